@@ -1,0 +1,407 @@
+"""Benchmark of the B200 path-tracing core: Mrays/s on the 1920x1080, 4 spp,
+depth 8 workload (64 BLAS of 2k-64k triangles, 1024 instances, Lambertian +
+20 % mirror; seeded synthetic scene), one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step is one frame: camera rays for every pixel and sample, then per bounce a
+closest-hit trace, shading, and a shadow-ray trace, then accumulation.  The
+device-timed `value` counts closest + shadow rays (the reference's counting,
+rend.c:3154/3264) over the K frames with inputs resident on the device; `e2e`
+runs the same frames through the C ABI as a frame loop does for a changing
+scene (upload of the TLAS and instances from host memory, render, ARGB8
+image back to pinned host memory).  With --gpus N under torchrun every rank
+renders its own replica of the frame (the path does not shard across GPUs
+in a way that needs an exchange): value = all rays / max rank time.
+
+The reference arm (--impl reference) times the reference renderer's own CPU
+traversal (intersect_tlas / intersect_any_tlas compiled from its sources)
+inside the CPU restatement of the path tracer, on all host cores, on a
+bounded band of rows of the same frame.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(family=2, seed=1, width=1920, height=1080, spp=4, depth=8)
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--width", type=int, default=WORKLOAD["width"])
+    p.add_argument("--height", type=int, default=WORKLOAD["height"])
+    p.add_argument("--spp", type=int, default=WORKLOAD["spp"])
+    p.add_argument("--depth", type=int, default=WORKLOAD["depth"])
+    p.add_argument("--blas", type=int, default=0,
+                   help="BLAS count (0 = the workload's 64)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0,
+                   help="target CPU time of the bounded CPU sample")
+    return p.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def allreduce(x, op):
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized():
+        return x
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
+def barrier():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+
+
+def config_of(a, world):
+    return {"workload": "scale: 64 BLAS (displaced spheres / triangle soups, "
+            "2k-64k tris log-uniform), 1024 instances, Lambertian + 20%% "
+            "mirror, ground + quad light; %dx%d, %d spp, max depth %d"
+            % (a.width, a.height, a.spp, a.depth),
+            "scene_seed": WORKLOAD["seed"], "width": a.width,
+            "height": a.height, "spp": a.spp, "max_depth": a.depth,
+            "blas": a.blas or 64, "instances": 1024,
+            "parallelism": "replicas x%d" % world,
+            "l2": "flushed between frames (256 MiB write), frames timed "
+                  "individually with CUDA events on the library stream"}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profile():
+    """dram bytes per closest-hit launch from the committed ncu summary
+    (a line `trace_dram_bytes_per_ray: X`), scaled by rays per launch."""
+    path = os.path.join(ROOT, "profiles", "k_trace_scale.md")
+    try:
+        for line in open(path):
+            if line.startswith("trace_dram_bytes_per_ray:"):
+                return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(a, rd, lights, area, budget_s):
+    """Reference traversal (compiled from its sources) in the CPU path
+    tracer, all host cores, on a band of rows of the same frame; plus the
+    reference algorithm's visit counts (restated traversal) for the
+    roofline's bytes per ray."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    cores = ol.ncpu()
+    W, H = a.width, a.height
+    use_ref = ol.ref() is not None
+    # calibrate on 4 rows, then size the band to the time budget
+    t0 = time.perf_counter()
+    _, r0 = ol.orc_render(rd, lights, area, a.depth, seed=1,
+                          window=(0, H // 2, W, H // 2 + 4), use_ref=use_ref)
+    dt = time.perf_counter() - t0
+    rows = max(4, min(H, int(4 * budget_s / max(dt, 1e-3))))
+    y0 = max(0, H // 2 - rows // 2)
+    t0 = time.perf_counter()
+    _, rays = ol.orc_render(rd, lights, area, a.depth, seed=1,
+                            window=(0, y0, W, y0 + rows), use_ref=use_ref)
+    dt = time.perf_counter() - t0
+    # visit counts of the reference algorithm on a ~1% sample of rows
+    cnt = ol.Counts()
+    srows = max(2, rows // 100)
+    _, crays = ol.orc_render(rd, lights, area, a.depth, seed=1,
+                             window=(0, y0, W, y0 + srows), counts=cnt)
+    # counts cover closest-hit rays only: shadow rays of the sample are
+    # part of crays, so divide by the closest-hit share measured on the GPU
+    return {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": cores,
+            "kind": "reference" if use_ref else "port",
+            "sample": "rows %d..%d of the %dx%d frame (%d spp, depth %d): "
+                      "%d rays in %.1f s; reference intersect_tlas/"
+                      "intersect_any_tlas inside the restated path tracer"
+                      % (y0, y0 + rows, W, H, a.spp, a.depth, rays, dt),
+            "_counts": (cnt.nodes, cnt.leaves, cnt.insts, crays)}
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    from nodebleed_b200 import api
+
+    world, rank, local = dist_setup()
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    scene = api.Scene(WORKLOAD["family"], WORKLOAD["seed"], a.blas)
+    rd = api.RenderData(scene, a.width, a.height, a.spp)
+    gr = api.GpuRenderer(rd, max_depth=a.depth, seed=1 + rank, timing=True,
+                         device=dev).upload()
+    stream = torch.cuda.ExternalStream(gr.stream(), device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    lights, area = gr.lights()
+
+    for _ in range(a.warmup):
+        gr.frame()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(dev)
+    ev = []
+    rays = closest = 0
+    trace_ms = shadow_ms = 0.0
+    launches = trace_launches = 0
+    for _ in range(a.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), \
+                torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+        n = gr.frame()
+        with torch.cuda.stream(stream):
+            e.record(stream)
+        st = gr.stats()
+        rays += n
+        closest += st["closest_rays"]
+        trace_ms += st["ms_trace"]
+        shadow_ms += st["ms_shadow"]
+        launches += st["launches"]
+        trace_launches += st["trace_launches"]
+        ev.append((s, e))
+    torch.cuda.synchronize()
+    cl = clocks.stop()
+    barrier()
+    ms = sum(s.elapsed_time(e) for s, e in ev)
+    ms_max = allreduce(ms, torch.distributed.ReduceOp.MAX) if world > 1 else ms
+    rays_all = allreduce(rays, torch.distributed.ReduceOp.SUM) \
+        if world > 1 else rays
+    samples_all = a.width * a.height * a.spp * a.steps * world
+    value = rays_all / (ms_max / 1e3) / 1e6
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not a.no_e2e:
+        pinned = torch.empty(a.width * a.height, dtype=torch.int32,
+                             pin_memory=True)
+        rd.buf = pinned.numpy().view(np.uint32)
+        rd.rd.buf = pinned.data_ptr()
+        h2d = d2h = 0
+        e2e_rays = 0
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            gr.upload_dynamic()
+            h2d += gr.stats()["h2d_bytes"]
+            e2e_rays += gr.frame()
+            gr.readback(2)
+            d2h += gr.stats()["d2h_bytes"]
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        dt_max = allreduce(dt, torch.distributed.ReduceOp.MAX) \
+            if world > 1 else dt
+        e2e_all = allreduce(e2e_rays, torch.distributed.ReduceOp.SUM) \
+            if world > 1 else e2e_rays
+        e2e = {"value": e2e_all / dt_max / 1e6, "unit": "Mrays/s",
+               "h2d_bytes_per_step": h2d // a.steps,
+               "d2h_bytes_per_step": d2h // a.steps,
+               "timing": "wall clock around upload_dynamic + render + "
+                         "readback of the ARGB8 image (pinned host)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(a, rd, lights, area, a.cpu_seconds)
+
+    out = None
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        roof = None
+        if cpu is not None:
+            nodes, leaves, insts, crays = cpu.pop("_counts")
+            # closest-hit rays of the counted sample: the GPU's closest
+            # share applied to the sample's ray count
+            share = closest / max(rays, 1)
+            csample = max(crays * share, 1.0)
+            b_ray = (256.0 * nodes + 192.0 * leaves + 64.0 * insts) / \
+                csample + 48.0
+            per_launch_rays = closest / max(trace_launches, 1)
+            launch_ms = trace_ms / max(trace_launches, 1)
+            achieved = per_launch_rays * b_ray / (launch_ms / 1e3) / 1e9
+            traffic = traffic_from_profile()
+            roof = {"bound": "hbm", "achieved": achieved, "peak": peak,
+                    "unit": "GB/s", "frac": achieved / peak,
+                    "peak_source": peak_kind,
+                    "kernel": "k_trace (closest hit)",
+                    "bytes_per_ray": b_ray,
+                    "visits_per_ray": [nodes / csample, leaves / csample,
+                                       insts / csample],
+                    "traffic": traffic * per_launch_rays if traffic else None,
+                    "launch_ms": launch_ms, "rays_per_launch": per_launch_rays}
+        out = {"metric": "Mrays/s", "value": value, "unit": "Mrays/s",
+               "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+               "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded procedural scene)",
+               "config": config_of(a, world),
+               "samples_per_s": samples_all / (ms_max / 1e3),
+               "rays_per_frame": rays / a.steps,
+               "closest_rays_per_frame": closest / a.steps,
+               "ms_trace_per_frame": trace_ms / a.steps,
+               "ms_shadow_per_frame": shadow_ms / a.steps,
+               "gpu_launches": launches, "e2e": e2e, "roofline": roof,
+               "cpu_baseline": cpu, "clocks": cl,
+               "scene": {"unique_tris": scene.tris,
+                         "instanced_tris": scene.inst_tris,
+                         "instances": scene.insts}}
+        print(json.dumps(out), flush=True)
+    gr.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return out
+
+
+def run_reference(a):
+    # rank 0 alone times the CPU reference; other ranks exit without work
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    from nodebleed_b200 import api
+    scene = api.Scene(WORKLOAD["family"], WORKLOAD["seed"], a.blas)
+    rd = api.RenderData(scene, a.width, a.height, a.spp)
+    # light table: the same emitters the GPU arm samples (FP64, numpy)
+    from test_oracle import _lights_numpy
+    lights, area = _lights_numpy(rd)
+    use_ref = ol.ref() is not None
+    W, H = a.width, a.height
+    t0 = time.perf_counter()
+    ol.orc_render(rd, lights, area, a.depth, seed=1,
+                  window=(0, H // 2, W, H // 2 + 2), use_ref=use_ref)
+    dt = time.perf_counter() - t0
+    per_step = max(10.0, 60.0 / max(a.steps + a.warmup, 1))
+    rows = max(2, min(H, int(2 * per_step / max(dt, 1e-3))))
+    y0 = max(0, H // 2 - rows // 2)
+    for _ in range(a.warmup):
+        ol.orc_render(rd, lights, area, a.depth, seed=1,
+                      window=(0, y0, W, y0 + max(2, rows // 8)),
+                      use_ref=use_ref)
+    tot_rays, tot_s = 0, 0.0
+    for k in range(a.steps):
+        t0 = time.perf_counter()
+        _, n = ol.orc_render(rd, lights, area, a.depth, seed=1 + k,
+                             window=(0, y0, W, y0 + rows), use_ref=use_ref)
+        tot_s += time.perf_counter() - t0
+        tot_rays += n
+    v = tot_rays / tot_s / 1e6
+    sample = ("rows %d..%d of the %dx%d frame per step (%d spp, depth %d); "
+              "reference intersect_tlas/intersect_any_tlas inside the "
+              "restated path tracer" % (y0, y0 + rows, W, H, a.spp, a.depth))
+    out = {"impl": "reference", "metric": "Mrays/s", "value": v,
+           "unit": "Mrays/s", "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": tot_s / a.steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+           "config": config_of(a, world),
+           "cpu_baseline": {"value": v, "unit": "Mrays/s",
+                            "cores": ol.ncpu(),
+                            "kind": "reference" if use_ref else "port",
+                            "sample": sample},
+           "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

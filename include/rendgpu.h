@@ -1,0 +1,169 @@
+/*
+ * rendgpu.h - C ABI of the B200 path-tracing core for nodebleed.
+ *
+ * A drop-in beside the reference renderer API (rend.h:149-162).  The
+ * application keeps its own host side: scene import, `struct rdata`
+ * (rend.h:119-147), rend_init, rend_prepstatic / rend_prepdynamic (the BVH8
+ * build) and rend_resaccum.  It then hands the same `struct rdata *` to the
+ * calls below, which upload the BVH/triangles/instances in a GPU layout and
+ * render on the GPU.  `rendgpu_render` has the thrd_start_t shape of
+ * `rend_render` (rend.c:3603), so a frame loop that does
+ *     for i < nthreads: thrd_create(&t[i], rend_render, &rd);
+ * can do the same with rendgpu_render: the first caller renders the frame,
+ * later callers of the same frame return at once (rd->blknum is the claim,
+ * as in rend.c:3623).  The caller then resets blknum/rays and bumps samples
+ * exactly as main.c:424-426 does.
+ *
+ * All calls return 0 on success or a negative RENDGPU_E* code; nothing
+ * exits or asserts.  rendgpu_strerror() describes the last error.
+ * Pointers in signatures are host pointers unless the name says _device.
+ */
+#ifndef RENDGPU_H
+#define RENDGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct rdata; /* rend.h:119-147, layout mirrored in nb_rdata.h */
+
+enum rendgpu_status {
+	RENDGPU_OK = 0,
+	RENDGPU_EINVAL = -1,   /* bad argument or state */
+	RENDGPU_ENOMEM = -2,   /* device or host allocation failed */
+	RENDGPU_ECUDA = -3,    /* CUDA runtime error */
+	RENDGPU_ELIMIT = -4,   /* scene exceeds a documented limit */
+	RENDGPU_ESTATE = -5,   /* call order (init/upload/resaccum) violated */
+	RENDGPU_EDEVICE = -6,  /* device-side error flag (e.g. stack overflow) */
+	RENDGPU_ENODEV = -7    /* no CUDA device */
+};
+
+enum rendgpu_mode {
+	RENDGPU_MODE_PATH = 0,    /* path tracing: NEE + cosine/mirror bounces */
+	RENDGPU_MODE_PRIMARY = 1  /* reference live shading: (n+1)/2 * albedo */
+};
+
+enum rendgpu_flags {
+	RENDGPU_FLAG_TIMING = 1u << 0  /* record per-kernel CUDA events */
+};
+
+struct rendgpu_cfg {
+	uint32_t size;       /* sizeof(struct rendgpu_cfg) */
+	uint32_t max_depth;  /* closest-hit rays per path (>= 1) */
+	uint32_t mode;       /* enum rendgpu_mode */
+	uint32_t flags;      /* enum rendgpu_flags */
+	uint64_t seed;       /* PCG32 seed of the path streams */
+	int32_t  device;     /* CUDA device ordinal */
+	uint32_t block;      /* threads per block of the trace kernels (0 = auto) */
+	uint32_t reserved[8];
+};
+
+/* A ray for the batch calls: origin, tmax, direction (32 bytes). */
+struct rendgpu_ray {
+	float ox, oy, oz, tmax;
+	float dx, dy, dz, pad;
+};
+
+/* A hit: t (FLT_MAX on a miss), barycentrics u/v of v1/v2, and
+ * id = tri << 12 | inst as in rend.c:890 (16 bytes). */
+struct rendgpu_hit {
+	float    t, u, v;
+	uint32_t id;
+};
+
+struct rendgpu_stats {
+	uint64_t rays;           /* closest + shadow rays of the last frame */
+	uint64_t closest_rays;
+	uint64_t shadow_rays;
+	uint32_t trace_launches; /* closest-hit trace launches of the frame */
+	uint32_t launches;       /* all kernel launches of the frame */
+	float    ms_frame;       /* device time of the frame (TIMING flag) */
+	float    ms_trace;       /* sum over closest-hit trace launches */
+	float    ms_shadow;      /* sum over shadow (any-hit) launches */
+	float    ms_shade;       /* gen + shade + accumulate */
+	uint32_t device_errors;  /* rays abandoned by a device error */
+	uint32_t max_stack;      /* traversal stack entries the scene needs */
+	uint64_t device_bytes;   /* device memory held by this context */
+	uint64_t h2d_bytes;      /* host->device bytes of the last upload/render */
+	uint64_t d2h_bytes;      /* device->host bytes of the last readback */
+};
+
+/* Create the GPU context of `rd` (one per rdata).  Replaces nothing in the
+ * reference; pairs with rend_init (rend.c:3000). */
+int rendgpu_init(struct rdata *rd, const struct rendgpu_cfg *cfg);
+
+/* Free everything of `rd`'s GPU context (pairs with rend_release,
+ * rend.c:3025). */
+int rendgpu_release(struct rdata *rd);
+
+/* After rend_prepstatic (rend.c:3033): upload every BLAS reachable from
+ * rd->insts (converted to the GPU node layout), triangles, normals and
+ * materials. */
+int rendgpu_upload_static(struct rdata *rd);
+
+/* After rend_prepdynamic (rend.c:3073): upload the TLAS, the instance
+ * transforms and the light table. */
+int rendgpu_upload_dynamic(struct rdata *rd);
+
+/* After rend_resaccum (rend.c:3092): size the device accumulator and the
+ * path/ray queues for rd->width x rd->height x rd->spp. */
+int rendgpu_resaccum(struct rdata *rd);
+
+/* Zero the device accumulator (rend_clraccum, rend.c:3103). */
+int rendgpu_clraccum(struct rdata *rd);
+
+/* Render one frame of rd->spp samples per pixel into the device
+ * accumulator (rend_render, rend.c:3603).  rd->samples keys the random
+ * streams and normalises the ARGB8 resolve, rd->rays receives the ray
+ * count.  Returns 0 (int, thrd_start_t shape); errors are reported by
+ * rendgpu_last_error(). */
+int rendgpu_render(void *rd);
+
+/* Copy the device accumulator to rd->acc and/or the ARGB8 image to rd->buf
+ * (which = 1: acc, 2: buf, 3: both); NULL host pointers are skipped. */
+int rendgpu_readback(struct rdata *rd, int which);
+
+/* Closest hits of n host rays (ray exchange with intersect_tlas,
+ * rend.c:1976); hits to host memory. */
+int rendgpu_trace_rays(struct rdata *rd, const struct rendgpu_ray *rays,
+                       uint32_t n, struct rendgpu_hit *hits);
+
+/* Occlusion of n host rays up to their tmax (intersect_any_tlas,
+ * rend.c:2883): occl[i] = 1 if anything is hit in (0, tmax). */
+int rendgpu_occluded(struct rdata *rd, const struct rendgpu_ray *rays,
+                     uint32_t n, uint8_t *occl);
+
+/* Device-pointer forms of the two calls above, on the context's stream;
+ * return without synchronising. */
+int rendgpu_trace_rays_device(struct rdata *rd, const void *rays_device,
+                              uint32_t n, void *hits_device);
+int rendgpu_occluded_device(struct rdata *rd, const void *rays_device,
+                            uint32_t n, void *occl_device);
+
+/* Wait for all work of the context. */
+int rendgpu_sync(struct rdata *rd);
+
+/* The cudaStream_t every call of this context runs on (for callers that
+ * order their own work or CUDA events against it). */
+int rendgpu_get_stream(struct rdata *rd, void **stream);
+
+/* Statistics of the last rendgpu_render / trace call. */
+int rendgpu_get_stats(struct rdata *rd, struct rendgpu_stats *st);
+
+/* The light table uploaded by rendgpu_upload_dynamic: n entries of 20
+ * floats (v0, e0, e1, n, emit, cdf, area, pad x3); returns the count, or a
+ * negative code.  `out` may be NULL to query the count. */
+int rendgpu_get_lights(struct rdata *rd, float *out, uint32_t cap,
+                       float *total_area);
+
+/* Last error of any call on this thread's most recent context. */
+int         rendgpu_last_error(struct rdata *rd);
+const char *rendgpu_strerror(struct rdata *rd);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

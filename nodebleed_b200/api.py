@@ -1,0 +1,351 @@
+"""ctypes bindings of libnbhost.so and libnbgpu.so (include/rendgpu.h)."""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+SCENE_SMALL, SCENE_SCALE, SCENE_BATCH, SCENE_STRESS, SCENE_TINY = 1, 2, 3, 5, 9
+MODE_PATH, MODE_PRIMARY = 0, 1
+FLAG_TIMING = 1
+
+# struct rendgpu_ray / rendgpu_hit (32 / 16 bytes)
+RAY_DTYPE = np.dtype([("o", "<f4", (3,)), ("tmax", "<f4"), ("d", "<f4", (3,)),
+                      ("pad", "<u4")])
+HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("id", "<u4")])
+
+STATUS = {0: "ok", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ELIMIT",
+          -5: "ESTATE", -6: "EDEVICE", -7: "ENODEV"}
+
+
+class RendgpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rendgpu {STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _load(name):
+    path = os.path.join(HERE, name)
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is not built; run "
+                           "`python -m nodebleed_b200.build`")
+    return C.CDLL(path)
+
+
+class RData(C.Structure):
+    """struct rdata (rend.h:119-147), 800 bytes."""
+    _fields_ = [
+        ("mtls", C.c_void_p), ("tris", C.c_void_p), ("nrms", C.c_void_p),
+        ("instcnt", C.c_uint32), ("insts", C.c_void_p),
+        ("aabbs", C.c_void_p), ("bnodes", C.c_void_p),
+        ("tlasofs", C.c_uint32), ("_pad0", C.c_uint32),
+        ("cam", C.c_ubyte * 672), ("bgcol", C.c_float * 3),
+        ("width", C.c_uint32), ("height", C.c_uint32),
+        ("acc", C.c_void_p), ("buf", C.c_void_p), ("blknum", C.c_int32),
+        ("rays", C.c_uint32), ("spp", C.c_uint32), ("samples", C.c_uint32),
+        ("_pad1", C.c_ubyte * 8)]
+
+
+class SceneStruct(C.Structure):
+    """struct nbh_scene (nb_host.h)."""
+    _fields_ = [
+        ("meshcnt", C.c_uint32), ("meshes", C.c_void_p),
+        ("mtlcnt", C.c_uint32), ("mtls", C.c_void_p),
+        ("instcnt", C.c_uint32), ("insts", C.c_void_p),
+        ("cam", C.c_float * 16), ("bgcol", C.c_float * 3),
+        ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+        ("depth", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class RendgpuCfg(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("max_depth", C.c_uint32),
+                ("mode", C.c_uint32), ("flags", C.c_uint32),
+                ("seed", C.c_uint64), ("device", C.c_int32),
+                ("block", C.c_uint32), ("reserved", C.c_uint32 * 8)]
+
+
+class RendgpuStats(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("closest_rays", C.c_uint64),
+                ("shadow_rays", C.c_uint64), ("trace_launches", C.c_uint32),
+                ("launches", C.c_uint32), ("ms_frame", C.c_float),
+                ("ms_trace", C.c_float), ("ms_shadow", C.c_float),
+                ("ms_shade", C.c_float), ("device_errors", C.c_uint32),
+                ("max_stack", C.c_uint32), ("device_bytes", C.c_uint64),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class HostLib:
+    def __init__(self):
+        L = _load("libnbhost.so")
+        vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+        L.nbh_scene_gen.argtypes = [vp, C.c_int, u64, u32]
+        L.nbh_scene_free.argtypes = [vp]
+        L.nbh_scene_tricnt.argtypes = [vp]
+        L.nbh_scene_tricnt.restype = u32
+        L.nbh_scene_instcnt.argtypes = [vp]
+        L.nbh_scene_instcnt.restype = u32
+        L.nbh_scene_insttris.argtypes = [vp]
+        L.nbh_scene_insttris.restype = C.c_double
+        L.nbh_rdata_new.restype = vp
+        L.nbh_rdata_delete.argtypes = [vp]
+        L.nbh_rend_init.argtypes = [vp, u32, u32, u32, u32]
+        L.nbh_rend_release.argtypes = [vp]
+        L.nbh_rend_resaccum.argtypes = [vp, u32, u32]
+        L.nbh_rend_clraccum.argtypes = [vp]
+        L.nbh_cpy_rdata.argtypes = [vp, vp]
+        L.nbh_upd_rinsts.argtypes = [vp, vp]
+        L.nbh_upd_rcam.argtypes = [vp, vp, C.c_float, C.c_float]
+        L.nbh_prepstatic.argtypes = [vp]
+        L.nbh_prepdynamic.argtypes = [vp]
+        L.nbh_rdata_from_scene.argtypes = [vp, vp]
+        self.L = L
+
+
+class GpuLib:
+    def __init__(self):
+        L = _load("libnbgpu.so")
+        vp, u32 = C.c_void_p, C.c_uint32
+        for fn, args in [
+                ("rendgpu_init", [vp, vp]), ("rendgpu_release", [vp]),
+                ("rendgpu_upload_static", [vp]),
+                ("rendgpu_upload_dynamic", [vp]),
+                ("rendgpu_resaccum", [vp]), ("rendgpu_clraccum", [vp]),
+                ("rendgpu_render", [vp]), ("rendgpu_readback", [vp, C.c_int]),
+                ("rendgpu_trace_rays", [vp, vp, u32, vp]),
+                ("rendgpu_occluded", [vp, vp, u32, vp]),
+                ("rendgpu_trace_rays_device", [vp, vp, u32, vp]),
+                ("rendgpu_occluded_device", [vp, vp, u32, vp]),
+                ("rendgpu_sync", [vp]), ("rendgpu_get_stats", [vp, vp]),
+                ("rendgpu_get_lights", [vp, vp, u32, vp]),
+                ("rendgpu_get_stream", [vp, vp]),
+                ("rendgpu_last_error", [vp])]:
+            f = getattr(L, fn)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.rendgpu_strerror.argtypes = [vp]
+        L.rendgpu_strerror.restype = C.c_char_p
+        self.L = L
+
+
+_HOST = None
+_GPU = None
+
+
+def host_lib():
+    global _HOST
+    if _HOST is None:
+        _HOST = HostLib()
+    return _HOST
+
+
+def gpu_lib():
+    global _GPU
+    if _GPU is None:
+        _GPU = GpuLib()
+    return _GPU
+
+
+class Scene:
+    """A seeded synthetic scene (nbh_scene_gen)."""
+
+    def __init__(self, family, seed=1, param=0):
+        self.h = host_lib().L
+        self.s = SceneStruct()
+        rc = self.h.nbh_scene_gen(C.byref(self.s), family, seed, param)
+        if rc != 0:
+            raise RuntimeError(f"nbh_scene_gen({family}, {seed}) = {rc}")
+        self.family, self.seed, self.param = family, seed, param
+
+    @property
+    def ptr(self):
+        return C.addressof(self.s)
+
+    @property
+    def tris(self):
+        return self.h.nbh_scene_tricnt(self.ptr)
+
+    @property
+    def insts(self):
+        return self.h.nbh_scene_instcnt(self.ptr)
+
+    @property
+    def inst_tris(self):
+        return self.h.nbh_scene_insttris(self.ptr)
+
+    def settings(self):
+        s = self.s
+        return dict(width=s.width, height=s.height, spp=s.spp, depth=s.depth)
+
+    def close(self):
+        if self.s is not None:
+            self.h.nbh_scene_free(self.ptr)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RenderData:
+    """A `struct rdata` filled from a scene by the host library (rend_init,
+    cpy_rdata, prepstatic, upd_rinsts, prepdynamic, resaccum, upd_rcam)."""
+
+    def __init__(self, scene, width=None, height=None, spp=None):
+        self.h = host_lib().L
+        self.ptr = self.h.nbh_rdata_new()
+        if not self.ptr:
+            raise MemoryError("nbh_rdata_new")
+        rc = self.h.nbh_rdata_from_scene(self.ptr, scene.ptr)
+        if rc != 0:
+            raise RuntimeError(f"nbh_rdata_from_scene = {rc}")
+        self.scene = scene
+        self.buf = None
+        if width or height or spp:
+            self.resize(width or self.rd.width, height or self.rd.height,
+                        spp or self.rd.spp)
+        self.attach_buf()
+
+    @property
+    def rd(self):
+        return RData.from_address(self.ptr)
+
+    def resize(self, w, h, spp=None):
+        if spp is not None:
+            self.rd.spp = spp
+        self.h.nbh_rend_resaccum(self.ptr, w, h)
+        camp = C.addressof(self.scene.s) + SceneStruct.cam.offset
+        self.h.nbh_upd_rcam(self.ptr, camp, float(w), float(h))
+        self.attach_buf()
+
+    def attach_buf(self):
+        n = self.rd.width * self.rd.height
+        self.buf = np.zeros(n, np.uint32)
+        self.rd.buf = self.buf.ctypes.data
+
+    def acc(self):
+        n = self.rd.width * self.rd.height * 3
+        a = (C.c_float * n).from_address(self.rd.acc)
+        return np.ctypeslib.as_array(a).reshape(self.rd.height,
+                                                self.rd.width, 3)
+
+    def eye(self):
+        return np.frombuffer(bytes(self.rd.cam[:12]), np.float32).copy()
+
+    def close(self):
+        if self.ptr:
+            self.h.nbh_rend_release(self.ptr)
+            self.h.nbh_rdata_delete(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuRenderer:
+    """The rendgpu C ABI on one RenderData."""
+
+    def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
+                 timing=False, device=0):
+        self.g = gpu_lib().L
+        self.rdata = rdata
+        self.ptr = rdata.ptr
+        cfg = RendgpuCfg()
+        cfg.size = C.sizeof(RendgpuCfg)
+        cfg.max_depth = max_depth
+        cfg.mode = mode
+        cfg.flags = FLAG_TIMING if timing else 0
+        cfg.seed = seed
+        cfg.device = device
+        rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
+        if rc != 0:
+            raise RendgpuError(rc, "rendgpu_init")
+        self.live = True
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            raise RendgpuError(rc, f"{what}: "
+                               f"{self.g.rendgpu_strerror(self.ptr).decode()}")
+
+    def upload(self):
+        self._ck(self.g.rendgpu_upload_static(self.ptr), "upload_static")
+        self._ck(self.g.rendgpu_upload_dynamic(self.ptr), "upload_dynamic")
+        self._ck(self.g.rendgpu_resaccum(self.ptr), "resaccum")
+        return self
+
+    def upload_dynamic(self):
+        self._ck(self.g.rendgpu_upload_dynamic(self.ptr), "upload_dynamic")
+
+    def clraccum(self):
+        self._ck(self.g.rendgpu_clraccum(self.ptr), "clraccum")
+
+    def frame(self):
+        """One frame and main.c's bookkeeping after the join
+        (main.c:424-426).  Returns the frame's ray count."""
+        rd = self.rdata.rd
+        self.g.rendgpu_render(self.ptr)
+        self._ck(self.g.rendgpu_last_error(self.ptr), "render")
+        st = self.stats()
+        rd.blknum = 0
+        rd.rays = 0
+        rd.samples += rd.spp
+        return st["rays"]
+
+    def readback(self, which=3):
+        self._ck(self.g.rendgpu_readback(self.ptr, which), "readback")
+
+    def trace(self, rays):
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(len(rays), HIT_DTYPE)
+        self._ck(self.g.rendgpu_trace_rays(self.ptr, rays.ctypes.data,
+                                           len(rays), hits.ctypes.data),
+                 "trace_rays")
+        return hits
+
+    def occluded(self, rays):
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        occl = np.zeros(len(rays), np.uint8)
+        self._ck(self.g.rendgpu_occluded(self.ptr, rays.ctypes.data,
+                                         len(rays), occl.ctypes.data),
+                 "occluded")
+        return occl
+
+    def stats(self):
+        st = RendgpuStats()
+        self._ck(self.g.rendgpu_get_stats(self.ptr, C.byref(st)), "stats")
+        return st.as_dict()
+
+    def stream(self):
+        """cudaStream_t of this context, as an integer handle."""
+        h = C.c_void_p()
+        self._ck(self.g.rendgpu_get_stream(self.ptr, C.byref(h)), "stream")
+        return h.value or 0
+
+    def lights(self):
+        area = C.c_float()
+        n = self.g.rendgpu_get_lights(self.ptr, None, 0, C.byref(area))
+        if n < 0:
+            self._ck(n, "get_lights")
+        out = np.zeros((max(n, 1), 20), np.float32)
+        self.g.rendgpu_get_lights(self.ptr, out.ctypes.data, n, C.byref(area))
+        return out[:n], area.value
+
+    def close(self):
+        if self.live:
+            self.g.rendgpu_release(self.ptr)
+            self.live = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,549 @@
+// Wavefront path-tracing kernels (sm_100a).
+//
+// One frame = gen, then per bounce: closest-hit trace of the ray queue,
+// shade (which appends next-bounce rays and shadow rays with warp-aggregated
+// atomics), any-hit trace of the shadow queue; finally accumulate.  Every
+// kernel is a grid-stride loop over a count it reads from device memory, so
+// the whole frame is a fixed launch sequence (capturable in a CUDA graph).
+//
+// The per-path arithmetic follows the CPU oracle operation by operation
+// (camera jitter, shading normal, next-event estimation, cosine bounce, PCG32
+// streams, sin/cos polynomials), compiled without contraction, so a path whose
+// hits agree with the oracle's produces the same bits.
+
+#ifndef NB_KERNELS_CUH
+#define NB_KERNELS_CUH
+
+#include "trace.cuh"
+
+namespace nb {
+
+constexpr float kEps2 = 1e-3f;          // util.h:8 EPS2
+constexpr float kInvPi = 0.318309886f;  // util.h:11 INV_PI
+
+struct FrameDev {
+	// queues: 2 float4 per ray: (o, tmax) (d, path as bits)
+	float4   *q[2];
+	float4   *hits;    // (t, u, v, id bits)
+	float4   *shadow;  // 3 float4: (o, tfar) (d, path) (c, 0)
+	float4   *pT;      // (T.rgb, spec flag)
+	float4   *pL;      // (L.rgb, 0)
+	uint2    *rng;     // PCG32 state
+	float    *acc;     // W*H*3
+	uint32_t *buf;     // W*H ARGB8
+	uint32_t *cnt;     // [0],[1] ray queues, [2] shadow, [3] errors
+	unsigned long long *rays; // [0] closest, [1] shadow
+	uint32_t  W, H, spp, npaths;
+};
+
+struct FrameArgs {
+	uint64_t seed;
+	uint32_t frame;   // rd->samples
+	uint32_t depth;
+	uint32_t mode;
+	// camera (rcam fields)
+	float eye[3], ri[3], up[3], fwd[3];
+	float rw, rh, fovfdist, aspect, fdist, focrad, tanfangle;
+};
+
+// ------------------------------------------------------------- sampling --
+
+__device__ __forceinline__ uint32_t pcg_next(uint64_t &st, uint64_t inc)
+{
+	uint64_t old = st;
+	st = old * 6364136223846793005ull + inc;
+	uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+	uint32_t rot = (uint32_t)(old >> 59u);
+	return (xs >> rot) | (xs << ((32u - rot) & 31u));
+}
+
+__device__ __forceinline__ uint64_t pcg_inc(uint32_t path)
+{
+	return ((uint64_t)path << 1u) | 1u;
+}
+
+__device__ __forceinline__ uint64_t pcg_start(uint64_t seed, uint32_t frame,
+                                              uint32_t path)
+{
+	uint64_t inc = pcg_inc(path), st = 0;
+	pcg_next(st, inc);
+	st += seed + 0x9e3779b97f4a7c15ull * ((uint64_t)frame + 1u);
+	pcg_next(st, inc);
+	return st;
+}
+
+__device__ __forceinline__ float rnd01(uint64_t &st, uint64_t inc)
+{
+	return __fmul_rn((float)(pcg_next(st, inc) >> 8), 0x1p-24f);
+}
+
+// sin and cos of 2*pi*u, u in [0,1): quadrant from 4u, Taylor polynomials
+// of sin/cos(pi/2 f) on [0,1) (same constants and order as the oracle).
+__device__ __forceinline__ void sincos2pi(float u, float *s, float *c)
+{
+	float u4 = __fmul_rn(u, 4.0f);
+	int q = (int)u4;
+	float f = __fsub_rn(u4, (float)q);
+	float f2 = __fmul_rn(f, f);
+	float sp = __fmul_rn(f, __fadd_rn(1.57079633f, __fmul_rn(f2,
+	  __fadd_rn(-0.645964098f, __fmul_rn(f2, __fadd_rn(0.0796926262f,
+	  __fmul_rn(f2, __fadd_rn(-0.00468175414f, __fmul_rn(f2,
+	  __fadd_rn(0.000160441185f, __fmul_rn(f2, -3.59884324e-06f)))))))))));
+	float cp = __fadd_rn(1.0f, __fmul_rn(f2, __fadd_rn(-1.23370055f,
+	  __fmul_rn(f2, __fadd_rn(0.253669508f, __fmul_rn(f2,
+	  __fadd_rn(-0.0208634808f, __fmul_rn(f2, __fadd_rn(0.000919260275f,
+	  __fmul_rn(f2, __fadd_rn(-2.52020424e-05f,
+	  __fmul_rn(f2, 4.71087478e-07f))))))))))));
+	switch (q & 3) {
+	case 0: *s = sp; *c = cp; break;
+	case 1: *s = cp; *c = -sp; break;
+	case 2: *s = -sp; *c = -cp; break;
+	default: *s = -cp; *c = sp; break;
+	}
+}
+
+// Warp-aggregated append: returns this lane's slot in the queue.
+__device__ __forceinline__ uint32_t append(uint32_t *counter, bool want)
+{
+	uint32_t mask = __ballot_sync(__activemask(), want);
+	if (!want)
+		return 0;
+	uint32_t lane = threadIdx.x & 31u;
+	uint32_t leader = __ffs(mask) - 1;
+	uint32_t base = 0;
+	if (lane == leader)
+		base = atomicAdd(counter, (uint32_t)__popc(mask));
+	base = __shfl_sync(mask, base, leader);
+	return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// Pixel of queue slot i: 8x4 pixel tiles, spp consecutive samples.
+__device__ __forceinline__ bool tile_pixel(uint32_t i, uint32_t W,
+                                           uint32_t H, uint32_t spp,
+                                           uint32_t *x, uint32_t *y,
+                                           uint32_t *s)
+{
+	uint32_t p = i / spp;
+	*s = i - p * spp;
+	uint32_t tile = p >> 5, in = p & 31u;
+	uint32_t tpr = (W + 7u) >> 3;
+	*x = (tile % tpr) * 8u + (in & 7u);
+	*y = (tile / tpr) * 4u + (in >> 3);
+	return *x < W && *y < H;
+}
+
+// --------------------------------------------------------------- kernels --
+
+// Camera rays (rend.c:3293-3402, one lane) and path state.
+__global__ void __launch_bounds__(256) k_gen(FrameDev F, FrameArgs A)
+{
+	uint32_t tiles_w = (F.W + 7u) >> 3, tiles_h = (F.H + 3u) >> 2;
+	uint32_t total = tiles_w * tiles_h * 32u * F.spp;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	     i - threadIdx.x < total; i += gridDim.x * blockDim.x) {
+		uint32_t x = 0, y = 0, s = 0;
+		bool live = i < total && tile_pixel(i, F.W, F.H, F.spp, &x, &y, &s);
+		uint32_t path = (y * F.W + x) * F.spp + s;
+		float o[3] = {0, 0, 0}, d[3] = {0, 0, 1};
+		uint64_t st = 0;
+		if (live) {
+			uint64_t inc = pcg_inc(path);
+			st = pcg_start(A.seed, A.frame, path);
+			float u0 = rnd01(st, inc), u1 = rnd01(st, inc);
+			float sx = __fadd_rn((float)x, __fsub_rn(u0, 0.5f));
+			float sy = __fadd_rn((float)y, __fsub_rn(u1, 0.5f));
+			sx = __fmaf_rn(sx, A.rw, -0.5f);
+			sy = __fmaf_rn(sy, A.rh, -0.5f);
+			sx = __fmul_rn(sx, A.fovfdist);
+			sy = __fmul_rn(sy, A.fovfdist);
+			sx = __fmul_rn(sx, A.aspect);
+			float ups[3], riup[3], td[3];
+			for (int a = 0; a < 3; a++) {
+				ups[a] = __fmul_rn(A.up[a], sy);
+				riup[a] = __fmaf_rn(A.ri[a], sx, -ups[a]);
+			}
+			if (A.tanfangle > 0.0f) {
+				float u2 = rnd01(st, inc), u3 = rnd01(st, inc);
+				float rad = __fsqrt_rn(u2), sn, cs;
+				sincos2pi(u3, &sn, &cs);
+				float lx = __fmul_rn(cs, rad), ly = __fmul_rn(sn, rad);
+				for (int a = 0; a < 3; a++) {
+					o[a] = __fmaf_rn(__fmaf_rn(A.ri[a], lx,
+					  __fmul_rn(A.up[a], ly)), A.focrad, A.eye[a]);
+					float fe = __fmaf_rn(A.fwd[a], A.fdist, A.eye[a]);
+					td[a] = __fsub_rn(__fadd_rn(fe, riup[a]), o[a]);
+				}
+			} else {
+				for (int a = 0; a < 3; a++) {
+					o[a] = A.eye[a];
+					td[a] = __fmaf_rn(A.fwd[a], A.fdist, riup[a]);
+				}
+			}
+			float l2 = __fmaf_rn(td[0], td[0], __fmaf_rn(td[1], td[1],
+			  __fmul_rn(td[2], td[2])));
+			float il = __fdiv_rn(1.0f, __fsqrt_rn(l2));
+			for (int a = 0; a < 3; a++)
+				d[a] = __fmul_rn(td[a], il);
+			F.pT[path] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+			F.pL[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+			F.rng[path] = make_uint2((uint32_t)st, (uint32_t)(st >> 32));
+		}
+		uint32_t slot = append(&F.cnt[0], live);
+		if (live) {
+			F.q[0][2u * slot] = make_float4(o[0], o[1], o[2], FLT_MAX);
+			F.q[0][2u * slot + 1u] = make_float4(d[0], d[1], d[2],
+			  __uint_as_float(path));
+		}
+	}
+}
+
+// Closest-hit trace of a ray queue (count in *count).
+template <int STACK>
+__global__ void __launch_bounds__(128) k_trace(DScene S, const float4 *rays,
+                                               const uint32_t *count,
+                                               float4 *hits, uint32_t *errs,
+                                               unsigned long long *nrays)
+{
+	extern __shared__ uint2 sstk[];
+	uint2 *stk = sstk + threadIdx.x;
+	uint32_t n = *count;
+	if (blockIdx.x == 0 && threadIdx.x == 0 && nrays)
+		atomicAdd(nrays, (unsigned long long)n);
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+	     i += gridDim.x * blockDim.x) {
+		float4 a = rays[2u * i], b = rays[2u * i + 1u];
+		THit h;
+		uint32_t err = 0;
+		float4 out = make_float4(FLT_MAX, 0.0f, 0.0f, 0.0f);
+		if (traverse<false, STACK>(S, a.x, a.y, a.z, b.x, b.y, b.z, a.w,
+		  stk, blockDim.x, h, err))
+			out = finish_hit(S, a.x, a.y, a.z, b.x, b.y, b.z, h);
+		if (err)
+			atomicAdd(errs, 1u);
+		hits[i] = out;
+	}
+}
+
+// Any-hit trace of host/API rays: occl[i] = hit in (0, tmax).
+template <int STACK>
+__global__ void __launch_bounds__(128) k_occluded(DScene S,
+                                                  const float4 *rays,
+                                                  uint32_t n, uint8_t *occl,
+                                                  uint32_t *errs)
+{
+	extern __shared__ uint2 sstk[];
+	uint2 *stk = sstk + threadIdx.x;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+	     i += gridDim.x * blockDim.x) {
+		float4 a = rays[2u * i], b = rays[2u * i + 1u];
+		THit h;
+		uint32_t err = 0;
+		bool hit = traverse<true, STACK>(S, a.x, a.y, a.z, b.x, b.y, b.z,
+		  a.w, stk, blockDim.x, h, err);
+		if (err)
+			atomicAdd(errs, 1u);
+		occl[i] = hit ? 1 : 0;
+	}
+}
+
+// Shadow queue: add the carried contribution when unoccluded.
+template <int STACK>
+__global__ void __launch_bounds__(128) k_shadow(DScene S, FrameDev F)
+{
+	extern __shared__ uint2 sstk[];
+	uint2 *stk = sstk + threadIdx.x;
+	uint32_t n = F.cnt[2];
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		atomicAdd(&F.rays[1], (unsigned long long)n);
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+	     i += gridDim.x * blockDim.x) {
+		float4 a = F.shadow[3u * i], b = F.shadow[3u * i + 1u];
+		THit h;
+		uint32_t err = 0;
+		bool hit = traverse<true, STACK>(S, a.x, a.y, a.z, b.x, b.y, b.z,
+		  a.w, stk, blockDim.x, h, err);
+		if (err)
+			atomicAdd(&F.cnt[3], 1u);
+		if (!hit && !err) {
+			float4 c = F.shadow[3u * i + 2u];
+			uint32_t path = __float_as_uint(b.w);
+			float4 L = F.pL[path];
+			L.x = __fadd_rn(L.x, c.x);
+			L.y = __fadd_rn(L.y, c.y);
+			L.z = __fadd_rn(L.z, c.z);
+			F.pL[path] = L;
+		}
+	}
+}
+
+// Shade the hits of queue `cur` at bounce k; append next rays to queue
+// 1-cur and shadow rays to the shadow queue.
+__global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
+                                               FrameArgs A, uint32_t cur,
+                                               uint32_t k)
+{
+	uint32_t n = F.cnt[cur];
+	const float4 *rays = F.q[cur];
+	float4 *next = F.q[cur ^ 1u];
+	for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n;
+	     i0 += gridDim.x * blockDim.x) {
+		uint32_t i = i0 + threadIdx.x;
+		bool live = i < n;
+		bool want_ray = false, want_shadow = false;
+		float no[3] = {0, 0, 0}, nd[3] = {0, 0, 0};
+		float so[3] = {0, 0, 0}, sd[3] = {0, 0, 0}, sc[3] = {0, 0, 0};
+		float tfar = 0.0f;
+		uint32_t path = 0;
+		if (live) {
+			float4 ra = rays[2u * i], rb = rays[2u * i + 1u];
+			float4 h = F.hits[i];
+			path = __float_as_uint(rb.w);
+			float4 T = F.pT[path];
+			float4 L = F.pL[path];
+			if (h.x == FLT_MAX) {
+				L.x = __fadd_rn(L.x, __fmul_rn(T.x, S.bg[0]));
+				L.y = __fadd_rn(L.y, __fmul_rn(T.y, S.bg[1]));
+				L.z = __fadd_rn(L.z, __fmul_rn(T.z, S.bg[2]));
+				F.pL[path] = L;
+			} else {
+				uint32_t id = __float_as_uint(h.w);
+				uint32_t inst = id & NB_INST_ID_MASK;
+				uint32_t prim = id >> NB_INST_ID_BITS;
+				const float4 *ip = S.insts + 4u * inst;
+				float4 m0 = __ldg(ip), m1 = __ldg(ip + 1);
+				float4 m2 = __ldg(ip + 2);
+				uint32_t triofs = __float_as_uint(__ldg(ip + 3).y);
+				const nb_rnrm *rn = S.nrms + triofs + prim;
+				const float4 *rnv = reinterpret_cast<const float4 *>(rn);
+				float4 n0 = __ldg(rnv), n1 = __ldg(rnv + 1);
+				float4 n2 = __ldg(rnv + 2);
+				uint32_t mtlid = __float_as_uint(n0.w);
+				const float4 *mv = reinterpret_cast<const float4 *>(
+				  S.mtls + mtlid);
+				float4 mc = __ldg(mv), mf = __ldg(mv + 1);
+				uint32_t mflags = __float_as_uint(mf.z);
+				float col[3] = {mc.x, mc.y, mc.z};
+				// shading normal (rend.c:3109 with the transpose)
+				float u = h.y, v = h.z;
+				float w = __fsub_rn(__fsub_rn(1.0f, u), v);
+				float nn[3];
+				nn[0] = __fadd_rn(__fmul_rn(n1.x, u), __fadd_rn(
+				  __fmul_rn(n2.x, v), __fmul_rn(n0.x, w)));
+				nn[1] = __fadd_rn(__fmul_rn(n1.y, u), __fadd_rn(
+				  __fmul_rn(n2.y, v), __fmul_rn(n0.y, w)));
+				nn[2] = __fadd_rn(__fmul_rn(n1.z, u), __fadd_rn(
+				  __fmul_rn(n2.z, v), __fmul_rn(n0.z, w)));
+				float mm[3];
+				mm[0] = __fadd_rn(__fadd_rn(__fmul_rn(m0.x, nn[0]),
+				  __fmul_rn(m1.x, nn[1])), __fmul_rn(m2.x, nn[2]));
+				mm[1] = __fadd_rn(__fadd_rn(__fmul_rn(m0.y, nn[0]),
+				  __fmul_rn(m1.y, nn[1])), __fmul_rn(m2.y, nn[2]));
+				mm[2] = __fadd_rn(__fadd_rn(__fmul_rn(m0.z, nn[0]),
+				  __fmul_rn(m1.z, nn[1])), __fmul_rn(m2.z, nn[2]));
+				float ml = __fadd_rn(__fadd_rn(__fmul_rn(mm[0], mm[0]),
+				  __fmul_rn(mm[1], mm[1])), __fmul_rn(mm[2], mm[2]));
+				float il = __fdiv_rn(1.0f, __fsqrt_rn(ml));
+				float n[3] = {__fmul_rn(mm[0], il), __fmul_rn(mm[1], il),
+				  __fmul_rn(mm[2], il)};
+				if (A.mode == 1u) {
+					// rend.c:3435-3441
+					L.x = __fmul_rn(__fmul_rn(__fadd_rn(n[0], 1.0f),
+					  0.5f), col[0]);
+					L.y = __fmul_rn(__fmul_rn(__fadd_rn(n[1], 1.0f),
+					  0.5f), col[1]);
+					L.z = __fmul_rn(__fmul_rn(__fadd_rn(n[2], 1.0f),
+					  0.5f), col[2]);
+					F.pL[path] = L;
+				} else {
+					float d[3] = {rb.x, rb.y, rb.z};
+					float pos[3] = {__fmaf_rn(d[0], h.x, ra.x),
+					  __fmaf_rn(d[1], h.x, ra.y),
+					  __fmaf_rn(d[2], h.x, ra.z)};
+					float dn = __fadd_rn(__fadd_rn(__fmul_rn(n[0], d[0]),
+					  __fmul_rn(n[1], d[1])), __fmul_rn(n[2], d[2]));
+					bool front = dn < 0.0f;
+					if (!front) {
+						n[0] = __fmul_rn(n[0], -1.0f);
+						n[1] = __fmul_rn(n[1], -1.0f);
+						n[2] = __fmul_rn(n[2], -1.0f);
+					}
+					uint2 rs = F.rng[path];
+					uint64_t st = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
+					uint64_t inc = pcg_inc(path);
+					float rl = rnd01(st, inc), ra_ = rnd01(st, inc);
+					float rb_ = rnd01(st, inc), r0 = rnd01(st, inc);
+					float r1 = rnd01(st, inc);
+					F.rng[path] = make_uint2((uint32_t)st,
+					  (uint32_t)(st >> 32));
+					bool spec = T.w != 0.0f;
+					if (mflags & NB_FLAG_EMISSIVE) {
+						if ((k == 0u || spec) && front) {
+							L.x = __fadd_rn(L.x, __fmul_rn(T.x, col[0]));
+							L.y = __fadd_rn(L.y, __fmul_rn(T.y, col[1]));
+							L.z = __fadd_rn(L.z, __fmul_rn(T.z, col[2]));
+							F.pL[path] = L;
+						}
+					} else if (mc.w >= 0.5f) {
+						// perfect mirror
+						float dd = __fadd_rn(__fadd_rn(__fmul_rn(d[0],
+						  n[0]), __fmul_rn(d[1], n[1])),
+						  __fmul_rn(d[2], n[2]));
+						float s2 = __fmul_rn(2.0f, dd);
+						for (int a = 0; a < 3; a++) {
+							nd[a] = __fsub_rn(d[a], __fmul_rn(n[a], s2));
+							no[a] = __fmaf_rn(nd[a], kEps2, pos[a]);
+						}
+						T.x = __fmul_rn(T.x, col[0]);
+						T.y = __fmul_rn(T.y, col[1]);
+						T.z = __fmul_rn(T.z, col[2]);
+						T.w = 1.0f;
+						F.pT[path] = T;
+						want_ray = k + 1u < A.depth;
+					} else {
+						T.w = 0.0f;
+						if (S.nlights) {
+							// pick an emitting triangle by area
+							uint32_t lo = 0, hi = S.nlights - 1u;
+							while (lo < hi) {
+								uint32_t mid = (lo + hi) >> 1;
+								float cdf = __ldg(&S.lights[5u * mid + 3u]).w;
+								if (rl < cdf)
+									hi = mid;
+								else
+									lo = mid + 1u;
+							}
+							const float4 *lp = S.lights + 5u * lo;
+							float4 l0 = __ldg(lp), l1 = __ldg(lp + 1);
+							float4 l2 = __ldg(lp + 2), l3 = __ldg(lp + 3);
+							// v0 = l0.xyz, e0 = (l0.w, l1.x, l1.y),
+							// e1 = (l1.z, l1.w, l2.x), n = (l2.y, l2.z, l2.w)
+							// emit = l3.xyz
+							float su = __fsqrt_rn(ra_);
+							float b1 = __fmul_rn(su, __fsub_rn(1.0f, rb_));
+							float b2 = __fmul_rn(su, rb_);
+							float e0[3] = {l0.w, l1.x, l1.y};
+							float e1[3] = {l1.z, l1.w, l2.x};
+							float lv0[3] = {l0.x, l0.y, l0.z};
+							float lnm[3] = {l2.y, l2.z, l2.w};
+							float ld[3];
+							for (int a = 0; a < 3; a++) {
+								float p = __fadd_rn(__fadd_rn(lv0[a],
+								  __fmul_rn(e0[a], b1)),
+								  __fmul_rn(e1[a], b2));
+								ld[a] = __fsub_rn(p, pos[a]);
+							}
+							float l2s = __fadd_rn(__fadd_rn(
+							  __fmul_rn(ld[0], ld[0]),
+							  __fmul_rn(ld[1], ld[1])),
+							  __fmul_rn(ld[2], ld[2]));
+							float ldist = __fsqrt_rn(l2s);
+							float ilr = __fdiv_rn(1.0f, ldist);
+							for (int a = 0; a < 3; a++)
+								ld[a] = __fmul_rn(ld[a], ilr);
+							float ndotl = __fadd_rn(__fadd_rn(
+							  __fmul_rn(n[0], ld[0]),
+							  __fmul_rn(n[1], ld[1])),
+							  __fmul_rn(n[2], ld[2]));
+							float cosl = -__fadd_rn(__fadd_rn(
+							  __fmul_rn(lnm[0], ld[0]),
+							  __fmul_rn(lnm[1], ld[1])),
+							  __fmul_rn(lnm[2], ld[2]));
+							tfar = __fsub_rn(ldist, __fmul_rn(2.0f, kEps2));
+							if (ndotl > 0.0f && cosl > 0.0f &&
+							    tfar > 0.0f) {
+								float wgt = __fmul_rn(ndotl, cosl);
+								wgt = __fmul_rn(wgt, __fmul_rn(kInvPi,
+								  S.light_area));
+								wgt = __fdiv_rn(wgt, l2s);
+								float em[3] = {l3.x, l3.y, l3.z};
+								float tc[3] = {T.x, T.y, T.z};
+								for (int a = 0; a < 3; a++) {
+									sc[a] = __fmul_rn(__fmul_rn(
+									  __fmul_rn(tc[a], col[a]), em[a]),
+									  wgt);
+									so[a] = __fmaf_rn(ld[a], kEps2,
+									  pos[a]);
+									sd[a] = ld[a];
+								}
+								want_shadow = true;
+							}
+						}
+						if (k + 1u < A.depth) {
+							float sn, cs;
+							sincos2pi(r0, &sn, &cs);
+							float s1 = __fsqrt_rn(r1);
+							float lx = __fmul_rn(cs, s1);
+							float ly = __fmul_rn(sn, s1);
+							float lz = __fsqrt_rn(__fsub_rn(1.0f, r1));
+							// onb (rend.c:3126)
+							float sgn = copysignf(1.0f, n[2]);
+							float oa = __fdiv_rn(-1.0f, __fadd_rn(sgn, n[2]));
+							float ob = __fmul_rn(__fmul_rn(n[0], n[1]), oa);
+							float ta[3] = {__fadd_rn(1.0f, __fmul_rn(
+							  __fmul_rn(__fmul_rn(sgn, n[0]), n[0]), oa)),
+							  __fmul_rn(sgn, ob), __fmul_rn(-sgn, n[0])};
+							float tb[3] = {ob, __fadd_rn(sgn, __fmul_rn(
+							  __fmul_rn(n[1], n[1]), oa)), -n[1]};
+							for (int a = 0; a < 3; a++) {
+								nd[a] = __fadd_rn(__fadd_rn(
+								  __fmul_rn(ta[a], lx),
+								  __fmul_rn(tb[a], ly)),
+								  __fmul_rn(n[a], lz));
+								no[a] = __fmaf_rn(nd[a], kEps2, pos[a]);
+							}
+							T.x = __fmul_rn(T.x, col[0]);
+							T.y = __fmul_rn(T.y, col[1]);
+							T.z = __fmul_rn(T.z, col[2]);
+							want_ray = true;
+						}
+						F.pT[path] = T;
+					}
+				}
+			}
+		}
+		uint32_t rs_ = append(&F.cnt[cur ^ 1u], want_ray);
+		if (want_ray) {
+			next[2u * rs_] = make_float4(no[0], no[1], no[2], FLT_MAX);
+			next[2u * rs_ + 1u] = make_float4(nd[0], nd[1], nd[2],
+			  __uint_as_float(path));
+		}
+		uint32_t ss = append(&F.cnt[2], want_shadow);
+		if (want_shadow) {
+			F.shadow[3u * ss] = make_float4(so[0], so[1], so[2], tfar);
+			F.shadow[3u * ss + 1u] = make_float4(sd[0], sd[1], sd[2],
+			  __uint_as_float(path));
+			F.shadow[3u * ss + 2u] = make_float4(sc[0], sc[1], sc[2], 0.0f);
+		}
+	}
+}
+
+// acc += sum over the pixel's samples; ARGB8 resolve (rend.c:3565-3580).
+__global__ void __launch_bounds__(256) k_accum(FrameDev F, float inv)
+{
+	uint32_t npix = F.W * F.H;
+	for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix;
+	     p += gridDim.x * blockDim.x) {
+		float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+		for (uint32_t s = 0; s < F.spp; s++) {
+			float4 L = F.pL[p * F.spp + s];
+			sx = __fadd_rn(sx, L.x);
+			sy = __fadd_rn(sy, L.y);
+			sz = __fadd_rn(sz, L.z);
+		}
+		float ax = __fadd_rn(F.acc[3u * p], sx);
+		float ay = __fadd_rn(F.acc[3u * p + 1u], sy);
+		float az = __fadd_rn(F.acc[3u * p + 2u], sz);
+		F.acc[3u * p] = ax;
+		F.acc[3u * p + 1u] = ay;
+		F.acc[3u * p + 2u] = az;
+		uint32_t cx = (uint32_t)__fmul_rn(255.0f, __fmul_rn(ax, inv));
+		uint32_t cy = (uint32_t)__fmul_rn(255.0f, __fmul_rn(ay, inv));
+		uint32_t cz = (uint32_t)__fmul_rn(255.0f, __fmul_rn(az, inv));
+		F.buf[p] = 0xff000000u | (cx & 0xffu) << 16 | (cy & 0xffu) << 8 |
+		  (cz & 0xffu);
+	}
+}
+
+} // namespace nb
+
+#endif

@@ -1,0 +1,46 @@
+// Host conversion of the reference BVH8 (bnode8/leaf4 byte trees in
+// rd->bnodes) into the GPU layout of gpulayout.h, and the light table.
+
+#ifndef NB_LAYOUT_HPP
+#define NB_LAYOUT_HPP
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "gpulayout.h"
+#include "host/nb_rdata.h"
+
+namespace nb {
+
+struct bvh_stats {
+	uint32_t depth = 0;  // longest root-to-leaf chain of nodes
+	uint32_t nodes = 0;
+	uint32_t items = 0;
+};
+
+// Append the BLAS rooted at bnodes[2 * triofs] to `nodes`/`tris`; returns
+// the root node index.  Triangles come from rd->tris (original vertices).
+// Returns false with `err` set on a malformed tree.
+bool convert_blas(const nb_rdata *rd, uint32_t triofs,
+                  std::vector<nb_qnode> &nodes, std::vector<nb_gtri> &tris,
+                  uint32_t *root, bvh_stats *st, std::string *err);
+
+// TLAS rooted at bnodes[tlasofs] into `nodes` (root at index 0) and
+// instance references `irefs`.
+bool convert_tlas(const nb_rdata *rd, std::vector<nb_qnode> &nodes,
+                  std::vector<uint32_t> &irefs, bvh_stats *st,
+                  std::string *err);
+
+// World-space emitting triangles of instances whose material is EMISSIVE,
+// with an area CDF; returns the total area.
+float build_lights(const nb_rdata *rd, std::vector<nb_glight> &lights);
+
+// Quantise one node: child boxes (min/max per slot; empty slots have
+// min > max) into n (origin, exponents, qlo/qhi).  Exposed for tests.
+void quantise_node(const float cmin[8][3], const float cmax[8][3],
+                   nb_qnode *n);
+
+} // namespace nb
+
+#endif

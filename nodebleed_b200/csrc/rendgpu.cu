@@ -1,0 +1,848 @@
+// C ABI of the B200 path-tracing core (include/rendgpu.h).
+//
+// One context per `struct rdata`, found through a small registry keyed by
+// the rdata pointer (the reference API passes only that pointer).  Uploads
+// convert the reference BVH8 to the GPU layout (layout.cpp); a frame is the
+// fixed launch sequence of kernels.cuh on the context's stream.
+
+#include <cfloat>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/rendgpu.h"
+#include "kernels.cuh"
+#include "layout.hpp"
+
+namespace nb {
+namespace {
+
+constexpr int kStackSmall = 24;
+constexpr int kStackLarge = 48;
+constexpr int kTraceBlock = 128;
+
+// Device allocation that grows on demand.
+struct DevBuf {
+	void  *p = nullptr;
+	size_t cap = 0;
+	cudaError_t ensure(size_t bytes)
+	{
+		if (bytes <= cap && p)
+			return cudaSuccess;
+		if (p)
+			cudaFree(p);
+		p = nullptr;
+		cap = 0;
+		size_t b = bytes ? bytes : 16;
+		cudaError_t e = cudaMalloc(&p, b);
+		if (e == cudaSuccess)
+			cap = b;
+		return e;
+	}
+	void release()
+	{
+		if (p)
+			cudaFree(p);
+		p = nullptr;
+		cap = 0;
+	}
+	template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+struct Ctx {
+	nb_rdata    *rd = nullptr;
+	rendgpu_cfg  cfg{};
+	int          device = 0;
+	int          nsm = 148;
+	cudaStream_t stream = nullptr;
+	// scene
+	DevBuf blas, tris, tlas, irefs, insts, nrms, mtls, lights;
+	std::unordered_map<uint32_t, uint32_t> root_of; // triofs -> BLAS root
+	std::unordered_map<uint32_t, uint32_t> depth_of; // triofs -> BLAS depth
+	uint32_t blas_depth = 0, tlas_depth = 0;
+	std::vector<nb_glight> host_lights;
+	float    light_area = 0.0f;
+	bool     have_static = false, have_dynamic = false;
+	uint32_t ntris = 0, nnodes = 0;
+	// frame
+	DevBuf q0, q1, hits, shadow, pT, pL, rng, acc, buf, cnt, rays;
+	uint32_t W = 0, H = 0, spp = 0, npaths = 0;
+	bool     have_frame = false;
+	// batch scratch
+	DevBuf brays, bhits, berr;
+	// stats / errors
+	rendgpu_stats st{};
+	int          last = 0;
+	std::string  msg;
+	cudaEvent_t  ev[64] = {};
+	int          nev = 0;
+};
+
+std::mutex g_mu;
+std::unordered_map<const void *, Ctx *> g_ctx;
+
+Ctx *find_ctx(const void *rd)
+{
+	std::lock_guard<std::mutex> lk(g_mu);
+	auto it = g_ctx.find(rd);
+	return it == g_ctx.end() ? nullptr : it->second;
+}
+
+int fail(Ctx *c, int code, const std::string &m)
+{
+	if (c) {
+		c->last = code;
+		c->msg = m;
+	}
+	return code;
+}
+
+int cuda_fail(Ctx *c, cudaError_t e, const char *where)
+{
+	return fail(c, RENDGPU_ECUDA, std::string(where) + ": " +
+	  cudaGetErrorString(e));
+}
+
+#define NB_CK(c, call)                                                   \
+	do {                                                              \
+		cudaError_t e_ = (call);                                  \
+		if (e_ != cudaSuccess)                                    \
+			return cuda_fail((c), e_, #call);                 \
+	} while (0)
+
+uint32_t need_stack(const Ctx *c)
+{
+	return c->tlas_depth + c->blas_depth + 2u;
+}
+
+DScene scene_of(const Ctx *c)
+{
+	DScene S;
+	S.blas = c->blas.as<nb_qnode>();
+	S.tris = c->tris.as<float4>();
+	S.tlas = c->tlas.as<nb_qnode>();
+	S.irefs = c->irefs.as<uint32_t>();
+	S.insts = c->insts.as<float4>();
+	S.nrms = c->nrms.as<nb_rnrm>();
+	S.mtls = c->mtls.as<nb_rmtl>();
+	S.lights = c->lights.as<float4>();
+	S.nlights = (uint32_t)c->host_lights.size();
+	S.light_area = c->light_area;
+	S.bg[0] = c->rd->bgcol.x;
+	S.bg[1] = c->rd->bgcol.y;
+	S.bg[2] = c->rd->bgcol.z;
+	return S;
+}
+
+int trace_grid(Ctx *c, const void *fn, int stack)
+{
+	int per_sm = 0;
+	size_t smem = (size_t)stack * kTraceBlock * sizeof(uint2);
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
+	  kTraceBlock, smem) != cudaSuccess || per_sm < 1)
+		per_sm = 1;
+	return per_sm * c->nsm;
+}
+
+// Launch a closest-hit trace of `count` (device) rays.
+int launch_trace(Ctx *c, const float4 *rays, const uint32_t *count,
+                 float4 *hits, uint32_t *errs, unsigned long long *nrays)
+{
+	DScene S = scene_of(c);
+	uint32_t need = need_stack(c);
+	if (need <= (uint32_t)kStackSmall) {
+		auto fn = k_trace<kStackSmall>;
+		size_t smem = (size_t)kStackSmall * kTraceBlock * sizeof(uint2);
+		fn<<<trace_grid(c, (const void *)fn, kStackSmall), kTraceBlock,
+		  smem, c->stream>>>(S, rays, count, hits, errs, nrays);
+	} else if (need <= (uint32_t)kStackLarge) {
+		auto fn = k_trace<kStackLarge>;
+		size_t smem = (size_t)kStackLarge * kTraceBlock * sizeof(uint2);
+		fn<<<trace_grid(c, (const void *)fn, kStackLarge), kTraceBlock,
+		  smem, c->stream>>>(S, rays, count, hits, errs, nrays);
+	} else {
+		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
+		  "stack");
+	}
+	NB_CK(c, cudaGetLastError());
+	return 0;
+}
+
+int launch_shadow(Ctx *c, FrameDev &F)
+{
+	DScene S = scene_of(c);
+	uint32_t need = need_stack(c);
+	if (need <= (uint32_t)kStackSmall) {
+		auto fn = k_shadow<kStackSmall>;
+		size_t smem = (size_t)kStackSmall * kTraceBlock * sizeof(uint2);
+		fn<<<trace_grid(c, (const void *)fn, kStackSmall), kTraceBlock,
+		  smem, c->stream>>>(S, F);
+	} else if (need <= (uint32_t)kStackLarge) {
+		auto fn = k_shadow<kStackLarge>;
+		size_t smem = (size_t)kStackLarge * kTraceBlock * sizeof(uint2);
+		fn<<<trace_grid(c, (const void *)fn, kStackLarge), kTraceBlock,
+		  smem, c->stream>>>(S, F);
+	} else {
+		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
+		  "stack");
+	}
+	NB_CK(c, cudaGetLastError());
+	return 0;
+}
+
+int launch_occluded(Ctx *c, const float4 *rays, uint32_t n, uint8_t *occl,
+                    uint32_t *errs)
+{
+	DScene S = scene_of(c);
+	uint32_t need = need_stack(c);
+	if (need <= (uint32_t)kStackSmall) {
+		auto fn = k_occluded<kStackSmall>;
+		size_t smem = (size_t)kStackSmall * kTraceBlock * sizeof(uint2);
+		fn<<<trace_grid(c, (const void *)fn, kStackSmall), kTraceBlock,
+		  smem, c->stream>>>(S, rays, n, occl, errs);
+	} else if (need <= (uint32_t)kStackLarge) {
+		auto fn = k_occluded<kStackLarge>;
+		size_t smem = (size_t)kStackLarge * kTraceBlock * sizeof(uint2);
+		fn<<<trace_grid(c, (const void *)fn, kStackLarge), kTraceBlock,
+		  smem, c->stream>>>(S, rays, n, occl, errs);
+	} else {
+		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
+		  "stack");
+	}
+	NB_CK(c, cudaGetLastError());
+	return 0;
+}
+
+FrameDev frame_of(Ctx *c)
+{
+	FrameDev F;
+	F.q[0] = c->q0.as<float4>();
+	F.q[1] = c->q1.as<float4>();
+	F.hits = c->hits.as<float4>();
+	F.shadow = c->shadow.as<float4>();
+	F.pT = c->pT.as<float4>();
+	F.pL = c->pL.as<float4>();
+	F.rng = c->rng.as<uint2>();
+	F.acc = c->acc.as<float>();
+	F.buf = c->buf.as<uint32_t>();
+	F.cnt = c->cnt.as<uint32_t>();
+	F.rays = c->rays.as<unsigned long long>();
+	F.W = c->W;
+	F.H = c->H;
+	F.spp = c->spp;
+	F.npaths = c->npaths;
+	return F;
+}
+
+int ready(Ctx *c, bool frame)
+{
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->have_static || !c->have_dynamic)
+		return fail(c, RENDGPU_ESTATE, "upload_static and upload_dynamic "
+		  "must come first");
+	if (frame && !c->have_frame)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_resaccum must come first");
+	return 0;
+}
+
+int grid_for(const Ctx *c, uint32_t n, int block)
+{
+	uint32_t g = (n + (uint32_t)block - 1u) / (uint32_t)block;
+	uint32_t cap = (uint32_t)c->nsm * 8u;
+	return (int)(g < 1u ? 1u : (g > cap ? cap : g));
+}
+
+void ev_record(Ctx *c)
+{
+	if (!(c->cfg.flags & RENDGPU_FLAG_TIMING) || c->nev >= 64)
+		return;
+	if (!c->ev[c->nev])
+		cudaEventCreate(&c->ev[c->nev]);
+	cudaEventRecord(c->ev[c->nev], c->stream);
+	c->nev++;
+}
+
+float ev_ms(Ctx *c, int a, int b)
+{
+	float ms = 0.0f;
+	if (a < c->nev && b < c->nev)
+		cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]);
+	return ms;
+}
+
+int render_frame(Ctx *c)
+{
+	int rc = ready(c, true);
+	if (rc)
+		return rc;
+	nb_rdata *rd = c->rd;
+	if (rd->width != c->W || rd->height != c->H || rd->spp != c->spp)
+		return fail(c, RENDGPU_ESTATE, "rdata size changed since "
+		  "rendgpu_resaccum");
+	FrameDev F = frame_of(c);
+	FrameArgs A;
+	A.seed = c->cfg.seed;
+	A.frame = rd->samples;
+	A.depth = c->cfg.mode == RENDGPU_MODE_PRIMARY ? 1u : c->cfg.max_depth;
+	A.mode = c->cfg.mode;
+	const nb_rcam &cam = rd->cam;
+	A.eye[0] = cam.eye.x; A.eye[1] = cam.eye.y; A.eye[2] = cam.eye.z;
+	A.ri[0] = cam.ri.x; A.ri[1] = cam.ri.y; A.ri[2] = cam.ri.z;
+	A.up[0] = cam.up.x; A.up[1] = cam.up.y; A.up[2] = cam.up.z;
+	A.fwd[0] = cam.fwd.x; A.fwd[1] = cam.fwd.y; A.fwd[2] = cam.fwd.z;
+	A.rw = cam.rw8[0];
+	A.rh = cam.rh8[0];
+	A.fovfdist = cam.fovfdist8[0];
+	A.aspect = cam.aspect8[0];
+	A.fdist = cam.fdist8[0];
+	A.focrad = cam.focrad8[0];
+	A.tanfangle = cam.tanfangle;
+	DScene S = scene_of(c);
+	c->nev = 0;
+	c->st.launches = 0;
+	c->st.trace_launches = 0;
+	NB_CK(c, cudaMemsetAsync(c->cnt.p, 0, 4 * sizeof(uint32_t), c->stream));
+	NB_CK(c, cudaMemsetAsync(c->rays.p, 0, 2 * sizeof(unsigned long long),
+	  c->stream));
+	ev_record(c); // 0
+	uint32_t tiles = ((c->W + 7u) >> 3) * ((c->H + 3u) >> 2) * 32u * c->spp;
+	k_gen<<<grid_for(c, tiles, 256), 256, 0, c->stream>>>(F, A);
+	NB_CK(c, cudaGetLastError());
+	c->st.launches++;
+	ev_record(c); // 1
+	std::vector<int> trace_ev, shadow_ev;
+	for (uint32_t k = 0; k < A.depth; k++) {
+		uint32_t cur = k & 1u;
+		trace_ev.push_back(c->nev);
+		ev_record(c);
+		rc = launch_trace(c, F.q[cur], F.cnt + cur, F.hits, F.cnt + 3,
+		  F.rays);
+		if (rc)
+			return rc;
+		ev_record(c);
+		c->st.launches++;
+		c->st.trace_launches++;
+		NB_CK(c, cudaMemsetAsync(F.cnt + (cur ^ 1u), 0, sizeof(uint32_t),
+		  c->stream));
+		NB_CK(c, cudaMemsetAsync(F.cnt + 2, 0, sizeof(uint32_t),
+		  c->stream));
+		k_shade<<<grid_for(c, c->npaths, 256), 256, 0, c->stream>>>(S, F,
+		  A, cur, k);
+		NB_CK(c, cudaGetLastError());
+		c->st.launches++;
+		if (A.mode == RENDGPU_MODE_PATH) {
+			shadow_ev.push_back(c->nev);
+			ev_record(c);
+			rc = launch_shadow(c, F);
+			if (rc)
+				return rc;
+			ev_record(c);
+			c->st.launches++;
+		}
+	}
+	int acc_ev = c->nev;
+	ev_record(c);
+	float inv = 1.0f / (float)(rd->samples + rd->spp);
+	k_accum<<<grid_for(c, c->W * c->H, 256), 256, 0, c->stream>>>(F, inv);
+	NB_CK(c, cudaGetLastError());
+	c->st.launches++;
+	ev_record(c);
+	unsigned long long hr[2];
+	uint32_t hc[4];
+	NB_CK(c, cudaMemcpyAsync(hr, c->rays.p, sizeof(hr),
+	  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaMemcpyAsync(hc, c->cnt.p, sizeof(hc),
+	  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	c->st.closest_rays = hr[0];
+	c->st.shadow_rays = hr[1];
+	c->st.rays = hr[0] + hr[1];
+	c->st.device_errors = hc[3];
+	c->st.max_stack = need_stack(c);
+	if (c->cfg.flags & RENDGPU_FLAG_TIMING) {
+		c->st.ms_frame = ev_ms(c, 0, c->nev - 1);
+		float tr = 0.0f, sh = 0.0f;
+		for (int e : trace_ev)
+			tr += ev_ms(c, e, e + 1);
+		for (int e : shadow_ev)
+			sh += ev_ms(c, e, e + 1);
+		c->st.ms_trace = tr;
+		c->st.ms_shadow = sh;
+		c->st.ms_shade = c->st.ms_frame - tr - sh;
+		(void)acc_ev;
+	}
+	if (hc[3])
+		return fail(c, RENDGPU_EDEVICE, "rays abandoned on the device "
+		  "(traversal stack overflow)");
+	return 0;
+}
+
+void free_ctx(Ctx *c)
+{
+	DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs, &c->insts,
+	  &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits, &c->shadow,
+	  &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt, &c->rays,
+	  &c->brays, &c->bhits, &c->berr};
+	for (DevBuf *b : bufs)
+		b->release();
+	for (int i = 0; i < 64; i++)
+		if (c->ev[i])
+			cudaEventDestroy(c->ev[i]);
+	if (c->stream)
+		cudaStreamDestroy(c->stream);
+	delete c;
+}
+
+uint64_t held_bytes(const Ctx *c)
+{
+	const DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs,
+	  &c->insts, &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits,
+	  &c->shadow, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
+	  &c->rays, &c->brays, &c->bhits, &c->berr};
+	uint64_t s = 0;
+	for (const DevBuf *b : bufs)
+		s += b->cap;
+	return s;
+}
+
+} // namespace
+} // namespace nb
+
+using namespace nb;
+
+extern "C" {
+
+int rendgpu_init(struct rdata *rdp, const struct rendgpu_cfg *cfg)
+{
+	if (!rdp || !cfg || cfg->size < sizeof(rendgpu_cfg) - 8 * sizeof(uint32_t))
+		return RENDGPU_EINVAL;
+	if (find_ctx(rdp))
+		return RENDGPU_ESTATE;
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+		return RENDGPU_ENODEV;
+	if (cfg->device < 0 || cfg->device >= ndev)
+		return RENDGPU_EINVAL;
+	if (cfg->mode > RENDGPU_MODE_PRIMARY || cfg->max_depth < 1 ||
+	  cfg->max_depth > 1024)
+		return RENDGPU_EINVAL;
+	Ctx *c = new Ctx;
+	c->rd = reinterpret_cast<nb_rdata *>(rdp);
+	c->cfg = *cfg;
+	c->device = cfg->device;
+	if (cudaSetDevice(c->device) != cudaSuccess ||
+	  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount,
+	  c->device) != cudaSuccess ||
+	  cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) !=
+	  cudaSuccess) {
+		free_ctx(c);
+		return RENDGPU_ECUDA;
+	}
+	if (c->cnt.ensure(16 * sizeof(uint32_t)) != cudaSuccess ||
+	  c->rays.ensure(4 * sizeof(unsigned long long)) != cudaSuccess ||
+	  c->berr.ensure(16) != cudaSuccess) {
+		free_ctx(c);
+		return RENDGPU_ENOMEM;
+	}
+	// dynamic smem above 48 KB for the deep-stack variants
+	size_t big = (size_t)kStackLarge * kTraceBlock * sizeof(uint2);
+	cudaFuncSetAttribute(k_trace<kStackLarge>,
+	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+	cudaFuncSetAttribute(k_shadow<kStackLarge>,
+	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+	cudaFuncSetAttribute(k_occluded<kStackLarge>,
+	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+	std::lock_guard<std::mutex> lk(g_mu);
+	g_ctx[rdp] = c;
+	return 0;
+}
+
+int rendgpu_release(struct rdata *rdp)
+{
+	Ctx *c = nullptr;
+	{
+		std::lock_guard<std::mutex> lk(g_mu);
+		auto it = g_ctx.find(rdp);
+		if (it == g_ctx.end())
+			return RENDGPU_EINVAL;
+		c = it->second;
+		g_ctx.erase(it);
+	}
+	cudaSetDevice(c->device);
+	cudaStreamSynchronize(c->stream);
+	free_ctx(c);
+	return 0;
+}
+
+int rendgpu_upload_static(struct rdata *rdp)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	nb_rdata *rd = c->rd;
+	if (!rd->bnodes || !rd->tris || !rd->nrms || !rd->mtls || !rd->insts)
+		return fail(c, RENDGPU_EINVAL, "render data not initialised");
+	if (rd->instcnt == 0 || rd->instcnt > (1u << NB_INST_ID_BITS))
+		return fail(c, RENDGPU_ELIMIT, "instance count outside 1..4096 "
+		  "(INST_ID_BITS = 12, rend.c:24)");
+	std::vector<nb_qnode> nodes;
+	std::vector<nb_gtri> tris;
+	c->root_of.clear();
+	c->depth_of.clear();
+	c->blas_depth = 0;
+	uint32_t maxtri = 0, maxmtl = 0;
+	for (uint32_t i = 0; i < rd->instcnt; i++) {
+		const nb_rinst &ri = rd->insts[i];
+		if (ri.tricnt == 0)
+			return fail(c, RENDGPU_EINVAL, "instance without triangles");
+		if (ri.tricnt > (1u << (32 - NB_INST_ID_BITS)))
+			return fail(c, RENDGPU_ELIMIT, "mesh above 2^20 triangles");
+		maxtri = std::max(maxtri, ri.triofs + ri.tricnt);
+		if (c->root_of.count(ri.triofs))
+			continue;
+		uint32_t root = 0;
+		bvh_stats bs;
+		std::string err;
+		if (!convert_blas(rd, ri.triofs, nodes, tris, &root, &bs, &err))
+			return fail(c, RENDGPU_EINVAL, "BLAS of triofs " +
+			  std::to_string(ri.triofs) + ": " + err);
+		c->root_of[ri.triofs] = root;
+		c->depth_of[ri.triofs] = bs.depth;
+		c->blas_depth = std::max(c->blas_depth, bs.depth);
+	}
+	for (uint32_t t = 0; t < maxtri; t++)
+		maxmtl = std::max(maxmtl, rd->nrms[t].mtlid + 1u);
+	NB_CK(c, c->blas.ensure(nodes.size() * sizeof(nb_qnode)));
+	NB_CK(c, c->tris.ensure(tris.size() * sizeof(nb_gtri)));
+	NB_CK(c, c->nrms.ensure((size_t)maxtri * sizeof(nb_rnrm)));
+	NB_CK(c, c->mtls.ensure((size_t)maxmtl * sizeof(nb_rmtl)));
+	NB_CK(c, cudaMemcpyAsync(c->blas.p, nodes.data(), nodes.size() *
+	  sizeof(nb_qnode), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemcpyAsync(c->tris.p, tris.data(), tris.size() *
+	  sizeof(nb_gtri), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemcpyAsync(c->nrms.p, rd->nrms, (size_t)maxtri *
+	  sizeof(nb_rnrm), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemcpyAsync(c->mtls.p, rd->mtls, (size_t)maxmtl *
+	  sizeof(nb_rmtl), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	c->ntris = (uint32_t)tris.size();
+	c->nnodes = (uint32_t)nodes.size();
+	c->have_static = true;
+	c->have_dynamic = false;
+	return 0;
+}
+
+int rendgpu_upload_dynamic(struct rdata *rdp)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->have_static)
+		return fail(c, RENDGPU_ESTATE, "upload_static must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	nb_rdata *rd = c->rd;
+	std::vector<nb_qnode> nodes;
+	std::vector<uint32_t> irefs;
+	bvh_stats bs;
+	std::string err;
+	if (!convert_tlas(rd, nodes, irefs, &bs, &err))
+		return fail(c, RENDGPU_EINVAL, "TLAS: " + err);
+	c->tlas_depth = bs.depth;
+	std::vector<nb_ginst> gi(rd->instcnt);
+	for (uint32_t i = 0; i < rd->instcnt; i++) {
+		const nb_rinst &ri = rd->insts[i];
+		auto it = c->root_of.find(ri.triofs);
+		if (it == c->root_of.end())
+			return fail(c, RENDGPU_ESTATE, "instance mesh not uploaded "
+			  "by upload_static");
+		std::memcpy(gi[i].m, ri.globinv, sizeof(gi[i].m));
+		gi[i].root = it->second;
+		gi[i].triofs = ri.triofs;
+		gi[i].flags = ri.flags;
+		gi[i].pad = 0;
+	}
+	c->light_area = build_lights(rd, c->host_lights);
+	NB_CK(c, c->tlas.ensure(nodes.size() * sizeof(nb_qnode)));
+	NB_CK(c, c->irefs.ensure(irefs.size() * sizeof(uint32_t)));
+	NB_CK(c, c->insts.ensure(gi.size() * sizeof(nb_ginst)));
+	NB_CK(c, c->lights.ensure(c->host_lights.size() * sizeof(nb_glight)));
+	NB_CK(c, cudaMemcpyAsync(c->tlas.p, nodes.data(), nodes.size() *
+	  sizeof(nb_qnode), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemcpyAsync(c->irefs.p, irefs.data(), irefs.size() *
+	  sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemcpyAsync(c->insts.p, gi.data(), gi.size() *
+	  sizeof(nb_ginst), cudaMemcpyHostToDevice, c->stream));
+	if (!c->host_lights.empty())
+		NB_CK(c, cudaMemcpyAsync(c->lights.p, c->host_lights.data(),
+		  c->host_lights.size() * sizeof(nb_glight),
+		  cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	c->st.h2d_bytes = nodes.size() * sizeof(nb_qnode) + irefs.size() *
+	  sizeof(uint32_t) + gi.size() * sizeof(nb_ginst) +
+	  c->host_lights.size() * sizeof(nb_glight);
+	c->have_dynamic = true;
+	if (need_stack(c) > (uint32_t)kStackLarge)
+		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
+		  "stack");
+	return 0;
+}
+
+int rendgpu_resaccum(struct rdata *rdp)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	nb_rdata *rd = c->rd;
+	uint64_t np = (uint64_t)rd->width * rd->height * (rd->spp ? rd->spp : 1);
+	if (np == 0 || np > 0x7fffffffull)
+		return fail(c, RENDGPU_ELIMIT, "width*height*spp outside "
+		  "1..2^31-1");
+	uint64_t npix = (uint64_t)rd->width * rd->height;
+	NB_CK(c, c->q0.ensure(np * 32));
+	NB_CK(c, c->q1.ensure(np * 32));
+	NB_CK(c, c->hits.ensure(np * 16));
+	NB_CK(c, c->shadow.ensure(np * 48));
+	NB_CK(c, c->pT.ensure(np * 16));
+	NB_CK(c, c->pL.ensure(np * 16));
+	NB_CK(c, c->rng.ensure(np * 8));
+	NB_CK(c, c->acc.ensure(npix * 12));
+	NB_CK(c, c->buf.ensure(npix * 4));
+	c->W = rd->width;
+	c->H = rd->height;
+	c->spp = rd->spp ? rd->spp : 1;
+	c->npaths = (uint32_t)np;
+	c->have_frame = true;
+	NB_CK(c, cudaMemsetAsync(c->acc.p, 0, npix * 12, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->buf.p, 0, npix * 4, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	return 0;
+}
+
+int rendgpu_clraccum(struct rdata *rdp)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->have_frame)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_resaccum must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	NB_CK(c, cudaMemsetAsync(c->acc.p, 0, (size_t)c->W * c->H * 12,
+	  c->stream));
+	return 0;
+}
+
+int rendgpu_render(void *rdp)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return 0;
+	nb_rdata *rd = c->rd;
+	// Claim the frame as rend_render claims blocks (rend.c:3623): only
+	// the first caller of a frame renders.
+	if (__atomic_fetch_add(&rd->blknum, 1, __ATOMIC_SEQ_CST) != 0)
+		return 0;
+	if (cudaSetDevice(c->device) != cudaSuccess) {
+		fail(c, RENDGPU_ECUDA, "cudaSetDevice");
+		return 0;
+	}
+	c->last = 0;
+	int rc = render_frame(c);
+	if (rc) {
+		c->last = rc;
+		return 0;
+	}
+	__atomic_fetch_add(&rd->rays, (unsigned int)c->st.rays,
+	  __ATOMIC_SEQ_CST);
+	return 0;
+}
+
+int rendgpu_readback(struct rdata *rdp, int which)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->have_frame)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_resaccum must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	nb_rdata *rd = c->rd;
+	size_t npix = (size_t)c->W * c->H;
+	c->st.d2h_bytes = 0;
+	if ((which & 1) && rd->acc) {
+		NB_CK(c, cudaMemcpyAsync(rd->acc, c->acc.p, npix * 12,
+		  cudaMemcpyDeviceToHost, c->stream));
+		c->st.d2h_bytes += npix * 12;
+	}
+	if ((which & 2) && rd->buf) {
+		NB_CK(c, cudaMemcpyAsync(rd->buf, c->buf.p, npix * 4,
+		  cudaMemcpyDeviceToHost, c->stream));
+		c->st.d2h_bytes += npix * 4;
+	}
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	return 0;
+}
+
+int rendgpu_trace_rays_device(struct rdata *rdp, const void *rays,
+                              uint32_t n, void *hits)
+{
+	Ctx *c = find_ctx(rdp);
+	int rc = ready(c, false);
+	if (rc)
+		return rc;
+	if (n == 0)
+		return 0;
+	NB_CK(c, cudaSetDevice(c->device));
+	// count lives in the batch scratch: [0] count, [1] errors
+	NB_CK(c, cudaMemcpyAsync(c->berr.p, &n, sizeof(n),
+	  cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->berr.as<uint32_t>() + 1, 0, 4, c->stream));
+	return launch_trace(c, static_cast<const float4 *>(rays),
+	  c->berr.as<uint32_t>(), static_cast<float4 *>(hits),
+	  c->berr.as<uint32_t>() + 1, nullptr);
+}
+
+int rendgpu_occluded_device(struct rdata *rdp, const void *rays, uint32_t n,
+                            void *occl)
+{
+	Ctx *c = find_ctx(rdp);
+	int rc = ready(c, false);
+	if (rc)
+		return rc;
+	if (n == 0)
+		return 0;
+	NB_CK(c, cudaSetDevice(c->device));
+	NB_CK(c, cudaMemsetAsync(c->berr.as<uint32_t>() + 1, 0, 4, c->stream));
+	return launch_occluded(c, static_cast<const float4 *>(rays), n,
+	  static_cast<uint8_t *>(occl), c->berr.as<uint32_t>() + 1);
+}
+
+static int batch_errors(Ctx *c)
+{
+	uint32_t e = 0;
+	NB_CK(c, cudaMemcpyAsync(&e, c->berr.as<uint32_t>() + 1, 4,
+	  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	c->st.device_errors = e;
+	if (e)
+		return fail(c, RENDGPU_EDEVICE, "rays abandoned on the device "
+		  "(traversal stack overflow)");
+	return 0;
+}
+
+int rendgpu_trace_rays(struct rdata *rdp, const struct rendgpu_ray *rays,
+                       uint32_t n, struct rendgpu_hit *hits)
+{
+	Ctx *c = find_ctx(rdp);
+	int rc = ready(c, false);
+	if (rc)
+		return rc;
+	if (n == 0)
+		return 0;
+	if (!rays || !hits)
+		return fail(c, RENDGPU_EINVAL, "null pointer");
+	NB_CK(c, cudaSetDevice(c->device));
+	NB_CK(c, c->brays.ensure((size_t)n * 32));
+	NB_CK(c, c->bhits.ensure((size_t)n * 16));
+	NB_CK(c, cudaMemcpyAsync(c->brays.p, rays, (size_t)n * 32,
+	  cudaMemcpyHostToDevice, c->stream));
+	rc = rendgpu_trace_rays_device(rdp, c->brays.p, n, c->bhits.p);
+	if (rc)
+		return rc;
+	NB_CK(c, cudaMemcpyAsync(hits, c->bhits.p, (size_t)n * 16,
+	  cudaMemcpyDeviceToHost, c->stream));
+	return batch_errors(c);
+}
+
+int rendgpu_occluded(struct rdata *rdp, const struct rendgpu_ray *rays,
+                     uint32_t n, uint8_t *occl)
+{
+	Ctx *c = find_ctx(rdp);
+	int rc = ready(c, false);
+	if (rc)
+		return rc;
+	if (n == 0)
+		return 0;
+	if (!rays || !occl)
+		return fail(c, RENDGPU_EINVAL, "null pointer");
+	NB_CK(c, cudaSetDevice(c->device));
+	NB_CK(c, c->brays.ensure((size_t)n * 32));
+	NB_CK(c, c->bhits.ensure((size_t)n));
+	NB_CK(c, cudaMemcpyAsync(c->brays.p, rays, (size_t)n * 32,
+	  cudaMemcpyHostToDevice, c->stream));
+	rc = rendgpu_occluded_device(rdp, c->brays.p, n, c->bhits.p);
+	if (rc)
+		return rc;
+	NB_CK(c, cudaMemcpyAsync(occl, c->bhits.p, (size_t)n,
+	  cudaMemcpyDeviceToHost, c->stream));
+	return batch_errors(c);
+}
+
+int rendgpu_sync(struct rdata *rdp)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	return 0;
+}
+
+int rendgpu_get_stream(struct rdata *rdp, void **stream)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c || !stream)
+		return RENDGPU_EINVAL;
+	*stream = (void *)c->stream;
+	return 0;
+}
+
+int rendgpu_get_stats(struct rdata *rdp, struct rendgpu_stats *st)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c || !st)
+		return RENDGPU_EINVAL;
+	c->st.device_bytes = held_bytes(c);
+	c->st.max_stack = need_stack(c);
+	*st = c->st;
+	return 0;
+}
+
+int rendgpu_get_lights(struct rdata *rdp, float *out, uint32_t cap,
+                       float *total_area)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->have_dynamic)
+		return fail(c, RENDGPU_ESTATE, "upload_dynamic must come first");
+	uint32_t n = (uint32_t)c->host_lights.size();
+	if (out) {
+		uint32_t m = n < cap ? n : cap;
+		std::memcpy(out, c->host_lights.data(), (size_t)m *
+		  sizeof(nb_glight));
+	}
+	if (total_area)
+		*total_area = c->light_area;
+	return (int)n;
+}
+
+int rendgpu_last_error(struct rdata *rdp)
+{
+	Ctx *c = find_ctx(rdp);
+	return c ? c->last : RENDGPU_EINVAL;
+}
+
+const char *rendgpu_strerror(struct rdata *rdp)
+{
+	Ctx *c = find_ctx(rdp);
+	return c ? c->msg.c_str() : "no GPU context for this rdata";
+}
+
+} // extern "C"

@@ -1,0 +1,306 @@
+// Test infrastructure only: a headless driver for the reference renderer.
+//
+// Compiled together with the reference's own rend.c/util.c/... (see Makefile)
+// into _ref/libnbref.so.  It replaces the SDL2 frame loop of main.c with
+// plain entry points that tests and the CPU baseline call through ctypes:
+//
+//   refh_layout        sizeof/offsetof of the reference structs (rend.h:17-147)
+//   refh_render_frame  N threads on rend_render, as main.c:409-412,424-426
+//   refh_trace         intersect_tlas (rend.c:1976) over a ray batch, threaded
+//   refh_trace_pckts   intersect_pckts_tlas (rend.c:2472) over 8-ray packets
+//   refh_occluded      intersect_any_tlas (rend.c:2883) over a ray batch
+//   refh_camrays       make_camray_pckt (rend.c:3293) for one image block
+//
+// Nothing here changes the reference's arithmetic; it only calls it.
+
+#include <pthread.h>
+#include <stddef.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#include <math.h>
+
+#include "rend.h"
+#include "util.h"
+
+// Non-static functions of rend.c that rend.h does not declare.
+void intersect_tlas(float *t, float *u, float *v, unsigned int *id,
+                    float ox, float oy, float oz,
+                    float dx, float dy, float dz,
+                    struct bnode8 *nodes, struct rinst *insts,
+                    unsigned int tlasofs);
+void intersect_pckts_tlas(__m256 *t8, __m256 *u8, __m256 *v8, __m256i *id8,
+                          __m256 *ox8, __m256 *oy8, __m256 *oz8,
+                          __m256 *dx8, __m256 *dy8, __m256 *dz8,
+                          unsigned char pcnt,
+                          struct bnode8 *nodes, struct rinst *insts,
+                          unsigned int tlasofs);
+bool intersect_any_tlas(float tfar, float ox, float oy, float oz, float dx,
+                        float dy, float dz, struct bnode8 *nodes,
+                        struct rinst *insts, unsigned int tlasofs);
+void make_camray_pckt(__m256 *ox8, __m256 *oy8, __m256 *oz8,
+                      __m256 *dx8, __m256 *dy8, __m256 *dz8,
+                      unsigned int x, unsigned int y,
+                      __m256 xofs8, __m256 yofs8,
+                      struct rcam *c, struct rngstate8 *rngstate);
+
+#define OFS(T, f) ((unsigned long long)offsetof(struct T, f))
+
+// Layout of the reference structs, for the C-ABI mirror check.
+int refh_layout(unsigned long long *out, int cap)
+{
+	unsigned long long v[] = {
+	  sizeof(struct rdata), OFS(rdata, mtls), OFS(rdata, tris),
+	  OFS(rdata, nrms), OFS(rdata, instcnt), OFS(rdata, insts),
+	  OFS(rdata, aabbs), OFS(rdata, bnodes), OFS(rdata, tlasofs),
+	  OFS(rdata, cam), OFS(rdata, bgcol), OFS(rdata, width),
+	  OFS(rdata, height), OFS(rdata, acc), OFS(rdata, buf),
+	  OFS(rdata, blknum), OFS(rdata, rays), OFS(rdata, spp),
+	  OFS(rdata, samples),
+	  sizeof(struct rcam), OFS(rcam, eyex8), OFS(rcam, focrad8),
+	  sizeof(struct bnode8), sizeof(struct leaf4), sizeof(struct rinst),
+	  sizeof(struct rtri), sizeof(struct rnrm), sizeof(struct rmtl),
+	  sizeof(struct aabb), OFS(leaf4, id4), OFS(leaf4, tricnt),
+	  OFS(rinst, flags), OFS(rinst, triofs), OFS(rinst, tricnt)};
+	int n = (int)(sizeof(v) / sizeof(*v));
+	for (int i = 0; i < n && i < cap; i++)
+		out[i] = v[i];
+	return n;
+}
+
+struct frame_arg {
+	struct rdata *rd;
+};
+
+static void *render_thread(void *a)
+{
+	rend_render(((struct frame_arg *)a)->rd);
+	return NULL;
+}
+
+// One frame of the live renderer on nthreads threads (main.c:409-412), then
+// the bookkeeping main.c does after the join (main.c:424-426).  Returns the
+// ray count of the frame.
+unsigned int refh_render_frame(struct rdata *rd, int nthreads)
+{
+	if (nthreads < 1)
+		nthreads = 1;
+	pthread_t *th = malloc(sizeof(*th) * (size_t)nthreads);
+	struct frame_arg fa = {rd};
+	for (int i = 0; i < nthreads; i++)
+		pthread_create(&th[i], NULL, render_thread, &fa);
+	for (int i = 0; i < nthreads; i++)
+		pthread_join(th[i], NULL);
+	free(th);
+	unsigned int rays = rd->rays;
+	rd->blknum = 0;
+	rd->rays = 0;
+	rd->samples += rd->spp;
+	return rays;
+}
+
+// Rays: 8 floats each (ox oy oz tmax dx dy dz pad).  Hits: 4 words each
+// (t u v id) with id = tri << 12 | inst as in rend.c:2109/890.
+struct batch {
+	const float *rays;
+	unsigned int *hits; // t,u,v as float bits + id
+	unsigned char *occl;
+	unsigned int n;
+	struct rdata *rd;
+	int next; // atomic chunk counter
+	int mode; // 0 closest, 1 any, 2 packets
+};
+
+#define CHUNK 256
+
+// Direction-sign mask shared by the 8 rays of a packet, or -1 if they
+// differ (iscohval3, rend.c:225-247).
+static int packet_mask(const float *r)
+{
+	int m = -1;
+	for (int k = 0; k < 8; k++) {
+		const float *q = r + 8 * k;
+		int mk = (int)signbit(q[4]) | (int)signbit(q[5]) << 1 |
+		  (int)signbit(q[6]) << 2;
+		if (m >= 0 && mk != m)
+			return -1;
+		m = mk;
+	}
+	return m;
+}
+
+static void trace_single(struct batch *b, unsigned int s, unsigned int e)
+{
+	struct rdata *rd = b->rd;
+	for (unsigned int i = s; i < e; i++) {
+		const float *r = b->rays + 8ull * i;
+		float t = r[3], u = 0.0f, v = 0.0f;
+		unsigned int id = 0;
+		intersect_tlas(&t, &u, &v, &id, r[0], r[1], r[2], r[4], r[5],
+		  r[6], rd->bnodes, rd->insts, rd->tlasofs);
+		unsigned int *h = b->hits + 4ull * i;
+		memcpy(&h[0], &t, 4);
+		memcpy(&h[1], &u, 4);
+		memcpy(&h[2], &v, 4);
+		h[3] = id;
+	}
+}
+
+static void trace_packets(struct batch *b, unsigned int p, unsigned int pc)
+{
+	struct rdata *rd = b->rd;
+	__m256 ox8[16], oy8[16], oz8[16];
+	__m256 dx8[16], dy8[16], dz8[16];
+	__m256 t8[16], u8[16], v8[16];
+	__m256i id8[16];
+	for (unsigned int j = 0; j < pc; j++) {
+		for (int k = 0; k < 8; k++) {
+			const float *r = b->rays + 8ull * (p + 8 * j + k);
+			ox8[j][k] = r[0];
+			oy8[j][k] = r[1];
+			oz8[j][k] = r[2];
+			dx8[j][k] = r[4];
+			dy8[j][k] = r[5];
+			dz8[j][k] = r[6];
+			t8[j][k] = r[3];
+			u8[j][k] = 0.0f;
+			v8[j][k] = 0.0f;
+		}
+		id8[j] = _mm256_setzero_si256();
+	}
+	intersect_pckts_tlas(t8, u8, v8, id8, ox8, oy8, oz8, dx8, dy8, dz8,
+	  (unsigned char)pc, rd->bnodes, rd->insts, rd->tlasofs);
+	for (unsigned int j = 0; j < pc; j++)
+		for (int k = 0; k < 8; k++) {
+			unsigned int *h = b->hits + 4ull * (p + 8 * j + k);
+			memcpy(&h[0], &t8[j][k], 4);
+			memcpy(&h[1], &u8[j][k], 4);
+			memcpy(&h[2], &v8[j][k], 4);
+			h[3] = ((unsigned int *)&id8[j])[k];
+		}
+}
+
+static void *trace_thread(void *a)
+{
+	struct batch *b = a;
+	struct rdata *rd = b->rd;
+	while (1) {
+		int c = __atomic_fetch_add(&b->next, 1, __ATOMIC_SEQ_CST);
+		unsigned int s = (unsigned int)c * CHUNK;
+		if (s >= b->n)
+			break;
+		unsigned int e = s + CHUNK < b->n ? s + CHUNK : b->n;
+		if (b->mode == 2) {
+			// Packets of 8 consecutive rays, traced the way rend_render
+			// groups them (rend.c:3636-3700): runs of up to 16 packets
+			// whose rays all share one direction-sign mask go to
+			// intersect_pckts_tlas, an incoherent packet goes ray by ray
+			// to intersect_tlas.  n is a multiple of 8.
+			unsigned int p = s;
+			while (p < e) {
+				unsigned int run = 0;
+				int mask0 = -1;
+				while (p + 8 * run < e && run < 16) {
+					int m = packet_mask(b->rays + 8ull * (p + 8 * run));
+					if (m < 0 || (mask0 >= 0 && m != mask0))
+						break;
+					mask0 = m;
+					run++;
+				}
+				if (run == 0) {
+					trace_single(b, p, p + 8);
+					p += 8;
+					continue;
+				}
+				trace_packets(b, p, run);
+				p += 8 * run;
+			}
+			continue;
+		}
+		for (unsigned int i = s; i < e; i++) {
+			const float *r = b->rays + 8ull * i;
+			if (b->mode == 1) {
+				b->occl[i] = intersect_any_tlas(r[3], r[0],
+				  r[1], r[2], r[4], r[5], r[6], rd->bnodes,
+				  rd->insts, rd->tlasofs);
+				continue;
+			}
+			float t = r[3], u = 0.0f, v = 0.0f;
+			unsigned int id = 0;
+			intersect_tlas(&t, &u, &v, &id, r[0], r[1], r[2],
+			  r[4], r[5], r[6], rd->bnodes, rd->insts,
+			  rd->tlasofs);
+			unsigned int *h = b->hits + 4ull * i;
+			memcpy(&h[0], &t, 4);
+			memcpy(&h[1], &u, 4);
+			memcpy(&h[2], &v, 4);
+			h[3] = id;
+		}
+	}
+	return NULL;
+}
+
+static void run_batch(struct batch *b, int nthreads)
+{
+	if (nthreads < 1)
+		nthreads = 1;
+	pthread_t *th = malloc(sizeof(*th) * (size_t)nthreads);
+	for (int i = 0; i < nthreads; i++)
+		pthread_create(&th[i], NULL, trace_thread, b);
+	for (int i = 0; i < nthreads; i++)
+		pthread_join(th[i], NULL);
+	free(th);
+}
+
+void refh_trace(struct rdata *rd, const float *rays, unsigned int n,
+                unsigned int *hits, int nthreads)
+{
+	struct batch b = {rays, hits, NULL, n, rd, 0, 0};
+	run_batch(&b, nthreads);
+}
+
+void refh_trace_pckts(struct rdata *rd, const float *rays, unsigned int n,
+                      unsigned int *hits, int nthreads)
+{
+	struct batch b = {rays, hits, NULL, n, rd, 0, 2};
+	run_batch(&b, nthreads);
+}
+
+void refh_occluded(struct rdata *rd, const float *rays, unsigned int n,
+                   unsigned char *occl, int nthreads)
+{
+	struct batch b = {rays, NULL, occl, n, rd, 0, 1};
+	run_batch(&b, nthreads);
+}
+
+// Camera rays of one 4x2 packet at pixel (x, y), drawn the way rend_render
+// draws them (rend.c:3627, 3642): the caller passes the reseed values.
+// Output: 8 rays of 8 floats (ox oy oz FLT_MAX dx dy dz 0), packet lane order
+// pcktxofs8/pcktyofs8 (rend.c:131-132): lanes 0-3 row y, lanes 4-7 row y+1.
+void refh_camrays(struct rdata *rd, unsigned int x, unsigned int y,
+                  unsigned long long seed0, unsigned long long seed1,
+                  unsigned int npckts, const unsigned int *pxy, float *out)
+{
+	struct rngstate8 rng;
+	rand8_init(&rng, seed0, seed1);
+	__m256 xo = _mm256_set_ps(3, 2, 1, 0, 3, 2, 1, 0);
+	__m256 yo = _mm256_set_ps(1, 1, 1, 1, 0, 0, 0, 0);
+	for (unsigned int p = 0; p < npckts; p++) {
+		__m256 ox8, oy8, oz8, dx8, dy8, dz8;
+		unsigned int px = pxy ? pxy[2 * p] : x;
+		unsigned int py = pxy ? pxy[2 * p + 1] : y;
+		make_camray_pckt(&ox8, &oy8, &oz8, &dx8, &dy8, &dz8, px, py,
+		  xo, yo, &rd->cam, &rng);
+		for (int k = 0; k < 8; k++) {
+			float *r = out + 64ull * p + 8 * k;
+			r[0] = ox8[k];
+			r[1] = oy8[k];
+			r[2] = oz8[k];
+			r[3] = FLT_MAX;
+			r[4] = dx8[k];
+			r[5] = dy8[k];
+			r[6] = dz8[k];
+			r[7] = 0.0f;
+		}
+	}
+}

@@ -1,0 +1,238 @@
+"""ctypes access to the CPU checkers under oracle/ (test infrastructure).
+
+* ``oracle/liboracle.so``: the plain-C restatement (oracle/oracle.h);
+* ``oracle/_ref/libnbref.so``: the reference renderer compiled from its own
+  sources plus a headless driver (oracle/ref_harness.c).
+
+Both are built by ``make -C oracle``.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from nodebleed_b200.api import HIT_DTYPE, RAY_DTYPE
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE = os.path.join(ROOT, "oracle", "liboracle.so")
+REF = os.path.join(ROOT, "oracle", "_ref", "libnbref.so")
+
+FLT_MAX = np.float32(np.finfo(np.float32).max)
+
+
+class Counts(C.Structure):
+    _fields_ = [("nodes", C.c_uint64), ("leaves", C.c_uint64),
+                ("insts", C.c_uint64), ("rays", C.c_uint64)]
+
+
+class PtCfg(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("depth", C.c_uint32),
+                ("mode", C.c_uint32), ("nthreads", C.c_int),
+                ("nlights", C.c_uint32), ("lights", C.c_void_p),
+                ("light_area", C.c_float), ("x0", C.c_uint32),
+                ("y0", C.c_uint32), ("x1", C.c_uint32), ("y1", C.c_uint32),
+                ("closest", C.c_void_p), ("any", C.c_void_p),
+                ("counts", C.c_void_p)]
+
+
+_ORC = None
+_REF = None
+
+
+def oracle():
+    global _ORC
+    if _ORC is None:
+        L = C.CDLL(ORACLE)
+        vp, u32 = C.c_void_p, C.c_uint32
+        L.orc_trace.argtypes = [vp, vp, u32, vp, vp, C.c_int]
+        L.orc_occluded.argtypes = [vp, vp, u32, vp, C.c_int]
+        L.orc_refine.argtypes = [vp, vp, u32, vp]
+        L.orc_reintersect_f64.argtypes = [vp, vp, vp, u32, vp, vp]
+        L.orc_render.argtypes = [vp, vp, vp]
+        L.orc_render.restype = C.c_uint64
+        L.orc_accumulate.argtypes = [vp, vp]
+        L.orc_pcg_first.argtypes = [C.c_uint64, u32, C.c_uint64, u32, vp]
+        L.orc_sincos2pi.argtypes = [C.c_float, vp, vp]
+        _ORC = L
+    return _ORC
+
+
+def ref():
+    global _REF
+    if _REF is None:
+        if not os.path.exists(REF):
+            return None
+        L = C.CDLL(REF)
+        vp, u32 = C.c_void_p, C.c_uint32
+        L.refh_layout.argtypes = [vp, C.c_int]
+        L.refh_render_frame.argtypes = [vp, C.c_int]
+        L.refh_render_frame.restype = u32
+        L.refh_trace.argtypes = [vp, vp, u32, vp, C.c_int]
+        L.refh_trace_pckts.argtypes = [vp, vp, u32, vp, C.c_int]
+        L.refh_occluded.argtypes = [vp, vp, u32, vp, C.c_int]
+        L.refh_camrays.argtypes = [vp, u32, u32, C.c_uint64, C.c_uint64,
+                                   u32, vp, vp]
+        L.rend_staticinit.argtypes = [u32, u32]
+        L.rend_prepstatic.argtypes = [vp]
+        L.rend_prepdynamic.argtypes = [vp]
+        L.rend_staticinit(16, 8)
+        _REF = L
+    return _REF
+
+
+def fn_addr(lib, name):
+    return C.cast(getattr(lib, name), C.c_void_p).value
+
+
+def ncpu():
+    return os.cpu_count() or 1
+
+
+def orc_trace(rd_ptr, rays, counts=False, nthreads=None):
+    L = oracle()
+    rays = np.ascontiguousarray(rays, RAY_DTYPE)
+    hits = np.zeros(len(rays), HIT_DTYPE)
+    cnt = Counts()
+    L.orc_trace(rd_ptr, rays.ctypes.data, len(rays), hits.ctypes.data,
+                C.byref(cnt) if counts else None, nthreads or ncpu())
+    return (hits, cnt) if counts else hits
+
+
+def orc_refine(rd_ptr, rays, hits):
+    rays = np.ascontiguousarray(rays, RAY_DTYPE)
+    hits = hits.copy()
+    oracle().orc_refine(rd_ptr, rays.ctypes.data, len(rays), hits.ctypes.data)
+    return hits
+
+
+def orc_occluded(rd_ptr, rays, nthreads=None):
+    rays = np.ascontiguousarray(rays, RAY_DTYPE)
+    out = np.zeros(len(rays), np.uint8)
+    oracle().orc_occluded(rd_ptr, rays.ctypes.data, len(rays),
+                          out.ctypes.data, nthreads or ncpu())
+    return out
+
+
+def reintersect(rd_ptr, rays, ids):
+    rays = np.ascontiguousarray(rays, RAY_DTYPE)
+    ids = np.ascontiguousarray(ids, np.uint32)
+    t = np.zeros(len(rays))
+    b = np.zeros((len(rays), 3))
+    oracle().orc_reintersect_f64(rd_ptr, rays.ctypes.data, ids.ctypes.data,
+                                 len(rays), t.ctypes.data, b.ctypes.data)
+    return t, b
+
+
+def ref_trace(rd_ptr, rays, packets=False, nthreads=None):
+    L = ref()
+    rays = np.ascontiguousarray(rays, RAY_DTYPE)
+    hits = np.zeros(len(rays), HIT_DTYPE)
+    f = L.refh_trace_pckts if packets else L.refh_trace
+    f(rd_ptr, rays.ctypes.data, len(rays), hits.ctypes.data,
+      nthreads or ncpu())
+    return hits
+
+
+def ref_occluded(rd_ptr, rays, nthreads=None):
+    rays = np.ascontiguousarray(rays, RAY_DTYPE)
+    out = np.zeros(len(rays), np.uint8)
+    ref().refh_occluded(rd_ptr, rays.ctypes.data, len(rays), out.ctypes.data,
+                        nthreads or ncpu())
+    return out
+
+
+def orc_render(rd, lights, light_area, depth, mode=0, seed=1, window=None,
+               nthreads=None, use_ref=False, counts=None):
+    """Frame radiance (H, W, 3) of the oracle path tracer; traversal by the
+    restatement or, with use_ref, by the compiled reference."""
+    L = oracle()
+    r = rd.rd
+    W, H = r.width, r.height
+    cfg = PtCfg()
+    cfg.seed = seed
+    cfg.depth = depth
+    cfg.mode = mode
+    cfg.nthreads = nthreads or ncpu()
+    lights = np.ascontiguousarray(lights, np.float32)
+    cfg.nlights = len(lights)
+    cfg.lights = lights.ctypes.data if len(lights) else None
+    cfg.light_area = light_area
+    x0, y0, x1, y1 = window or (0, 0, W, H)
+    cfg.x0, cfg.y0, cfg.x1, cfg.y1 = x0, y0, x1, y1
+    if use_ref:
+        R = ref()
+        cfg.closest = fn_addr(R, "intersect_tlas")
+        cfg.any = fn_addr(R, "intersect_any_tlas")
+    if counts is not None:
+        cfg.counts = C.addressof(counts)
+    rad = np.zeros((H, W, 3), np.float32)
+    rays = L.orc_render(rd.ptr, C.byref(cfg), rad.ctypes.data)
+    return rad, rays
+
+
+def classify(rd_ptr, rays, ha, hb, eps_t, eps_b):
+    """Compare two hit sets on the same rays.  Returns (n_same, ties,
+    bad): disagreements are ties when an FP64 re-intersection shows the
+    two candidates within eps_t relative in t, or a candidate's
+    barycentrics within eps_b of an edge (or outside by less)."""
+    miss_a = ha["t"] == FLT_MAX
+    miss_b = hb["t"] == FLT_MAX
+    same = (miss_a & miss_b) | (~miss_a & ~miss_b & (ha["id"] == hb["id"]))
+    idx = np.nonzero(~same)[0]
+    ties, bad = [], []
+    if len(idx):
+        ta, ba = reintersect(rd_ptr, rays[idx], ha["id"][idx])
+        tb, bb = reintersect(rd_ptr, rays[idx], hb["id"][idx])
+        for j, i in enumerate(idx):
+            near_a = (not miss_a[i]) and np.min(ba[j]) < eps_b
+            near_b = (not miss_b[i]) and np.min(bb[j]) < eps_b
+            close_t = (not miss_a[i] and not miss_b[i] and
+                       abs(ta[j] - tb[j]) <= eps_t * min(abs(ta[j]), abs(tb[j])))
+            if near_a or near_b or close_t:
+                ties.append(i)
+            else:
+                bad.append(i)
+    return int(same.sum()), ties, bad
+
+
+def random_rays(rd, n, seed=0, spread=8.0):
+    """Half camera-origin rays, half from random interior points; random
+    directions."""
+    rng = np.random.default_rng(seed)
+    eye = rd.eye()
+    rays = np.zeros(n, RAY_DTYPE)
+    org = rng.uniform(-spread, spread, (n, 3)).astype(np.float32)
+    cam = rng.random(n) < 0.5
+    org[cam] = eye
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays["o"] = org
+    rays["d"] = d.astype(np.float32)
+    rays["tmax"] = FLT_MAX
+    return rays
+
+
+def camera_rays(rd, n_side=None, seed=3):
+    """Rays through jittered pixel positions of the scene camera (a
+    numpy version of the pinhole model, for test ray sets)."""
+    r = rd.rd
+    cam = np.frombuffer(bytes(r.cam), np.float32)
+    eye, ri, up, fwd = cam[0:3], cam[4:7], cam[8:11], cam[12:15]
+    W, H = r.width, r.height
+    rng = np.random.default_rng(seed)
+    ys, xs = np.mgrid[0:H, 0:W]
+    xs = xs.ravel() + rng.random(W * H)
+    ys = ys.ravel() + rng.random(W * H)
+    fov = cam[16 + 8 * 16]  # fovfdist8[0]
+    aspect = cam[16 + 8 * 14]
+    fd = cam[16 + 8 * 15]
+    sx = (xs / W - 0.5) * fov * aspect
+    sy = (ys / H - 0.5) * fov
+    d = fwd[None] * fd + ri[None] * sx[:, None] - up[None] * sy[:, None]
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.zeros(W * H, RAY_DTYPE)
+    rays["o"] = eye
+    rays["d"] = d.astype(np.float32)
+    rays["tmax"] = FLT_MAX
+    return rays

