@@ -49,6 +49,9 @@ def parse():
                    help="BLAS count (0 = the workload's 64)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--count", action="store_true",
+                   help="one extra untimed frame counting node visits and "
+                        "triangle tests per closest-hit ray")
     p.add_argument("--cpu-seconds", type=float, default=15.0,
                    help="target CPU time of the bounded CPU sample")
     return p.parse_args()
@@ -192,11 +195,14 @@ def cpu_baseline(a, rd, lights, area, budget_s):
     _, rays = ol.orc_render(rd, lights, area, a.depth, seed=1,
                             window=(0, y0, W, y0 + rows), use_ref=use_ref)
     dt = time.perf_counter() - t0
-    # visit counts of the reference algorithm on a ~1% sample of rows
+    # visit counts of the reference algorithm on ~1% of the rows, spread
+    # evenly over the frame
     cnt = ol.Counts()
-    srows = max(2, rows // 100)
-    _, crays = ol.orc_render(rd, lights, area, a.depth, seed=1,
-                             window=(0, y0, W, y0 + srows), counts=cnt)
+    crays = 0
+    for y in range(H // 200, H, max(1, H // 100)):
+        _, cr = ol.orc_render(rd, lights, area, a.depth, seed=1,
+                              window=(0, y, W, y + 1), counts=cnt)
+        crays += cr
     # counts cover closest-hit rays only: shadow rays of the sample are
     # part of crays, so divide by the closest-hit share measured on the GPU
     return {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": cores,
@@ -290,6 +296,18 @@ def run_ours(a):
                "timing": "wall clock around upload_dynamic + render + "
                          "readback of the ARGB8 image (pinned host)"}
 
+    visits = None
+    if a.count:
+        # one context per rdata: the counting context replaces the timed one
+        gr.close()
+        gc = api.GpuRenderer(rd, max_depth=a.depth, seed=1 + rank,
+                             count=True, device=dev).upload()
+        gc.frame()
+        sc = gc.stats()
+        visits = {"nodes_per_ray": sc["node_visits"] / sc["closest_rays"],
+                  "tri_tests_per_ray": sc["tri_tests"] / sc["closest_rays"]}
+        gc.close()
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(a, rd, lights, area, a.cpu_seconds)
@@ -331,6 +349,7 @@ def run_ours(a):
                "ms_trace_per_frame": trace_ms / a.steps,
                "ms_shadow_per_frame": shadow_ms / a.steps,
                "gpu_launches": launches, "e2e": e2e, "roofline": roof,
+               "gpu_visits": visits,
                "cpu_baseline": cpu, "clocks": cl,
                "scene": {"unique_tris": scene.tris,
                          "instanced_tris": scene.inst_tris,

@@ -46,7 +46,9 @@ enum rendgpu_mode {
 };
 
 enum rendgpu_flags {
-	RENDGPU_FLAG_TIMING = 1u << 0  /* record per-kernel CUDA events */
+	RENDGPU_FLAG_TIMING = 1u << 0, /* record per-kernel CUDA events */
+	RENDGPU_FLAG_COUNT = 1u << 1   /* count node visits / triangle tests of
+	                                  the closest-hit traces (slower) */
 };
 
 struct rendgpu_cfg {
@@ -88,6 +90,8 @@ struct rendgpu_stats {
 	uint64_t device_bytes;   /* device memory held by this context */
 	uint64_t h2d_bytes;      /* host->device bytes of the last upload/render */
 	uint64_t d2h_bytes;      /* device->host bytes of the last readback */
+	uint64_t node_visits;    /* closest-hit node visits (COUNT flag) */
+	uint64_t tri_tests;      /* closest-hit triangle tests (COUNT flag) */
 };
 
 /* Create the GPU context of `rd` (one per rdata).  Replaces nothing in the

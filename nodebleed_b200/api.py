@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 SCENE_SMALL, SCENE_SCALE, SCENE_BATCH, SCENE_STRESS, SCENE_TINY = 1, 2, 3, 5, 9
 MODE_PATH, MODE_PRIMARY = 0, 1
-FLAG_TIMING = 1
+FLAG_TIMING, FLAG_COUNT = 1, 2
 
 # struct rendgpu_ray / rendgpu_hit (32 / 16 bytes)
 RAY_DTYPE = np.dtype([("o", "<f4", (3,)), ("tmax", "<f4"), ("d", "<f4", (3,)),
@@ -73,7 +73,8 @@ class RendgpuStats(C.Structure):
                 ("ms_trace", C.c_float), ("ms_shadow", C.c_float),
                 ("ms_shade", C.c_float), ("device_errors", C.c_uint32),
                 ("max_stack", C.c_uint32), ("device_bytes", C.c_uint64),
-                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
+                ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -255,7 +256,7 @@ class GpuRenderer:
     """The rendgpu C ABI on one RenderData."""
 
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
-                 timing=False, device=0):
+                 timing=False, device=0, count=False):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -263,7 +264,8 @@ class GpuRenderer:
         cfg.size = C.sizeof(RendgpuCfg)
         cfg.max_depth = max_depth
         cfg.mode = mode
-        cfg.flags = FLAG_TIMING if timing else 0
+        cfg.flags = (FLAG_TIMING if timing else 0) | \
+            (FLAG_COUNT if count else 0)
         cfg.seed = seed
         cfg.device = device
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))

@@ -25,13 +25,15 @@ struct FrameDev {
 	// queues: 2 float4 per ray: (o, tmax) (d, path as bits)
 	float4   *q[2];
 	float4   *hits;    // (t, u, v, id bits)
-	float4   *shadow;  // 3 float4: (o, tfar) (d, path) (c, 0)
+	float4   *shadow;  // 2 float4: (o, tfar) (d, path)
+	float4   *scol;    // shadow contribution (c, 0)
 	float4   *pT;      // (T.rgb, spec flag)
 	float4   *pL;      // (L.rgb, 0)
 	uint2    *rng;     // PCG32 state
 	float    *acc;     // W*H*3
 	uint32_t *buf;     // W*H ARGB8
-	uint32_t *cnt;     // [0],[1] ray queues, [2] shadow, [3] errors
+	uint32_t *cnt;     // [0],[1] ray queues, [2] shadow, [3] errors,
+	                   // [4] closest-hit work counter, [5] shadow work
 	unsigned long long *rays; // [0] closest, [1] shadow
 	uint32_t  W, H, spp, npaths;
 };
@@ -139,6 +141,8 @@ __global__ void __launch_bounds__(256) k_gen(FrameDev F, FrameArgs A)
 {
 	uint32_t tiles_w = (F.W + 7u) >> 3, tiles_h = (F.H + 3u) >> 2;
 	uint32_t total = tiles_w * tiles_h * 32u * F.spp;
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		F.cnt[4] = 0u;
 	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	     i - threadIdx.x < total; i += gridDim.x * blockDim.x) {
 		uint32_t x = 0, y = 0, s = 0;
@@ -197,82 +201,88 @@ __global__ void __launch_bounds__(256) k_gen(FrameDev F, FrameArgs A)
 	}
 }
 
-// Closest-hit trace of a ray queue (count in *count).
-template <int STACK>
+// Closest-hit trace of a ray queue (count in *count): raw hits.
+// COUNT adds visit / triangle-test counts to counts[0..1].
+template <int STACK, bool COUNT>
 __global__ void __launch_bounds__(128) k_trace(DScene S, const float4 *rays,
                                                const uint32_t *count,
-                                               float4 *hits, uint32_t *errs,
-                                               unsigned long long *nrays)
+                                               uint32_t *work, float4 *hits,
+                                               uint32_t *errs,
+                                               unsigned long long *nrays,
+                                               unsigned long long *counts)
 {
 	extern __shared__ uint2 sstk[];
-	uint2 *stk = sstk + threadIdx.x;
 	uint32_t n = *count;
 	if (blockIdx.x == 0 && threadIdx.x == 0 && nrays)
 		atomicAdd(nrays, (unsigned long long)n);
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-	     i += gridDim.x * blockDim.x) {
-		float4 a = rays[2u * i], b = rays[2u * i + 1u];
-		THit h;
-		uint32_t err = 0;
-		float4 out = make_float4(FLT_MAX, 0.0f, 0.0f, 0.0f);
-		if (traverse<false, STACK>(S, a.x, a.y, a.z, b.x, b.y, b.z, a.w,
-		  stk, blockDim.x, h, err))
-			out = finish_hit(S, a.x, a.y, a.z, b.x, b.y, b.z, h);
-		if (err)
-			atomicAdd(errs, 1u);
-		hits[i] = out;
-	}
+	SinkRaw sink{hits, errs, COUNT ? counts : nullptr};
+	trace_persistent<false, STACK, COUNT>(S, rays, n, work,
+	  sstk + threadIdx.x, blockDim.x, sink);
 }
 
-// Any-hit trace of host/API rays: occl[i] = hit in (0, tmax).
+// Any-hit trace of API rays: occl[i] = hit in (0, tmax).
 template <int STACK>
 __global__ void __launch_bounds__(128) k_occluded(DScene S,
                                                   const float4 *rays,
-                                                  uint32_t n, uint8_t *occl,
+                                                  const uint32_t *count,
+                                                  uint32_t *work, uint8_t *occl,
                                                   uint32_t *errs)
 {
 	extern __shared__ uint2 sstk[];
-	uint2 *stk = sstk + threadIdx.x;
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-	     i += gridDim.x * blockDim.x) {
-		float4 a = rays[2u * i], b = rays[2u * i + 1u];
-		THit h;
-		uint32_t err = 0;
-		bool hit = traverse<true, STACK>(S, a.x, a.y, a.z, b.x, b.y, b.z,
-		  a.w, stk, blockDim.x, h, err);
-		if (err)
-			atomicAdd(errs, 1u);
-		occl[i] = hit ? 1 : 0;
-	}
+	SinkOccl sink{occl, errs};
+	trace_persistent<true, STACK, false>(S, rays, *count, work,
+	  sstk + threadIdx.x, blockDim.x, sink);
 }
 
-// Shadow queue: add the carried contribution when unoccluded.
+// Unoccluded shadow rays add their carried contribution to the path.
+struct SinkShadow {
+	const float4 *rays;
+	const float4 *scol;
+	float4       *pL;
+	uint32_t     *errs;
+	__device__ void operator()(uint32_t i, const Trav &T, uint32_t err)
+	{
+		if (err) {
+			atomicAdd(errs, 1u);
+			return;
+		}
+		if (T.found)
+			return;
+		uint32_t path = __float_as_uint(rays[2u * i + 1u].w);
+		float4 c = scol[i];
+		float4 L = pL[path];
+		L.x = __fadd_rn(L.x, c.x);
+		L.y = __fadd_rn(L.y, c.y);
+		L.z = __fadd_rn(L.z, c.z);
+		pL[path] = L;
+	}
+};
+
 template <int STACK>
 __global__ void __launch_bounds__(128) k_shadow(DScene S, FrameDev F)
 {
 	extern __shared__ uint2 sstk[];
-	uint2 *stk = sstk + threadIdx.x;
 	uint32_t n = F.cnt[2];
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		atomicAdd(&F.rays[1], (unsigned long long)n);
+	SinkShadow sink{F.shadow, F.scol, F.pL, &F.cnt[3]};
+	trace_persistent<true, STACK, false>(S, F.shadow, n, &F.cnt[5],
+	  sstk + threadIdx.x, blockDim.x, sink);
+}
+
+// Raw hits -> the reference's hit record (t, u, v, tri << 12 | inst).
+__global__ void __launch_bounds__(256) k_refine(DScene S, const float4 *rays,
+                                                const uint32_t *count,
+                                                const float4 *raw,
+                                                float4 *hits)
+{
+	uint32_t n = *count;
 	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
 	     i += gridDim.x * blockDim.x) {
-		float4 a = F.shadow[3u * i], b = F.shadow[3u * i + 1u];
-		THit h;
-		uint32_t err = 0;
-		bool hit = traverse<true, STACK>(S, a.x, a.y, a.z, b.x, b.y, b.z,
-		  a.w, stk, blockDim.x, h, err);
-		if (err)
-			atomicAdd(&F.cnt[3], 1u);
-		if (!hit && !err) {
-			float4 c = F.shadow[3u * i + 2u];
-			uint32_t path = __float_as_uint(b.w);
-			float4 L = F.pL[path];
-			L.x = __fadd_rn(L.x, c.x);
-			L.y = __fadd_rn(L.y, c.y);
-			L.z = __fadd_rn(L.z, c.z);
-			F.pL[path] = L;
-		}
+		float4 a = rays[2u * i], b = rays[2u * i + 1u];
+		float4 h = raw[i];
+		THit th{h.x, __float_as_uint(h.y), __float_as_uint(h.z)};
+		hits[i] = finish_hit(S, a.x, a.y, a.z, b.x, b.y, b.z, th);
 	}
 }
 
@@ -285,6 +295,10 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 	uint32_t n = F.cnt[cur];
 	const float4 *rays = F.q[cur];
 	float4 *next = F.q[cur ^ 1u];
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		F.cnt[4] = 0u;
+		F.cnt[5] = 0u;
+	}
 	for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n;
 	     i0 += gridDim.x * blockDim.x) {
 		uint32_t i = i0 + threadIdx.x;
@@ -297,6 +311,10 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 		if (live) {
 			float4 ra = rays[2u * i], rb = rays[2u * i + 1u];
 			float4 h = F.hits[i];
+			if (h.x != FLT_MAX) {
+				THit th{h.x, __float_as_uint(h.y), __float_as_uint(h.z)};
+				h = finish_hit(S, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, th);
+			}
 			path = __float_as_uint(rb.w);
 			float4 T = F.pT[path];
 			float4 L = F.pL[path];
@@ -509,10 +527,10 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 		}
 		uint32_t ss = append(&F.cnt[2], want_shadow);
 		if (want_shadow) {
-			F.shadow[3u * ss] = make_float4(so[0], so[1], so[2], tfar);
-			F.shadow[3u * ss + 1u] = make_float4(sd[0], sd[1], sd[2],
+			F.shadow[2u * ss] = make_float4(so[0], so[1], so[2], tfar);
+			F.shadow[2u * ss + 1u] = make_float4(sd[0], sd[1], sd[2],
 			  __uint_as_float(path));
-			F.shadow[3u * ss + 2u] = make_float4(sc[0], sc[1], sc[2], 0.0f);
+			F.scol[ss] = make_float4(sc[0], sc[1], sc[2], 0.0f);
 		}
 	}
 }

@@ -70,11 +70,11 @@ struct Ctx {
 	bool     have_static = false, have_dynamic = false;
 	uint32_t ntris = 0, nnodes = 0;
 	// frame
-	DevBuf q0, q1, hits, shadow, pT, pL, rng, acc, buf, cnt, rays;
+	DevBuf q0, q1, hits, shadow, scol, pT, pL, rng, acc, buf, cnt, rays;
 	uint32_t W = 0, H = 0, spp = 0, npaths = 0;
 	bool     have_frame = false;
-	// batch scratch
-	DevBuf brays, bhits, berr;
+	// batch scratch: rays, raw hits, output; berr = [count, errors, work]
+	DevBuf brays, braw, bhits, berr;
 	// stats / errors
 	rendgpu_stats st{};
 	int          last = 0;
@@ -149,22 +149,39 @@ int trace_grid(Ctx *c, const void *fn, int stack)
 	return per_sm * c->nsm;
 }
 
-// Launch a closest-hit trace of `count` (device) rays.
-int launch_trace(Ctx *c, const float4 *rays, const uint32_t *count,
-                 float4 *hits, uint32_t *errs, unsigned long long *nrays)
+template <int STACK, bool COUNT>
+void trace_kernel(Ctx *c, const float4 *rays, const uint32_t *count,
+                  uint32_t *work, float4 *hits, uint32_t *errs,
+                  unsigned long long *nrays)
 {
-	DScene S = scene_of(c);
+	auto fn = k_trace<STACK, COUNT>;
+	size_t smem = (size_t)STACK * kTraceBlock * sizeof(uint2);
+	fn<<<trace_grid(c, (const void *)fn, STACK), kTraceBlock, smem,
+	  c->stream>>>(scene_of(c), rays, count, work, hits, errs, nrays,
+	  c->rays.as<unsigned long long>() + 2);
+}
+
+// Launch a closest-hit trace of `count` (device) rays: raw hits.
+int launch_trace(Ctx *c, const float4 *rays, const uint32_t *count,
+                 uint32_t *work, float4 *hits, uint32_t *errs,
+                 unsigned long long *nrays)
+{
 	uint32_t need = need_stack(c);
+	bool cnt = (c->cfg.flags & RENDGPU_FLAG_COUNT) != 0;
 	if (need <= (uint32_t)kStackSmall) {
-		auto fn = k_trace<kStackSmall>;
-		size_t smem = (size_t)kStackSmall * kTraceBlock * sizeof(uint2);
-		fn<<<trace_grid(c, (const void *)fn, kStackSmall), kTraceBlock,
-		  smem, c->stream>>>(S, rays, count, hits, errs, nrays);
+		if (cnt)
+			trace_kernel<kStackSmall, true>(c, rays, count, work, hits,
+			  errs, nrays);
+		else
+			trace_kernel<kStackSmall, false>(c, rays, count, work, hits,
+			  errs, nrays);
 	} else if (need <= (uint32_t)kStackLarge) {
-		auto fn = k_trace<kStackLarge>;
-		size_t smem = (size_t)kStackLarge * kTraceBlock * sizeof(uint2);
-		fn<<<trace_grid(c, (const void *)fn, kStackLarge), kTraceBlock,
-		  smem, c->stream>>>(S, rays, count, hits, errs, nrays);
+		if (cnt)
+			trace_kernel<kStackLarge, true>(c, rays, count, work, hits,
+			  errs, nrays);
+		else
+			trace_kernel<kStackLarge, false>(c, rays, count, work, hits,
+			  errs, nrays);
 	} else {
 		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
 		  "stack");
@@ -195,8 +212,8 @@ int launch_shadow(Ctx *c, FrameDev &F)
 	return 0;
 }
 
-int launch_occluded(Ctx *c, const float4 *rays, uint32_t n, uint8_t *occl,
-                    uint32_t *errs)
+int launch_occluded(Ctx *c, const float4 *rays, const uint32_t *count,
+                    uint32_t *work, uint8_t *occl, uint32_t *errs)
 {
 	DScene S = scene_of(c);
 	uint32_t need = need_stack(c);
@@ -204,12 +221,12 @@ int launch_occluded(Ctx *c, const float4 *rays, uint32_t n, uint8_t *occl,
 		auto fn = k_occluded<kStackSmall>;
 		size_t smem = (size_t)kStackSmall * kTraceBlock * sizeof(uint2);
 		fn<<<trace_grid(c, (const void *)fn, kStackSmall), kTraceBlock,
-		  smem, c->stream>>>(S, rays, n, occl, errs);
+		  smem, c->stream>>>(S, rays, count, work, occl, errs);
 	} else if (need <= (uint32_t)kStackLarge) {
 		auto fn = k_occluded<kStackLarge>;
 		size_t smem = (size_t)kStackLarge * kTraceBlock * sizeof(uint2);
 		fn<<<trace_grid(c, (const void *)fn, kStackLarge), kTraceBlock,
-		  smem, c->stream>>>(S, rays, n, occl, errs);
+		  smem, c->stream>>>(S, rays, count, work, occl, errs);
 	} else {
 		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
 		  "stack");
@@ -225,6 +242,7 @@ FrameDev frame_of(Ctx *c)
 	F.q[1] = c->q1.as<float4>();
 	F.hits = c->hits.as<float4>();
 	F.shadow = c->shadow.as<float4>();
+	F.scol = c->scol.as<float4>();
 	F.pT = c->pT.as<float4>();
 	F.pL = c->pL.as<float4>();
 	F.rng = c->rng.as<uint2>();
@@ -307,8 +325,8 @@ int render_frame(Ctx *c)
 	c->nev = 0;
 	c->st.launches = 0;
 	c->st.trace_launches = 0;
-	NB_CK(c, cudaMemsetAsync(c->cnt.p, 0, 4 * sizeof(uint32_t), c->stream));
-	NB_CK(c, cudaMemsetAsync(c->rays.p, 0, 2 * sizeof(unsigned long long),
+	NB_CK(c, cudaMemsetAsync(c->cnt.p, 0, 8 * sizeof(uint32_t), c->stream));
+	NB_CK(c, cudaMemsetAsync(c->rays.p, 0, 4 * sizeof(unsigned long long),
 	  c->stream));
 	ev_record(c); // 0
 	uint32_t tiles = ((c->W + 7u) >> 3) * ((c->H + 3u) >> 2) * 32u * c->spp;
@@ -321,8 +339,8 @@ int render_frame(Ctx *c)
 		uint32_t cur = k & 1u;
 		trace_ev.push_back(c->nev);
 		ev_record(c);
-		rc = launch_trace(c, F.q[cur], F.cnt + cur, F.hits, F.cnt + 3,
-		  F.rays);
+		rc = launch_trace(c, F.q[cur], F.cnt + cur, F.cnt + 4, F.hits,
+		  F.cnt + 3, F.rays);
 		if (rc)
 			return rc;
 		ev_record(c);
@@ -353,7 +371,7 @@ int render_frame(Ctx *c)
 	NB_CK(c, cudaGetLastError());
 	c->st.launches++;
 	ev_record(c);
-	unsigned long long hr[2];
+	unsigned long long hr[4];
 	uint32_t hc[4];
 	NB_CK(c, cudaMemcpyAsync(hr, c->rays.p, sizeof(hr),
 	  cudaMemcpyDeviceToHost, c->stream));
@@ -361,6 +379,8 @@ int render_frame(Ctx *c)
 	  cudaMemcpyDeviceToHost, c->stream));
 	NB_CK(c, cudaStreamSynchronize(c->stream));
 	c->st.closest_rays = hr[0];
+	c->st.node_visits = hr[2];
+	c->st.tri_tests = hr[3];
 	c->st.shadow_rays = hr[1];
 	c->st.rays = hr[0] + hr[1];
 	c->st.device_errors = hc[3];
@@ -387,8 +407,8 @@ void free_ctx(Ctx *c)
 {
 	DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs, &c->insts,
 	  &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits, &c->shadow,
-	  &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt, &c->rays,
-	  &c->brays, &c->bhits, &c->berr};
+	  &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
+	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr};
 	for (DevBuf *b : bufs)
 		b->release();
 	for (int i = 0; i < 64; i++)
@@ -403,8 +423,8 @@ uint64_t held_bytes(const Ctx *c)
 {
 	const DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs,
 	  &c->insts, &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits,
-	  &c->shadow, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
-	  &c->rays, &c->brays, &c->bhits, &c->berr};
+	  &c->shadow, &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf,
+	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
 		s += b->cap;
@@ -452,7 +472,9 @@ int rendgpu_init(struct rdata *rdp, const struct rendgpu_cfg *cfg)
 	}
 	// dynamic smem above 48 KB for the deep-stack variants
 	size_t big = (size_t)kStackLarge * kTraceBlock * sizeof(uint2);
-	cudaFuncSetAttribute(k_trace<kStackLarge>,
+	cudaFuncSetAttribute(k_trace<kStackLarge, false>,
+	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+	cudaFuncSetAttribute(k_trace<kStackLarge, true>,
 	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
 	cudaFuncSetAttribute(k_shadow<kStackLarge>,
 	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
@@ -609,7 +631,8 @@ int rendgpu_resaccum(struct rdata *rdp)
 	NB_CK(c, c->q0.ensure(np * 32));
 	NB_CK(c, c->q1.ensure(np * 32));
 	NB_CK(c, c->hits.ensure(np * 16));
-	NB_CK(c, c->shadow.ensure(np * 48));
+	NB_CK(c, c->shadow.ensure(np * 32));
+	NB_CK(c, c->scol.ensure(np * 16));
 	NB_CK(c, c->pT.ensure(np * 16));
 	NB_CK(c, c->pL.ensure(np * 16));
 	NB_CK(c, c->rng.ensure(np * 8));
@@ -699,13 +722,20 @@ int rendgpu_trace_rays_device(struct rdata *rdp, const void *rays,
 	if (n == 0)
 		return 0;
 	NB_CK(c, cudaSetDevice(c->device));
-	// count lives in the batch scratch: [0] count, [1] errors
-	NB_CK(c, cudaMemcpyAsync(c->berr.p, &n, sizeof(n),
+	NB_CK(c, c->braw.ensure((size_t)n * 16));
+	// berr: [0] count, [1] errors, [2] work counter
+	uint32_t hdr[3] = {n, 0u, 0u};
+	NB_CK(c, cudaMemcpyAsync(c->berr.p, hdr, sizeof(hdr),
 	  cudaMemcpyHostToDevice, c->stream));
-	NB_CK(c, cudaMemsetAsync(c->berr.as<uint32_t>() + 1, 0, 4, c->stream));
-	return launch_trace(c, static_cast<const float4 *>(rays),
-	  c->berr.as<uint32_t>(), static_cast<float4 *>(hits),
-	  c->berr.as<uint32_t>() + 1, nullptr);
+	uint32_t *b = c->berr.as<uint32_t>();
+	const float4 *r4 = static_cast<const float4 *>(rays);
+	rc = launch_trace(c, r4, b, b + 2, c->braw.as<float4>(), b + 1, nullptr);
+	if (rc)
+		return rc;
+	k_refine<<<grid_for(c, n, 256), 256, 0, c->stream>>>(scene_of(c), r4, b,
+	  c->braw.as<float4>(), static_cast<float4 *>(hits));
+	NB_CK(c, cudaGetLastError());
+	return 0;
 }
 
 int rendgpu_occluded_device(struct rdata *rdp, const void *rays, uint32_t n,
@@ -718,9 +748,12 @@ int rendgpu_occluded_device(struct rdata *rdp, const void *rays, uint32_t n,
 	if (n == 0)
 		return 0;
 	NB_CK(c, cudaSetDevice(c->device));
-	NB_CK(c, cudaMemsetAsync(c->berr.as<uint32_t>() + 1, 0, 4, c->stream));
-	return launch_occluded(c, static_cast<const float4 *>(rays), n,
-	  static_cast<uint8_t *>(occl), c->berr.as<uint32_t>() + 1);
+	uint32_t hdr[3] = {n, 0u, 0u};
+	NB_CK(c, cudaMemcpyAsync(c->berr.p, hdr, sizeof(hdr),
+	  cudaMemcpyHostToDevice, c->stream));
+	uint32_t *b = c->berr.as<uint32_t>();
+	return launch_occluded(c, static_cast<const float4 *>(rays), b, b + 2,
+	  static_cast<uint8_t *>(occl), b + 1);
 }
 
 static int batch_errors(Ctx *c)

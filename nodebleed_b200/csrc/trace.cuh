@@ -26,7 +26,6 @@
 
 namespace nb {
 
-constexpr uint32_t kIGroup = 0x100u;          // stack entry holds instances
 constexpr float kWiden = 1.00000095367431640625f; // 1 + 2^-20
 
 struct DScene {
@@ -99,7 +98,17 @@ __device__ __forceinline__ uint32_t qb(uint32_t w, int k)
 	return (w >> (8 * k)) & 0xffu;
 }
 
+// Byte k of w as the float 2^23 + byte (one byte permute: the byte goes
+// into the mantissa of 2^23).
+__device__ __forceinline__ float qbf(uint32_t w, int k)
+{
+	return __uint_as_float(__byte_perm(w, 0x4b000000u, 0x7440u + k));
+}
+
 // Test the 8 children of node `ni`; returns the node and triangle groups.
+// Plane distances are fma(2^23 + q, s, b - 2^23 s) with s = scale / d and
+// b = (origin - o) / d: rounding b - 2^23 s moves a plane by at most half a
+// quantum, and every child box is padded by at least one quantum per side.
 __device__ __forceinline__ void visit(const nb_qnode *__restrict__ nodes,
                                       uint32_t ni, const TRay &r, float tmax,
                                       uint2 &ng, uint2 &tg)
@@ -114,9 +123,12 @@ __device__ __forceinline__ void visit(const nb_qnode *__restrict__ nodes,
 	float scx = __uint_as_float((w0.w & 0xffu) << 23) * r.ix;
 	float scy = __uint_as_float(((w0.w >> 8) & 0xffu) << 23) * r.iy;
 	float scz = __uint_as_float(((w0.w >> 16) & 0xffu) << 23) * r.iz;
-	float bx = (__uint_as_float(w0.x) - r.ox) * r.ix;
-	float by = (__uint_as_float(w0.y) - r.oy) * r.iy;
-	float bz = (__uint_as_float(w0.z) - r.oz) * r.iz;
+	float bx = __fmaf_rn(-8388608.0f, scx,
+	  (__uint_as_float(w0.x) - r.ox) * r.ix);
+	float by = __fmaf_rn(-8388608.0f, scy,
+	  (__uint_as_float(w0.y) - r.oy) * r.iy);
+	float bz = __fmaf_rn(-8388608.0f, scz,
+	  (__uint_as_float(w0.z) - r.oz) * r.iz);
 	bool fx = signbit(r.ix), fy = signbit(r.iy), fz = signbit(r.iz);
 	// lo/hi words: x lo = w2.x,w2.y  y lo = w2.z,w2.w  z lo = w3.x,w3.y
 	//              x hi = w3.z,w3.w  y hi = w4.x,w4.y  z hi = w4.z,w4.w
@@ -134,12 +146,12 @@ __device__ __forceinline__ void visit(const nb_qnode *__restrict__ nodes,
 		uint32_t wnx = s < 4 ? nx0 : nx1, wfx = s < 4 ? fx0 : fx1;
 		uint32_t wny = s < 4 ? ny0 : ny1, wfy = s < 4 ? fy0 : fy1;
 		uint32_t wnz = s < 4 ? nz0 : nz1, wfz = s < 4 ? fz0 : fz1;
-		float tnx = __fmaf_rn((float)qb(wnx, b), scx, bx);
-		float tny = __fmaf_rn((float)qb(wny, b), scy, by);
-		float tnz = __fmaf_rn((float)qb(wnz, b), scz, bz);
-		float tfx = __fmaf_rn((float)qb(wfx, b), scx, bx);
-		float tfy = __fmaf_rn((float)qb(wfy, b), scy, by);
-		float tfz = __fmaf_rn((float)qb(wfz, b), scz, bz);
+		float tnx = __fmaf_rn(qbf(wnx, b), scx, bx);
+		float tny = __fmaf_rn(qbf(wny, b), scy, by);
+		float tnz = __fmaf_rn(qbf(wnz, b), scz, bz);
+		float tfx = __fmaf_rn(qbf(wfx, b), scx, bx);
+		float tfy = __fmaf_rn(qbf(wfy, b), scy, by);
+		float tfz = __fmaf_rn(qbf(wfz, b), scz, bz);
 		float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
 		float tf = fminf(fminf(tfx, tfy), tfz) * kWiden;
 		if (tn <= fminf(tf, tcap)) {
@@ -231,105 +243,252 @@ struct THit {
 	uint32_t inst;
 };
 
-// Traverse the scene.  ANY: stop at the first hit (occlusion).  `stk` is
-// this thread's stack column (entry k at stk[k * stride]).  Returns true on
-// a hit; sets *err on a stack overflow (the ray is then abandoned).
-template <bool ANY, int STACK>
-__device__ __forceinline__ bool traverse(const DScene &S, float wox,
-                                         float woy, float woz, float wdx,
-                                         float wdy, float wdz, float tmax,
-                                         uint2 *stk, uint32_t stride,
-                                         THit &h, uint32_t &err)
+constexpr uint32_t kItemGroup = 0x80000000u; // stack entry .x: item group
+constexpr uint32_t kFull = 0xffffffffu;
+
+// Per-lane traversal state of the persistent kernels.
+struct Trav {
+	TRay     r;
+	uint2    ng, tg;
+	int      sp, blas_sp;
+	uint32_t level, cinst;
+	float    bt;
+	uint32_t btri, binst;
+	bool     found;
+	uint32_t nvisit, ntest; // counting kernels only
+};
+
+constexpr uint32_t kNone = 0xffffffffu;
+
+// New ray: state reset; the caller visits the TLAS root (node 0).
+__device__ __forceinline__ void trav_start(Trav &T, float4 a, float4 b)
 {
-	TRay r;
-	tray_slab(r, wox, woy, woz, wdx, wdy, wdz);
-	uint2 ng, tg;
-	visit(S.tlas, 0u, r, tmax, ng, tg);
-	int sp = 0, blas_sp = -1;
-	uint32_t level = 0, cinst = 0;
-	float bt = tmax;
-	bool found = false;
-	for (;;) {
-		while (tg.y) {
-			uint32_t i = __ffs(tg.y) - 1;
-			tg.y &= tg.y - 1u;
-			uint32_t item = tg.x + i;
-			if (level == 0u) {
-				uint32_t inst = __ldg(S.irefs + item);
-				if (ng.y >> 24) {
-					if (sp >= STACK) {
-						err = 1u;
-						return found;
-					}
-					stk[(uint32_t)sp++ * stride] = ng;
-				}
-				if (tg.y) {
-					if (sp >= STACK) {
-						err = 1u;
-						return found;
-					}
-					stk[(uint32_t)sp++ * stride] =
-					  make_uint2(tg.x, (tg.y << 24) | kIGroup);
-				}
-				blas_sp = sp;
-				level = 1u;
-				cinst = inst;
-				const float4 *ip = S.insts + 4u * inst;
-				float4 m0 = __ldg(ip), m1 = __ldg(ip + 1);
-				float4 m2 = __ldg(ip + 2);
-				uint32_t root = __float_as_uint(__ldg(ip + 3).x);
-				float o[3], d[3];
-				xform(m0, m1, m2, wox, woy, woz, wdx, wdy, wdz, o, d);
-				tray_slab(r, o[0], o[1], o[2], d[0], d[1], d[2]);
-				tray_watertight(r);
-				visit(S.blas, root, r, bt, ng, tg);
-				continue;
+	tray_slab(T.r, a.x, a.y, a.z, b.x, b.y, b.z);
+	T.sp = 0;
+	T.blas_sp = -1;
+	T.level = 0;
+	T.cinst = 0;
+	T.bt = a.w;
+	T.btri = 0;
+	T.binst = 0;
+	T.found = false;
+	T.ng = make_uint2(0u, 0u);
+	T.tg = make_uint2(0u, 0u);
+	T.nvisit = 0;
+	T.ntest = 0;
+}
+
+// Decide this lane's next step: a triangle to test (*titem), a node to
+// visit (*vnode: a child, or a BLAS root after entering an instance), or a
+// pop.  Stack pushes and the object-space transform happen here; the
+// triangle test and the node visit run afterwards in one place for the whole
+// warp.  `postpone`: this lane's triangle group goes on the stack so the
+// warp keeps visiting nodes together.  Returns true when the ray is done.
+template <int STACK>
+__device__ __forceinline__ bool trav_decide(Trav &T, const DScene &S,
+                                            const float4 *rays, uint32_t ridx,
+                                            uint2 *stk, uint32_t stride,
+                                            bool postpone, uint32_t &err,
+                                            uint32_t *vnode, uint32_t *titem)
+{
+	bool has_nodes = (T.ng.y >> 24) != 0u;
+	if (T.tg.y && has_nodes && postpone) {
+		if (T.sp >= STACK) {
+			err = 1u;
+			return true;
+		}
+		stk[(uint32_t)T.sp++ * stride] = make_uint2(T.tg.x | kItemGroup,
+		  T.tg.y);
+		T.tg.y = 0u;
+	}
+	if (T.tg.y) {
+		uint32_t i = __ffs(T.tg.y) - 1;
+		T.tg.y &= T.tg.y - 1u;
+		uint32_t item = T.tg.x + i;
+		if (T.level != 0u) {
+			*titem = item;
+			return false;
+		}
+		// enter an instance: keep the TLAS work on the stack
+		uint32_t inst = __ldg(S.irefs + item);
+		if (has_nodes) {
+			if (T.sp >= STACK) {
+				err = 1u;
+				return true;
 			}
-			float t;
-			if (tri_hit(S.tris, item, r, bt, &t)) {
-				bt = t;
-				h.t = t;
-				h.tri = item;
-				h.inst = cinst;
-				found = true;
-				if (ANY)
-					return true;
+			stk[(uint32_t)T.sp++ * stride] = T.ng;
+		}
+		if (T.tg.y) {
+			if (T.sp >= STACK) {
+				err = 1u;
+				return true;
+			}
+			stk[(uint32_t)T.sp++ * stride] =
+			  make_uint2(T.tg.x | kItemGroup, T.tg.y);
+		}
+		T.blas_sp = T.sp;
+		T.level = 1u;
+		T.cinst = inst;
+		const float4 *ip = S.insts + 4u * inst;
+		float4 m0 = __ldg(ip), m1 = __ldg(ip + 1);
+		float4 m2 = __ldg(ip + 2);
+		*vnode = __float_as_uint(__ldg(ip + 3).x);
+		float o[3], d[3];
+		xform(m0, m1, m2, T.r.ox, T.r.oy, T.r.oz, T.r.dx, T.r.dy, T.r.dz,
+		  o, d);
+		tray_slab(T.r, o[0], o[1], o[2], d[0], d[1], d[2]);
+		tray_watertight(T.r);
+		return false;
+	}
+	if (has_nodes) {
+		uint32_t hm = T.ng.y >> 24;
+		uint32_t key = __ffs(hm) - 1;
+		hm &= hm - 1u;
+		uint32_t slot = key ^ T.r.oct;
+		*vnode = T.ng.x + __popc(T.ng.y & ((1u << slot) - 1u) & 0xffu);
+		T.ng.y = (hm << 24) | (T.ng.y & 0xffu);
+		if (hm) {
+			if (T.sp >= STACK) {
+				err = 1u;
+				return true;
+			}
+			stk[(uint32_t)T.sp++ * stride] = T.ng;
+		}
+		return false;
+	}
+	if (T.level == 1u && T.sp == T.blas_sp) {
+		T.level = 0u;
+		float4 a = rays[2u * ridx], b = rays[2u * ridx + 1u];
+		tray_slab(T.r, a.x, a.y, a.z, b.x, b.y, b.z);
+	}
+	if (T.sp == 0)
+		return true;
+	uint2 e = stk[(uint32_t)(--T.sp) * stride];
+	if (e.x & kItemGroup) {
+		T.tg = make_uint2(e.x & ~kItemGroup, e.y);
+		T.ng = make_uint2(0u, 0u);
+	} else {
+		T.ng = e;
+		T.tg.y = 0u;
+	}
+	return false;
+}
+
+// Persistent traversal of `n` rays (2 float4 each: (o, tmax),
+// (d, payload)).  Each warp refills its idle lanes from a global work
+// counter once at least kRefill of them are idle, so lanes stay busy while
+// rays of very different cost finish at different times; when fewer than a
+// fifth of the active lanes want triangle tests, those lanes push their
+// triangle group and visit nodes with the rest (Ylitie, Karras and Laine,
+// HPG 2017).  Per iteration every lane does at most one triangle test and
+// one node visit, each from a single call site.  `sink` gets every
+// finished ray: (ray index, state, error).
+constexpr int kRefill = 8;
+
+template <bool ANY, int STACK, bool COUNT, class Sink>
+__device__ __forceinline__ void trace_persistent(const DScene &S,
+                                                 const float4 *rays,
+                                                 uint32_t n, uint32_t *work,
+                                                 uint2 *stk, uint32_t stride,
+                                                 Sink &sink)
+{
+	const uint32_t lane = threadIdx.x & 31u;
+	bool active = false, exhausted = false;
+	uint32_t ridx = 0, err = 0;
+	Trav T;
+	for (;;) {
+		uint32_t vnode = kNone, titem = kNone;
+		uint32_t idle = __ballot_sync(kFull, !active);
+		if (!exhausted && __popc(idle) >= kRefill) {
+			uint32_t cnt = __popc(idle);
+			uint32_t leader = __ffs(idle) - 1;
+			uint32_t base = 0;
+			if (lane == leader)
+				base = atomicAdd(work, cnt);
+			base = __shfl_sync(kFull, base, leader);
+			if (base + cnt >= n)
+				exhausted = true;
+			if (!active) {
+				uint32_t my = base + __popc(idle & ((1u << lane) - 1u));
+				if (my < n) {
+					ridx = my;
+					err = 0;
+					trav_start(T, rays[2u * my], rays[2u * my + 1u]);
+					vnode = 0u;
+					active = true;
+				}
 			}
 		}
-		uint32_t hm = ng.y >> 24;
-		if (hm) {
-			uint32_t key = __ffs(hm) - 1;
-			hm &= hm - 1u;
-			uint32_t slot = key ^ r.oct;
-			uint32_t child = ng.x + __popc(ng.y & ((1u << slot) - 1u) &
-			  0xffu);
-			ng.y = (hm << 24) | (ng.y & 0xffu);
-			if (hm) {
-				if (sp >= STACK) {
-					err = 1u;
-					return found;
-				}
-				stk[(uint32_t)sp++ * stride] = ng;
-			}
-			visit(level ? S.blas : S.tlas, child, r, bt, ng, tg);
+		uint32_t act = __ballot_sync(kFull, active);
+		if (!act) {
+			if (exhausted)
+				return;
 			continue;
 		}
-		if (level == 1u && sp == blas_sp) {
-			level = 0u;
-			tray_slab(r, wox, woy, woz, wdx, wdy, wdz);
+		uint32_t want_tri = __ballot_sync(kFull, active && T.tg.y != 0u);
+		bool postpone = __popc(want_tri) * 5u < __popc(act);
+		if (active && vnode == kNone) {
+			if (trav_decide<STACK>(T, S, rays, ridx, stk, stride, postpone,
+			  err, &vnode, &titem)) {
+				sink(ridx, T, err);
+				active = false;
+			}
 		}
-		if (sp == 0)
-			return found;
-		uint2 e = stk[(uint32_t)(--sp) * stride];
-		if (e.y & kIGroup) {
-			tg = make_uint2(e.x, e.y >> 24);
-			ng = make_uint2(0u, 0u);
-		} else {
-			ng = e;
-			tg.y = 0u;
+		if (titem != kNone) {
+			float t;
+			if (COUNT)
+				T.ntest++;
+			if (tri_hit(S.tris, titem, T.r, T.bt, &t)) {
+				T.bt = t;
+				T.btri = titem;
+				T.binst = T.cinst;
+				T.found = true;
+				if (ANY) {
+					sink(ridx, T, err);
+					active = false;
+				}
+			}
+		}
+		if (vnode != kNone) {
+			if (COUNT)
+				T.nvisit++;
+			visit(T.level ? S.blas : S.tlas, vnode, T.r, T.bt, T.ng, T.tg);
 		}
 	}
 }
+
+// --------------------------------------------------------------- sinks --
+
+// Raw closest hit: (t, triangle index, instance, 0); t = FLT_MAX on a miss
+// or on a device error (counted in errs).
+struct SinkRaw {
+	float4   *hits;
+	uint32_t *errs;
+	unsigned long long *counts; // visits, tests (counting kernels)
+	__device__ void operator()(uint32_t i, const Trav &T, uint32_t err)
+	{
+		if (counts) {
+			atomicAdd(&counts[0], (unsigned long long)T.nvisit);
+			atomicAdd(&counts[1], (unsigned long long)T.ntest);
+		}
+		if (err)
+			atomicAdd(errs, 1u);
+		hits[i] = (T.found && !err) ? make_float4(T.bt,
+		  __uint_as_float(T.btri), __uint_as_float(T.binst), 0.0f) :
+		  make_float4(FLT_MAX, 0.0f, 0.0f, 0.0f);
+	}
+};
+
+struct SinkOccl {
+	uint8_t  *occl;
+	uint32_t *errs;
+	__device__ void operator()(uint32_t i, const Trav &T, uint32_t err)
+	{
+		if (err)
+			atomicAdd(errs, 1u);
+		occl[i] = T.found ? 1 : 0;
+	}
+};
 
 // ---------------------------------------------------------- refinement --
 
@@ -437,6 +596,8 @@ __device__ __forceinline__ float4 finish_hit(const DScene &S, float wox,
                                              float wdy, float wdz,
                                              const THit &h)
 {
+	if (h.t == FLT_MAX)
+		return make_float4(FLT_MAX, 0.0f, 0.0f, 0.0f);
 	const float4 *ip = S.insts + 4u * h.inst;
 	float o[3], d[3];
 	xform(__ldg(ip), __ldg(ip + 1), __ldg(ip + 2), wox, woy, woz, wdx, wdy,

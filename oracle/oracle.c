@@ -579,6 +579,149 @@ void orc_reintersect_f64(const struct nb_rdata *rd, const float *rays,
 	}
 }
 
+static double vlen3(const double *a)
+{
+	return sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+}
+
+static double absdot3(const double *a, const double *b)
+{
+	return fabs(a[0] * b[0]) + fabs(a[1] * b[1]) + fabs(a[2] * b[2]);
+}
+
+void orc_mt_bounds(const struct nb_rdata *rd, const float *rays,
+                   const uint32_t *ids, uint32_t n, double *out)
+{
+	const double eps = 8.0 * ldexp(1.0, -24);
+	for (uint32_t i = 0; i < n; i++) {
+		const float *r = rays + 8ull * i;
+		uint32_t inst = ids[i] & INST_MASK, prim = ids[i] >> INST_BITS;
+		if (inst >= rd->instcnt) {
+			out[3 * i] = out[3 * i + 1] = out[3 * i + 2] = 0.0;
+			continue;
+		}
+		float o[3] = {r[0], r[1], r[2]}, d[3] = {r[4], r[5], r[6]};
+		float oo[3], od[3], v0[3], v1[3], v2[3];
+		orc_object_ray(rd, inst, o, d, oo, od);
+		tri_verts(rd, inst, prim, v0, v1, v2);
+		double e0[3], e1[3], tv[3], dd[3], pv[3], qv[3];
+		for (int a = 0; a < 3; a++) {
+			e0[a] = (double)v1[a] - v0[a];
+			e1[a] = (double)v2[a] - v0[a];
+			tv[a] = (double)oo[a] - v0[a];
+			dd[a] = od[a];
+		}
+		pv[0] = dd[1] * e1[2] - dd[2] * e1[1];
+		pv[1] = dd[2] * e1[0] - dd[0] * e1[2];
+		pv[2] = dd[0] * e1[1] - dd[1] * e1[0];
+		qv[0] = tv[1] * e0[2] - tv[2] * e0[1];
+		qv[1] = tv[2] * e0[0] - tv[0] * e0[2];
+		qv[2] = tv[0] * e0[1] - tv[1] * e0[0];
+		double det = e0[0] * pv[0] + e0[1] * pv[1] + e0[2] * pv[2];
+		double adet = fabs(det);
+		if (adet == 0.0) {
+			out[3 * i] = out[3 * i + 1] = out[3 * i + 2] = INFINITY;
+			continue;
+		}
+		double u = (tv[0] * pv[0] + tv[1] * pv[1] + tv[2] * pv[2]) / det;
+		double v = (dd[0] * qv[0] + dd[1] * qv[1] + dd[2] * qv[2]) / det;
+		double t = (e1[0] * qv[0] + e1[1] * qv[1] + e1[2] * qv[2]) / det;
+		double ld = vlen3(dd), l0 = vlen3(e0), l1 = vlen3(e1);
+		double lt = vlen3(tv);
+		double rdet = eps * (absdot3(e0, pv) + l0 * ld * l1) / adet;
+		out[3 * i] = eps * (absdot3(tv, pv) + lt * ld * l1) / adet +
+		  fabs(u) * rdet;
+		out[3 * i + 1] = eps * (absdot3(dd, qv) + ld * lt * l0) / adet +
+		  fabs(v) * rdet;
+		out[3 * i + 2] = eps * (absdot3(e1, qv) + l1 * lt * l0) / adet +
+		  fabs(t) * rdet;
+	}
+}
+
+static int slab_f64(const double *o, const double *d, const struct nb_aabb *b,
+                    double tbest)
+{
+	double lo = 0.0, hi = tbest;
+	const float mn[3] = {b->min.x, b->min.y, b->min.z};
+	const float mx[3] = {b->max.x, b->max.y, b->max.z};
+	for (int a = 0; a < 3; a++) {
+		if (d[a] == 0.0) {
+			if (o[a] < mn[a] || o[a] > mx[a])
+				return 0;
+			continue;
+		}
+		double t0 = (mn[a] - o[a]) / d[a], t1 = (mx[a] - o[a]) / d[a];
+		if (t0 > t1) {
+			double x = t0;
+			t0 = t1;
+			t1 = x;
+		}
+		lo = t0 > lo ? t0 : lo;
+		hi = t1 < hi ? t1 : hi;
+	}
+	return lo <= hi * (1.0 + 1e-9);
+}
+
+void orc_bruteforce_f64(const struct nb_rdata *rd, const float *rays,
+                        uint32_t n, uint32_t *ids, double *tout)
+{
+	for (uint32_t i = 0; i < n; i++) {
+		const float *r = rays + 8ull * i;
+		double o[3] = {r[0], r[1], r[2]}, d[3] = {r[4], r[5], r[6]};
+		double best = r[3] == FLT_MAX ? INFINITY : (double)r[3];
+		uint32_t bid = 0;
+		for (uint32_t k = 0; k < rd->instcnt; k++) {
+			if (!slab_f64(o, d, &rd->aabbs[k], best))
+				continue;
+			const struct nb_rinst *ri = &rd->insts[k];
+			const float *g = ri->globinv;
+			double oo[3], od[3];
+			for (int a = 0; a < 3; a++) {
+				oo[a] = g[4 * a] * o[0] + g[4 * a + 1] * o[1] +
+				  g[4 * a + 2] * o[2] + g[4 * a + 3];
+				od[a] = g[4 * a] * d[0] + g[4 * a + 1] * d[1] +
+				  g[4 * a + 2] * d[2];
+			}
+			for (uint32_t p = 0; p < ri->tricnt; p++) {
+				const struct nb_rtri *t = &rd->tris[ri->triofs + p];
+				double v0[3] = {t->v0.x, t->v0.y, t->v0.z};
+				double e0[3] = {t->v1.x - v0[0], t->v1.y - v0[1],
+				  t->v1.z - v0[2]};
+				double e1[3] = {t->v2.x - v0[0], t->v2.y - v0[1],
+				  t->v2.z - v0[2]};
+				double pv[3] = {od[1] * e1[2] - od[2] * e1[1],
+				  od[2] * e1[0] - od[0] * e1[2],
+				  od[0] * e1[1] - od[1] * e1[0]};
+				double det = e0[0] * pv[0] + e0[1] * pv[1] +
+				  e0[2] * pv[2];
+				if (det == 0.0)
+					continue;
+				double tv[3] = {oo[0] - v0[0], oo[1] - v0[1],
+				  oo[2] - v0[2]};
+				double u = (tv[0] * pv[0] + tv[1] * pv[1] +
+				  tv[2] * pv[2]) / det;
+				if (u < 0.0 || u > 1.0)
+					continue;
+				double qv[3] = {tv[1] * e0[2] - tv[2] * e0[1],
+				  tv[2] * e0[0] - tv[0] * e0[2],
+				  tv[0] * e0[1] - tv[1] * e0[0]};
+				double v = (od[0] * qv[0] + od[1] * qv[1] +
+				  od[2] * qv[2]) / det;
+				if (v < 0.0 || u + v > 1.0)
+					continue;
+				double tt = (e1[0] * qv[0] + e1[1] * qv[1] +
+				  e1[2] * qv[2]) / det;
+				if (tt > 0.0 && tt < best) {
+					best = tt;
+					bid = (p << INST_BITS) | k;
+				}
+			}
+		}
+		ids[i] = bid;
+		tout[i] = best;
+	}
+}
+
 // ------------------------------------------------- batches -----------------
 
 struct tbatch {

@@ -75,6 +75,20 @@ void orc_reintersect_f64(const struct nb_rdata *rd, const float *rays,
                          const uint32_t *ids, uint32_t n, double *t64,
                          double *bary64);
 
+// First-order forward error bounds of Moeller-Trumbore evaluated in FP32
+// (rend.c:843-926) for triangle `id` of each ray: out[3i..3i+2] = bounds on
+// |du|, |dv| and |dt| (8 units of 2^-24 per rounded term, plus the relative
+// error of det carried into u, v, t).  Large for grazing rays and for
+// triangles small against their distance from the ray origin.
+void orc_mt_bounds(const struct nb_rdata *rd, const float *rays,
+                   const uint32_t *ids, uint32_t n, double *out);
+
+// Closest hit in FP64 by testing every triangle of every instance whose
+// world box the ray enters (ground truth for a handful of rays): id and t per
+// ray, t = INFINITY and id = 0 on a miss.
+void orc_bruteforce_f64(const struct nb_rdata *rd, const float *rays,
+                        uint32_t n, uint32_t *ids, double *t);
+
 // Light table entry: 20 floats = v0[3] e0[3] e1[3] n[3] emit[3] cdf area
 // pad[3] (world space; n the emitting side; cdf the running area fraction).
 #define ORC_LIGHT_FLOATS 20

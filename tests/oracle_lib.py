@@ -54,6 +54,8 @@ def oracle():
         L.orc_accumulate.argtypes = [vp, vp]
         L.orc_pcg_first.argtypes = [C.c_uint64, u32, C.c_uint64, u32, vp]
         L.orc_sincos2pi.argtypes = [C.c_float, vp, vp]
+        L.orc_mt_bounds.argtypes = [vp, vp, vp, u32, vp]
+        L.orc_bruteforce_f64.argtypes = [vp, vp, u32, vp, vp]
         _ORC = L
     return _ORC
 
@@ -171,29 +173,90 @@ def orc_render(rd, lights, light_area, depth, mode=0, seed=1, window=None,
     return rad, rays
 
 
+def mt_bounds(rd_ptr, rays, ids):
+    """Forward error bounds (du, dv, dt) of FP32 Moeller-Trumbore for the
+    given (ray, triangle) pairs (orc_mt_bounds)."""
+    rays = np.ascontiguousarray(rays, RAY_DTYPE)
+    ids = np.ascontiguousarray(ids, np.uint32)
+    out = np.zeros((len(rays), 3))
+    oracle().orc_mt_bounds(rd_ptr, rays.ctypes.data, ids.ctypes.data,
+                           len(rays), out.ctypes.data)
+    return out
+
+
+def bruteforce(rd_ptr, rays):
+    """FP64 closest hit over every triangle of every entered instance."""
+    rays = np.ascontiguousarray(rays, RAY_DTYPE)
+    ids = np.zeros(len(rays), np.uint32)
+    t = np.zeros(len(rays))
+    oracle().orc_bruteforce_f64(rd_ptr, rays.ctypes.data, len(rays),
+                                ids.ctypes.data, t.ctypes.data)
+    return ids, t
+
+
 def classify(rd_ptr, rays, ha, hb, eps_t, eps_b):
     """Compare two hit sets on the same rays.  Returns (n_same, ties,
-    bad): disagreements are ties when an FP64 re-intersection shows the
-    two candidates within eps_t relative in t, or a candidate's
-    barycentrics within eps_b of an edge (or outside by less)."""
+    bad).  A disagreement is a tie when an FP64 re-intersection of both
+    candidates shows either
+
+    * the two within eps_t relative in t (plus the FP32 Moeller-Trumbore
+      error bounds of both), or
+    * a candidate within eps_b (plus its Moeller-Trumbore error bound) of
+      an edge, or outside by less.
+
+    The Moeller-Trumbore bounds cover the reference's and the oracle's own
+    evaluation of the test; eps_t/eps_b cover the reference's rcpps."""
     miss_a = ha["t"] == FLT_MAX
     miss_b = hb["t"] == FLT_MAX
     same = (miss_a & miss_b) | (~miss_a & ~miss_b & (ha["id"] == hb["id"]))
     idx = np.nonzero(~same)[0]
     ties, bad = [], []
     if len(idx):
-        ta, ba = reintersect(rd_ptr, rays[idx], ha["id"][idx])
-        tb, bb = reintersect(rd_ptr, rays[idx], hb["id"][idx])
+        r = rays[idx]
+        ta, ba = reintersect(rd_ptr, r, ha["id"][idx])
+        tb, bb = reintersect(rd_ptr, r, hb["id"][idx])
+        ea = mt_bounds(rd_ptr, r, ha["id"][idx])
+        eb = mt_bounds(rd_ptr, r, hb["id"][idx])
+
+        def near(b, e):
+            return (b[1] < eps_b + e[0] or b[2] < eps_b + e[1] or
+                    b[0] < eps_b + e[0] + e[1])
         for j, i in enumerate(idx):
-            near_a = (not miss_a[i]) and np.min(ba[j]) < eps_b
-            near_b = (not miss_b[i]) and np.min(bb[j]) < eps_b
+            near_a = (not miss_a[i]) and near(ba[j], ea[j])
+            near_b = (not miss_b[i]) and near(bb[j], eb[j])
             close_t = (not miss_a[i] and not miss_b[i] and
-                       abs(ta[j] - tb[j]) <= eps_t * min(abs(ta[j]), abs(tb[j])))
+                       abs(ta[j] - tb[j]) <= eps_t * min(abs(ta[j]),
+                                                         abs(tb[j])) +
+                       ea[j][2] + eb[j][2])
             if near_a or near_b or close_t:
                 ties.append(i)
             else:
                 bad.append(i)
     return int(same.sum()), ties, bad
+
+
+def agrees_with_truth(rd_ptr, rays, hits, rel=1e-6):
+    """For each ray: does `hits` hold a closest hit as close as the FP64
+    brute-force one (same triangle, or FP64 t within `rel`), or miss where
+    the truth's triangle is hit within `rel` of an edge?"""
+    tid, tt = bruteforce(rd_ptr, rays)
+    ok = np.zeros(len(rays), bool)
+    th, bh = reintersect(rd_ptr, rays, hits["id"])
+    _, btruth = reintersect(rd_ptr, rays, tid)
+    for i in range(len(rays)):
+        truth_miss = not np.isfinite(tt[i])
+        hit_miss = hits["t"][i] == FLT_MAX
+        if truth_miss and hit_miss:
+            ok[i] = True
+        elif hit_miss:
+            ok[i] = np.min(btruth[i]) < rel
+        elif truth_miss:
+            ok[i] = np.min(bh[i]) > -rel and False
+        else:
+            ok[i] = (hits["id"][i] == tid[i] or
+                     abs(th[i] - tt[i]) <= rel * abs(tt[i]) or
+                     np.min(btruth[i]) < rel)
+    return ok
 
 
 def random_rays(rd, n, seed=0, spread=8.0):

@@ -15,8 +15,12 @@ def relmse(x, ref):
 
 
 def _gpu_frame(rd, depth, mode, seed):
+    """One GPU frame; rd.samples is left at its value before the frame so
+    the oracle renders the same random streams."""
     gr = api.GpuRenderer(rd, max_depth=depth, mode=mode, seed=seed).upload()
+    samples = rd.rd.samples
     rays = gr.frame()
+    rd.rd.samples = samples
     gr.readback(3)
     acc = rd.acc().copy()
     lights, area = gr.lights()

@@ -34,6 +34,11 @@ def _check_against_oracle(rd, rays, hits):
     same, ties, bad = ol.classify(rd.ptr, rays, hits, ref, TIGHT_T, TIGHT_B)
     assert not bad, f"{len(bad)} non-tie mismatches, e.g. {bad[:5]}"
     assert len(ties) <= max(2, len(rays) // 2000)
+    # where they differ, the GPU holds the FP64 ground truth
+    if ties:
+        pick = np.array(ties[:32])
+        ok = ol.agrees_with_truth(rd.ptr, rays[pick], hits[pick])
+        assert ok.mean() >= 0.9, (ok.mean(), pick[~ok][:5])
     # where the triangle agrees, the refined hit is bit-identical
     m = (hits["id"] == ref["id"]) & (hits["t"] < ol.FLT_MAX)
     assert np.array_equal(hits["t"][m].view(np.uint32),
@@ -104,11 +109,11 @@ def test_trace_edge_cases(gpu):
     gr = api.GpuRenderer(rd).upload()
     assert len(gr.trace(np.zeros(0, api.RAY_DTYPE))) == 0
     rays = ol.random_rays(rd, 64, seed=9)
-    # zero tmax: nothing can be hit; axis-parallel directions
+    # zero tmax: nothing lies in (0, tmax)
     z = rays.copy()
     z["tmax"] = 0.0
-    assert (gr.trace(z)["t"] == 0.0).all() or \
-        (gr.trace(z)["t"] >= ol.FLT_MAX).all() or True
+    assert (gr.trace(z)["t"] == ol.FLT_MAX).all()
+    assert (gr.occluded(z) == 0).all()
     axis = rays[:6].copy()
     axis["d"] = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0],
                           [0, 0, 1], [0, 0, -1]], np.float32)
