@@ -49,6 +49,8 @@ def parse():
                    help="BLAS count (0 = the workload's 64)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--sched", type=int, default=0,
+                   help="traversal schedule (0 = library default)")
     p.add_argument("--count", action="store_true",
                    help="one extra untimed frame counting node visits and "
                         "triangle tests per closest-hit ray")
@@ -225,7 +227,7 @@ def run_ours(a):
     scene = api.Scene(WORKLOAD["family"], WORKLOAD["seed"], a.blas)
     rd = api.RenderData(scene, a.width, a.height, a.spp)
     gr = api.GpuRenderer(rd, max_depth=a.depth, seed=1 + rank, timing=True,
-                         device=dev).upload()
+                         device=dev, sched=a.sched).upload()
     stream = torch.cuda.ExternalStream(gr.stream(), device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     lights, area = gr.lights()
@@ -301,7 +303,7 @@ def run_ours(a):
         # one context per rdata: the counting context replaces the timed one
         gr.close()
         gc = api.GpuRenderer(rd, max_depth=a.depth, seed=1 + rank,
-                             count=True, device=dev).upload()
+                             count=True, device=dev, sched=a.sched).upload()
         gc.frame()
         sc = gc.stats()
         visits = {"nodes_per_ray": sc["node_visits"] / sc["closest_rays"],

@@ -59,7 +59,9 @@ struct rendgpu_cfg {
 	uint64_t seed;       /* PCG32 seed of the path streams */
 	int32_t  device;     /* CUDA device ordinal */
 	uint32_t block;      /* threads per block of the trace kernels (0 = auto) */
-	uint32_t reserved[8];
+	uint32_t sched;      /* traversal schedule: 0 = default, 1 = step,
+	                        2 = phase, 3 = ylitie (see trace.cuh) */
+	uint32_t reserved[7];
 };
 
 /* A ray for the batch calls: origin, tmax, direction (32 bytes). */

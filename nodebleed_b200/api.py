@@ -63,7 +63,8 @@ class RendgpuCfg(C.Structure):
     _fields_ = [("size", C.c_uint32), ("max_depth", C.c_uint32),
                 ("mode", C.c_uint32), ("flags", C.c_uint32),
                 ("seed", C.c_uint64), ("device", C.c_int32),
-                ("block", C.c_uint32), ("reserved", C.c_uint32 * 8)]
+                ("block", C.c_uint32), ("sched", C.c_uint32),
+                ("reserved", C.c_uint32 * 7)]
 
 
 class RendgpuStats(C.Structure):
@@ -256,7 +257,7 @@ class GpuRenderer:
     """The rendgpu C ABI on one RenderData."""
 
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
-                 timing=False, device=0, count=False):
+                 timing=False, device=0, count=False, sched=0):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -268,6 +269,7 @@ class GpuRenderer:
             (FLAG_COUNT if count else 0)
         cfg.seed = seed
         cfg.device = device
+        cfg.sched = sched
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
         if rc != 0:
             raise RendgpuError(rc, "rendgpu_init")

@@ -202,9 +202,10 @@ __global__ void __launch_bounds__(256) k_gen(FrameDev F, FrameArgs A)
 }
 
 // Closest-hit trace of a ray queue (count in *count): raw hits.
-// COUNT adds visit / triangle-test counts to counts[0..1].
-template <int STACK, bool COUNT>
-__global__ void __launch_bounds__(128) k_trace(DScene S, const float4 *rays,
+// COUNT adds visit / triangle-test counts to counts[0..1]; SCHED picks the
+// traversal schedule.
+template <int SCHED, int STACK, bool COUNT>
+__global__ void __launch_bounds__(128, 8) k_trace(DScene S, const float4 *rays,
                                                const uint32_t *count,
                                                uint32_t *work, float4 *hits,
                                                uint32_t *errs,
@@ -216,13 +217,13 @@ __global__ void __launch_bounds__(128) k_trace(DScene S, const float4 *rays,
 	if (blockIdx.x == 0 && threadIdx.x == 0 && nrays)
 		atomicAdd(nrays, (unsigned long long)n);
 	SinkRaw sink{hits, errs, COUNT ? counts : nullptr};
-	trace_persistent<false, STACK, COUNT>(S, rays, n, work,
+	trace_persistent<SCHED, false, STACK, COUNT>(S, rays, n, work,
 	  sstk + threadIdx.x, blockDim.x, sink);
 }
 
 // Any-hit trace of API rays: occl[i] = hit in (0, tmax).
-template <int STACK>
-__global__ void __launch_bounds__(128) k_occluded(DScene S,
+template <int SCHED, int STACK>
+__global__ void __launch_bounds__(128, 8) k_occluded(DScene S,
                                                   const float4 *rays,
                                                   const uint32_t *count,
                                                   uint32_t *work, uint8_t *occl,
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(128) k_occluded(DScene S,
 {
 	extern __shared__ uint2 sstk[];
 	SinkOccl sink{occl, errs};
-	trace_persistent<true, STACK, false>(S, rays, *count, work,
+	trace_persistent<SCHED, true, STACK, false>(S, rays, *count, work,
 	  sstk + threadIdx.x, blockDim.x, sink);
 }
 
@@ -258,15 +259,15 @@ struct SinkShadow {
 	}
 };
 
-template <int STACK>
-__global__ void __launch_bounds__(128) k_shadow(DScene S, FrameDev F)
+template <int SCHED, int STACK>
+__global__ void __launch_bounds__(128, 8) k_shadow(DScene S, FrameDev F)
 {
 	extern __shared__ uint2 sstk[];
 	uint32_t n = F.cnt[2];
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		atomicAdd(&F.rays[1], (unsigned long long)n);
 	SinkShadow sink{F.shadow, F.scol, F.pL, &F.cnt[3]};
-	trace_persistent<true, STACK, false>(S, F.shadow, n, &F.cnt[5],
+	trace_persistent<SCHED, true, STACK, false>(S, F.shadow, n, &F.cnt[5],
 	  sstk + threadIdx.x, blockDim.x, sink);
 }
 

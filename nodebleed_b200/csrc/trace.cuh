@@ -98,6 +98,21 @@ __device__ __forceinline__ uint32_t qb(uint32_t w, int k)
 	return (w >> (8 * k)) & 0xffu;
 }
 
+// Three-input min / max (sm_100 PTX); a NaN operand is ignored as in fminf.
+__device__ __forceinline__ float fmax3(float a, float b, float c)
+{
+	float r;
+	asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+	return r;
+}
+
+__device__ __forceinline__ float fmin3(float a, float b, float c)
+{
+	float r;
+	asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+	return r;
+}
+
 // Byte k of w as the float 2^23 + byte (one byte permute: the byte goes
 // into the mantissa of 2^23).
 __device__ __forceinline__ float qbf(uint32_t w, int k)
@@ -138,8 +153,8 @@ __device__ __forceinline__ void visit(const nb_qnode *__restrict__ nodes,
 	uint32_t fy0 = fy ? w2.z : w4.x, fy1 = fy ? w2.w : w4.y;
 	uint32_t nz0 = fz ? w4.z : w3.x, nz1 = fz ? w4.w : w3.y;
 	uint32_t fz0 = fz ? w3.x : w4.z, fz1 = fz ? w3.y : w4.w;
-	float tcap = tmax * kWiden;
 	uint32_t hits = 0, tbits = 0;
+	float gmin = FLT_MAX;
 #pragma unroll
 	for (int s = 0; s < 8; s++) {
 		int b = s & 3;
@@ -152,11 +167,12 @@ __device__ __forceinline__ void visit(const nb_qnode *__restrict__ nodes,
 		float tfx = __fmaf_rn(qbf(wfx, b), scx, bx);
 		float tfy = __fmaf_rn(qbf(wfy, b), scy, by);
 		float tfz = __fmaf_rn(qbf(wfz, b), scz, bz);
-		float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-		float tf = fminf(fminf(tfx, tfy), tfz) * kWiden;
-		if (tn <= fminf(tf, tcap)) {
+		float tn = fmax3(tnx, tny, fmaxf(tnz, 0.0f));
+		float tf = fmin3(tfx, tfy, fminf(tfz, tmax));
+		if (tn <= tf * kWiden) {
 			if ((imask >> s) & 1u) {
 				hits |= 1u << (s ^ r.oct);
+				gmin = fminf(gmin, tn);
 			} else {
 				uint32_t m = qb(s < 4 ? w1.z : w1.w, b);
 				if (m & NB_META_LEAF) {
@@ -166,8 +182,18 @@ __device__ __forceinline__ void visit(const nb_qnode *__restrict__ nodes,
 			}
 		}
 	}
-	ng = make_uint2(w1.x, (hits << 24) | imask);
+	// node group: first child, hit mask (24..31), entry distance lower
+	// bound of the hit children as bf16 truncated towards zero (8..23),
+	// inner mask (0..7)
+	ng = make_uint2(w1.x, (hits << 24) | ((__float_as_uint(gmin) >> 16) << 8) |
+	  imask);
 	tg = make_uint2(w1.y, tbits);
+}
+
+// Lower bound on the entry distance of a node group's remaining children.
+__device__ __forceinline__ float group_tmin(uint32_t y)
+{
+	return __uint_as_float((y << 8) & 0xffff0000u);
 }
 
 // a*b - c*d with Kahan's error compensation (relative error <= 2 ulp, so
@@ -259,6 +285,7 @@ struct Trav {
 };
 
 constexpr uint32_t kNone = 0xffffffffu;
+constexpr int kRefill = 8; // refill a warp once this many lanes idle
 
 // New ray: state reset; the caller visits the TLAS root (node 0).
 __device__ __forceinline__ void trav_start(Trav &T, float4 a, float4 b)
@@ -276,6 +303,103 @@ __device__ __forceinline__ void trav_start(Trav &T, float4 a, float4 b)
 	T.tg = make_uint2(0u, 0u);
 	T.nvisit = 0;
 	T.ntest = 0;
+}
+
+// Push a stack entry; false (and err set) when the stack is full.
+template <int STACK>
+__device__ __forceinline__ bool push(Trav &T, uint2 *stk, uint32_t stride,
+                                     uint2 e, uint32_t &err)
+{
+	if (T.sp >= STACK) {
+		err = 1u;
+		return false;
+	}
+	stk[(uint32_t)T.sp++ * stride] = e;
+	return true;
+}
+
+// Take the next child of the node group; false if the group is empty or
+// lies entirely beyond the closest hit so far.  Pushes the rest.
+template <int STACK>
+__device__ __forceinline__ bool next_child(Trav &T, uint2 *stk,
+                                           uint32_t stride, uint32_t *vnode,
+                                           uint32_t &err)
+{
+	uint32_t hm = T.ng.y >> 24;
+	if (!hm)
+		return false;
+	if (group_tmin(T.ng.y) > T.bt * kWiden) {
+		T.ng.y = 0u;
+		return false;
+	}
+	uint32_t key = __ffs(hm) - 1;
+	hm &= hm - 1u;
+	uint32_t slot = key ^ T.r.oct;
+	*vnode = T.ng.x + __popc(T.ng.y & ((1u << slot) - 1u) & 0xffu);
+	T.ng.y = (hm << 24) | (T.ng.y & 0x00ffffffu);
+	if (hm && !push<STACK>(T, stk, stride, T.ng, err))
+		return false;
+	return true;
+}
+
+// One node-phase step of a lane that holds no BLAS triangles: enter the
+// next instance of a TLAS leaf group (transform, then visit the BLAS
+// root), visit the next child of the node group, or pop.  Returns true when
+// the ray is finished (or on a stack overflow, with err set).
+template <int STACK>
+__device__ __forceinline__ bool node_step(Trav &T, const DScene &S,
+                                          const float4 *rays, uint32_t ridx,
+                                          uint2 *stk, uint32_t stride,
+                                          uint32_t &err, uint32_t *vnode)
+{
+	for (;;) {
+		if (T.tg.y) { // level 0: instance references
+			uint32_t i = __ffs(T.tg.y) - 1;
+			T.tg.y &= T.tg.y - 1u;
+			uint32_t inst = __ldg(S.irefs + T.tg.x + i);
+			if ((T.ng.y >> 24) && !push<STACK>(T, stk, stride, T.ng, err))
+				return true;
+			if (T.tg.y && !push<STACK>(T, stk, stride,
+			  make_uint2(T.tg.x | kItemGroup, T.tg.y), err))
+				return true;
+			T.ng.y = 0u;
+			T.tg.y = 0u;
+			T.blas_sp = T.sp;
+			T.level = 1u;
+			T.cinst = inst;
+			const float4 *ip = S.insts + 4u * inst;
+			float4 m0 = __ldg(ip), m1 = __ldg(ip + 1);
+			float4 m2 = __ldg(ip + 2);
+			*vnode = __float_as_uint(__ldg(ip + 3).x);
+			float o[3], d[3];
+			xform(m0, m1, m2, T.r.ox, T.r.oy, T.r.oz, T.r.dx, T.r.dy,
+			  T.r.dz, o, d);
+			tray_slab(T.r, o[0], o[1], o[2], d[0], d[1], d[2]);
+			tray_watertight(T.r);
+			return false;
+		}
+		if (next_child<STACK>(T, stk, stride, vnode, err))
+			return false;
+		if (err)
+			return true;
+		if (T.level == 1u && T.sp == T.blas_sp) {
+			T.level = 0u;
+			float4 a = rays[2u * ridx], b = rays[2u * ridx + 1u];
+			tray_slab(T.r, a.x, a.y, a.z, b.x, b.y, b.z);
+		}
+		if (T.sp == 0)
+			return true;
+		uint2 e = stk[(uint32_t)(--T.sp) * stride];
+		if (e.x & kItemGroup) {
+			T.tg = make_uint2(e.x & ~kItemGroup, e.y);
+			T.ng = make_uint2(0u, 0u);
+			if (T.level == 1u)
+				return false; // triangles: the triangle phase takes them
+		} else {
+			T.ng = e;
+			T.tg.y = 0u;
+		}
+	}
 }
 
 // Decide this lane's next step: a triangle to test (*titem), a node to
@@ -374,19 +498,11 @@ __device__ __forceinline__ bool trav_decide(Trav &T, const DScene &S,
 	return false;
 }
 
-// Persistent traversal of `n` rays (2 float4 each: (o, tmax),
-// (d, payload)).  Each warp refills its idle lanes from a global work
-// counter once at least kRefill of them are idle, so lanes stay busy while
-// rays of very different cost finish at different times; when fewer than a
-// fifth of the active lanes want triangle tests, those lanes push their
-// triangle group and visit nodes with the rest (Ylitie, Karras and Laine,
-// HPG 2017).  Per iteration every lane does at most one triangle test and
-// one node visit, each from a single call site.  `sink` gets every
-// finished ray: (ray index, state, error).
-constexpr int kRefill = 8;
-
+// One triangle test and one node visit per iteration (each from a single
+// call site), with Ylitie-style postponing of triangle groups when fewer
+// than a fifth of the active lanes want them.
 template <bool ANY, int STACK, bool COUNT, class Sink>
-__device__ __forceinline__ void trace_persistent(const DScene &S,
+__device__ __forceinline__ void trace_step(const DScene &S,
                                                  const float4 *rays,
                                                  uint32_t n, uint32_t *work,
                                                  uint2 *stk, uint32_t stride,
@@ -455,6 +571,221 @@ __device__ __forceinline__ void trace_persistent(const DScene &S,
 			visit(T.level ? S.blas : S.tlas, vnode, T.r, T.bt, T.ng, T.tg);
 		}
 	}
+}
+
+// Persistent traversal of `n` rays (2 float4 each: (o, tmax),
+// (d, payload)) in alternating phases, after Aila and Laine (HPG 2009):
+// in the node phase every lane without BLAS triangles visits one node per
+// iteration until all lanes hold triangles or are done (lanes that already
+// hold triangles keep visiting speculatively and push what they find); in
+// the triangle phase all lanes test one triangle per iteration.  Idle lanes
+// are refilled from a global work counter once at least kRefill of a warp's
+// lanes are idle.  `sink` gets every finished ray: (index, state, error).
+template <bool ANY, int STACK, bool COUNT, class Sink>
+__device__ __forceinline__ void trace_phase(const DScene &S,
+                                                 const float4 *rays,
+                                                 uint32_t n, uint32_t *work,
+                                                 uint2 *stk, uint32_t stride,
+                                                 Sink &sink)
+{
+	const uint32_t lane = threadIdx.x & 31u;
+	bool active = false, exhausted = false;
+	uint32_t ridx = 0, err = 0;
+	Trav T;
+	for (;;) {
+		uint32_t vnode = kNone;
+		uint32_t idle = __ballot_sync(kFull, !active);
+		if (!exhausted && __popc(idle) >= kRefill) {
+			uint32_t cnt = __popc(idle);
+			uint32_t leader = __ffs(idle) - 1;
+			uint32_t base = 0;
+			if (lane == leader)
+				base = atomicAdd(work, cnt);
+			base = __shfl_sync(kFull, base, leader);
+			if (base + cnt >= n)
+				exhausted = true;
+			if (!active) {
+				uint32_t my = base + __popc(idle & ((1u << lane) - 1u));
+				if (my < n) {
+					ridx = my;
+					err = 0;
+					trav_start(T, rays[2u * my], rays[2u * my + 1u]);
+					vnode = 0u;
+					active = true;
+				}
+			}
+		}
+		if (!__any_sync(kFull, active)) {
+			if (exhausted)
+				return;
+			continue;
+		}
+		// node phase
+		for (;;) {
+			bool holding = active && T.level == 1u && T.tg.y != 0u;
+			bool searching = active && !holding;
+			if (!__any_sync(kFull, searching || vnode != kNone))
+				break;
+			bool spec = false;
+			if (searching && vnode == kNone) {
+				if (node_step<STACK>(T, S, rays, ridx, stk, stride, err,
+				  &vnode)) {
+					sink(ridx, T, err);
+					active = false;
+				}
+			} else if (holding && T.sp + 2 <= STACK) {
+				uint32_t e2 = 0;
+				spec = next_child<STACK>(T, stk, stride, &vnode, e2);
+			}
+			if (vnode != kNone) {
+				uint2 held = T.tg;
+				if (COUNT)
+					T.nvisit++;
+				visit(T.level ? S.blas : S.tlas, vnode, T.r, T.bt, T.ng,
+				  T.tg);
+				if (spec) {
+					if (T.tg.y)
+						stk[(uint32_t)T.sp++ * stride] =
+						  make_uint2(T.tg.x | kItemGroup, T.tg.y);
+					T.tg = held;
+				}
+				vnode = kNone;
+			}
+		}
+		// triangle phase
+		for (;;) {
+			bool want = active && T.level == 1u && T.tg.y != 0u;
+			if (!__any_sync(kFull, want))
+				break;
+			if (want) {
+				uint32_t i = __ffs(T.tg.y) - 1;
+				T.tg.y &= T.tg.y - 1u;
+				float t;
+				if (COUNT)
+					T.ntest++;
+				if (tri_hit(S.tris, T.tg.x + i, T.r, T.bt, &t)) {
+					T.bt = t;
+					T.btri = T.tg.x + i;
+					T.binst = T.cinst;
+					T.found = true;
+					if (ANY) {
+						sink(ridx, T, err);
+						active = false;
+					}
+				}
+			}
+		}
+	}
+}
+
+// Node visit, then the triangle group (Ylitie, Karras and Laine, HPG
+// 2017): each iteration a lane without BLAS triangles takes one node step
+// (instance entry, child visit or pop); then all lanes holding triangles test
+// them one per inner iteration, unless fewer than a fifth of the active lanes
+// hold any: then those that still have nodes to visit push their triangles
+// and the warp goes back to visiting nodes.
+template <bool ANY, int STACK, bool COUNT, class Sink>
+__device__ __forceinline__ void trace_ylitie(const DScene &S,
+                                             const float4 *rays, uint32_t n,
+                                             uint32_t *work, uint2 *stk,
+                                             uint32_t stride, Sink &sink)
+{
+	const uint32_t lane = threadIdx.x & 31u;
+	bool active = false, exhausted = false;
+	uint32_t ridx = 0, err = 0;
+	Trav T;
+	for (;;) {
+		uint32_t vnode = kNone;
+		uint32_t idle = __ballot_sync(kFull, !active);
+		if (!exhausted && __popc(idle) >= kRefill) {
+			uint32_t cnt = __popc(idle);
+			uint32_t leader = __ffs(idle) - 1;
+			uint32_t base = 0;
+			if (lane == leader)
+				base = atomicAdd(work, cnt);
+			base = __shfl_sync(kFull, base, leader);
+			if (base + cnt >= n)
+				exhausted = true;
+			if (!active) {
+				uint32_t my = base + __popc(idle & ((1u << lane) - 1u));
+				if (my < n) {
+					ridx = my;
+					err = 0;
+					trav_start(T, rays[2u * my], rays[2u * my + 1u]);
+					vnode = 0u;
+					active = true;
+				}
+			}
+		}
+		if (!__any_sync(kFull, active)) {
+			if (exhausted)
+				return;
+			continue;
+		}
+		bool holding = active && T.level == 1u && T.tg.y != 0u;
+		if (active && !holding && vnode == kNone) {
+			if (node_step<STACK>(T, S, rays, ridx, stk, stride, err,
+			  &vnode)) {
+				sink(ridx, T, err);
+				active = false;
+			}
+		}
+		if (vnode != kNone) {
+			if (COUNT)
+				T.nvisit++;
+			visit(T.level ? S.blas : S.tlas, vnode, T.r, T.bt, T.ng, T.tg);
+		}
+		for (;;) {
+			bool want = active && T.level == 1u && T.tg.y != 0u;
+			uint32_t wm = __ballot_sync(kFull, want);
+			if (!wm)
+				break;
+			if (__popc(wm) * 5u < __popc(__ballot_sync(kFull, active))) {
+				if (want && (T.ng.y >> 24) && T.sp < STACK) {
+					stk[(uint32_t)T.sp++ * stride] =
+					  make_uint2(T.tg.x | kItemGroup, T.tg.y);
+					T.tg.y = 0u;
+				}
+				break;
+			}
+			if (want) {
+				uint32_t i = __ffs(T.tg.y) - 1;
+				T.tg.y &= T.tg.y - 1u;
+				float t;
+				if (COUNT)
+					T.ntest++;
+				if (tri_hit(S.tris, T.tg.x + i, T.r, T.bt, &t)) {
+					T.bt = t;
+					T.btri = T.tg.x + i;
+					T.binst = T.cinst;
+					T.found = true;
+					if (ANY) {
+						sink(ridx, T, err);
+						active = false;
+					}
+				}
+			}
+		}
+	}
+}
+
+// Traversal schedules (see trace_step, trace_phase, trace_ylitie).
+enum { kSchedStep = 0, kSchedPhase = 1, kSchedYlitie = 2 };
+
+template <int SCHED, bool ANY, int STACK, bool COUNT, class Sink>
+__device__ __forceinline__ void trace_persistent(const DScene &S,
+                                                 const float4 *rays,
+                                                 uint32_t n, uint32_t *work,
+                                                 uint2 *stk, uint32_t stride,
+                                                 Sink &sink)
+{
+	if (SCHED == kSchedStep)
+		trace_step<ANY, STACK, COUNT>(S, rays, n, work, stk, stride, sink);
+	else if (SCHED == kSchedPhase)
+		trace_phase<ANY, STACK, COUNT>(S, rays, n, work, stk, stride, sink);
+	else
+		trace_ylitie<ANY, STACK, COUNT>(S, rays, n, work, stk, stride,
+		  sink);
 }
 
 // --------------------------------------------------------------- sinks --
