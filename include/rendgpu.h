@@ -148,6 +148,27 @@ int rendgpu_trace_rays_device(struct rdata *rd, const void *rays_device,
 int rendgpu_occluded_device(struct rdata *rd, const void *rays_device,
                             uint32_t n, void *occl_device);
 
+/* Closest hits of n device rays into device hits, like
+ * rendgpu_trace_rays_device, but the call allocates no device memory.
+ * No counterpart in the reference (it has no device memory at all).  It
+ * exists for callers that cannot let a library call cudaMalloc or cudaFree
+ * while they run: applications that hand out all device memory from their
+ * own arena sized at start-up, and frame loops that cannot absorb the device
+ * synchronisation an allocation or free can imply.  Its scratch (the raw hits
+ * of at most RENDGPU_NOALLOC_MAX_RAYS rays plus three counters, 4 MiB +
+ * 256 B) is one static device array that every GPU loading the library keeps
+ * until the process exits.  n above the maximum returns RENDGPU_ELIMIT.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU (two
+ * contexts, two streams, or two host threads) race on it; calls on one
+ * context are ordered by its stream.  Rays the device had to abandon come
+ * back as misses.  Returns without synchronising. */
+#define RENDGPU_NOALLOC_MAX_RAYS (1u << 18)
+int rendgpu_trace_rays_device_noalloc(struct rdata *rd,
+                                      const void *rays_device, uint32_t n,
+                                      void *hits_device);
+
 /* Wait for all work of the context. */
 int rendgpu_sync(struct rdata *rd);
 

@@ -122,6 +122,7 @@ class GpuLib:
                 ("rendgpu_occluded", [vp, vp, u32, vp]),
                 ("rendgpu_trace_rays_device", [vp, vp, u32, vp]),
                 ("rendgpu_occluded_device", [vp, vp, u32, vp]),
+                ("rendgpu_trace_rays_device_noalloc", [vp, vp, u32, vp]),
                 ("rendgpu_sync", [vp]), ("rendgpu_get_stats", [vp, vp]),
                 ("rendgpu_get_lights", [vp, vp, u32, vp]),
                 ("rendgpu_get_stream", [vp, vp]),

@@ -490,6 +490,54 @@ uint64_t held_bytes(const Ctx *c)
 	return s;
 }
 
+// ------------------------------------------------ allocation-free tracing --
+//
+// rendgpu_trace_rays_device_noalloc keeps its scratch (three counters and the
+// raw hits of up to kNoAllocMaxRays rays, 4 MiB + 256 B) in this file-scope
+// device array instead of context buffers that grow with cudaMalloc.  Every
+// GPU that loads the library holds the array until the process exits.  Host
+// code only ever sees a host-side stand-in under the array's name, so the
+// device address is looked up with cudaGetSymbolAddress once per device and
+// cached.
+
+constexpr uint32_t kNoAllocMaxRays = 1u << 18;
+constexpr size_t kNoAllocHeader = 256;
+
+static __device__ __align__(256) unsigned char
+  g_noalloc_scratch[kNoAllocHeader + (size_t)kNoAllocMaxRays * 16];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[64];
+
+// Device address of the scratch array on the current device `dev` (first
+// use on a device performs the lookup).
+int noalloc_scratch(Ctx *c, int dev, unsigned char **base)
+{
+	if (dev < 0 || dev >= 64)
+		return fail(c, RENDGPU_EINVAL, "device ordinal above 63");
+	std::lock_guard<std::mutex> lk(g_noalloc_mu);
+	if (!g_noalloc_addr[dev]) {
+		void *p = nullptr;
+		cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		if (e != cudaSuccess || !p)
+			return cuda_fail(c, e, "cudaGetSymbolAddress(scratch)");
+		g_noalloc_addr[dev] = p;
+	}
+	*base = static_cast<unsigned char *>(g_noalloc_addr[dev]);
+	return 0;
+}
+
+// Count, error and work counters of one call, written on the device so the
+// call needs no host-to-device copy.
+__global__ void k_noalloc_begin(uint32_t *hdr, uint32_t n)
+{
+	if (threadIdx.x == 0) {
+		hdr[0] = n;
+		hdr[1] = 0u;
+		hdr[2] = 0u;
+	}
+}
+
 } // namespace
 } // namespace nb
 
@@ -803,6 +851,40 @@ int rendgpu_occluded_device(struct rdata *rdp, const void *rays, uint32_t n,
 	uint32_t *b = c->berr.as<uint32_t>();
 	return launch_occluded(c, static_cast<const float4 *>(rays), b, b + 2,
 	  static_cast<uint8_t *>(occl), b + 1);
+}
+
+int rendgpu_trace_rays_device_noalloc(struct rdata *rdp, const void *rays,
+                                      uint32_t n, void *hits)
+{
+	Ctx *c = find_ctx(rdp);
+	int rc = ready(c, false);
+	if (rc)
+		return rc;
+	if (n == 0)
+		return 0;
+	if (n > kNoAllocMaxRays)
+		return fail(c, RENDGPU_ELIMIT, "rendgpu_trace_rays_device_noalloc: "
+		  "n = " + std::to_string(n) + " exceeds the fixed scratch of " +
+		  std::to_string(kNoAllocMaxRays) + " rays; split the batch");
+	if (!rays || !hits)
+		return fail(c, RENDGPU_EINVAL, "null pointer");
+	NB_CK(c, cudaSetDevice(c->device));
+	unsigned char *base = nullptr;
+	rc = noalloc_scratch(c, c->device, &base);
+	if (rc)
+		return rc;
+	uint32_t *hdr = reinterpret_cast<uint32_t *>(base);
+	float4 *raw = reinterpret_cast<float4 *>(base + kNoAllocHeader);
+	k_noalloc_begin<<<1, 32, 0, c->stream>>>(hdr, n);
+	NB_CK(c, cudaGetLastError());
+	const float4 *r4 = static_cast<const float4 *>(rays);
+	rc = launch_trace(c, r4, hdr, hdr + 2, raw, hdr + 1, nullptr);
+	if (rc)
+		return rc;
+	k_refine<<<grid_for(c, n, 256), 256, 0, c->stream>>>(scene_of(c), r4,
+	  hdr, raw, static_cast<float4 *>(hits));
+	NB_CK(c, cudaGetLastError());
+	return 0;
 }
 
 static int batch_errors(Ctx *c)
