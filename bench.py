@@ -348,6 +348,8 @@ def run_ours(a):
                "samples_per_s": samples_all / (ms_max / 1e3),
                "rays_per_frame": rays / a.steps,
                "closest_rays_per_frame": closest / a.steps,
+               "rays_per_bounce": {"closest": st["bounce_closest"][:a.depth],
+                                   "shadow": st["bounce_shadow"][:a.depth]},
                "ms_trace_per_frame": trace_ms / a.steps,
                "ms_shadow_per_frame": shadow_ms / a.steps,
                "gpu_launches": launches, "e2e": e2e, "roofline": roof,

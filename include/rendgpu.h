@@ -94,6 +94,8 @@ struct rendgpu_stats {
 	uint64_t d2h_bytes;      /* device->host bytes of the last readback */
 	uint64_t node_visits;    /* closest-hit node visits (COUNT flag) */
 	uint64_t tri_tests;      /* closest-hit triangle tests (COUNT flag) */
+	uint32_t bounce_closest[16]; /* closest-hit rays per bounce */
+	uint32_t bounce_shadow[16];  /* shadow rays per bounce */
 };
 
 /* Create the GPU context of `rd` (one per rdata).  Replaces nothing in the

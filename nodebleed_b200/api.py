@@ -75,10 +75,16 @@ class RendgpuStats(C.Structure):
                 ("ms_shade", C.c_float), ("device_errors", C.c_uint32),
                 ("max_stack", C.c_uint32), ("device_bytes", C.c_uint64),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
-                ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64)]
+                ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
+                ("bounce_closest", C.c_uint32 * 16),
+                ("bounce_shadow", C.c_uint32 * 16)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            d[k] = list(v) if hasattr(v, "__len__") else v
+        return d
 
 
 class HostLib:

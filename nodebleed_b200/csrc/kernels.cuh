@@ -33,7 +33,9 @@ struct FrameDev {
 	float    *acc;     // W*H*3
 	uint32_t *buf;     // W*H ARGB8
 	uint32_t *cnt;     // [0],[1] ray queues, [2] shadow, [3] errors,
-	                   // [4] closest-hit work counter, [5] shadow work
+	                   // [4] closest-hit work counter, [5] shadow work,
+	                   // [6] shadow launches, [8+k] / [24+k] closest /
+	                   // shadow rays of bounce k
 	unsigned long long *rays; // [0] closest, [1] shadow
 	uint32_t  W, H, spp, npaths;
 };
@@ -264,8 +266,13 @@ __global__ void __launch_bounds__(128, 8) k_shadow(DScene S, FrameDev F)
 {
 	extern __shared__ uint2 sstk[];
 	uint32_t n = F.cnt[2];
-	if (blockIdx.x == 0 && threadIdx.x == 0)
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
 		atomicAdd(&F.rays[1], (unsigned long long)n);
+		atomicAdd(&F.cnt[6], 1u);
+		uint32_t k = F.cnt[6] - 1u; // bounce of this shadow launch
+		if (k < 16u)
+			F.cnt[24u + k] = n;
+	}
 	SinkShadow sink{F.shadow, F.scol, F.pL, &F.cnt[3]};
 	trace_persistent<SCHED, true, STACK, false>(S, F.shadow, n, &F.cnt[5],
 	  sstk + threadIdx.x, blockDim.x, sink);
@@ -299,6 +306,8 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 	if (blockIdx.x == 0 && threadIdx.x == 0) {
 		F.cnt[4] = 0u;
 		F.cnt[5] = 0u;
+		if (k < 16u)
+			F.cnt[8u + k] = n; // closest-hit rays of bounce k
 	}
 	for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n;
 	     i0 += gridDim.x * blockDim.x) {

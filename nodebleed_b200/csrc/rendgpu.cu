@@ -384,7 +384,7 @@ int render_frame(Ctx *c)
 	c->nev = 0;
 	c->st.launches = 0;
 	c->st.trace_launches = 0;
-	NB_CK(c, cudaMemsetAsync(c->cnt.p, 0, 8 * sizeof(uint32_t), c->stream));
+	NB_CK(c, cudaMemsetAsync(c->cnt.p, 0, 64 * sizeof(uint32_t), c->stream));
 	NB_CK(c, cudaMemsetAsync(c->rays.p, 0, 4 * sizeof(unsigned long long),
 	  c->stream));
 	ev_record(c); // 0
@@ -431,7 +431,7 @@ int render_frame(Ctx *c)
 	c->st.launches++;
 	ev_record(c);
 	unsigned long long hr[4];
-	uint32_t hc[4];
+	uint32_t hc[64];
 	NB_CK(c, cudaMemcpyAsync(hr, c->rays.p, sizeof(hr),
 	  cudaMemcpyDeviceToHost, c->stream));
 	NB_CK(c, cudaMemcpyAsync(hc, c->cnt.p, sizeof(hc),
@@ -443,6 +443,10 @@ int render_frame(Ctx *c)
 	c->st.shadow_rays = hr[1];
 	c->st.rays = hr[0] + hr[1];
 	c->st.device_errors = hc[3];
+	for (int k = 0; k < 16; k++) {
+		c->st.bounce_closest[k] = hc[8 + k];
+		c->st.bounce_shadow[k] = hc[24 + k];
+	}
 	c->st.max_stack = need_stack(c);
 	if (c->cfg.flags & RENDGPU_FLAG_TIMING) {
 		c->st.ms_frame = ev_ms(c, 0, c->nev - 1);
@@ -571,7 +575,7 @@ int rendgpu_init(struct rdata *rdp, const struct rendgpu_cfg *cfg)
 		free_ctx(c);
 		return RENDGPU_ECUDA;
 	}
-	if (c->cnt.ensure(16 * sizeof(uint32_t)) != cudaSuccess ||
+	if (c->cnt.ensure(64 * sizeof(uint32_t)) != cudaSuccess ||
 	  c->rays.ensure(4 * sizeof(unsigned long long)) != cudaSuccess ||
 	  c->berr.ensure(16) != cudaSuccess) {
 		free_ctx(c);
