@@ -61,7 +61,8 @@ struct rendgpu_cfg {
 	uint32_t block;      /* threads per block of the trace kernels (0 = auto) */
 	uint32_t sched;      /* traversal schedule: 0 = default, 1 = step,
 	                        2 = phase, 3 = ylitie (see trace.cuh) */
-	uint32_t reserved[7];
+	uint32_t reserved[7]; /* [0]: float bits of the cache's Adam learning
+	                         rate (0 = 1e-2) */
 };
 
 /* A ray for the batch calls: origin, tmax, direction (32 bytes). */
@@ -170,6 +171,33 @@ int rendgpu_occluded_device(struct rdata *rd, const void *rays_device,
 int rendgpu_trace_rays_device_noalloc(struct rdata *rd,
                                       const void *rays_device, uint32_t n,
                                       void *hits_device);
+
+/* Neural radiance cache (no counterpart in the reference).  A 64-input MLP
+ * with 5 hidden layers of 64 ReLU units and 3 linear outputs, BF16 on the
+ * tensor cores with FP32 master weights and Adam (beta 0.9/0.99, eps 1e-15).
+ * Parameters: RENDGPU_NRC_PARAMS floats, layer l (0..4: 64x64, 5: 8x64 of
+ * which 3 rows are used) stored [out][in] at offset l * 4096. */
+#define RENDGPU_NRC_PARAMS (5 * 4096 + 8 * 64)
+
+/* (Re)initialise the weights (Xavier uniform from `seed`), zero Adam. */
+int rendgpu_nrc_reset(struct rdata *rd, uint64_t seed);
+/* Copy the FP32 master weights out (write = 0) or in (write = 1). */
+int rendgpu_nrc_weights(struct rdata *rd, float *host, int write);
+/* 12 floats per query (world position, outgoing direction, normal,
+ * albedo) -> 64 BF16 features (frequency-encoded position in the scene
+ * box, encoded direction, normal, albedo, zero padding). */
+int rendgpu_nrc_encode_device(struct rdata *rd, const float *raw_device,
+                              uint32_t n, void *feats_device);
+/* MLP outputs (r, g, b, 0) per query. */
+int rendgpu_nrc_infer_device(struct rdata *rd, const void *feats_device,
+                             uint32_t n, float *out_device);
+/* Gradient of the relative L2 loss mean((y-t)^2 / (y^2 + 0.01)) over a
+ * batch (targets: 4 floats per query, the 4th unused); update = 1 takes
+ * one Adam step.  grad_device (RENDGPU_NRC_PARAMS floats) and loss_host
+ * may be NULL; a non-NULL loss_host synchronises. */
+int rendgpu_nrc_train_device(struct rdata *rd, const void *feats_device,
+                             const float *targets_device, uint32_t n,
+                             int update, float *grad_device, float *loss_host);
 
 /* Wait for all work of the context. */
 int rendgpu_sync(struct rdata *rd);

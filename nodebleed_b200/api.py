@@ -129,6 +129,12 @@ class GpuLib:
                 ("rendgpu_trace_rays_device", [vp, vp, u32, vp]),
                 ("rendgpu_occluded_device", [vp, vp, u32, vp]),
                 ("rendgpu_trace_rays_device_noalloc", [vp, vp, u32, vp]),
+                ("rendgpu_nrc_reset", [vp, C.c_uint64]),
+                ("rendgpu_nrc_weights", [vp, vp, C.c_int]),
+                ("rendgpu_nrc_encode_device", [vp, vp, u32, vp]),
+                ("rendgpu_nrc_infer_device", [vp, vp, u32, vp]),
+                ("rendgpu_nrc_train_device", [vp, vp, vp, u32, C.c_int, vp,
+                                              vp]),
                 ("rendgpu_sync", [vp]), ("rendgpu_get_stats", [vp, vp]),
                 ("rendgpu_get_lights", [vp, vp, u32, vp]),
                 ("rendgpu_get_stream", [vp, vp]),
@@ -334,6 +340,23 @@ class GpuRenderer:
         st = RendgpuStats()
         self._ck(self.g.rendgpu_get_stats(self.ptr, C.byref(st)), "stats")
         return st.as_dict()
+
+    # ---- neural radiance cache
+    NRC_PARAMS = 5 * 4096 + 8 * 64
+
+    def nrc_reset(self, seed=1):
+        self._ck(self.g.rendgpu_nrc_reset(self.ptr, seed), "nrc_reset")
+
+    def nrc_weights(self, w=None):
+        """Get (w is None) or set the FP32 master weights."""
+        if w is None:
+            out = np.zeros(self.NRC_PARAMS, np.float32)
+            self._ck(self.g.rendgpu_nrc_weights(self.ptr, out.ctypes.data, 0),
+                     "nrc_weights")
+            return out
+        w = np.ascontiguousarray(w, np.float32)
+        self._ck(self.g.rendgpu_nrc_weights(self.ptr, w.ctypes.data, 1),
+                 "nrc_weights")
 
     def stream(self):
         """cudaStream_t of this context, as an integer handle."""

@@ -1,0 +1,498 @@
+// Neural radiance cache MLP (sm_100a): 64 inputs, 5 hidden layers of 64
+// ReLU units, 3 linear outputs, no biases; BF16 operands on the tensor cores
+// with FP32 accumulation, FP32 master weights updated by Adam.
+//
+// Weights of layer l are stored [out][in] (row-major), so a row of 8..64
+// outputs is the "col" B operand of mma.m16n8k16.row.col directly; the
+// backward pass reads a transposed copy [in][out].  The output layer has 3
+// outputs padded to 8 (forward) / 16 (transposed copy) with zero rows.
+//
+// Forward: a warp owns 16 rows; the FP32 C fragments of two adjacent
+// 8-column tiles repack into the BF16 A fragment of the next layer's 16-wide
+// k tile in registers (thread layout of m16n8k16), so activations never leave
+// the register file.  Training additionally keeps each layer's input in shared
+// memory for the weight gradients, which use ldmatrix.trans to form the
+// transposed operands.
+
+#ifndef NB_NRC_CUH
+#define NB_NRC_CUH
+
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace nb {
+
+constexpr int kMlpIn = 64;
+constexpr int kMlpHidden = 64;
+constexpr int kMlpSquare = 5;              // 64x64 matrices
+constexpr int kMlpOutPad = 8;              // output rows in the fwd copy
+constexpr int kMlpOutPadT = 16;            // output cols in the bwd copy
+constexpr int kMlpSq = kMlpHidden * kMlpHidden;
+// parameter offsets (elements) of the FP32 master / forward BF16 copy
+constexpr int kMlpParams = kMlpSquare * kMlpSq + kMlpOutPad * kMlpHidden;
+// transposed BF16 copy: 5 square + [64][16]
+constexpr int kMlpParamsT = kMlpSquare * kMlpSq + kMlpHidden * kMlpOutPadT;
+constexpr int kMlpRowPad = 72;             // smem row stride (bf16), no bank conflicts
+
+// ------------------------------------------------------------ mma helpers --
+
+__device__ __forceinline__ void mma16816(float *c, const uint32_t *a,
+                                         uint32_t b0, uint32_t b1)
+{
+	asm volatile(
+	  "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+	  "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+	  : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+	  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+	__nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+	return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t *r, const void *p)
+{
+	uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+	asm volatile(
+	  "ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+	  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+
+__device__ __forceinline__ void ldsm_x2_trans(uint32_t *r, const void *p)
+{
+	uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+	asm volatile(
+	  "ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
+	  : "=r"(r[0]), "=r"(r[1]) : "r"(a));
+}
+
+// A fragment (16 rows x 16 k) of a row-major bf16 tile in shared memory
+// with row stride kMlpRowPad.
+__device__ __forceinline__ void lda_smem(uint32_t *a, const __nv_bfloat16 *t,
+                                         int kt, int lane)
+{
+	int r = lane >> 2, c = (lane & 3) * 2 + kt * 16;
+	a[0] = *reinterpret_cast<const uint32_t *>(t + r * kMlpRowPad + c);
+	a[1] = *reinterpret_cast<const uint32_t *>(t + (r + 8) * kMlpRowPad + c);
+	a[2] = *reinterpret_cast<const uint32_t *>(t + r * kMlpRowPad + c + 8);
+	a[3] = *reinterpret_cast<const uint32_t *>(t + (r + 8) * kMlpRowPad + c +
+	  8);
+}
+
+// B fragment (16 k x 8 n) from weights stored [n][k] with row length K
+// (shared or global memory).
+__device__ __forceinline__ void ldb_w(uint32_t *b, const __nv_bfloat16 *w,
+                                      int K, int nt, int kt, int lane)
+{
+	int n = nt * 8 + (lane >> 2), k = kt * 16 + (lane & 3) * 2;
+	b[0] = *reinterpret_cast<const uint32_t *>(w + n * K + k);
+	b[1] = *reinterpret_cast<const uint32_t *>(w + n * K + k + 8);
+}
+
+// Repack 8 FP32 C tiles (16 x 64) into 4 BF16 A fragments (k tiles), with
+// ReLU when relu is set.
+__device__ __forceinline__ void c_to_a(const float c[8][4], uint32_t a[4][4],
+                                       bool relu)
+{
+#pragma unroll
+	for (int kt = 0; kt < 4; kt++) {
+		const float *lo = c[2 * kt], *hi = c[2 * kt + 1];
+		float v[8];
+#pragma unroll
+		for (int i = 0; i < 4; i++) {
+			v[i] = relu ? fmaxf(lo[i], 0.0f) : lo[i];
+			v[4 + i] = relu ? fmaxf(hi[i], 0.0f) : hi[i];
+		}
+		a[kt][0] = pack_bf16(v[0], v[1]);
+		a[kt][1] = pack_bf16(v[2], v[3]);
+		a[kt][2] = pack_bf16(v[4], v[5]);
+		a[kt][3] = pack_bf16(v[6], v[7]);
+	}
+}
+
+// Store 4 A fragments (16 x 64 bf16) to a padded shared-memory tile.
+__device__ __forceinline__ void st_a(__nv_bfloat16 *t, const uint32_t a[4][4],
+                                     int lane)
+{
+	int r = lane >> 2;
+#pragma unroll
+	for (int kt = 0; kt < 4; kt++) {
+		int c = (lane & 3) * 2 + kt * 16;
+		*reinterpret_cast<uint32_t *>(t + r * kMlpRowPad + c) = a[kt][0];
+		*reinterpret_cast<uint32_t *>(t + (r + 8) * kMlpRowPad + c) = a[kt][1];
+		*reinterpret_cast<uint32_t *>(t + r * kMlpRowPad + c + 8) = a[kt][2];
+		*reinterpret_cast<uint32_t *>(t + (r + 8) * kMlpRowPad + c + 8) =
+		  a[kt][3];
+	}
+}
+
+// A fragments of one 16-row tile of BF16 features [n][64] in global memory;
+// rows beyond n read as zero.
+__device__ __forceinline__ void lda_global(uint32_t a[4][4],
+                                           const __nv_bfloat16 *f,
+                                           uint32_t row0, uint32_t n, int lane)
+{
+	uint32_t r0 = row0 + (lane >> 2), r1 = r0 + 8;
+#pragma unroll
+	for (int kt = 0; kt < 4; kt++) {
+		int c = (lane & 3) * 2 + kt * 16;
+		a[kt][0] = r0 < n ? __ldg(reinterpret_cast<const uint32_t *>(
+		  f + (size_t)r0 * kMlpIn + c)) : 0u;
+		a[kt][1] = r1 < n ? __ldg(reinterpret_cast<const uint32_t *>(
+		  f + (size_t)r1 * kMlpIn + c)) : 0u;
+		a[kt][2] = r0 < n ? __ldg(reinterpret_cast<const uint32_t *>(
+		  f + (size_t)r0 * kMlpIn + c + 8)) : 0u;
+		a[kt][3] = r1 < n ? __ldg(reinterpret_cast<const uint32_t *>(
+		  f + (size_t)r1 * kMlpIn + c + 8)) : 0u;
+	}
+}
+
+// One square layer: c = a x W^T (W [64][64] bf16 in shared memory).
+__device__ __forceinline__ void layer_sq(float c[8][4], const uint32_t a[4][4],
+                                         const __nv_bfloat16 *w, int lane)
+{
+#pragma unroll
+	for (int nt = 0; nt < 8; nt++) {
+		c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0f;
+#pragma unroll
+		for (int kt = 0; kt < 4; kt++) {
+			uint32_t b[2];
+			ldb_w(b, w, 64, nt, kt, lane);
+			mma16816(c[nt], a[kt], b[0], b[1]);
+		}
+	}
+}
+
+// Output layer: c (16 x 8, first 3 columns valid) = a x W5^T.
+__device__ __forceinline__ void layer_out(float c[4], const uint32_t a[4][4],
+                                          const __nv_bfloat16 *w5, int lane)
+{
+	c[0] = c[1] = c[2] = c[3] = 0.0f;
+#pragma unroll
+	for (int kt = 0; kt < 4; kt++) {
+		uint32_t b[2];
+		ldb_w(b, w5, 64, 0, kt, lane);
+		mma16816(c, a[kt], b[0], b[1]);
+	}
+}
+
+// ------------------------------------------------------------- inference --
+
+// out[i] = (r, g, b, 0) = MLP(feats[i]) for i < n.  Persistent CTAs of 4
+// warps; the forward BF16 weights (41 KB) are staged in shared memory once.
+__global__ void __launch_bounds__(128) k_mlp_fwd(const __nv_bfloat16 *wbf,
+                                                 const __nv_bfloat16 *feats,
+                                                 uint32_t n, float4 *out)
+{
+	extern __shared__ __align__(16) unsigned char mlp_smem[];
+	__nv_bfloat16 *w = reinterpret_cast<__nv_bfloat16 *>(mlp_smem);
+	for (int i = threadIdx.x; i < kMlpParams / 8; i += blockDim.x)
+		reinterpret_cast<uint4 *>(w)[i] =
+		  __ldg(reinterpret_cast<const uint4 *>(wbf) + i);
+	__syncthreads();
+	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	uint32_t tiles = (n + 15u) / 16u;
+	for (uint32_t t = blockIdx.x * 4u + warp; t < tiles;
+	     t += gridDim.x * 4u) {
+		uint32_t a[4][4];
+		float c[8][4];
+		lda_global(a, feats, t * 16u, n, lane);
+#pragma unroll 1
+		for (int l = 0; l < kMlpSquare; l++) {
+			layer_sq(c, a, w + l * kMlpSq, lane);
+			c_to_a(c, a, true);
+		}
+		float o[4];
+		layer_out(o, a, w + kMlpSquare * kMlpSq, lane);
+		// thread holds rows lane/4 (cols 2q, 2q+1) and lane/4+8
+		int q = lane & 3;
+		uint32_t r0 = t * 16u + (lane >> 2), r1 = r0 + 8u;
+		// gather the 3 valid columns of each row into lanes with q == 0
+		float x1 = __shfl_down_sync(0xffffffffu, o[0], 1);
+		float x3 = __shfl_down_sync(0xffffffffu, o[2], 1);
+		if (q == 0) {
+			// cols 0,1 from this lane, col 2 from lane+1 (its col 2q = 2)
+			if (r0 < n)
+				out[r0] = make_float4(o[0], o[1], x1, 0.0f);
+			if (r1 < n)
+				out[r1] = make_float4(o[2], o[3], x3, 0.0f);
+		}
+	}
+}
+
+// --------------------------------------------------------------- training --
+
+// Shared memory of the training kernel (per CTA of 4 warps).
+struct MlpTrainSmem {
+	__nv_bfloat16 w[kMlpParams];         // forward copy [out][in]
+	__nv_bfloat16 act[4][6][16 * kMlpRowPad]; // inputs of layers 0..5
+	__nv_bfloat16 dz[4][16 * kMlpRowPad]; // gradient of one layer's output
+	float dw[kMlpParams];                // weight-gradient accumulators
+	float loss;
+};
+
+// Relative L2 loss mean((y - t)^2 / (y^2 + 0.01)) over the batch and three
+// channels (y detached in the denominator); gradients of a batch of n
+// samples into this CTA's partial gradient slice grad[blockIdx.x].
+__global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16 *wbf,
+                                                  const __nv_bfloat16 *wbt,
+                                                  const __nv_bfloat16 *feats,
+                                                  const float4 *targets,
+                                                  uint32_t n, float *grad,
+                                                  float *loss)
+{
+	extern __shared__ __align__(16) unsigned char mlp_smem[];
+	MlpTrainSmem &S = *reinterpret_cast<MlpTrainSmem *>(mlp_smem);
+	for (int i = threadIdx.x; i < kMlpParams / 8; i += blockDim.x)
+		reinterpret_cast<uint4 *>(S.w)[i] =
+		  __ldg(reinterpret_cast<const uint4 *>(wbf) + i);
+	for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x)
+		S.dw[i] = 0.0f;
+	if (threadIdx.x == 0)
+		S.loss = 0.0f;
+	__syncthreads();
+	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const float inv = 1.0f / (3.0f * (float)n);
+	uint32_t tiles = (n + 15u) / 16u;
+	float lsum = 0.0f;
+	for (uint32_t t = blockIdx.x * 4u + warp; t < tiles;
+	     t += gridDim.x * 4u) {
+		uint32_t a[4][4];
+		float c[8][4];
+		lda_global(a, feats, t * 16u, n, lane);
+		st_a(S.act[warp][0], a, lane);
+		for (int l = 0; l < kMlpSquare; l++) {
+			layer_sq(c, a, S.w + l * kMlpSq, lane);
+			c_to_a(c, a, true);
+			st_a(S.act[warp][l + 1], a, lane);
+		}
+		float o[4];
+		layer_out(o, a, S.w + kMlpSquare * kMlpSq, lane);
+		// output gradient: thread holds rows r0 (cols 2q, 2q+1), r1
+		int q = lane & 3;
+		uint32_t r0 = t * 16u + (lane >> 2), r1 = r0 + 8u;
+		float g[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+		for (int i = 0; i < 4; i++) {
+			int col = 2 * q + (i & 1);
+			uint32_t row = i < 2 ? r0 : r1;
+			if (col < 3 && row < n) {
+				float4 tv = __ldg(targets + row);
+				float tt = col == 0 ? tv.x : (col == 1 ? tv.y : tv.z);
+				float y = o[i], d = y - tt, den = y * y + 0.01f;
+				lsum += d * d / den;
+				g[i] = 2.0f * d / den * inv;
+			}
+		}
+		// dz of the output layer as bf16, padded to 16 columns
+		__nv_bfloat16 *dz = S.dz[warp];
+		{
+			int r = lane >> 2, cc = 2 * q;
+			*reinterpret_cast<uint32_t *>(dz + r * kMlpRowPad + cc) =
+			  pack_bf16(g[0], g[1]);
+			*reinterpret_cast<uint32_t *>(dz + (r + 8) * kMlpRowPad + cc) =
+			  pack_bf16(g[2], g[3]);
+			*reinterpret_cast<uint32_t *>(dz + r * kMlpRowPad + cc + 8) = 0u;
+			*reinterpret_cast<uint32_t *>(dz + (r + 8) * kMlpRowPad + cc + 8) =
+			  0u;
+		}
+		__syncwarp();
+		// backward through the 6 layers
+		for (int l = kMlpSquare; l >= 0; l--) {
+			int nout = l == kMlpSquare ? 8 : 64;
+			const __nv_bfloat16 *act = S.act[warp][l];
+			float *dw = S.dw + l * kMlpSq;
+			// dW[out][in] += sum_rows dz[row][out] * act[row][in]:
+			// M = out, N = in, K = 16 rows
+			for (int mt = 0; mt < nout / 16 + (nout == 8); mt++) {
+				uint32_t af[4];
+				// A = dz^T (m = out, k = row): ldmatrix.trans of dz
+				// blocks (rows 0-7 | 8-15) x (out mt*16 + 0-7 | 8-15)
+				{
+					int blk = lane >> 3, rr = lane & 7;
+					int row = (blk >> 1) * 8 + rr;
+					int col = mt * 16 + (blk & 1) * 8;
+					ldsm_x4_trans(af, dz + row * kMlpRowPad + col);
+				}
+#pragma unroll
+				for (int nt = 0; nt < 8; nt++) {
+					// B = act (k = row, n = in): ldmatrix.trans
+					uint32_t bf[2];
+					int blk = (lane >> 3) & 1, rr = lane & 7;
+					ldsm_x2_trans(bf, act + (blk * 8 + rr) * kMlpRowPad +
+					  nt * 8);
+					float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+					mma16816(acc, af, bf[0], bf[1]);
+					int m0 = mt * 16 + (lane >> 2), nn = nt * 8 + 2 * q;
+					if (m0 < nout) {
+						atomicAdd(dw + m0 * 64 + nn, acc[0]);
+						atomicAdd(dw + m0 * 64 + nn + 1, acc[1]);
+					}
+					if (m0 + 8 < nout) {
+						atomicAdd(dw + (m0 + 8) * 64 + nn, acc[2]);
+						atomicAdd(dw + (m0 + 8) * 64 + nn + 1, acc[3]);
+					}
+				}
+			}
+			if (l == 0)
+				break;
+			// dA[row][in] = sum_out dz[row][out] * W[out][in]:
+			// M = 16 rows, N = 64 in, K = out (16 padded for the
+			// output layer); B from the transposed copy [in][out],
+			// read through L1 (it does not fit in shared memory too)
+			int kts = l == kMlpSquare ? 1 : 4;
+			int K = l == kMlpSquare ? kMlpOutPadT : 64;
+			const __nv_bfloat16 *wt = wbt + l * kMlpSq;
+			uint32_t dzf[4][4];
+			for (int kt = 0; kt < kts; kt++)
+				lda_smem(dzf[kt], dz, kt, lane);
+#pragma unroll
+			for (int nt = 0; nt < 8; nt++) {
+				c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0f;
+				for (int kt = 0; kt < kts; kt++) {
+					uint32_t b[2];
+					ldb_w(b, wt, K, nt, kt, lane);
+					mma16816(c[nt], dzf[kt], b[0], b[1]);
+				}
+			}
+			// dz of layer l-1 = dA * relu'(act_l), act_l = relu(z_{l-1})
+			__syncwarp();
+#pragma unroll
+			for (int nt = 0; nt < 8; nt++) {
+				int r = lane >> 2, cc = nt * 8 + 2 * q;
+				const __nv_bfloat16 *ap = act + r * kMlpRowPad + cc;
+				const __nv_bfloat16 *ap8 = act + (r + 8) * kMlpRowPad + cc;
+				float v0 = __bfloat162float(ap[0]) > 0.0f ? c[nt][0] : 0.0f;
+				float v1 = __bfloat162float(ap[1]) > 0.0f ? c[nt][1] : 0.0f;
+				float v2 = __bfloat162float(ap8[0]) > 0.0f ? c[nt][2] : 0.0f;
+				float v3 = __bfloat162float(ap8[1]) > 0.0f ? c[nt][3] : 0.0f;
+				*reinterpret_cast<uint32_t *>(dz + r * kMlpRowPad + cc) =
+				  pack_bf16(v0, v1);
+				*reinterpret_cast<uint32_t *>(dz + (r + 8) * kMlpRowPad +
+				  cc) = pack_bf16(v2, v3);
+			}
+			__syncwarp();
+		}
+	}
+	atomicAdd(&S.loss, lsum);
+	__syncthreads();
+	float *gp = grad + (size_t)blockIdx.x * kMlpParams;
+	for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x)
+		gp[i] = S.dw[i];
+	if (threadIdx.x == 0)
+		loss[blockIdx.x] = S.loss;
+}
+
+// Sum the per-CTA partial gradients; optionally write the sum (g_out) and
+// take one Adam step on the FP32 master weights, refreshing both BF16 copies.
+// Output-layer rows 3..7 stay zero.
+__global__ void k_mlp_adam(float *wf, float *m, float *v, const float *part,
+                           int nparts, float *g_out, int update, float lr,
+                           float beta1, float beta2, float eps, float bc1,
+                           float bc2, __nv_bfloat16 *wbf, __nv_bfloat16 *wbt)
+{
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kMlpParams;
+	     i += gridDim.x * blockDim.x) {
+		float g = 0.0f;
+		for (int p = 0; p < nparts; p++)
+			g += part[(size_t)p * kMlpParams + i];
+		int l = i / kMlpSq;
+		int o = (i - l * kMlpSq) / 64, in = i & 63;
+		bool pad = l == kMlpSquare && o >= 3;
+		if (pad)
+			g = 0.0f;
+		if (g_out)
+			g_out[i] = g;
+		float w = wf[i];
+		if (update && !pad) {
+			float mi = beta1 * m[i] + (1.0f - beta1) * g;
+			float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
+			m[i] = mi;
+			v[i] = vi;
+			w -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+			wf[i] = w;
+		}
+		__nv_bfloat16 wb = __float2bfloat16_rn(pad ? 0.0f : w);
+		wbf[i] = wb;
+		if (l < kMlpSquare)
+			wbt[l * kMlpSq + in * 64 + o] = wb;
+		else
+			wbt[kMlpSquare * kMlpSq + in * kMlpOutPadT + o] = wb;
+	}
+}
+
+// ------------------------------------------------------------- encoding --
+
+// Raw cache inputs (12 floats: world position, outgoing direction, shading
+// normal, albedo) -> 64 BF16 features:
+//   0..35  position in the scene box, per axis sin/cos(2^k pi x), k = 0..5
+//   36..43 direction (theta/pi, phi/2pi), sin/cos(2^k pi u), k = 0..1
+//   44..46 (normal + 1) / 2,  47..49 albedo,  50..63 zero
+struct NrcBox {
+	float lo[3], inv[3]; // position -> [0,1]^3
+};
+
+__device__ __forceinline__ void nrc_encode(const float *in, const NrcBox &B,
+                                           __nv_bfloat16 *out)
+{
+	float f[64];
+#pragma unroll
+	for (int i = 0; i < 64; i++)
+		f[i] = 0.0f;
+#pragma unroll
+	for (int a = 0; a < 3; a++) {
+		float x = fminf(fmaxf((in[a] - B.lo[a]) * B.inv[a], 0.0f), 1.0f);
+#pragma unroll
+		for (int k = 0; k < 6; k++) {
+			float s, c;
+			// sin/cos(2^k pi x) = sin/cos(2 pi * frac(x 2^(k-1)))
+			float u = x * ldexpf(1.0f, k - 1);
+			u = u - floorf(u);
+			sincospif(2.0f * u, &s, &c);
+			f[a * 12 + 2 * k] = s;
+			f[a * 12 + 2 * k + 1] = c;
+		}
+	}
+	float dz = fminf(fmaxf(in[5], -1.0f), 1.0f);
+	float th = acosf(dz) * 0.318309886f;
+	float ph = atan2f(in[4], in[3]) * 0.159154943f + 0.5f;
+	float ang[2] = {th, ph};
+#pragma unroll
+	for (int j = 0; j < 2; j++)
+#pragma unroll
+		for (int k = 0; k < 2; k++) {
+			float s, c;
+			sincospif(ldexpf(1.0f, k) * ang[j], &s, &c);
+			f[36 + j * 4 + 2 * k] = s;
+			f[36 + j * 4 + 2 * k + 1] = c;
+		}
+#pragma unroll
+	for (int a = 0; a < 3; a++) {
+		f[44 + a] = 0.5f * (in[6 + a] + 1.0f);
+		f[47 + a] = in[9 + a];
+	}
+#pragma unroll
+	for (int i = 0; i < 64; i += 8) {
+		uint4 v;
+		v.x = pack_bf16(f[i], f[i + 1]);
+		v.y = pack_bf16(f[i + 2], f[i + 3]);
+		v.z = pack_bf16(f[i + 4], f[i + 5]);
+		v.w = pack_bf16(f[i + 6], f[i + 7]);
+		*reinterpret_cast<uint4 *>(out + i) = v;
+	}
+}
+
+__global__ void k_nrc_encode(const float *raw, uint32_t n, NrcBox B,
+                             __nv_bfloat16 *feats)
+{
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+	     i += gridDim.x * blockDim.x)
+		nrc_encode(raw + 12ull * i, B, feats + 64ull * i);
+}
+
+} // namespace nb
+
+#endif

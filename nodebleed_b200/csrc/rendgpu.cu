@@ -18,6 +18,7 @@
 #include "../../include/rendgpu.h"
 #include "kernels.cuh"
 #include "layout.hpp"
+#include "nrc.cuh"
 
 namespace nb {
 namespace {
@@ -75,6 +76,12 @@ struct Ctx {
 	bool     have_frame = false;
 	// batch scratch: rays, raw hits, output; berr = [count, errors, work]
 	DevBuf brays, braw, bhits, berr;
+	// neural radiance cache: FP32 master weights, Adam moments, BF16
+	// forward / transposed copies, per-CTA gradient partials and losses
+	DevBuf mlp_wf, mlp_m, mlp_v, mlp_wbf, mlp_wbt, mlp_part, mlp_loss;
+	uint32_t mlp_step = 0;
+	bool     mlp_ready = false;
+	NrcBox   box{};
 	// stats / errors
 	rendgpu_stats st{};
 	int          last = 0;
@@ -471,7 +478,9 @@ void free_ctx(Ctx *c)
 	DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs, &c->insts,
 	  &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits, &c->shadow,
 	  &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
-	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr};
+	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_wf,
+	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
+	  &c->mlp_loss};
 	for (DevBuf *b : bufs)
 		b->release();
 	for (int i = 0; i < 64; i++)
@@ -487,11 +496,134 @@ uint64_t held_bytes(const Ctx *c)
 	const DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs,
 	  &c->insts, &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits,
 	  &c->shadow, &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf,
-	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr};
+	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
+	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
+	  &c->mlp_part, &c->mlp_loss};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
 		s += b->cap;
 	return s;
+}
+
+// ------------------------------------------------ neural radiance cache --
+
+constexpr float kAdamBeta1 = 0.9f, kAdamBeta2 = 0.99f, kAdamEps = 1e-15f;
+
+float nrc_lr(const Ctx *c)
+{
+	float lr;
+	std::memcpy(&lr, &c->cfg.reserved[0], sizeof(lr));
+	return lr > 0.0f ? lr : 1e-2f;
+}
+
+// Xavier-uniform FP32 master weights from a seeded PCG32 stream, zero Adam
+// moments, BF16 copies refreshed on the device.
+int nrc_reset(Ctx *c, uint64_t seed)
+{
+	NB_CK(c, c->mlp_wf.ensure(kMlpParams * sizeof(float)));
+	NB_CK(c, c->mlp_m.ensure(kMlpParams * sizeof(float)));
+	NB_CK(c, c->mlp_v.ensure(kMlpParams * sizeof(float)));
+	NB_CK(c, c->mlp_wbf.ensure(kMlpParams * sizeof(__nv_bfloat16)));
+	NB_CK(c, c->mlp_wbt.ensure(kMlpParamsT * sizeof(__nv_bfloat16)));
+	NB_CK(c, c->mlp_loss.ensure(1024 * sizeof(float)));
+	std::vector<float> w(kMlpParams, 0.0f);
+	uint64_t st = 0, inc = (seed << 1) | 1u;
+	auto next = [&]() {
+		uint64_t old = st;
+		st = old * 6364136223846793005ull + inc;
+		uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+		uint32_t rot = (uint32_t)(old >> 59u);
+		return (xs >> rot) | (xs << ((32u - rot) & 31u));
+	};
+	next();
+	st += 0x853c49e6748fea9bull;
+	next();
+	for (int l = 0; l <= kMlpSquare; l++) {
+		int nout = l == kMlpSquare ? 3 : 64;
+		float bound = std::sqrt(6.0f / (64.0f + (float)nout));
+		for (int o = 0; o < nout; o++)
+			for (int i = 0; i < 64; i++) {
+				float u = (float)(next() >> 8) * 0x1p-24f;
+				w[l * kMlpSq + o * 64 + i] = (2.0f * u - 1.0f) * bound;
+			}
+	}
+	NB_CK(c, cudaMemcpyAsync(c->mlp_wf.p, w.data(), w.size() * 4,
+	  cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->mlp_m.p, 0, kMlpParams * 4, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->mlp_v.p, 0, kMlpParams * 4, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->mlp_wbt.p, 0, kMlpParamsT * 2, c->stream));
+	k_mlp_adam<<<grid_for(c, kMlpParams, 256), 256, 0, c->stream>>>(
+	  c->mlp_wf.as<float>(), c->mlp_m.as<float>(), c->mlp_v.as<float>(),
+	  nullptr, 0, nullptr, 0, 0.0f, kAdamBeta1, kAdamBeta2, kAdamEps, 1.0f,
+	  1.0f, c->mlp_wbf.as<__nv_bfloat16>(), c->mlp_wbt.as<__nv_bfloat16>());
+	NB_CK(c, cudaGetLastError());
+	c->mlp_step = 0;
+	c->mlp_ready = true;
+	return 0;
+}
+
+int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out)
+{
+	if (n == 0)
+		return 0;
+	int per_sm = 0;
+	size_t smem = kMlpParams * sizeof(__nv_bfloat16);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_fwd, 128,
+	  smem);
+	uint32_t tiles = (n + 15u) / 16u;
+	uint32_t grid = std::min<uint32_t>((tiles + 3u) / 4u,
+	  (uint32_t)std::max(per_sm, 1) * (uint32_t)c->nsm);
+	k_mlp_fwd<<<grid, 128, smem, c->stream>>>(c->mlp_wbf.as<__nv_bfloat16>(),
+	  static_cast<const __nv_bfloat16 *>(feats), n, out);
+	NB_CK(c, cudaGetLastError());
+	return 0;
+}
+
+// Gradient of a batch (and optionally one Adam step).  g_out (device,
+// kMlpParams floats) receives the summed gradient when not null; *loss the
+// batch loss when not null (synchronises).
+int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
+              int update, float *g_out, float *loss)
+{
+	if (n == 0)
+		return 0;
+	static bool attr = false;
+	size_t smem = sizeof(MlpTrainSmem);
+	if (!attr) {
+		NB_CK(c, cudaFuncSetAttribute(k_mlp_grad,
+		  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		attr = true;
+	}
+	uint32_t tiles = (n + 15u) / 16u;
+	uint32_t grid = std::min<uint32_t>((tiles + 15u) / 16u,
+	  (uint32_t)c->nsm);
+	grid = std::max(grid, 1u);
+	NB_CK(c, c->mlp_part.ensure((size_t)grid * kMlpParams * sizeof(float)));
+	k_mlp_grad<<<grid, 128, smem, c->stream>>>(c->mlp_wbf.as<__nv_bfloat16>(),
+	  c->mlp_wbt.as<__nv_bfloat16>(), static_cast<const __nv_bfloat16 *>(feats),
+	  targets, n, c->mlp_part.as<float>(), c->mlp_loss.as<float>());
+	NB_CK(c, cudaGetLastError());
+	if (update)
+		c->mlp_step++;
+	float bc1 = 1.0f - std::pow(kAdamBeta1, (float)std::max(c->mlp_step, 1u));
+	float bc2 = 1.0f - std::pow(kAdamBeta2, (float)std::max(c->mlp_step, 1u));
+	k_mlp_adam<<<grid_for(c, kMlpParams, 256), 256, 0, c->stream>>>(
+	  c->mlp_wf.as<float>(), c->mlp_m.as<float>(), c->mlp_v.as<float>(),
+	  c->mlp_part.as<float>(), (int)grid, g_out, update, nrc_lr(c),
+	  kAdamBeta1, kAdamBeta2, kAdamEps, bc1, bc2,
+	  c->mlp_wbf.as<__nv_bfloat16>(), c->mlp_wbt.as<__nv_bfloat16>());
+	NB_CK(c, cudaGetLastError());
+	if (loss) {
+		std::vector<float> l(grid);
+		NB_CK(c, cudaMemcpyAsync(l.data(), c->mlp_loss.p, grid * 4,
+		  cudaMemcpyDeviceToHost, c->stream));
+		NB_CK(c, cudaStreamSynchronize(c->stream));
+		double sum = 0.0;
+		for (float x : l)
+			sum += x;
+		*loss = (float)(sum / (3.0 * n));
+	}
+	return 0;
 }
 
 // ------------------------------------------------ allocation-free tracing --
@@ -692,6 +824,23 @@ int rendgpu_upload_dynamic(struct rdata *rdp)
 		gi[i].pad = 0;
 	}
 	c->light_area = build_lights(rd, c->host_lights);
+	{
+		float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+		float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+		for (uint32_t i = 0; i < rd->instcnt; i++) {
+			const nb_aabb &b = rd->aabbs[i];
+			float bl[3] = {b.min.x, b.min.y, b.min.z};
+			float bh[3] = {b.max.x, b.max.y, b.max.z};
+			for (int a = 0; a < 3; a++) {
+				lo[a] = std::min(lo[a], bl[a]);
+				hi[a] = std::max(hi[a], bh[a]);
+			}
+		}
+		for (int a = 0; a < 3; a++) {
+			c->box.lo[a] = lo[a];
+			c->box.inv[a] = hi[a] > lo[a] ? 1.0f / (hi[a] - lo[a]) : 1.0f;
+		}
+	}
 	NB_CK(c, c->tlas.ensure(nodes.size() * sizeof(nb_qnode)));
 	NB_CK(c, c->irefs.ensure(irefs.size() * sizeof(uint32_t)));
 	NB_CK(c, c->insts.ensure(gi.size() * sizeof(nb_ginst)));
@@ -950,6 +1099,83 @@ int rendgpu_occluded(struct rdata *rdp, const struct rendgpu_ray *rays,
 	NB_CK(c, cudaMemcpyAsync(occl, c->bhits.p, (size_t)n,
 	  cudaMemcpyDeviceToHost, c->stream));
 	return batch_errors(c);
+}
+
+int rendgpu_nrc_reset(struct rdata *rdp, uint64_t seed)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	return nrc_reset(c, seed);
+}
+
+int rendgpu_nrc_weights(struct rdata *rdp, float *host, int write)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c || !host)
+		return RENDGPU_EINVAL;
+	if (!c->mlp_ready)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_nrc_reset must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	if (write) {
+		NB_CK(c, cudaMemcpyAsync(c->mlp_wf.p, host, kMlpParams * 4,
+		  cudaMemcpyHostToDevice, c->stream));
+		k_mlp_adam<<<grid_for(c, kMlpParams, 256), 256, 0, c->stream>>>(
+		  c->mlp_wf.as<float>(), c->mlp_m.as<float>(), c->mlp_v.as<float>(),
+		  nullptr, 0, nullptr, 0, 0.0f, kAdamBeta1, kAdamBeta2, kAdamEps,
+		  1.0f, 1.0f, c->mlp_wbf.as<__nv_bfloat16>(),
+		  c->mlp_wbt.as<__nv_bfloat16>());
+		NB_CK(c, cudaGetLastError());
+	} else {
+		NB_CK(c, cudaMemcpyAsync(host, c->mlp_wf.p, kMlpParams * 4,
+		  cudaMemcpyDeviceToHost, c->stream));
+	}
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	return 0;
+}
+
+int rendgpu_nrc_encode_device(struct rdata *rdp, const float *raw, uint32_t n,
+                              void *feats)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->have_dynamic)
+		return fail(c, RENDGPU_ESTATE, "upload_dynamic must come first");
+	if (n == 0)
+		return 0;
+	NB_CK(c, cudaSetDevice(c->device));
+	k_nrc_encode<<<grid_for(c, n, 128), 128, 0, c->stream>>>(raw, n, c->box,
+	  static_cast<__nv_bfloat16 *>(feats));
+	NB_CK(c, cudaGetLastError());
+	return 0;
+}
+
+int rendgpu_nrc_infer_device(struct rdata *rdp, const void *feats, uint32_t n,
+                             float *out)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->mlp_ready)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_nrc_reset must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	return nrc_infer(c, feats, n, reinterpret_cast<float4 *>(out));
+}
+
+int rendgpu_nrc_train_device(struct rdata *rdp, const void *feats,
+                             const float *targets, uint32_t n, int update,
+                             float *grad, float *loss)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->mlp_ready)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_nrc_reset must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	return nrc_train(c, feats, reinterpret_cast<const float4 *>(targets), n,
+	  update, grad, loss);
 }
 
 int rendgpu_sync(struct rdata *rdp)

@@ -1,0 +1,176 @@
+"""Neural radiance cache kernels on the GPU (rendgpu_nrc_*) against the FP64
+oracle (oracle/nrc_oracle.py): encoding, forward pass, gradients, Adam."""
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from nodebleed_b200 import api
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(
+    os.path.abspath(__file__))), "oracle"))
+import nrc_oracle as no  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(seed=7):
+    scene = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd).upload()
+    gr.nrc_reset(seed)
+    return rd, gr
+
+
+def _box(rd):
+    r = rd.rd
+    a = np.ctypeslib.as_array((C.c_float * (8 * r.instcnt)).from_address(
+        r.aabbs)).reshape(-1, 8)
+    return a[:, 0:3].min(0).astype(np.float64), \
+        a[:, 4:7].max(0).astype(np.float64)
+
+
+def _dev(x, dtype=None):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(x))
+    return t.cuda() if dtype is None else t.to(dtype).cuda()
+
+
+def _feats_dev(f64):
+    """BF16 features on the device (torch bfloat16), and their exact
+    values as float64."""
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(f64, np.float32)).to(
+        torch.bfloat16).cuda()
+    return t, t.float().cpu().numpy().astype(np.float64)
+
+
+def _random_raw(rd, n, seed=0):
+    rng = np.random.default_rng(seed)
+    lo, hi = _box(rd)
+    raw = np.zeros((n, 12), np.float32)
+    raw[:, 0:3] = rng.uniform(lo, hi, (n, 3))
+    for s in (3, 6):
+        d = rng.normal(size=(n, 3))
+        raw[:, s:s + 3] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    raw[:, 9:12] = rng.uniform(0, 1, (n, 3))
+    return raw
+
+
+def test_encode_matches_oracle(gpu):
+    import torch
+    rd, gr = _setup()
+    raw = _random_raw(rd, 4099)
+    out = torch.zeros((len(raw), 64), dtype=torch.bfloat16, device="cuda")
+    d_raw = _dev(raw)
+    torch.cuda.synchronize()
+    gr._ck(gr.g.rendgpu_nrc_encode_device(gr.ptr, d_raw.data_ptr(), len(raw),
+                                          out.data_ptr()), "encode")
+    gr.g.rendgpu_sync(gr.ptr)
+    got = out.float().cpu().numpy()
+    lo, hi = _box(rd)
+    ref = no.encode(raw, lo.astype(np.float32), hi.astype(np.float32))
+    assert np.abs(got - ref).max() < 8e-3
+    assert (got[:, 50:] == 0).all()
+    gr.close()
+
+
+def test_forward_matches_oracle(gpu):
+    import torch
+    rd, gr = _setup()
+    rng = np.random.default_rng(1)
+    n = 3001  # not a multiple of the 16-row tiles
+    f, f64 = _feats_dev(rng.uniform(0, 1, (n, 64)))
+    out = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    gr._ck(gr.g.rendgpu_nrc_infer_device(gr.ptr, f.data_ptr(), n,
+                                         out.data_ptr()), "infer")
+    gr.g.rendgpu_sync(gr.ptr)
+    got = out.cpu().numpy()[:, :3]
+    w = gr.nrc_weights()
+    _, ref = no.forward(w, f64, bf=True)
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() < 1e-2 * scale
+    assert np.mean(np.abs(got - ref)) < 1e-3 * scale
+    gr.close()
+
+
+def test_gradients_match_oracle(gpu):
+    import torch
+    rd, gr = _setup(11)
+    rng = np.random.default_rng(2)
+    n = 2048
+    f, f64 = _feats_dev(rng.uniform(0, 1, (n, 64)))
+    t = rng.uniform(0, 2, (n, 4)).astype(np.float32)
+    d_t = _dev(t)
+    g = torch.zeros(no.NPARAMS, dtype=torch.float32, device="cuda")
+    loss = C.c_float()
+    torch.cuda.synchronize()
+    gr._ck(gr.g.rendgpu_nrc_train_device(gr.ptr, f.data_ptr(), d_t.data_ptr(),
+                                         n, 0, g.data_ptr(), C.byref(loss)),
+           "train")
+    gr.g.rendgpu_sync(gr.ptr)
+    got = g.cpu().numpy().astype(np.float64)
+    w = gr.nrc_weights()
+    ref_loss, ref = no.loss_grad(w, f64, t, bf=True)
+    assert abs(loss.value - ref_loss) < 1e-3 * ref_loss
+    for l in range(6):
+        sl = slice(l * no.SQ, (l + 1) * no.SQ) if l < 5 else \
+            slice(5 * no.SQ, 5 * no.SQ + 3 * 64)
+        err = np.linalg.norm(got[sl] - ref[sl]) / np.linalg.norm(ref[sl])
+        assert err < 3e-2, (l, err)
+    assert (got[5 * no.SQ + 3 * 64:] == 0).all()
+    # the weights did not move (update = 0)
+    assert np.array_equal(gr.nrc_weights(), w)
+    gr.close()
+
+
+def test_adam_step_matches_oracle(gpu):
+    import torch
+    rd, gr = _setup(3)
+    w0 = no.xavier(5).astype(np.float32)
+    gr.nrc_weights(w0)
+    rng = np.random.default_rng(3)
+    n = 1024
+    f, f64 = _feats_dev(rng.uniform(0, 1, (n, 64)))
+    d_t = _dev(rng.uniform(0, 2, (n, 4)).astype(np.float32))
+    g = torch.zeros(no.NPARAMS, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    gr._ck(gr.g.rendgpu_nrc_train_device(gr.ptr, f.data_ptr(), d_t.data_ptr(),
+                                         n, 1, g.data_ptr(), None), "train")
+    gr.g.rendgpu_sync(gr.ptr)
+    w1 = gr.nrc_weights().astype(np.float64)
+    gg = g.cpu().numpy().astype(np.float64)
+    ref, _, _ = no.adam(w0.astype(np.float64), np.zeros(no.NPARAMS),
+                        np.zeros(no.NPARAMS), gg, 1)
+    assert np.abs(w1 - ref).max() < 1e-6
+    gr.close()
+
+
+def test_training_fits_a_smooth_target(gpu):
+    import torch
+    rd, gr = _setup(21)
+    rng = np.random.default_rng(4)
+    n = 8192
+    x = rng.uniform(0, 1, (n, 64))
+    x[:, 50:] = 0
+    f, f64 = _feats_dev(x)
+    tgt = np.stack([0.5 + 0.4 * np.sin(3 * f64[:, 0] + f64[:, 1]),
+                    0.5 + 0.4 * np.cos(2 * f64[:, 2] - f64[:, 3]),
+                    0.3 + 0.2 * f64[:, 4] * f64[:, 5],
+                    np.zeros(n)], 1).astype(np.float32)
+    d_t = _dev(tgt)
+    losses = []
+    torch.cuda.synchronize()
+    for step in range(300):
+        lv = C.c_float()
+        gr._ck(gr.g.rendgpu_nrc_train_device(
+            gr.ptr, f.data_ptr(), d_t.data_ptr(), n, 1, None,
+            C.byref(lv) if step % 50 == 0 or step == 299 else None), "train")
+        if step % 50 == 0 or step == 299:
+            losses.append(lv.value)
+    assert losses[-1] < 0.1 * losses[0], losses
+    gr.close()
