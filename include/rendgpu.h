@@ -42,7 +42,10 @@ enum rendgpu_status {
 
 enum rendgpu_mode {
 	RENDGPU_MODE_PATH = 0,    /* path tracing: NEE + cosine/mirror bounces */
-	RENDGPU_MODE_PRIMARY = 1  /* reference live shading: (n+1)/2 * albedo */
+	RENDGPU_MODE_PRIMARY = 1, /* reference live shading: (n+1)/2 * albedo */
+	RENDGPU_MODE_NRC = 2      /* path tracing ended by the radiance cache at
+	                             the first diffuse vertex after the primary
+	                             hit; 2^16 unbiased paths per frame train it */
 };
 
 enum rendgpu_flags {
@@ -62,7 +65,8 @@ struct rendgpu_cfg {
 	uint32_t sched;      /* traversal schedule: 0 = default, 1 = step,
 	                        2 = phase, 3 = ylitie (see trace.cuh) */
 	uint32_t reserved[7]; /* [0]: float bits of the cache's Adam learning
-	                         rate (0 = 1e-2) */
+	                         rate (0 = 1e-2); [1]: radiance-cache warm-up
+	                         frames of unbiased tracing (0 = 8) */
 };
 
 /* A ray for the batch calls: origin, tmax, direction (32 bytes). */
@@ -97,6 +101,10 @@ struct rendgpu_stats {
 	uint64_t tri_tests;      /* closest-hit triangle tests (COUNT flag) */
 	uint32_t bounce_closest[16]; /* closest-hit rays per bounce */
 	uint32_t bounce_shadow[16];  /* shadow rays per bounce */
+	uint32_t nrc_queries;    /* radiance-cache queries of the frame */
+	uint32_t nrc_records;    /* training vertices recorded in the frame */
+	float    ms_nrc;         /* cache inference + training (TIMING flag) */
+	float    nrc_loss;       /* loss of the frame's last training step */
 };
 
 /* Create the GPU context of `rd` (one per rdata).  Replaces nothing in the
@@ -198,6 +206,12 @@ int rendgpu_nrc_infer_device(struct rdata *rd, const void *feats_device,
 int rendgpu_nrc_train_device(struct rdata *rd, const void *feats_device,
                              const float *targets_device, uint32_t n,
                              int update, float *grad_device, float *loss_host);
+
+/* relMSE of this context's accumulated image (acc / rd->samples) against a
+ * reference image (W*H*3 floats, device memory): mean over pixels and
+ * channels of (x - r)^2 / (r^2 + 0.01), reduced in FP64 on the device. */
+int rendgpu_relmse_device(struct rdata *rd, const float *ref_device,
+                          double *out);
 
 /* Wait for all work of the context. */
 int rendgpu_sync(struct rdata *rd);

@@ -8,7 +8,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 SCENE_SMALL, SCENE_SCALE, SCENE_BATCH, SCENE_STRESS, SCENE_TINY = 1, 2, 3, 5, 9
-MODE_PATH, MODE_PRIMARY = 0, 1
+MODE_PATH, MODE_PRIMARY, MODE_NRC = 0, 1, 2
 FLAG_TIMING, FLAG_COUNT = 1, 2
 
 # struct rendgpu_ray / rendgpu_hit (32 / 16 bytes)
@@ -77,7 +77,9 @@ class RendgpuStats(C.Structure):
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
                 ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
                 ("bounce_closest", C.c_uint32 * 16),
-                ("bounce_shadow", C.c_uint32 * 16)]
+                ("bounce_shadow", C.c_uint32 * 16),
+                ("nrc_queries", C.c_uint32), ("nrc_records", C.c_uint32),
+                ("ms_nrc", C.c_float), ("nrc_loss", C.c_float)]
 
     def as_dict(self):
         d = {}
@@ -130,6 +132,7 @@ class GpuLib:
                 ("rendgpu_occluded_device", [vp, vp, u32, vp]),
                 ("rendgpu_trace_rays_device_noalloc", [vp, vp, u32, vp]),
                 ("rendgpu_nrc_reset", [vp, C.c_uint64]),
+                ("rendgpu_relmse_device", [vp, vp, vp]),
                 ("rendgpu_nrc_weights", [vp, vp, C.c_int]),
                 ("rendgpu_nrc_encode_device", [vp, vp, u32, vp]),
                 ("rendgpu_nrc_infer_device", [vp, vp, u32, vp]),
@@ -270,7 +273,8 @@ class GpuRenderer:
     """The rendgpu C ABI on one RenderData."""
 
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
-                 timing=False, device=0, count=False, sched=0):
+                 timing=False, device=0, count=False, sched=0,
+                 nrc_warmup=0, nrc_lr=0.0):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -283,6 +287,9 @@ class GpuRenderer:
         cfg.seed = seed
         cfg.device = device
         cfg.sched = sched
+        cfg.reserved[0] = C.c_uint32.from_buffer_copy(
+            C.c_float(nrc_lr)).value
+        cfg.reserved[1] = nrc_warmup
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
         if rc != 0:
             raise RendgpuError(rc, "rendgpu_init")
@@ -357,6 +364,14 @@ class GpuRenderer:
         w = np.ascontiguousarray(w, np.float32)
         self._ck(self.g.rendgpu_nrc_weights(self.ptr, w.ctypes.data, 1),
                  "nrc_weights")
+
+    def relmse(self, ref_device_ptr):
+        """relMSE of the accumulated image against a device reference
+        image (W*H*3 floats), reduced in FP64 on the device."""
+        out = C.c_double()
+        self._ck(self.g.rendgpu_relmse_device(self.ptr, ref_device_ptr,
+                                              C.byref(out)), "relmse")
+        return out.value
 
     def stream(self):
         """cudaStream_t of this context, as an integer handle."""

@@ -14,6 +14,7 @@
 #ifndef NB_KERNELS_CUH
 #define NB_KERNELS_CUH
 
+#include "nrc.cuh"
 #include "trace.cuh"
 
 namespace nb {
@@ -38,13 +39,24 @@ struct FrameDev {
 	                   // shadow rays of bounce k
 	unsigned long long *rays; // [0] closest, [1] shadow
 	uint32_t  W, H, spp, npaths;
+	// neural radiance cache (mode 2): queries (4 float4: (pos, path),
+	// (wo, T.x), (n, T.y), (albedo, T.z)) counted in cnt[40], training
+	// records (6 float4: (pos, path), wo, n, albedo, L before, T) in cnt[41]
+	float4   *nq;
+	float4   *nrec;
+	uint32_t  nq_cap, nrec_cap;
 };
+
+// Path flags kept in the bits of pT.w.
+constexpr uint32_t kPathSpec = 1u;   // arrived by a mirror bounce
+constexpr uint32_t kPathTrain = 2u;  // unbiased cache-training path
 
 struct FrameArgs {
 	uint64_t seed;
 	uint32_t frame;   // rd->samples
 	uint32_t depth;
-	uint32_t mode;
+	uint32_t mode;      // 0 path, 1 primary, 2 path with radiance cache
+	uint32_t nrc_stride, nrc_offset; // training paths: (path + offset) % stride == 0
 	// camera (rcam fields)
 	float eye[3], ri[3], up[3], fwd[3];
 	float rw, rh, fovfdist, aspect, fdist, focrad, tanfangle;
@@ -190,7 +202,10 @@ __global__ void __launch_bounds__(256) k_gen(FrameDev F, FrameArgs A)
 			float il = __fdiv_rn(1.0f, __fsqrt_rn(l2));
 			for (int a = 0; a < 3; a++)
 				d[a] = __fmul_rn(td[a], il);
-			F.pT[path] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+			uint32_t flags = (A.mode == 2u && (path + A.nrc_offset) %
+			  A.nrc_stride == 0u) ? kPathTrain : 0u;
+			F.pT[path] = make_float4(1.0f, 1.0f, 1.0f,
+			  __uint_as_float(flags));
 			F.pL[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 			F.rng[path] = make_uint2((uint32_t)st, (uint32_t)(st >> 32));
 		}
@@ -403,15 +418,52 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 					float r1 = rnd01(st, inc);
 					F.rng[path] = make_uint2((uint32_t)st,
 					  (uint32_t)(st >> 32));
-					bool spec = T.w != 0.0f;
-					if (mflags & NB_FLAG_EMISSIVE) {
+					uint32_t pflags = __float_as_uint(T.w);
+					bool spec = (pflags & kPathSpec) != 0u;
+					bool train = (pflags & kPathTrain) != 0u;
+					bool emissive = (mflags & NB_FLAG_EMISSIVE) != 0u;
+					bool mirror = mc.w >= 0.5f;
+					bool queried = false;
+					if (A.mode == 2u && k >= 1u && !emissive) {
+						if (!train && !mirror) {
+							// radiance cache query: the path ends here
+							uint32_t qi = atomicAdd(&F.cnt[40], 1u);
+							if (qi < F.nq_cap) {
+								float4 *q = F.nq + 4u * qi;
+								q[0] = make_float4(pos[0], pos[1], pos[2],
+								  __uint_as_float(path));
+								q[1] = make_float4(-d[0], -d[1], -d[2], T.x);
+								q[2] = make_float4(n[0], n[1], n[2], T.y);
+								q[3] = make_float4(col[0], col[1], col[2],
+								  T.z);
+							}
+							queried = true;
+						}
+						if (train) {
+							uint32_t ri = atomicAdd(&F.cnt[41], 1u);
+							if (ri < F.nrec_cap) {
+								float4 *q = F.nrec + 6u * ri;
+								q[0] = make_float4(pos[0], pos[1], pos[2],
+								  __uint_as_float(path));
+								q[1] = make_float4(-d[0], -d[1], -d[2], 0.0f);
+								q[2] = make_float4(n[0], n[1], n[2], 0.0f);
+								q[3] = make_float4(col[0], col[1], col[2],
+								  0.0f);
+								q[4] = make_float4(L.x, L.y, L.z, 0.0f);
+								q[5] = make_float4(T.x, T.y, T.z, 0.0f);
+							}
+						}
+					}
+					if (queried) {
+						// the cache supplies the rest of the path
+					} else if (emissive) {
 						if ((k == 0u || spec) && front) {
 							L.x = __fadd_rn(L.x, __fmul_rn(T.x, col[0]));
 							L.y = __fadd_rn(L.y, __fmul_rn(T.y, col[1]));
 							L.z = __fadd_rn(L.z, __fmul_rn(T.z, col[2]));
 							F.pL[path] = L;
 						}
-					} else if (mc.w >= 0.5f) {
+					} else if (mirror) {
 						// perfect mirror
 						float dd = __fadd_rn(__fadd_rn(__fmul_rn(d[0],
 						  n[0]), __fmul_rn(d[1], n[1])),
@@ -424,11 +476,11 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 						T.x = __fmul_rn(T.x, col[0]);
 						T.y = __fmul_rn(T.y, col[1]);
 						T.z = __fmul_rn(T.z, col[2]);
-						T.w = 1.0f;
+						T.w = __uint_as_float(pflags | kPathSpec);
 						F.pT[path] = T;
 						want_ray = k + 1u < A.depth;
 					} else {
-						T.w = 0.0f;
+						T.w = __uint_as_float(pflags & ~kPathSpec);
 						if (S.nlights) {
 							// pick an emitting triangle by area
 							uint32_t lo = 0, hi = S.nlights - 1u;
@@ -542,6 +594,34 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 			  __uint_as_float(path));
 			F.scol[ss] = make_float4(sc[0], sc[1], sc[2], 0.0f);
 		}
+	}
+}
+
+// relMSE of the accumulated image (acc / samples) against a reference
+// image: mean over pixels and channels of (x - r)^2 / (r^2 + 0.01),
+// accumulated in FP64 (the only double-precision arithmetic on the device).
+__global__ void __launch_bounds__(256) k_relmse(const float *acc, float inv,
+                                                const float *ref,
+                                                uint32_t n, double *out)
+{
+	double s = 0.0;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+	     i += gridDim.x * blockDim.x) {
+		double x = (double)acc[i] * (double)inv, r = ref[i];
+		double d = x - r;
+		s += d * d / (r * r + 0.01);
+	}
+	for (int o = 16; o > 0; o >>= 1)
+		s += __shfl_down_sync(0xffffffffu, s, o);
+	__shared__ double part[8];
+	if ((threadIdx.x & 31) == 0)
+		part[threadIdx.x >> 5] = s;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+			t += part[w];
+		atomicAdd(out, t);
 	}
 }
 

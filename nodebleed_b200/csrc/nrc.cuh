@@ -185,8 +185,11 @@ __device__ __forceinline__ void layer_out(float c[4], const uint32_t a[4][4],
 // warps; the forward BF16 weights (41 KB) are staged in shared memory once.
 __global__ void __launch_bounds__(128) k_mlp_fwd(const __nv_bfloat16 *wbf,
                                                  const __nv_bfloat16 *feats,
-                                                 uint32_t n, float4 *out)
+                                                 uint32_t n, float4 *out,
+                                                 const uint32_t *ncount)
 {
+	if (ncount)
+		n = min(*ncount, n); // count produced on the device
 	extern __shared__ __align__(16) unsigned char mlp_smem[];
 	__nv_bfloat16 *w = reinterpret_cast<__nv_bfloat16 *>(mlp_smem);
 	for (int i = threadIdx.x; i < kMlpParams / 8; i += blockDim.x)
@@ -237,13 +240,26 @@ struct MlpTrainSmem {
 // Relative L2 loss mean((y - t)^2 / (y^2 + 0.01)) over the batch and three
 // channels (y detached in the denominator); gradients of a batch of n
 // samples into this CTA's partial gradient slice grad[blockIdx.x].
+// With ncount set, the batch is samples [off, off + n) of the
+// min(*ncount, cap) produced on the device, off = offset mod that count.
 __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16 *wbf,
                                                   const __nv_bfloat16 *wbt,
                                                   const __nv_bfloat16 *feats,
                                                   const float4 *targets,
                                                   uint32_t n, float *grad,
-                                                  float *loss)
+                                                  float *loss,
+                                                  const uint32_t *ncount,
+                                                  uint32_t offset,
+                                                  uint32_t cap)
 {
+	if (ncount) {
+		uint32_t total = min(*ncount, cap);
+		uint32_t off = total ? offset % total : 0u;
+		uint32_t avail = total - off;
+		feats += (size_t)off * kMlpIn;
+		targets += off;
+		n = min(n, avail);
+	}
 	extern __shared__ __align__(16) unsigned char mlp_smem[];
 	MlpTrainSmem &S = *reinterpret_cast<MlpTrainSmem *>(mlp_smem);
 	for (int i = threadIdx.x; i < kMlpParams / 8; i += blockDim.x)
@@ -255,7 +271,7 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16 *wbf,
 		S.loss = 0.0f;
 	__syncthreads();
 	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const float inv = 1.0f / (3.0f * (float)n);
+	const float inv = n ? 1.0f / (3.0f * (float)n) : 0.0f;
 	uint32_t tiles = (n + 15u) / 16u;
 	float lsum = 0.0f;
 	for (uint32_t t = blockIdx.x * 4u + warp; t < tiles;
@@ -491,6 +507,62 @@ __global__ void k_nrc_encode(const float *raw, uint32_t n, NrcBox B,
 	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
 	     i += gridDim.x * blockDim.x)
 		nrc_encode(raw + 12ull * i, B, feats + 64ull * i);
+}
+
+// Features of cache queries / training records produced by k_shade: the
+// first four float4 of each entry (stride float4s) hold position, outgoing
+// direction, normal and albedo in .xyz.
+__global__ void k_nrc_encode_entries(const float4 *e, uint32_t stride,
+                                     const uint32_t *count, uint32_t cap,
+                                     NrcBox B, __nv_bfloat16 *feats)
+{
+	uint32_t n = min(*count, cap);
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+	     i += gridDim.x * blockDim.x) {
+		const float4 *q = e + (size_t)stride * i;
+		float4 a = q[0], b = q[1], c = q[2], d = q[3];
+		float raw[12] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z,
+		  d.x, d.y, d.z};
+		nrc_encode(raw, B, feats + 64ull * i);
+	}
+}
+
+// L[path] += T * max(cache(x), 0) for every query.
+__global__ void k_nrc_apply(const float4 *q, const uint32_t *count,
+                            uint32_t cap, const float4 *pred, float4 *pL)
+{
+	uint32_t n = min(*count, cap);
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+	     i += gridDim.x * blockDim.x) {
+		const float4 *e = q + 4u * i;
+		uint32_t path = __float_as_uint(e[0].w);
+		float4 y = pred[i];
+		float4 L = pL[path];
+		L.x += e[1].w * fmaxf(y.x, 0.0f);
+		L.y += e[2].w * fmaxf(y.y, 0.0f);
+		L.z += e[3].w * fmaxf(y.z, 0.0f);
+		pL[path] = L;
+	}
+}
+
+// Training target of a record: the radiance its path gathered from this
+// vertex on, divided by the throughput on arrival.
+__global__ void k_nrc_targets(const float4 *rec, const uint32_t *count,
+                              uint32_t cap, const float4 *pL, float4 *tgt)
+{
+	uint32_t n = min(*count, cap);
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+	     i += gridDim.x * blockDim.x) {
+		const float4 *e = rec + 6u * i;
+		uint32_t path = __float_as_uint(e[0].w);
+		float4 L = pL[path], Lb = e[4], T = e[5];
+		float4 t;
+		t.x = T.x > 0.0f ? (L.x - Lb.x) / T.x : 0.0f;
+		t.y = T.y > 0.0f ? (L.y - Lb.y) / T.y : 0.0f;
+		t.z = T.z > 0.0f ? (L.z - Lb.z) / T.z : 0.0f;
+		t.w = 0.0f;
+		tgt[i] = t;
+	}
 }
 
 } // namespace nb

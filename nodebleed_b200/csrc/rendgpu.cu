@@ -82,6 +82,10 @@ struct Ctx {
 	uint32_t mlp_step = 0;
 	bool     mlp_ready = false;
 	NrcBox   box{};
+	DevBuf   nq, nfeat, npred, nrec, rfeat, rtgt; // radiance-cache frame data
+	uint32_t nq_cap = 0, nrec_cap = 0, nrc_stride = 1;
+	uint32_t nrc_frames = 0; // radiance-cache frames rendered so far
+	uint32_t train_grid = 0; // CTAs of the last training step
 	// stats / errors
 	rendgpu_stats st{};
 	int          last = 0;
@@ -360,151 +364,6 @@ float ev_ms(Ctx *c, int a, int b)
 	return ms;
 }
 
-int render_frame(Ctx *c)
-{
-	int rc = ready(c, true);
-	if (rc)
-		return rc;
-	nb_rdata *rd = c->rd;
-	if (rd->width != c->W || rd->height != c->H || rd->spp != c->spp)
-		return fail(c, RENDGPU_ESTATE, "rdata size changed since "
-		  "rendgpu_resaccum");
-	FrameDev F = frame_of(c);
-	FrameArgs A;
-	A.seed = c->cfg.seed;
-	A.frame = rd->samples;
-	A.depth = c->cfg.mode == RENDGPU_MODE_PRIMARY ? 1u : c->cfg.max_depth;
-	A.mode = c->cfg.mode;
-	const nb_rcam &cam = rd->cam;
-	A.eye[0] = cam.eye.x; A.eye[1] = cam.eye.y; A.eye[2] = cam.eye.z;
-	A.ri[0] = cam.ri.x; A.ri[1] = cam.ri.y; A.ri[2] = cam.ri.z;
-	A.up[0] = cam.up.x; A.up[1] = cam.up.y; A.up[2] = cam.up.z;
-	A.fwd[0] = cam.fwd.x; A.fwd[1] = cam.fwd.y; A.fwd[2] = cam.fwd.z;
-	A.rw = cam.rw8[0];
-	A.rh = cam.rh8[0];
-	A.fovfdist = cam.fovfdist8[0];
-	A.aspect = cam.aspect8[0];
-	A.fdist = cam.fdist8[0];
-	A.focrad = cam.focrad8[0];
-	A.tanfangle = cam.tanfangle;
-	DScene S = scene_of(c);
-	c->nev = 0;
-	c->st.launches = 0;
-	c->st.trace_launches = 0;
-	NB_CK(c, cudaMemsetAsync(c->cnt.p, 0, 64 * sizeof(uint32_t), c->stream));
-	NB_CK(c, cudaMemsetAsync(c->rays.p, 0, 4 * sizeof(unsigned long long),
-	  c->stream));
-	ev_record(c); // 0
-	uint32_t tiles = ((c->W + 7u) >> 3) * ((c->H + 3u) >> 2) * 32u * c->spp;
-	k_gen<<<grid_for(c, tiles, 256), 256, 0, c->stream>>>(F, A);
-	NB_CK(c, cudaGetLastError());
-	c->st.launches++;
-	ev_record(c); // 1
-	std::vector<int> trace_ev, shadow_ev;
-	for (uint32_t k = 0; k < A.depth; k++) {
-		uint32_t cur = k & 1u;
-		trace_ev.push_back(c->nev);
-		ev_record(c);
-		rc = launch_trace(c, F.q[cur], F.cnt + cur, F.cnt + 4, F.hits,
-		  F.cnt + 3, F.rays);
-		if (rc)
-			return rc;
-		ev_record(c);
-		c->st.launches++;
-		c->st.trace_launches++;
-		NB_CK(c, cudaMemsetAsync(F.cnt + (cur ^ 1u), 0, sizeof(uint32_t),
-		  c->stream));
-		NB_CK(c, cudaMemsetAsync(F.cnt + 2, 0, sizeof(uint32_t),
-		  c->stream));
-		k_shade<<<grid_for(c, c->npaths, 256), 256, 0, c->stream>>>(S, F,
-		  A, cur, k);
-		NB_CK(c, cudaGetLastError());
-		c->st.launches++;
-		if (A.mode == RENDGPU_MODE_PATH) {
-			shadow_ev.push_back(c->nev);
-			ev_record(c);
-			rc = launch_shadow(c, F);
-			if (rc)
-				return rc;
-			ev_record(c);
-			c->st.launches++;
-		}
-	}
-	int acc_ev = c->nev;
-	ev_record(c);
-	float inv = 1.0f / (float)(rd->samples + rd->spp);
-	k_accum<<<grid_for(c, c->W * c->H, 256), 256, 0, c->stream>>>(F, inv);
-	NB_CK(c, cudaGetLastError());
-	c->st.launches++;
-	ev_record(c);
-	unsigned long long hr[4];
-	uint32_t hc[64];
-	NB_CK(c, cudaMemcpyAsync(hr, c->rays.p, sizeof(hr),
-	  cudaMemcpyDeviceToHost, c->stream));
-	NB_CK(c, cudaMemcpyAsync(hc, c->cnt.p, sizeof(hc),
-	  cudaMemcpyDeviceToHost, c->stream));
-	NB_CK(c, cudaStreamSynchronize(c->stream));
-	c->st.closest_rays = hr[0];
-	c->st.node_visits = hr[2];
-	c->st.tri_tests = hr[3];
-	c->st.shadow_rays = hr[1];
-	c->st.rays = hr[0] + hr[1];
-	c->st.device_errors = hc[3];
-	for (int k = 0; k < 16; k++) {
-		c->st.bounce_closest[k] = hc[8 + k];
-		c->st.bounce_shadow[k] = hc[24 + k];
-	}
-	c->st.max_stack = need_stack(c);
-	if (c->cfg.flags & RENDGPU_FLAG_TIMING) {
-		c->st.ms_frame = ev_ms(c, 0, c->nev - 1);
-		float tr = 0.0f, sh = 0.0f;
-		for (int e : trace_ev)
-			tr += ev_ms(c, e, e + 1);
-		for (int e : shadow_ev)
-			sh += ev_ms(c, e, e + 1);
-		c->st.ms_trace = tr;
-		c->st.ms_shadow = sh;
-		c->st.ms_shade = c->st.ms_frame - tr - sh;
-		(void)acc_ev;
-	}
-	if (hc[3])
-		return fail(c, RENDGPU_EDEVICE, "rays abandoned on the device "
-		  "(traversal stack overflow)");
-	return 0;
-}
-
-void free_ctx(Ctx *c)
-{
-	DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs, &c->insts,
-	  &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits, &c->shadow,
-	  &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
-	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_wf,
-	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
-	  &c->mlp_loss};
-	for (DevBuf *b : bufs)
-		b->release();
-	for (int i = 0; i < 64; i++)
-		if (c->ev[i])
-			cudaEventDestroy(c->ev[i]);
-	if (c->stream)
-		cudaStreamDestroy(c->stream);
-	delete c;
-}
-
-uint64_t held_bytes(const Ctx *c)
-{
-	const DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs,
-	  &c->insts, &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits,
-	  &c->shadow, &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf,
-	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
-	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
-	  &c->mlp_part, &c->mlp_loss};
-	uint64_t s = 0;
-	for (const DevBuf *b : bufs)
-		s += b->cap;
-	return s;
-}
-
 // ------------------------------------------------ neural radiance cache --
 
 constexpr float kAdamBeta1 = 0.9f, kAdamBeta2 = 0.99f, kAdamEps = 1e-15f;
@@ -538,8 +397,10 @@ int nrc_reset(Ctx *c, uint64_t seed)
 	next();
 	st += 0x853c49e6748fea9bull;
 	next();
-	for (int l = 0; l <= kMlpSquare; l++) {
-		int nout = l == kMlpSquare ? 3 : 64;
+	// Xavier uniform for the hidden layers; the output layer starts at
+	// zero so an untrained cache adds no energy
+	for (int l = 0; l < kMlpSquare; l++) {
+		int nout = 64;
 		float bound = std::sqrt(6.0f / (64.0f + (float)nout));
 		for (int o = 0; o < nout; o++)
 			for (int i = 0; i < 64; i++) {
@@ -562,7 +423,48 @@ int nrc_reset(Ctx *c, uint64_t seed)
 	return 0;
 }
 
-int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out)
+// Frames of unbiased tracing that train the cache before it ends paths
+// (cfg.reserved[1]; 0 = 8).
+uint32_t nrc_warmup(const Ctx *c)
+{
+	return c->cfg.reserved[1] ? c->cfg.reserved[1] : 8u;
+}
+
+constexpr uint32_t kNrcBatch = 16384;    // training samples per Adam step
+constexpr uint32_t kNrcSteps = 4;        // Adam steps per frame
+constexpr uint32_t kNrcTrainPaths = 65536; // training paths per frame (2^16)
+
+// Radiance-cache buffers of a frame: queries and their features/outputs
+// for every path, records for the training paths' vertices.
+int nrc_frame_buffers(Ctx *c)
+{
+	if (!c->mlp_ready) {
+		int rc = nrc_reset(c, c->cfg.seed);
+		if (rc)
+			return rc;
+	}
+	uint32_t np = c->npaths;
+	// about 2^16 training paths, and never more than 1 path in 16
+	c->nrc_stride = std::max(16u, np / kNrcTrainPaths);
+	uint32_t verts = c->cfg.max_depth > 1 ? c->cfg.max_depth - 1 : 1;
+	// warm-up frames record from every path; later frames overwrite the
+	// capacity-limited prefix only, so cap at 4 batches per frame worth of
+	// vertices beyond the steady-state need
+	uint32_t ntrain = np / c->nrc_stride + 1;
+	c->nq_cap = np;
+	c->nrec_cap = std::max(ntrain * verts + 64, kNrcSteps * kNrcBatch);
+	NB_CK(c, c->nq.ensure((size_t)np * 64));
+	NB_CK(c, c->nfeat.ensure((size_t)np * 128));
+	NB_CK(c, c->npred.ensure((size_t)np * 16));
+	NB_CK(c, c->nrec.ensure((size_t)c->nrec_cap * 96));
+	NB_CK(c, c->rfeat.ensure((size_t)c->nrec_cap * 128));
+	NB_CK(c, c->rtgt.ensure((size_t)c->nrec_cap * 16));
+	return 0;
+}
+
+// Forward pass of n (or, with ncount, of min(*ncount, n)) queries.
+int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out,
+              const uint32_t *ncount = nullptr)
 {
 	if (n == 0)
 		return 0;
@@ -574,7 +476,7 @@ int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out)
 	uint32_t grid = std::min<uint32_t>((tiles + 3u) / 4u,
 	  (uint32_t)std::max(per_sm, 1) * (uint32_t)c->nsm);
 	k_mlp_fwd<<<grid, 128, smem, c->stream>>>(c->mlp_wbf.as<__nv_bfloat16>(),
-	  static_cast<const __nv_bfloat16 *>(feats), n, out);
+	  static_cast<const __nv_bfloat16 *>(feats), n, out, ncount);
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -583,7 +485,9 @@ int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out)
 // kMlpParams floats) receives the summed gradient when not null; *loss the
 // batch loss when not null (synchronises).
 int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
-              int update, float *g_out, float *loss)
+              int update, float *g_out, float *loss,
+              const uint32_t *ncount = nullptr, uint32_t offset = 0,
+              uint32_t cap = 0)
 {
 	if (n == 0)
 		return 0;
@@ -599,9 +503,11 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 	  (uint32_t)c->nsm);
 	grid = std::max(grid, 1u);
 	NB_CK(c, c->mlp_part.ensure((size_t)grid * kMlpParams * sizeof(float)));
+	c->train_grid = grid;
 	k_mlp_grad<<<grid, 128, smem, c->stream>>>(c->mlp_wbf.as<__nv_bfloat16>(),
 	  c->mlp_wbt.as<__nv_bfloat16>(), static_cast<const __nv_bfloat16 *>(feats),
-	  targets, n, c->mlp_part.as<float>(), c->mlp_loss.as<float>());
+	  targets, n, c->mlp_part.as<float>(), c->mlp_loss.as<float>(), ncount,
+	  offset, cap);
 	NB_CK(c, cudaGetLastError());
 	if (update)
 		c->mlp_step++;
@@ -624,6 +530,225 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 		*loss = (float)(sum / (3.0 * n));
 	}
 	return 0;
+}
+
+int render_frame(Ctx *c)
+{
+	int rc = ready(c, true);
+	if (rc)
+		return rc;
+	nb_rdata *rd = c->rd;
+	if (rd->width != c->W || rd->height != c->H || rd->spp != c->spp)
+		return fail(c, RENDGPU_ESTATE, "rdata size changed since "
+		  "rendgpu_resaccum");
+	FrameDev F = frame_of(c);
+	FrameArgs A;
+	A.seed = c->cfg.seed;
+	A.frame = rd->samples;
+	A.depth = c->cfg.mode == RENDGPU_MODE_PRIMARY ? 1u : c->cfg.max_depth;
+	A.mode = c->cfg.mode;
+	A.nrc_stride = 1;
+	A.nrc_offset = 0;
+	bool nrc = c->cfg.mode == RENDGPU_MODE_NRC;
+	if (nrc) {
+		int rc2 = nrc_frame_buffers(c);
+		if (rc2)
+			return rc2;
+		A.nrc_stride = c->nrc_stride;
+		A.nrc_offset = (rd->samples * 7919u) % c->nrc_stride;
+		// warm-up: the first frames trace every path unbiased (as
+		// training paths) while the cache trains
+		if (c->nrc_frames < nrc_warmup(c))
+			A.nrc_stride = 1;
+		c->nrc_frames++;
+	}
+	const nb_rcam &cam = rd->cam;
+	A.eye[0] = cam.eye.x; A.eye[1] = cam.eye.y; A.eye[2] = cam.eye.z;
+	A.ri[0] = cam.ri.x; A.ri[1] = cam.ri.y; A.ri[2] = cam.ri.z;
+	A.up[0] = cam.up.x; A.up[1] = cam.up.y; A.up[2] = cam.up.z;
+	A.fwd[0] = cam.fwd.x; A.fwd[1] = cam.fwd.y; A.fwd[2] = cam.fwd.z;
+	A.rw = cam.rw8[0];
+	A.rh = cam.rh8[0];
+	A.fovfdist = cam.fovfdist8[0];
+	A.aspect = cam.aspect8[0];
+	A.fdist = cam.fdist8[0];
+	A.focrad = cam.focrad8[0];
+	A.tanfangle = cam.tanfangle;
+	F.nq = c->nq.as<float4>();
+	F.nrec = c->nrec.as<float4>();
+	F.nq_cap = c->nq_cap;
+	F.nrec_cap = c->nrec_cap;
+	DScene S = scene_of(c);
+	c->nev = 0;
+	c->st.launches = 0;
+	c->st.trace_launches = 0;
+	NB_CK(c, cudaMemsetAsync(c->cnt.p, 0, 64 * sizeof(uint32_t), c->stream));
+	NB_CK(c, cudaMemsetAsync(c->rays.p, 0, 4 * sizeof(unsigned long long),
+	  c->stream));
+	ev_record(c); // 0
+	uint32_t tiles = ((c->W + 7u) >> 3) * ((c->H + 3u) >> 2) * 32u * c->spp;
+	k_gen<<<grid_for(c, tiles, 256), 256, 0, c->stream>>>(F, A);
+	NB_CK(c, cudaGetLastError());
+	c->st.launches++;
+	ev_record(c); // 1
+	std::vector<int> trace_ev, shadow_ev;
+	for (uint32_t k = 0; k < A.depth; k++) {
+		uint32_t cur = k & 1u;
+		trace_ev.push_back(c->nev);
+		ev_record(c);
+		rc = launch_trace(c, F.q[cur], F.cnt + cur, F.cnt + 4, F.hits,
+		  F.cnt + 3, F.rays);
+		if (rc)
+			return rc;
+		ev_record(c);
+		c->st.launches++;
+		c->st.trace_launches++;
+		NB_CK(c, cudaMemsetAsync(F.cnt + (cur ^ 1u), 0, sizeof(uint32_t),
+		  c->stream));
+		NB_CK(c, cudaMemsetAsync(F.cnt + 2, 0, sizeof(uint32_t),
+		  c->stream));
+		k_shade<<<grid_for(c, c->npaths, 256), 256, 0, c->stream>>>(S, F,
+		  A, cur, k);
+		NB_CK(c, cudaGetLastError());
+		c->st.launches++;
+		if (A.mode != RENDGPU_MODE_PRIMARY) {
+			shadow_ev.push_back(c->nev);
+			ev_record(c);
+			rc = launch_shadow(c, F);
+			if (rc)
+				return rc;
+			ev_record(c);
+			c->st.launches++;
+		}
+	}
+	int nrc_ev = c->nev;
+	if (nrc) {
+		// cache inference for the queries of this frame
+		ev_record(c);
+		k_nrc_encode_entries<<<grid_for(c, c->nq_cap, 128), 128, 0,
+		  c->stream>>>(F.nq, 4u, F.cnt + 40, c->nq_cap, c->box,
+		  c->nfeat.as<__nv_bfloat16>());
+		rc = nrc_infer(c, c->nfeat.p, c->nq_cap, c->npred.as<float4>(),
+		  F.cnt + 40);
+		if (rc)
+			return rc;
+		k_nrc_apply<<<grid_for(c, c->nq_cap, 256), 256, 0, c->stream>>>(
+		  F.nq, F.cnt + 40, c->nq_cap, c->npred.as<float4>(), F.pL);
+		NB_CK(c, cudaGetLastError());
+		c->st.launches += 3;
+		ev_record(c);
+	}
+	int acc_ev = c->nev;
+	ev_record(c);
+	float inv = 1.0f / (float)(rd->samples + rd->spp);
+	k_accum<<<grid_for(c, c->W * c->H, 256), 256, 0, c->stream>>>(F, inv);
+	NB_CK(c, cudaGetLastError());
+	c->st.launches++;
+	ev_record(c);
+	int train_ev = c->nev;
+	if (nrc) {
+		// train on this frame's records: targets from the finished paths,
+		// then kNrcSteps Adam steps of kNrcBatch samples each
+		ev_record(c);
+		k_nrc_targets<<<grid_for(c, c->nrec_cap, 256), 256, 0, c->stream>>>(
+		  F.nrec, F.cnt + 41, c->nrec_cap, F.pL, c->rtgt.as<float4>());
+		k_nrc_encode_entries<<<grid_for(c, c->nrec_cap, 128), 128, 0,
+		  c->stream>>>(F.nrec, 6u, F.cnt + 41, c->nrec_cap, c->box,
+		  c->rfeat.as<__nv_bfloat16>());
+		NB_CK(c, cudaGetLastError());
+		for (uint32_t s = 0; s < kNrcSteps; s++) {
+			rc = nrc_train(c, c->rfeat.p, c->rtgt.as<float4>(), kNrcBatch, 1,
+			  nullptr, nullptr, F.cnt + 41, s * kNrcBatch, c->nrec_cap);
+			if (rc)
+				return rc;
+		}
+		c->st.launches += 2 + 2 * kNrcSteps;
+		ev_record(c);
+	}
+	unsigned long long hr[4];
+	uint32_t hc[64];
+	NB_CK(c, cudaMemcpyAsync(hr, c->rays.p, sizeof(hr),
+	  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaMemcpyAsync(hc, c->cnt.p, sizeof(hc),
+	  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	c->st.closest_rays = hr[0];
+	c->st.node_visits = hr[2];
+	c->st.tri_tests = hr[3];
+	c->st.shadow_rays = hr[1];
+	c->st.rays = hr[0] + hr[1];
+	c->st.device_errors = hc[3];
+	if (nrc) {
+		// loss of the last Adam step (partials of its CTAs)
+		float lp[1024];
+		uint32_t ng = std::min<uint32_t>(c->train_grid, 1024);
+		NB_CK(c, cudaMemcpy(lp, c->mlp_loss.p, ng * 4,
+		  cudaMemcpyDeviceToHost));
+		double sl = 0.0;
+		for (uint32_t i = 0; i < ng; i++)
+			sl += lp[i];
+		uint32_t used = std::min(std::min(hc[41], c->nrec_cap), kNrcBatch);
+		c->st.nrc_loss = used ? (float)(sl / (3.0 * used)) : 0.0f;
+	}
+	c->st.nrc_queries = nrc ? std::min(hc[40], c->nq_cap) : 0;
+	c->st.nrc_records = nrc ? std::min(hc[41], c->nrec_cap) : 0;
+	for (int k = 0; k < 16; k++) {
+		c->st.bounce_closest[k] = hc[8 + k];
+		c->st.bounce_shadow[k] = hc[24 + k];
+	}
+	c->st.max_stack = need_stack(c);
+	if (c->cfg.flags & RENDGPU_FLAG_TIMING) {
+		c->st.ms_frame = ev_ms(c, 0, c->nev - 1);
+		float tr = 0.0f, sh = 0.0f;
+		for (int e : trace_ev)
+			tr += ev_ms(c, e, e + 1);
+		for (int e : shadow_ev)
+			sh += ev_ms(c, e, e + 1);
+		c->st.ms_trace = tr;
+		c->st.ms_shadow = sh;
+		c->st.ms_nrc = nrc ? ev_ms(c, nrc_ev, nrc_ev + 1) +
+		  ev_ms(c, train_ev, train_ev + 1) : 0.0f;
+		c->st.ms_shade = c->st.ms_frame - tr - sh - c->st.ms_nrc;
+		(void)acc_ev;
+	}
+	if (hc[3])
+		return fail(c, RENDGPU_EDEVICE, "rays abandoned on the device "
+		  "(traversal stack overflow)");
+	return 0;
+}
+
+void free_ctx(Ctx *c)
+{
+	DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs, &c->insts,
+	  &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits, &c->shadow,
+	  &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
+	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_wf,
+	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
+	  &c->mlp_loss, &c->nq, &c->nfeat, &c->npred, &c->nrec, &c->rfeat,
+	  &c->rtgt};
+	for (DevBuf *b : bufs)
+		b->release();
+	for (int i = 0; i < 64; i++)
+		if (c->ev[i])
+			cudaEventDestroy(c->ev[i]);
+	if (c->stream)
+		cudaStreamDestroy(c->stream);
+	delete c;
+}
+
+uint64_t held_bytes(const Ctx *c)
+{
+	const DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs,
+	  &c->insts, &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits,
+	  &c->shadow, &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf,
+	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
+	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
+	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nfeat, &c->npred, &c->nrec,
+	  &c->rfeat, &c->rtgt};
+	uint64_t s = 0;
+	for (const DevBuf *b : bufs)
+		s += b->cap;
+	return s;
 }
 
 // ------------------------------------------------ allocation-free tracing --
@@ -692,7 +817,7 @@ int rendgpu_init(struct rdata *rdp, const struct rendgpu_cfg *cfg)
 		return RENDGPU_ENODEV;
 	if (cfg->device < 0 || cfg->device >= ndev)
 		return RENDGPU_EINVAL;
-	if (cfg->mode > RENDGPU_MODE_PRIMARY || cfg->max_depth < 1 ||
+	if (cfg->mode > RENDGPU_MODE_NRC || cfg->max_depth < 1 ||
 	  cfg->max_depth > 1024 || cfg->sched > 3)
 		return RENDGPU_EINVAL;
 	Ctx *c = new Ctx;
@@ -1176,6 +1301,30 @@ int rendgpu_nrc_train_device(struct rdata *rdp, const void *feats,
 	NB_CK(c, cudaSetDevice(c->device));
 	return nrc_train(c, feats, reinterpret_cast<const float4 *>(targets), n,
 	  update, grad, loss);
+}
+
+int rendgpu_relmse_device(struct rdata *rdp, const float *ref, double *out)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c || !ref || !out)
+		return RENDGPU_EINVAL;
+	if (!c->have_frame)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_resaccum must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	uint32_t n = c->W * c->H * 3u;
+	NB_CK(c, c->mlp_loss.ensure(1024 * sizeof(float)));
+	double *d = reinterpret_cast<double *>(c->mlp_loss.p);
+	NB_CK(c, cudaMemsetAsync(d, 0, sizeof(double), c->stream));
+	uint32_t samples = c->rd->samples ? c->rd->samples : 1u;
+	k_relmse<<<grid_for(c, n, 256), 256, 0, c->stream>>>(c->acc.as<float>(),
+	  1.0f / (float)samples, ref, n, d);
+	NB_CK(c, cudaGetLastError());
+	double h = 0.0;
+	NB_CK(c, cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost,
+	  c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	*out = h / (double)n;
+	return 0;
 }
 
 int rendgpu_sync(struct rdata *rdp)

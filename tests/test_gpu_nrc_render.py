@@ -1,0 +1,42 @@
+"""Radiance-cache frames (RENDGPU_MODE_NRC) on the GPU: queries, training
+records, online training, and what the trained cache gains over the plain
+tracer at equal device time."""
+
+import numpy as np
+import pytest
+
+from nodebleed_b200 import api, nrc_eval
+
+pytestmark = pytest.mark.gpu
+
+
+def test_nrc_frames_produce_queries_and_records(gpu):
+    scene = api.Scene(api.SCENE_SMALL, 1)
+    rd = api.RenderData(scene, 160, 90, 1)
+    gr = api.GpuRenderer(rd, max_depth=5, mode=api.MODE_NRC, seed=3,
+                         timing=True).upload()
+    for _ in range(4):
+        rays = gr.frame()
+        st = gr.stats()
+        assert rays > 0 and st["device_errors"] == 0
+        assert st["nrc_queries"] > 0 and st["nrc_records"] > 0
+    gr.readback(1)
+    img = rd.acc()
+    assert np.isfinite(img).all() and (img >= 0).all()
+    gr.close()
+
+
+def test_nrc_relmse_reduction_is_reported(gpu):
+    """Against a 1024-spp plain reference: the FP64 relMSE of both methods
+    at equal device time.  The trained cache must not be worse than the
+    plain tracer by more than 20 % on this small scene, and the evaluation
+    must be self-consistent."""
+    scene = api.Scene(api.SCENE_SMALL, 1)
+    w, h, depth = 160, 90, 8
+    ref = nrc_eval.reference(scene, w, h, depth, 1024)
+    res = nrc_eval.equal_time(scene, w, h, depth, 24, ref)
+    print(res)
+    assert np.isfinite(res["nrc"]["relmse"]) and res["nrc"]["relmse"] > 0
+    assert np.isfinite(res["plain"]["relmse"]) and res["plain"]["relmse"] > 0
+    assert res["plain"]["ms"] >= res["nrc"]["ms"] or res["plain"]["frames"] == 1
+    assert res["nrc"]["relmse"] < 1.2 * res["plain"]["relmse"], res
