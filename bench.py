@@ -54,6 +54,14 @@ def parse():
     p.add_argument("--count", action="store_true",
                    help="one extra untimed frame counting node visits and "
                         "triangle tests per closest-hit ray")
+    p.add_argument("--no-nrc", action="store_true",
+                   help="skip the radiance-cache equal-time evaluation")
+    p.add_argument("--nrc-width", type=int, default=1920)
+    p.add_argument("--nrc-height", type=int, default=1080)
+    p.add_argument("--nrc-frames", type=int, default=64)
+    p.add_argument("--nrc-ref-spp", type=int, default=1024,
+                   help="reference samples per pixel (the workload asks "
+                        "for 4096; 1024 keeps the default run short)")
     p.add_argument("--cpu-seconds", type=float, default=15.0,
                    help="target CPU time of the bounded CPU sample")
     return p.parse_args()
@@ -310,6 +318,24 @@ def run_ours(a):
                   "tri_tests_per_ray": sc["tri_tests"] / sc["closest_rays"]}
         gc.close()
 
+    nrc = None
+    if rank == 0 and world == 1 and not a.no_nrc:
+        # radiance cache vs plain at equal device time, 1 spp per frame,
+        # both against a high-spp plain reference (relMSE in FP64 on the
+        # device); the same scene as the throughput workload
+        from nodebleed_b200 import nrc_eval
+        t0 = time.perf_counter()
+        ref = nrc_eval.reference(scene, a.nrc_width, a.nrc_height, a.depth,
+                                 a.nrc_ref_spp)
+        nrc = nrc_eval.equal_time(scene, a.nrc_width, a.nrc_height, a.depth,
+                                  a.nrc_frames, ref)
+        nrc["config"] = {"width": a.nrc_width, "height": a.nrc_height,
+                         "spp_per_frame": 1, "depth": a.depth,
+                         "reference_spp": a.nrc_ref_spp,
+                         "warmup_frames": 8, "train_paths_per_frame": 65536,
+                         "adam_lr": 1e-2}
+        nrc["wall_s"] = time.perf_counter() - t0
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(a, rd, lights, area, a.cpu_seconds)
@@ -353,7 +379,7 @@ def run_ours(a):
                "ms_trace_per_frame": trace_ms / a.steps,
                "ms_shadow_per_frame": shadow_ms / a.steps,
                "gpu_launches": launches, "e2e": e2e, "roofline": roof,
-               "gpu_visits": visits,
+               "gpu_visits": visits, "nrc": nrc,
                "cpu_baseline": cpu, "clocks": cl,
                "scene": {"unique_tris": scene.tris,
                          "instanced_tris": scene.inst_tris,

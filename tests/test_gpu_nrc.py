@@ -18,10 +18,13 @@ pytestmark = pytest.mark.gpu
 
 
 def _setup(seed=7):
+    """Renderer with Xavier-initialised weights in every layer (the
+    library starts the output layer at zero)."""
     scene = api.Scene(api.SCENE_TINY, 1)
     rd = api.RenderData(scene)
     gr = api.GpuRenderer(rd).upload()
     gr.nrc_reset(seed)
+    gr.nrc_weights(no.xavier(seed).astype(np.float32))
     return rd, gr
 
 
@@ -125,6 +128,17 @@ def test_gradients_match_oracle(gpu):
     assert (got[5 * no.SQ + 3 * 64:] == 0).all()
     # the weights did not move (update = 0)
     assert np.array_equal(gr.nrc_weights(), w)
+    gr.close()
+
+
+def test_reset_starts_output_layer_at_zero(gpu):
+    scene = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd).upload()
+    gr.nrc_reset(5)
+    w = gr.nrc_weights()
+    assert (w[5 * no.SQ:] == 0).all()
+    assert np.abs(w[:5 * no.SQ]).max() > 0.1
     gr.close()
 
 
