@@ -50,8 +50,13 @@ enum rendgpu_mode {
 
 enum rendgpu_flags {
 	RENDGPU_FLAG_TIMING = 1u << 0, /* record per-kernel CUDA events */
-	RENDGPU_FLAG_COUNT = 1u << 1   /* count node visits / triangle tests of
+	RENDGPU_FLAG_COUNT = 1u << 1,  /* count node visits / triangle tests of
 	                                  the closest-hit traces (slower) */
+	RENDGPU_FLAG_GRAPH = 1u << 2   /* capture the frame's launch sequence
+	                                  into a CUDA graph once and replay it
+	                                  (always on for batches; ignored in
+	                                  NRC mode); with TIMING only ms_frame
+	                                  is recorded */
 };
 
 struct rendgpu_cfg {
@@ -61,7 +66,8 @@ struct rendgpu_cfg {
 	uint32_t flags;      /* enum rendgpu_flags */
 	uint64_t seed;       /* PCG32 seed of the path streams */
 	int32_t  device;     /* CUDA device ordinal */
-	uint32_t block;      /* threads per block of the trace kernels (0 = auto) */
+	uint32_t block;      /* threads per block of the trace kernels: 64,
+	                        128 or 256 (0 = 128); see rendgpu_tune */
 	uint32_t sched;      /* traversal schedule: 0 = default, 1 = step,
 	                        2 = phase, 3 = ylitie (see trace.cuh) */
 	uint32_t reserved[7]; /* [0]: float bits of the cache's Adam learning
@@ -105,6 +111,30 @@ struct rendgpu_stats {
 	uint32_t nrc_records;    /* training vertices recorded in the frame */
 	float    ms_nrc;         /* cache inference + training (TIMING flag) */
 	float    nrc_loss;       /* loss of the frame's last training step */
+};
+
+/* Launch parameters of a context (rendgpu_set_tune / rendgpu_autotune).
+ * Zero fields take the defaults. */
+struct rendgpu_tune {
+	uint32_t block;  /* threads per block of the trace kernels: 64, 128
+	                    (default) or 256 */
+	uint32_t stack;  /* traversal stack entries per thread in shared memory:
+	                    24, 32 or 48; a depth below the scene's need (TLAS +
+	                    BLAS depth + 2) gives the smallest that fits */
+	uint32_t queue;  /* ray-queue capacity in camera slots: a frame runs in
+	                    waves of this many paths through all bounces
+	                    (0 = one wave of all paths) */
+	uint32_t sched;  /* traversal schedule as rendgpu_cfg.sched (0 = cfg's) */
+	float    ms;     /* autotune: median device ms per frame measured */
+	uint32_t reserved[3];
+};
+
+/* Per-scene counts of a batch frame. */
+struct rendgpu_scene_stats {
+	uint64_t closest_rays;
+	uint64_t shadow_rays;
+	uint64_t paths;   /* width * height * spp */
+	uint64_t pixels;
 };
 
 /* Create the GPU context of `rd` (one per rdata).  Replaces nothing in the
@@ -232,6 +262,59 @@ int rendgpu_get_lights(struct rdata *rd, float *out, uint32_t cap,
 /* Last error of any call on this thread's most recent context. */
 int         rendgpu_last_error(struct rdata *rd);
 const char *rendgpu_strerror(struct rdata *rd);
+
+/* Launch parameters (no counterpart in the reference).  set_tune with a new
+ * queue capacity re-sizes the queues and clears the accumulator; get_tune
+ * reports the settings in effect.  rendgpu_autotune renders `frames` timed
+ * frames (after one untimed) per candidate, tuning the schedule, the block
+ * size, the stack depth and the queue capacity one at a time (coordinate
+ * descent), keeps the fastest, and clears the accumulator; rd->samples is
+ * not advanced.  Every measured setting with its ms goes to log[0..cap)
+ * and their number to *nlog (either may be NULL).  Not in NRC mode. */
+int rendgpu_set_tune(struct rdata *rd, const struct rendgpu_tune *t);
+int rendgpu_get_tune(struct rdata *rd, struct rendgpu_tune *t);
+int rendgpu_autotune(struct rdata *rd, uint32_t frames,
+                     struct rendgpu_tune *best, struct rendgpu_tune *log,
+                     uint32_t cap, uint32_t *nlog);
+
+/* Batches (no counterpart in the reference, which renders one rdata per
+ * rend_render): n scenes of uneven triangle counts, resolutions, spp and
+ * depths rendered by one launch sequence over shared ray queues, captured
+ * once into a CUDA graph and replayed every frame.  Each rdata is prepared
+ * by the application exactly as for rendgpu_init (rend_prepstatic,
+ * rend_prepdynamic, rend_resaccum); max_depth[i] bounds scene i's paths
+ * (NULL: cfg->max_depth for all).  Every scene's image is bit-identical to
+ * the same scene rendered alone with the same cfg.  At most 4096 instances
+ * over all scenes (hit ids keep 12 instance bits); PATH and PRIMARY modes.
+ * batch_render renders one frame of every scene (rd->samples of each keys
+ * its random streams; the caller bumps samples afterwards, as main.c does)
+ * and adds each scene's rays to its rd->rays. */
+struct rendgpu_batch;
+int rendgpu_batch_init(struct rdata *const *rds, uint32_t n,
+                       const uint32_t *max_depth,
+                       const struct rendgpu_cfg *cfg,
+                       struct rendgpu_batch **out);
+int rendgpu_batch_release(struct rendgpu_batch *b);
+int rendgpu_batch_upload_static(struct rendgpu_batch *b);
+int rendgpu_batch_upload_dynamic(struct rendgpu_batch *b);
+int rendgpu_batch_resaccum(struct rendgpu_batch *b);
+int rendgpu_batch_clraccum(struct rendgpu_batch *b);
+int rendgpu_batch_render(struct rendgpu_batch *b);
+int rendgpu_batch_readback(struct rendgpu_batch *b, int which);
+/* Totals of the last frame, and per-scene counts into per[0..n). */
+int rendgpu_batch_get_stats(struct rendgpu_batch *b,
+                            struct rendgpu_stats *total,
+                            struct rendgpu_scene_stats *per, uint32_t n);
+int rendgpu_batch_set_tune(struct rendgpu_batch *b,
+                           const struct rendgpu_tune *t);
+int rendgpu_batch_get_tune(struct rendgpu_batch *b, struct rendgpu_tune *t);
+int rendgpu_batch_autotune(struct rendgpu_batch *b, uint32_t frames,
+                           struct rendgpu_tune *best,
+                           struct rendgpu_tune *log, uint32_t cap,
+                           uint32_t *nlog);
+int rendgpu_batch_get_stream(struct rendgpu_batch *b, void **stream);
+int         rendgpu_batch_last_error(struct rendgpu_batch *b);
+const char *rendgpu_batch_strerror(struct rendgpu_batch *b);
 
 #ifdef __cplusplus
 }

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 SCENE_SMALL, SCENE_SCALE, SCENE_BATCH, SCENE_STRESS, SCENE_TINY = 1, 2, 3, 5, 9
 MODE_PATH, MODE_PRIMARY, MODE_NRC = 0, 1, 2
-FLAG_TIMING, FLAG_COUNT = 1, 2
+FLAG_TIMING, FLAG_COUNT, FLAG_GRAPH = 1, 2, 4
 
 # struct rendgpu_ray / rendgpu_hit (32 / 16 bytes)
 RAY_DTYPE = np.dtype([("o", "<f4", (3,)), ("tmax", "<f4"), ("d", "<f4", (3,)),
@@ -89,6 +89,27 @@ class RendgpuStats(C.Structure):
         return d
 
 
+class RendgpuTune(C.Structure):
+    _fields_ = [("block", C.c_uint32), ("stack", C.c_uint32),
+                ("queue", C.c_uint32), ("sched", C.c_uint32),
+                ("ms", C.c_float), ("reserved", C.c_uint32 * 3)]
+
+    def as_dict(self):
+        return {"block": self.block, "stack": self.stack,
+                "queue": self.queue, "sched": self.sched, "ms": self.ms}
+
+    @classmethod
+    def make(cls, block=0, stack=0, queue=0, sched=0):
+        t = cls()
+        t.block, t.stack, t.queue, t.sched = block, stack, queue, sched
+        return t
+
+
+class RendgpuSceneStats(C.Structure):
+    _fields_ = [("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("paths", C.c_uint64), ("pixels", C.c_uint64)]
+
+
 class HostLib:
     def __init__(self):
         L = _load("libnbhost.so")
@@ -141,12 +162,31 @@ class GpuLib:
                 ("rendgpu_sync", [vp]), ("rendgpu_get_stats", [vp, vp]),
                 ("rendgpu_get_lights", [vp, vp, u32, vp]),
                 ("rendgpu_get_stream", [vp, vp]),
+                ("rendgpu_set_tune", [vp, vp]),
+                ("rendgpu_get_tune", [vp, vp]),
+                ("rendgpu_autotune", [vp, u32, vp, vp, u32, vp]),
+                ("rendgpu_batch_init", [vp, u32, vp, vp, vp]),
+                ("rendgpu_batch_release", [vp]),
+                ("rendgpu_batch_upload_static", [vp]),
+                ("rendgpu_batch_upload_dynamic", [vp]),
+                ("rendgpu_batch_resaccum", [vp]),
+                ("rendgpu_batch_clraccum", [vp]),
+                ("rendgpu_batch_render", [vp]),
+                ("rendgpu_batch_readback", [vp, C.c_int]),
+                ("rendgpu_batch_get_stats", [vp, vp, vp, u32]),
+                ("rendgpu_batch_set_tune", [vp, vp]),
+                ("rendgpu_batch_get_tune", [vp, vp]),
+                ("rendgpu_batch_autotune", [vp, u32, vp, vp, u32, vp]),
+                ("rendgpu_batch_get_stream", [vp, vp]),
+                ("rendgpu_batch_last_error", [vp]),
                 ("rendgpu_last_error", [vp])]:
             f = getattr(L, fn)
             f.argtypes = args
             f.restype = C.c_int
         L.rendgpu_strerror.argtypes = [vp]
         L.rendgpu_strerror.restype = C.c_char_p
+        L.rendgpu_batch_strerror.argtypes = [vp]
+        L.rendgpu_batch_strerror.restype = C.c_char_p
         self.L = L
 
 
@@ -269,24 +309,41 @@ class RenderData:
             pass
 
 
+def make_cfg(max_depth=5, mode=MODE_PATH, seed=1, timing=False, device=0,
+             count=False, sched=0, graph=False, block=0):
+    cfg = RendgpuCfg()
+    cfg.size = C.sizeof(RendgpuCfg)
+    cfg.max_depth = max_depth
+    cfg.mode = mode
+    cfg.flags = (FLAG_TIMING if timing else 0) | \
+        (FLAG_COUNT if count else 0) | (FLAG_GRAPH if graph else 0)
+    cfg.seed = seed
+    cfg.device = device
+    cfg.sched = sched
+    cfg.block = block
+    return cfg
+
+
+def _autotune(fn, handle, frames, cap, check):
+    best = RendgpuTune()
+    log = (RendgpuTune * cap)()
+    n = C.c_uint32()
+    check(fn(handle, frames, C.byref(best), log, cap, C.byref(n)))
+    return best.as_dict(), [log[i].as_dict() for i in range(min(n.value,
+                                                                 cap))]
+
+
 class GpuRenderer:
     """The rendgpu C ABI on one RenderData."""
 
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
                  timing=False, device=0, count=False, sched=0,
-                 nrc_warmup=0, nrc_lr=0.0):
+                 nrc_warmup=0, nrc_lr=0.0, graph=False, block=0):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
-        cfg = RendgpuCfg()
-        cfg.size = C.sizeof(RendgpuCfg)
-        cfg.max_depth = max_depth
-        cfg.mode = mode
-        cfg.flags = (FLAG_TIMING if timing else 0) | \
-            (FLAG_COUNT if count else 0)
-        cfg.seed = seed
-        cfg.device = device
-        cfg.sched = sched
+        cfg = make_cfg(max_depth, mode, seed, timing, device, count, sched,
+                       graph, block)
         cfg.reserved[0] = C.c_uint32.from_buffer_copy(
             C.c_float(nrc_lr)).value
         cfg.reserved[1] = nrc_warmup
@@ -348,6 +405,20 @@ class GpuRenderer:
         self._ck(self.g.rendgpu_get_stats(self.ptr, C.byref(st)), "stats")
         return st.as_dict()
 
+    def set_tune(self, **kw):
+        t = RendgpuTune.make(**kw)
+        self._ck(self.g.rendgpu_set_tune(self.ptr, C.byref(t)), "set_tune")
+
+    def get_tune(self):
+        t = RendgpuTune()
+        self._ck(self.g.rendgpu_get_tune(self.ptr, C.byref(t)), "get_tune")
+        return t.as_dict()
+
+    def autotune(self, frames=2, cap=64):
+        """Returns (best setting, every measured setting)."""
+        return _autotune(self.g.rendgpu_autotune, self.ptr, frames, cap,
+                         lambda rc: self._ck(rc, "autotune"))
+
     # ---- neural radiance cache
     NRC_PARAMS = 5 * 4096 + 8 * 64
 
@@ -391,6 +462,103 @@ class GpuRenderer:
     def close(self):
         if self.live:
             self.g.rendgpu_release(self.ptr)
+            self.live = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchRenderer:
+    """rendgpu_batch_*: several RenderData rendered by one captured launch
+    sequence over shared ray queues.  max_depth: one value for all scenes
+    or one per scene."""
+
+    def __init__(self, rdatas, max_depth=5, mode=MODE_PATH, seed=1,
+                 timing=False, device=0, sched=0, block=0):
+        self.g = gpu_lib().L
+        self.rdatas = list(rdatas)
+        n = len(self.rdatas)
+        depths = max_depth if hasattr(max_depth, "__len__") else \
+            [max_depth] * n
+        self.depths = (C.c_uint32 * n)(*depths)
+        ptrs = (C.c_void_p * n)(*[r.ptr for r in self.rdatas])
+        cfg = make_cfg(max(depths), mode, seed, timing, device, False, sched,
+                       True, block)
+        h = C.c_void_p()
+        rc = self.g.rendgpu_batch_init(ptrs, n, self.depths, C.byref(cfg),
+                                       C.byref(h))
+        if rc != 0:
+            raise RendgpuError(rc, "rendgpu_batch_init")
+        self.h = h.value
+        self.live = True
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            raise RendgpuError(rc, f"{what}: "
+                               f"{self.g.rendgpu_batch_strerror(self.h).decode()}")
+
+    def upload(self):
+        self._ck(self.g.rendgpu_batch_upload_static(self.h), "upload_static")
+        self._ck(self.g.rendgpu_batch_upload_dynamic(self.h),
+                 "upload_dynamic")
+        self._ck(self.g.rendgpu_batch_resaccum(self.h), "resaccum")
+        return self
+
+    def clraccum(self):
+        self._ck(self.g.rendgpu_batch_clraccum(self.h), "clraccum")
+
+    def frame(self):
+        """One frame of every scene, then main.c's bookkeeping on each
+        rdata.  Returns the frame's ray count over all scenes."""
+        self._ck(self.g.rendgpu_batch_render(self.h), "render")
+        total, _ = self.stats()
+        for r in self.rdatas:
+            rd = r.rd
+            rd.blknum = 0
+            rd.rays = 0
+            rd.samples += rd.spp
+        return total["rays"]
+
+    def readback(self, which=3):
+        self._ck(self.g.rendgpu_batch_readback(self.h, which), "readback")
+
+    def stats(self):
+        """(totals as GpuRenderer.stats, [per-scene counts])."""
+        n = len(self.rdatas)
+        st = RendgpuStats()
+        per = (RendgpuSceneStats * n)()
+        self._ck(self.g.rendgpu_batch_get_stats(self.h, C.byref(st), per, n),
+                 "stats")
+        return st.as_dict(), [{k: getattr(p, k) for k, _ in p._fields_}
+                              for p in per]
+
+    def set_tune(self, **kw):
+        t = RendgpuTune.make(**kw)
+        self._ck(self.g.rendgpu_batch_set_tune(self.h, C.byref(t)),
+                 "set_tune")
+
+    def get_tune(self):
+        t = RendgpuTune()
+        self._ck(self.g.rendgpu_batch_get_tune(self.h, C.byref(t)),
+                 "get_tune")
+        return t.as_dict()
+
+    def autotune(self, frames=2, cap=64):
+        return _autotune(self.g.rendgpu_batch_autotune, self.h, frames, cap,
+                         lambda rc: self._ck(rc, "autotune"))
+
+    def stream(self):
+        s = C.c_void_p()
+        self._ck(self.g.rendgpu_batch_get_stream(self.h, C.byref(s)),
+                 "stream")
+        return s.value or 0
+
+    def close(self):
+        if self.live:
+            self.g.rendgpu_batch_release(self.h)
             self.live = False
 
     def __del__(self):

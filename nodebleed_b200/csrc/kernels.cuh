@@ -38,7 +38,8 @@ struct FrameDev {
 	                   // [6] shadow launches, [8+k] / [24+k] closest /
 	                   // shadow rays of bounce k
 	unsigned long long *rays; // [0] closest, [1] shadow
-	uint32_t  W, H, spp, npaths;
+	unsigned long long *scn;  // per scene: [2s] closest, [2s+1] shadow rays
+	uint32_t  npaths, npix;   // all scenes
 	// neural radiance cache (mode 2): queries (4 float4: (pos, path),
 	// (wo, T.x), (n, T.y), (albedo, T.z)) counted in cnt[40], training
 	// records (6 float4: (pos, path), wo, n, albedo, L before, T) in cnt[41]
@@ -51,15 +52,11 @@ struct FrameDev {
 constexpr uint32_t kPathSpec = 1u;   // arrived by a mirror bounce
 constexpr uint32_t kPathTrain = 2u;  // unbiased cache-training path
 
+// Frame-wide arguments; everything per scene (camera, seed, sizes, depth,
+// the cache's training-path stride) is in the ScenePar table.
 struct FrameArgs {
-	uint64_t seed;
-	uint32_t frame;   // rd->samples
-	uint32_t depth;
-	uint32_t mode;      // 0 path, 1 primary, 2 path with radiance cache
-	uint32_t nrc_stride, nrc_offset; // training paths: (path + offset) % stride == 0
-	// camera (rcam fields)
-	float eye[3], ri[3], up[3], fwd[3];
-	float rw, rh, fovfdist, aspect, fdist, focrad, tanfangle;
+	uint32_t depth;   // bounces of the launch sequence: max over scenes
+	uint32_t mode;    // 0 path, 1 primary, 2 path with radiance cache
 };
 
 // ------------------------------------------------------------- sampling --
@@ -133,6 +130,21 @@ __device__ __forceinline__ uint32_t append(uint32_t *counter, bool want)
 	return base + __popc(mask & ((1u << lane) - 1u));
 }
 
+// Warp-aggregated count of the lanes with `want` into ctr[2 * scene + which]
+// (lanes of one warp mostly share a scene).
+__device__ __forceinline__ void count_scene(unsigned long long *ctr,
+                                            uint32_t scene, uint32_t which,
+                                            bool want)
+{
+	uint32_t mask = __ballot_sync(__activemask(), want);
+	if (!want)
+		return;
+	uint32_t peers = __match_any_sync(mask, scene);
+	if ((threadIdx.x & 31u) == (uint32_t)__ffs(peers) - 1u)
+		atomicAdd(ctr + 2u * scene + which,
+		  (unsigned long long)__popc(peers));
+}
+
 // Pixel of queue slot i: 8x4 pixel tiles, spp consecutive samples.
 __device__ __forceinline__ bool tile_pixel(uint32_t i, uint32_t W,
                                            uint32_t H, uint32_t spp,
@@ -150,51 +162,62 @@ __device__ __forceinline__ bool tile_pixel(uint32_t i, uint32_t W,
 
 // --------------------------------------------------------------- kernels --
 
-// Camera rays (rend.c:3293-3402, one lane) and path state.
-__global__ void __launch_bounds__(256) k_gen(FrameDev F, FrameArgs A)
+// Camera rays (rend.c:3293-3402, one lane) and path state for the camera
+// slots [slot_lo, slot_hi) of all scenes (one wave of the ray queue).
+__global__ void __launch_bounds__(256) k_gen(DScene S, FrameDev F,
+                                             FrameArgs A, uint32_t slot_lo,
+                                             uint32_t slot_hi)
 {
-	uint32_t tiles_w = (F.W + 7u) >> 3, tiles_h = (F.H + 3u) >> 2;
-	uint32_t total = tiles_w * tiles_h * 32u * F.spp;
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		F.cnt[4] = 0u;
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	     i - threadIdx.x < total; i += gridDim.x * blockDim.x) {
-		uint32_t x = 0, y = 0, s = 0;
-		bool live = i < total && tile_pixel(i, F.W, F.H, F.spp, &x, &y, &s);
-		uint32_t path = (y * F.W + x) * F.spp + s;
+	for (uint32_t i0 = slot_lo + blockIdx.x * blockDim.x; i0 < slot_hi;
+	     i0 += gridDim.x * blockDim.x) {
+		uint32_t i = i0 + threadIdx.x;
+		uint32_t x = 0, y = 0, smp = 0, sc = 0;
+		bool live = i < slot_hi;
+		if (live)
+			sc = scene_search(S, i, [](const ScenePar *p) {
+				return __ldg(&p->slot_base); });
+		const ScenePar *P = S.sp + sc;
+		uint32_t W = __ldg(&P->W), spp = __ldg(&P->spp);
+		live = live && tile_pixel(i - __ldg(&P->slot_base), W,
+		  __ldg(&P->H), spp, &x, &y, &smp);
+		uint32_t lpath = (y * W + x) * spp + smp;
+		uint32_t path = __ldg(&P->path_base) + lpath;
 		float o[3] = {0, 0, 0}, d[3] = {0, 0, 1};
 		uint64_t st = 0;
 		if (live) {
-			uint64_t inc = pcg_inc(path);
-			st = pcg_start(A.seed, A.frame, path);
+			ScenePar C = *P;
+			uint64_t inc = pcg_inc(lpath);
+			st = pcg_start(C.seed, C.frame, lpath);
 			float u0 = rnd01(st, inc), u1 = rnd01(st, inc);
 			float sx = __fadd_rn((float)x, __fsub_rn(u0, 0.5f));
 			float sy = __fadd_rn((float)y, __fsub_rn(u1, 0.5f));
-			sx = __fmaf_rn(sx, A.rw, -0.5f);
-			sy = __fmaf_rn(sy, A.rh, -0.5f);
-			sx = __fmul_rn(sx, A.fovfdist);
-			sy = __fmul_rn(sy, A.fovfdist);
-			sx = __fmul_rn(sx, A.aspect);
+			sx = __fmaf_rn(sx, C.rw, -0.5f);
+			sy = __fmaf_rn(sy, C.rh, -0.5f);
+			sx = __fmul_rn(sx, C.fovfdist);
+			sy = __fmul_rn(sy, C.fovfdist);
+			sx = __fmul_rn(sx, C.aspect);
 			float ups[3], riup[3], td[3];
 			for (int a = 0; a < 3; a++) {
-				ups[a] = __fmul_rn(A.up[a], sy);
-				riup[a] = __fmaf_rn(A.ri[a], sx, -ups[a]);
+				ups[a] = __fmul_rn(C.up[a], sy);
+				riup[a] = __fmaf_rn(C.ri[a], sx, -ups[a]);
 			}
-			if (A.tanfangle > 0.0f) {
+			if (C.tanfangle > 0.0f) {
 				float u2 = rnd01(st, inc), u3 = rnd01(st, inc);
 				float rad = __fsqrt_rn(u2), sn, cs;
 				sincos2pi(u3, &sn, &cs);
 				float lx = __fmul_rn(cs, rad), ly = __fmul_rn(sn, rad);
 				for (int a = 0; a < 3; a++) {
-					o[a] = __fmaf_rn(__fmaf_rn(A.ri[a], lx,
-					  __fmul_rn(A.up[a], ly)), A.focrad, A.eye[a]);
-					float fe = __fmaf_rn(A.fwd[a], A.fdist, A.eye[a]);
+					o[a] = __fmaf_rn(__fmaf_rn(C.ri[a], lx,
+					  __fmul_rn(C.up[a], ly)), C.focrad, C.eye[a]);
+					float fe = __fmaf_rn(C.fwd[a], C.fdist, C.eye[a]);
 					td[a] = __fsub_rn(__fadd_rn(fe, riup[a]), o[a]);
 				}
 			} else {
 				for (int a = 0; a < 3; a++) {
-					o[a] = A.eye[a];
-					td[a] = __fmaf_rn(A.fwd[a], A.fdist, riup[a]);
+					o[a] = C.eye[a];
+					td[a] = __fmaf_rn(C.fwd[a], C.fdist, riup[a]);
 				}
 			}
 			float l2 = __fmaf_rn(td[0], td[0], __fmaf_rn(td[1], td[1],
@@ -202,8 +225,8 @@ __global__ void __launch_bounds__(256) k_gen(FrameDev F, FrameArgs A)
 			float il = __fdiv_rn(1.0f, __fsqrt_rn(l2));
 			for (int a = 0; a < 3; a++)
 				d[a] = __fmul_rn(td[a], il);
-			uint32_t flags = (A.mode == 2u && (path + A.nrc_offset) %
-			  A.nrc_stride == 0u) ? kPathTrain : 0u;
+			uint32_t flags = (A.mode == 2u && (lpath + C.nrc_offset) %
+			  C.nrc_stride == 0u) ? kPathTrain : 0u;
 			F.pT[path] = make_float4(1.0f, 1.0f, 1.0f,
 			  __uint_as_float(flags));
 			F.pL[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -220,9 +243,10 @@ __global__ void __launch_bounds__(256) k_gen(FrameDev F, FrameArgs A)
 
 // Closest-hit trace of a ray queue (count in *count): raw hits.
 // COUNT adds visit / triangle-test counts to counts[0..1]; SCHED picks the
-// traversal schedule.
+// traversal schedule.  Blocks of 64, 128 or 256 threads (the launch bound
+// keeps 64 registers per thread for each).
 template <int SCHED, int STACK, bool COUNT>
-__global__ void __launch_bounds__(128, 8) k_trace(DScene S, const float4 *rays,
+__global__ void __launch_bounds__(256, 4) k_trace(DScene S, const float4 *rays,
                                                const uint32_t *count,
                                                uint32_t *work, float4 *hits,
                                                uint32_t *errs,
@@ -240,7 +264,7 @@ __global__ void __launch_bounds__(128, 8) k_trace(DScene S, const float4 *rays,
 
 // Any-hit trace of API rays: occl[i] = hit in (0, tmax).
 template <int SCHED, int STACK>
-__global__ void __launch_bounds__(128, 8) k_occluded(DScene S,
+__global__ void __launch_bounds__(256, 4) k_occluded(DScene S,
                                                   const float4 *rays,
                                                   const uint32_t *count,
                                                   uint32_t *work, uint8_t *occl,
@@ -277,16 +301,15 @@ struct SinkShadow {
 };
 
 template <int SCHED, int STACK>
-__global__ void __launch_bounds__(128, 8) k_shadow(DScene S, FrameDev F)
+__global__ void __launch_bounds__(256, 4) k_shadow(DScene S, FrameDev F,
+                                                  uint32_t k)
 {
 	extern __shared__ uint2 sstk[];
 	uint32_t n = F.cnt[2];
 	if (blockIdx.x == 0 && threadIdx.x == 0) {
 		atomicAdd(&F.rays[1], (unsigned long long)n);
-		atomicAdd(&F.cnt[6], 1u);
-		uint32_t k = F.cnt[6] - 1u; // bounce of this shadow launch
 		if (k < 16u)
-			F.cnt[24u + k] = n;
+			atomicAdd(&F.cnt[24u + k], n); // shadow rays of bounce k
 	}
 	SinkShadow sink{F.shadow, F.scol, F.pL, &F.cnt[3]};
 	trace_persistent<SCHED, true, STACK, false>(S, F.shadow, n, &F.cnt[5],
@@ -322,7 +345,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 		F.cnt[4] = 0u;
 		F.cnt[5] = 0u;
 		if (k < 16u)
-			F.cnt[8u + k] = n; // closest-hit rays of bounce k
+			atomicAdd(&F.cnt[8u + k], n); // closest-hit rays of bounce k
 	}
 	for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n;
 	     i0 += gridDim.x * blockDim.x) {
@@ -332,7 +355,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 		float no[3] = {0, 0, 0}, nd[3] = {0, 0, 0};
 		float so[3] = {0, 0, 0}, sd[3] = {0, 0, 0}, sc[3] = {0, 0, 0};
 		float tfar = 0.0f;
-		uint32_t path = 0;
+		uint32_t path = 0, sidx = 0;
 		if (live) {
 			float4 ra = rays[2u * i], rb = rays[2u * i + 1u];
 			float4 h = F.hits[i];
@@ -341,12 +364,16 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 				h = finish_hit(S, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z, th);
 			}
 			path = __float_as_uint(rb.w);
+			sidx = scene_of_path(S, path);
+			const ScenePar *P = S.sp + sidx;
+			uint32_t lpath = path - __ldg(&P->path_base);
+			uint32_t depth = __ldg(&P->depth);
 			float4 T = F.pT[path];
 			float4 L = F.pL[path];
 			if (h.x == FLT_MAX) {
-				L.x = __fadd_rn(L.x, __fmul_rn(T.x, S.bg[0]));
-				L.y = __fadd_rn(L.y, __fmul_rn(T.y, S.bg[1]));
-				L.z = __fadd_rn(L.z, __fmul_rn(T.z, S.bg[2]));
+				L.x = __fadd_rn(L.x, __fmul_rn(T.x, __ldg(&P->bg[0])));
+				L.y = __fadd_rn(L.y, __fmul_rn(T.y, __ldg(&P->bg[1])));
+				L.z = __fadd_rn(L.z, __fmul_rn(T.z, __ldg(&P->bg[2])));
 				F.pL[path] = L;
 			} else {
 				uint32_t id = __float_as_uint(h.w);
@@ -412,7 +439,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 					}
 					uint2 rs = F.rng[path];
 					uint64_t st = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
-					uint64_t inc = pcg_inc(path);
+					uint64_t inc = pcg_inc(lpath);
 					float rl = rnd01(st, inc), ra_ = rnd01(st, inc);
 					float rb_ = rnd01(st, inc), r0 = rnd01(st, inc);
 					float r1 = rnd01(st, inc);
@@ -478,21 +505,24 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 						T.z = __fmul_rn(T.z, col[2]);
 						T.w = __uint_as_float(pflags | kPathSpec);
 						F.pT[path] = T;
-						want_ray = k + 1u < A.depth;
+						want_ray = k + 1u < depth;
 					} else {
 						T.w = __uint_as_float(pflags & ~kPathSpec);
-						if (S.nlights) {
+						uint32_t nl = __ldg(&P->light_cnt);
+						if (nl) {
 							// pick an emitting triangle by area
-							uint32_t lo = 0, hi = S.nlights - 1u;
+							const float4 *lt = S.lights +
+							  5u * __ldg(&P->light_off);
+							uint32_t lo = 0, hi = nl - 1u;
 							while (lo < hi) {
 								uint32_t mid = (lo + hi) >> 1;
-								float cdf = __ldg(&S.lights[5u * mid + 3u]).w;
+								float cdf = __ldg(&lt[5u * mid + 3u]).w;
 								if (rl < cdf)
 									hi = mid;
 								else
 									lo = mid + 1u;
 							}
-							const float4 *lp = S.lights + 5u * lo;
+							const float4 *lp = lt + 5u * lo;
 							float4 l0 = __ldg(lp), l1 = __ldg(lp + 1);
 							float4 l2 = __ldg(lp + 2), l3 = __ldg(lp + 3);
 							// v0 = l0.xyz, e0 = (l0.w, l1.x, l1.y),
@@ -533,7 +563,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 							    tfar > 0.0f) {
 								float wgt = __fmul_rn(ndotl, cosl);
 								wgt = __fmul_rn(wgt, __fmul_rn(kInvPi,
-								  S.light_area));
+								  __ldg(&P->light_area)));
 								wgt = __fdiv_rn(wgt, l2s);
 								float em[3] = {l3.x, l3.y, l3.z};
 								float tc[3] = {T.x, T.y, T.z};
@@ -548,7 +578,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 								want_shadow = true;
 							}
 						}
-						if (k + 1u < A.depth) {
+						if (k + 1u < depth) {
 							float sn, cs;
 							sincos2pi(r0, &sn, &cs);
 							float s1 = __fsqrt_rn(r1);
@@ -580,6 +610,10 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 					}
 				}
 			}
+		}
+		if (S.nscenes > 1u) {
+			count_scene(F.scn, sidx, 0u, live);
+			count_scene(F.scn, sidx, 1u, want_shadow);
 		}
 		uint32_t rs_ = append(&F.cnt[cur ^ 1u], want_ray);
 		if (want_ray) {
@@ -626,14 +660,21 @@ __global__ void __launch_bounds__(256) k_relmse(const float *acc, float inv,
 }
 
 // acc += sum over the pixel's samples; ARGB8 resolve (rend.c:3565-3580).
-__global__ void __launch_bounds__(256) k_accum(FrameDev F, float inv)
+// Pixels of all scenes: acc and buf hold the scenes' images back to back.
+__global__ void __launch_bounds__(256) k_accum(DScene S, FrameDev F)
 {
-	uint32_t npix = F.W * F.H;
-	for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix;
+	for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < F.npix;
 	     p += gridDim.x * blockDim.x) {
+		uint32_t sc = scene_search(S, p, [](const ScenePar *q) {
+			return __ldg(&q->pix_base); });
+		const ScenePar *P = S.sp + sc;
+		uint32_t spp = __ldg(&P->spp);
+		float inv = __ldg(&P->inv);
+		const float4 *pl = F.pL + __ldg(&P->path_base) +
+		  (size_t)(p - __ldg(&P->pix_base)) * spp;
 		float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-		for (uint32_t s = 0; s < F.spp; s++) {
-			float4 L = F.pL[p * F.spp + s];
+		for (uint32_t s = 0; s < spp; s++) {
+			float4 L = pl[s];
 			sx = __fadd_rn(sx, L.x);
 			sy = __fadd_rn(sy, L.y);
 			sz = __fadd_rn(sz, L.z);

@@ -295,24 +295,24 @@ bool convert_blas(const nb_rdata *rd, uint32_t triofs,
 }
 
 bool convert_tlas(const nb_rdata *rd, std::vector<nb_qnode> &nodes,
-                  std::vector<uint32_t> &irefs, bvh_stats *st,
-                  std::string *err)
+                  std::vector<uint32_t> &irefs, uint32_t inst_base,
+                  uint32_t *root, bvh_stats *st, std::string *err)
 {
 	const uint8_t *base = (const uint8_t *)&rd->bnodes[rd->tlasofs];
 	uint64_t limit = (uint64_t)2 * (rd->instcnt ? rd->instcnt : 1) *
 	  sizeof(nb_bnode8);
-	nodes.clear();
-	irefs.clear();
+	*root = (uint32_t)nodes.size();
 	nodes.emplace_back();
+	uint32_t items0 = (uint32_t)irefs.size();
 	auto leaf = [&](uint32_t inst, uint32_t *first) -> uint32_t {
 		if (inst >= rd->instcnt)
 			return 0;
 		*first = (uint32_t)irefs.size();
-		irefs.push_back(inst);
+		irefs.push_back(inst_base + inst);
 		return 1;
 	};
-	bool ok = convert_tree(base, limit, nodes, 0, leaf, st, err);
-	st->items = (uint32_t)irefs.size();
+	bool ok = convert_tree(base, limit, nodes, *root, leaf, st, err);
+	st->items = (uint32_t)irefs.size() - items0;
 	return ok;
 }
 

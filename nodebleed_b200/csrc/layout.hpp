@@ -26,11 +26,11 @@ bool convert_blas(const nb_rdata *rd, uint32_t triofs,
                   std::vector<nb_qnode> &nodes, std::vector<nb_gtri> &tris,
                   uint32_t *root, bvh_stats *st, std::string *err);
 
-// TLAS rooted at bnodes[tlasofs] into `nodes` (root at index 0) and
-// instance references `irefs`.
+// Append the TLAS rooted at bnodes[tlasofs] to `nodes` (its root index in
+// *root) and its instance references, offset by inst_base, to `irefs`.
 bool convert_tlas(const nb_rdata *rd, std::vector<nb_qnode> &nodes,
-                  std::vector<uint32_t> &irefs, bvh_stats *st,
-                  std::string *err);
+                  std::vector<uint32_t> &irefs, uint32_t inst_base,
+                  uint32_t *root, bvh_stats *st, std::string *err);
 
 // World-space emitting triangles of instances whose material is EMISSIVE,
 // with an area CDF; returns the total area.

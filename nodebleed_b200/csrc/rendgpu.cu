@@ -1,16 +1,22 @@
 // C ABI of the B200 path-tracing core (include/rendgpu.h).
 //
 // One context per `struct rdata`, found through a small registry keyed by
-// the rdata pointer (the reference API passes only that pointer).  Uploads
-// convert the reference BVH8 to the GPU layout (layout.cpp); a frame is the
-// fixed launch sequence of kernels.cuh on the context's stream.
+// the rdata pointer (the reference API passes only that pointer), or one
+// context for a batch of rdatas (rendgpu_batch_*): a single-scene context
+// is a batch of one.  Uploads convert each scene's reference BVH8 to the GPU
+// layout (layout.cpp) and append it to shared arrays with its offsets baked
+// in; a frame is the fixed launch sequence of kernels.cuh over all scenes'
+// paths on the context's stream, optionally captured once into a CUDA graph
+// and replayed.
 
+#include <algorithm>
 #include <cfloat>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -23,9 +29,13 @@
 namespace nb {
 namespace {
 
-constexpr int kStackSmall = 24;
-constexpr int kStackLarge = 48;
+// Traversal stack depths with compiled kernel variants (entries of 8
+// bytes per thread in shared memory), and the default trace block size.
+constexpr int kStacks[3] = {24, 32, 48};
+constexpr int kStackMax = 48;
 constexpr int kTraceBlock = 128;
+constexpr uint32_t kMaxScenes = 4096;
+constexpr int kMaxEvents = 512;
 
 // Device allocation that grows on demand.
 struct DevBuf {
@@ -55,25 +65,47 @@ struct DevBuf {
 	template <class T> T *as() const { return static_cast<T *>(p); }
 };
 
+// One scene of a context: its render data and where its pieces sit in the
+// context's shared arrays.
+struct SceneHost {
+	nb_rdata *rd = nullptr;
+	std::unordered_map<uint32_t, uint32_t> root_of; // triofs -> BLAS root
+	uint32_t nrm_base = 0, mtl_base = 0, inst_base = 0, ntri = 0, nmtl = 0;
+	uint32_t blas_depth = 0, tlas_depth = 0, tlas_root = 0;
+	uint32_t depth = 1;   // max path depth of this scene
+	std::vector<nb_glight> lights;
+	uint32_t light_off = 0;
+	float    light_area = 0.0f;
+	// frame layout (rendgpu_resaccum)
+	uint32_t W = 0, H = 0, spp = 0;
+	uint32_t path_base = 0, pix_base = 0, slot_base = 0, nslots = 0;
+};
+
 struct Ctx {
-	nb_rdata    *rd = nullptr;
+	std::vector<SceneHost> sc;
+	nb_rdata    *rd = nullptr;  // sc[0].rd
+	bool         batch = false; // created by rendgpu_batch_init
 	rendgpu_cfg  cfg{};
+	rendgpu_tune tune{};        // 0 fields: defaults
 	int          device = 0;
 	int          nsm = 148;
 	cudaStream_t stream = nullptr;
-	// scene
-	DevBuf blas, tris, tlas, irefs, insts, nrms, mtls, lights;
-	std::unordered_map<uint32_t, uint32_t> root_of; // triofs -> BLAS root
-	std::unordered_map<uint32_t, uint32_t> depth_of; // triofs -> BLAS depth
-	uint32_t blas_depth = 0, tlas_depth = 0;
-	std::vector<nb_glight> host_lights;
-	float    light_area = 0.0f;
+	// scenes: BLAS nodes and triangles, TLAS nodes and instance refs,
+	// instances, normals, materials, lights; scene parameter table
+	DevBuf blas, tris, tlas, irefs, insts, nrms, mtls, lights, sp;
+	uint32_t blas_depth = 0, tlas_depth = 0; // max over scenes
 	bool     have_static = false, have_dynamic = false;
-	uint32_t ntris = 0, nnodes = 0;
-	// frame
-	DevBuf q0, q1, hits, shadow, scol, pT, pL, rng, acc, buf, cnt, rays;
-	uint32_t W = 0, H = 0, spp = 0, npaths = 0;
+	uint32_t ntris = 0, nnodes = 0, ninst = 0;
+	std::vector<ScenePar> par;  // host copy of the table
+	// frame: queues (capacity qcap entries), per-path state (npaths)
+	DevBuf q0, q1, hits, shadow, scol, pT, pL, rng, acc, buf, cnt, rays, scn;
+	uint32_t npaths = 0, npix = 0, nslots = 0, qcap = 0;
 	bool     have_frame = false;
+	// captured frame (RENDGPU_FLAG_GRAPH and batches)
+	cudaGraphExec_t graph = nullptr;
+	bool     capturing = false;
+	uint32_t graph_launches = 0, graph_trace_launches = 0;
+	std::vector<unsigned long long> scn_host;
 	// batch scratch: rays, raw hits, output; berr = [count, errors, work]
 	DevBuf brays, braw, bhits, berr;
 	// neural radiance cache: FP32 master weights, Adam moments, BF16
@@ -90,12 +122,20 @@ struct Ctx {
 	rendgpu_stats st{};
 	int          last = 0;
 	std::string  msg;
-	cudaEvent_t  ev[64] = {};
+	cudaEvent_t  ev[kMaxEvents] = {};
 	int          nev = 0;
 };
 
 std::mutex g_mu;
 std::unordered_map<const void *, Ctx *> g_ctx;
+std::unordered_set<const void *> g_batches; // live rendgpu_batch handles
+
+Ctx *find_batch(const rendgpu_batch *b)
+{
+	std::lock_guard<std::mutex> lk(g_mu);
+	return g_batches.count(b) ? reinterpret_cast<Ctx *>(
+	  const_cast<rendgpu_batch *>(b)) : nullptr;
+}
 
 Ctx *find_ctx(const void *rd)
 {
@@ -131,6 +171,27 @@ uint32_t need_stack(const Ctx *c)
 	return c->tlas_depth + c->blas_depth + 2u;
 }
 
+// Traversal stack of the trace kernels: the tuned depth when it holds the
+// deepest TLAS + BLAS chain, else the smallest compiled depth that does
+// (0: none does).
+int stack_of(const Ctx *c)
+{
+	uint32_t need = need_stack(c);
+	for (int st : kStacks)
+		if ((uint32_t)st == c->tune.stack && need <= (uint32_t)st)
+			return st;
+	for (int st : kStacks)
+		if (need <= (uint32_t)st)
+			return st;
+	return 0;
+}
+
+int block_of(const Ctx *c)
+{
+	uint32_t b = c->tune.block;
+	return b == 64u || b == 256u ? (int)b : kTraceBlock;
+}
+
 DScene scene_of(const Ctx *c)
 {
 	DScene S;
@@ -142,20 +203,17 @@ DScene scene_of(const Ctx *c)
 	S.nrms = c->nrms.as<nb_rnrm>();
 	S.mtls = c->mtls.as<nb_rmtl>();
 	S.lights = c->lights.as<float4>();
-	S.nlights = (uint32_t)c->host_lights.size();
-	S.light_area = c->light_area;
-	S.bg[0] = c->rd->bgcol.x;
-	S.bg[1] = c->rd->bgcol.y;
-	S.bg[2] = c->rd->bgcol.z;
+	S.sp = c->sp.as<ScenePar>();
+	S.nscenes = (uint32_t)c->sc.size();
 	return S;
 }
 
-// Schedule of the trace kernels: cfg.sched 1..3; 0 = the default, the
-// Ylitie-style schedule (fastest measured on the 1920x1080 4 spp workload:
-// 789 vs 664 (step) vs 544 (phase) Mrays/s).
+// Schedule of the trace kernels: tune.sched, else cfg.sched, 1..3; 0 = the
+// default, the Ylitie-style schedule (fastest measured on the 1920x1080
+// 4 spp workload: 789 vs 664 (step) vs 544 (phase) Mrays/s).
 int sched_of(const Ctx *c)
 {
-	switch (c->cfg.sched) {
+	switch (c->tune.sched ? c->tune.sched : c->cfg.sched) {
 	case 1: return kSchedStep;
 	case 2: return kSchedPhase;
 	default: return kSchedYlitie;
@@ -164,16 +222,15 @@ int sched_of(const Ctx *c)
 
 // Occupancy-sized persistent grid; allows dynamic shared memory above
 // 48 KB for the deep-stack variants on first use.
-int trace_grid(Ctx *c, const void *fn, int stack)
+int trace_grid(Ctx *c, const void *fn, int stack, int block)
 {
-	size_t smem0 = (size_t)stack * kTraceBlock * sizeof(uint2);
-	if (smem0 > 48 * 1024)
+	size_t smem = (size_t)stack * block * sizeof(uint2);
+	if (smem > 48 * 1024)
 		cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		  (int)smem0);
+		  (int)smem);
 	int per_sm = 0;
-	size_t smem = (size_t)stack * kTraceBlock * sizeof(uint2);
-	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
-	  kTraceBlock, smem) != cudaSuccess || per_sm < 1)
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block,
+	  smem) != cudaSuccess || per_sm < 1)
 		per_sm = 1;
 	return per_sm * c->nsm;
 }
@@ -184,8 +241,9 @@ void trace_kernel(Ctx *c, const float4 *rays, const uint32_t *count,
                   unsigned long long *nrays)
 {
 	auto fn = k_trace<SCHED, STACK, COUNT>;
-	size_t smem = (size_t)STACK * kTraceBlock * sizeof(uint2);
-	fn<<<trace_grid(c, (const void *)fn, STACK), kTraceBlock, smem,
+	int block = block_of(c);
+	size_t smem = (size_t)STACK * block * sizeof(uint2);
+	fn<<<trace_grid(c, (const void *)fn, STACK, block), block, smem,
 	  c->stream>>>(scene_of(c), rays, count, work, hits, errs, nrays,
 	  c->rays.as<unsigned long long>() + 2);
 }
@@ -223,59 +281,75 @@ void trace_kernel_s(Ctx *c, const float4 *rays, const uint32_t *count,
 	}
 }
 
+int too_deep(Ctx *c)
+{
+	return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal stack "
+	  "(TLAS + BLAS depth + 2 = " + std::to_string(need_stack(c)) +
+	  " > " + std::to_string(kStackMax) + ")");
+}
+
 // Launch a closest-hit trace of `count` (device) rays: raw hits.
 int launch_trace(Ctx *c, const float4 *rays, const uint32_t *count,
                  uint32_t *work, float4 *hits, uint32_t *errs,
                  unsigned long long *nrays)
 {
-	uint32_t need = need_stack(c);
-	if (need <= (uint32_t)kStackSmall)
-		trace_kernel_s<kStackSmall>(c, rays, count, work, hits, errs,
-		  nrays);
-	else if (need <= (uint32_t)kStackLarge)
-		trace_kernel_s<kStackLarge>(c, rays, count, work, hits, errs,
-		  nrays);
-	else
-		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
-		  "stack");
+	switch (stack_of(c)) {
+	case 24:
+		trace_kernel_s<24>(c, rays, count, work, hits, errs, nrays);
+		break;
+	case 32:
+		trace_kernel_s<32>(c, rays, count, work, hits, errs, nrays);
+		break;
+	case 48:
+		trace_kernel_s<48>(c, rays, count, work, hits, errs, nrays);
+		break;
+	default:
+		return too_deep(c);
+	}
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
 
 template <int SCHED, int STACK>
-void shadow_kernel(Ctx *c, FrameDev &F)
+void shadow_kernel(Ctx *c, FrameDev &F, uint32_t k)
 {
 	auto fn = k_shadow<SCHED, STACK>;
-	size_t smem = (size_t)STACK * kTraceBlock * sizeof(uint2);
-	fn<<<trace_grid(c, (const void *)fn, STACK), kTraceBlock, smem,
-	  c->stream>>>(scene_of(c), F);
+	int block = block_of(c);
+	size_t smem = (size_t)STACK * block * sizeof(uint2);
+	fn<<<trace_grid(c, (const void *)fn, STACK, block), block, smem,
+	  c->stream>>>(scene_of(c), F, k);
 }
 
 template <int STACK>
-void shadow_kernel_s(Ctx *c, FrameDev &F)
+void shadow_kernel_s(Ctx *c, FrameDev &F, uint32_t k)
 {
 	switch (sched_of(c)) {
 	case kSchedPhase:
-		shadow_kernel<kSchedPhase, STACK>(c, F);
+		shadow_kernel<kSchedPhase, STACK>(c, F, k);
 		break;
 	case kSchedYlitie:
-		shadow_kernel<kSchedYlitie, STACK>(c, F);
+		shadow_kernel<kSchedYlitie, STACK>(c, F, k);
 		break;
 	default:
-		shadow_kernel<kSchedStep, STACK>(c, F);
+		shadow_kernel<kSchedStep, STACK>(c, F, k);
 	}
 }
 
-int launch_shadow(Ctx *c, FrameDev &F)
+int launch_shadow(Ctx *c, FrameDev &F, uint32_t k)
 {
-	uint32_t need = need_stack(c);
-	if (need <= (uint32_t)kStackSmall)
-		shadow_kernel_s<kStackSmall>(c, F);
-	else if (need <= (uint32_t)kStackLarge)
-		shadow_kernel_s<kStackLarge>(c, F);
-	else
-		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
-		  "stack");
+	switch (stack_of(c)) {
+	case 24:
+		shadow_kernel_s<24>(c, F, k);
+		break;
+	case 32:
+		shadow_kernel_s<32>(c, F, k);
+		break;
+	case 48:
+		shadow_kernel_s<48>(c, F, k);
+		break;
+	default:
+		return too_deep(c);
+	}
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -285,22 +359,28 @@ void occl_kernel(Ctx *c, const float4 *rays, const uint32_t *count,
                  uint32_t *work, uint8_t *occl, uint32_t *errs)
 {
 	auto fn = k_occluded<kSchedYlitie, STACK>;
-	size_t smem = (size_t)STACK * kTraceBlock * sizeof(uint2);
-	fn<<<trace_grid(c, (const void *)fn, STACK), kTraceBlock, smem,
+	int block = block_of(c);
+	size_t smem = (size_t)STACK * block * sizeof(uint2);
+	fn<<<trace_grid(c, (const void *)fn, STACK, block), block, smem,
 	  c->stream>>>(scene_of(c), rays, count, work, occl, errs);
 }
 
 int launch_occluded(Ctx *c, const float4 *rays, const uint32_t *count,
                     uint32_t *work, uint8_t *occl, uint32_t *errs)
 {
-	uint32_t need = need_stack(c);
-	if (need <= (uint32_t)kStackSmall)
-		occl_kernel<kStackSmall>(c, rays, count, work, occl, errs);
-	else if (need <= (uint32_t)kStackLarge)
-		occl_kernel<kStackLarge>(c, rays, count, work, occl, errs);
-	else
-		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
-		  "stack");
+	switch (stack_of(c)) {
+	case 24:
+		occl_kernel<24>(c, rays, count, work, occl, errs);
+		break;
+	case 32:
+		occl_kernel<32>(c, rays, count, work, occl, errs);
+		break;
+	case 48:
+		occl_kernel<48>(c, rays, count, work, occl, errs);
+		break;
+	default:
+		return too_deep(c);
+	}
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -320,10 +400,13 @@ FrameDev frame_of(Ctx *c)
 	F.buf = c->buf.as<uint32_t>();
 	F.cnt = c->cnt.as<uint32_t>();
 	F.rays = c->rays.as<unsigned long long>();
-	F.W = c->W;
-	F.H = c->H;
-	F.spp = c->spp;
+	F.scn = c->scn.as<unsigned long long>();
 	F.npaths = c->npaths;
+	F.npix = c->npix;
+	F.nq = c->nq.as<float4>();
+	F.nrec = c->nrec.as<float4>();
+	F.nq_cap = c->nq_cap;
+	F.nrec_cap = c->nrec_cap;
 	return F;
 }
 
@@ -348,7 +431,8 @@ int grid_for(const Ctx *c, uint32_t n, int block)
 
 void ev_record(Ctx *c)
 {
-	if (!(c->cfg.flags & RENDGPU_FLAG_TIMING) || c->nev >= 64)
+	if (!(c->cfg.flags & RENDGPU_FLAG_TIMING) || c->capturing ||
+	  c->nev >= kMaxEvents)
 		return;
 	if (!c->ev[c->nev])
 		cudaEventCreate(&c->ev[c->nev]);
@@ -532,98 +616,137 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 	return 0;
 }
 
-int render_frame(Ctx *c)
+// Scene parameter table of this frame from each scene's render data (its
+// camera, frame number, sizes and lights); uploaded to the device.
+int frame_params(Ctx *c, bool nrc, FrameArgs *A)
 {
-	int rc = ready(c, true);
-	if (rc)
-		return rc;
-	nb_rdata *rd = c->rd;
-	if (rd->width != c->W || rd->height != c->H || rd->spp != c->spp)
-		return fail(c, RENDGPU_ESTATE, "rdata size changed since "
-		  "rendgpu_resaccum");
-	FrameDev F = frame_of(c);
-	FrameArgs A;
-	A.seed = c->cfg.seed;
-	A.frame = rd->samples;
-	A.depth = c->cfg.mode == RENDGPU_MODE_PRIMARY ? 1u : c->cfg.max_depth;
-	A.mode = c->cfg.mode;
-	A.nrc_stride = 1;
-	A.nrc_offset = 0;
-	bool nrc = c->cfg.mode == RENDGPU_MODE_NRC;
-	if (nrc) {
-		int rc2 = nrc_frame_buffers(c);
-		if (rc2)
-			return rc2;
-		A.nrc_stride = c->nrc_stride;
-		A.nrc_offset = (rd->samples * 7919u) % c->nrc_stride;
-		// warm-up: the first frames trace every path unbiased (as
-		// training paths) while the cache trains
-		if (c->nrc_frames < nrc_warmup(c))
-			A.nrc_stride = 1;
-		c->nrc_frames++;
+	size_t n = c->sc.size();
+	c->par.assign(n, ScenePar{});
+	A->mode = c->cfg.mode;
+	A->depth = 1;
+	for (size_t i = 0; i < n; i++) {
+		const SceneHost &h = c->sc[i];
+		const nb_rdata *rd = h.rd;
+		if (rd->width != h.W || rd->height != h.H ||
+		  (rd->spp ? rd->spp : 1u) != h.spp)
+			return fail(c, RENDGPU_ESTATE, "rdata size changed since "
+			  "rendgpu_resaccum");
+		ScenePar &P = c->par[i];
+		P.tlas_root = h.tlas_root;
+		P.light_off = h.light_off;
+		P.light_cnt = (uint32_t)h.lights.size();
+		P.depth = c->cfg.mode == RENDGPU_MODE_PRIMARY ? 1u : h.depth;
+		A->depth = std::max(A->depth, P.depth);
+		P.W = h.W;
+		P.H = h.H;
+		P.spp = h.spp;
+		P.frame = rd->samples;
+		P.path_base = h.path_base;
+		P.pix_base = h.pix_base;
+		P.slot_base = h.slot_base;
+		P.nrc_stride = 1;
+		P.nrc_offset = 0;
+		if (nrc) {
+			// warm-up: the first frames trace every path unbiased (as
+			// training paths) while the cache trains
+			P.nrc_stride = c->nrc_frames < nrc_warmup(c) ? 1u :
+			  c->nrc_stride;
+			P.nrc_offset = (rd->samples * 7919u) % P.nrc_stride;
+		}
+		P.light_area = h.light_area;
+		P.inv = 1.0f / (float)(rd->samples + rd->spp);
+		P.bg[0] = rd->bgcol.x;
+		P.bg[1] = rd->bgcol.y;
+		P.bg[2] = rd->bgcol.z;
+		const nb_rcam &cam = rd->cam;
+		P.eye[0] = cam.eye.x; P.eye[1] = cam.eye.y; P.eye[2] = cam.eye.z;
+		P.ri[0] = cam.ri.x; P.ri[1] = cam.ri.y; P.ri[2] = cam.ri.z;
+		P.up[0] = cam.up.x; P.up[1] = cam.up.y; P.up[2] = cam.up.z;
+		P.fwd[0] = cam.fwd.x; P.fwd[1] = cam.fwd.y; P.fwd[2] = cam.fwd.z;
+		P.rw = cam.rw8[0];
+		P.rh = cam.rh8[0];
+		P.fovfdist = cam.fovfdist8[0];
+		P.aspect = cam.aspect8[0];
+		P.fdist = cam.fdist8[0];
+		P.focrad = cam.focrad8[0];
+		P.tanfangle = cam.tanfangle;
+		P.seed = c->cfg.seed;
 	}
-	const nb_rcam &cam = rd->cam;
-	A.eye[0] = cam.eye.x; A.eye[1] = cam.eye.y; A.eye[2] = cam.eye.z;
-	A.ri[0] = cam.ri.x; A.ri[1] = cam.ri.y; A.ri[2] = cam.ri.z;
-	A.up[0] = cam.up.x; A.up[1] = cam.up.y; A.up[2] = cam.up.z;
-	A.fwd[0] = cam.fwd.x; A.fwd[1] = cam.fwd.y; A.fwd[2] = cam.fwd.z;
-	A.rw = cam.rw8[0];
-	A.rh = cam.rh8[0];
-	A.fovfdist = cam.fovfdist8[0];
-	A.aspect = cam.aspect8[0];
-	A.fdist = cam.fdist8[0];
-	A.focrad = cam.focrad8[0];
-	A.tanfangle = cam.tanfangle;
-	F.nq = c->nq.as<float4>();
-	F.nrec = c->nrec.as<float4>();
-	F.nq_cap = c->nq_cap;
-	F.nrec_cap = c->nrec_cap;
+	NB_CK(c, cudaMemcpyAsync(c->sp.p, c->par.data(), n * sizeof(ScenePar),
+	  cudaMemcpyHostToDevice, c->stream));
+	return 0;
+}
+
+void drop_graph(Ctx *c)
+{
+	if (c->graph)
+		cudaGraphExecDestroy(c->graph);
+	c->graph = nullptr;
+}
+
+// Event indices of the per-kernel timing of one directly launched frame.
+struct FrameEvents {
+	std::vector<int> trace, shadow;
+	int nrc = -1, train = -1;
+};
+
+// The launch sequence of one frame: every wave of camera slots through all
+// bounces (trace, shade, shadow), cache inference, accumulation, cache
+// training.  Sizes and counts are read on the device, so the sequence is
+// the same every frame and can be captured once.
+int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
+                  bool nrc, FrameEvents *E)
+{
 	DScene S = scene_of(c);
-	c->nev = 0;
+	int rc = 0;
 	c->st.launches = 0;
 	c->st.trace_launches = 0;
 	NB_CK(c, cudaMemsetAsync(c->cnt.p, 0, 64 * sizeof(uint32_t), c->stream));
 	NB_CK(c, cudaMemsetAsync(c->rays.p, 0, 4 * sizeof(unsigned long long),
 	  c->stream));
+	NB_CK(c, cudaMemsetAsync(c->scn.p, 0, c->sc.size() * 2 *
+	  sizeof(unsigned long long), c->stream));
 	ev_record(c); // 0
-	uint32_t tiles = ((c->W + 7u) >> 3) * ((c->H + 3u) >> 2) * 32u * c->spp;
-	k_gen<<<grid_for(c, tiles, 256), 256, 0, c->stream>>>(F, A);
-	NB_CK(c, cudaGetLastError());
-	c->st.launches++;
-	ev_record(c); // 1
-	std::vector<int> trace_ev, shadow_ev;
-	for (uint32_t k = 0; k < A.depth; k++) {
-		uint32_t cur = k & 1u;
-		trace_ev.push_back(c->nev);
-		ev_record(c);
-		rc = launch_trace(c, F.q[cur], F.cnt + cur, F.cnt + 4, F.hits,
-		  F.cnt + 3, F.rays);
-		if (rc)
-			return rc;
-		ev_record(c);
-		c->st.launches++;
-		c->st.trace_launches++;
-		NB_CK(c, cudaMemsetAsync(F.cnt + (cur ^ 1u), 0, sizeof(uint32_t),
-		  c->stream));
-		NB_CK(c, cudaMemsetAsync(F.cnt + 2, 0, sizeof(uint32_t),
-		  c->stream));
-		k_shade<<<grid_for(c, c->npaths, 256), 256, 0, c->stream>>>(S, F,
-		  A, cur, k);
+	for (uint32_t lo = 0; lo < c->nslots; lo += c->qcap) {
+		uint32_t hi = std::min(c->nslots, lo + c->qcap);
+		NB_CK(c, cudaMemsetAsync(F.cnt, 0, sizeof(uint32_t), c->stream));
+		k_gen<<<grid_for(c, hi - lo, 256), 256, 0, c->stream>>>(S, F, A, lo,
+		  hi);
 		NB_CK(c, cudaGetLastError());
 		c->st.launches++;
-		if (A.mode != RENDGPU_MODE_PRIMARY) {
-			shadow_ev.push_back(c->nev);
+		for (uint32_t k = 0; k < A.depth; k++) {
+			uint32_t cur = k & 1u;
+			E->trace.push_back(c->nev);
 			ev_record(c);
-			rc = launch_shadow(c, F);
+			rc = launch_trace(c, F.q[cur], F.cnt + cur, F.cnt + 4, F.hits,
+			  F.cnt + 3, F.rays);
 			if (rc)
 				return rc;
 			ev_record(c);
 			c->st.launches++;
+			c->st.trace_launches++;
+			NB_CK(c, cudaMemsetAsync(F.cnt + (cur ^ 1u), 0,
+			  sizeof(uint32_t), c->stream));
+			NB_CK(c, cudaMemsetAsync(F.cnt + 2, 0, sizeof(uint32_t),
+			  c->stream));
+			k_shade<<<grid_for(c, hi - lo, 256), 256, 0, c->stream>>>(S, F,
+			  A, cur, k);
+			NB_CK(c, cudaGetLastError());
+			c->st.launches++;
+			if (A.mode != RENDGPU_MODE_PRIMARY) {
+				E->shadow.push_back(c->nev);
+				ev_record(c);
+				rc = launch_shadow(c, const_cast<FrameDev &>(F), k);
+				if (rc)
+					return rc;
+				ev_record(c);
+				c->st.launches++;
+			}
 		}
 	}
-	int nrc_ev = c->nev;
 	if (nrc) {
 		// cache inference for the queries of this frame
+		E->nrc = c->nev;
 		ev_record(c);
 		k_nrc_encode_entries<<<grid_for(c, c->nq_cap, 128), 128, 0,
 		  c->stream>>>(F.nq, 4u, F.cnt + 40, c->nq_cap, c->box,
@@ -638,17 +761,13 @@ int render_frame(Ctx *c)
 		c->st.launches += 3;
 		ev_record(c);
 	}
-	int acc_ev = c->nev;
-	ev_record(c);
-	float inv = 1.0f / (float)(rd->samples + rd->spp);
-	k_accum<<<grid_for(c, c->W * c->H, 256), 256, 0, c->stream>>>(F, inv);
+	k_accum<<<grid_for(c, c->npix, 256), 256, 0, c->stream>>>(S, F);
 	NB_CK(c, cudaGetLastError());
 	c->st.launches++;
-	ev_record(c);
-	int train_ev = c->nev;
 	if (nrc) {
 		// train on this frame's records: targets from the finished paths,
 		// then kNrcSteps Adam steps of kNrcBatch samples each
+		E->train = c->nev;
 		ev_record(c);
 		k_nrc_targets<<<grid_for(c, c->nrec_cap, 256), 256, 0, c->stream>>>(
 		  F.nrec, F.cnt + 41, c->nrec_cap, F.pL, c->rtgt.as<float4>());
@@ -665,12 +784,93 @@ int render_frame(Ctx *c)
 		c->st.launches += 2 + 2 * kNrcSteps;
 		ev_record(c);
 	}
+	ev_record(c); // last
+	return 0;
+}
+
+// Capture the frame's launch sequence into a graph (once per layout).
+int capture_frame(Ctx *c, const FrameDev &F, const FrameArgs &A)
+{
+	FrameEvents E;
+	NB_CK(c, cudaStreamBeginCapture(c->stream,
+	  cudaStreamCaptureModeRelaxed));
+	c->capturing = true;
+	int rc = enqueue_frame(c, F, A, false, &E);
+	c->capturing = false;
+	cudaGraph_t g = nullptr;
+	cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+	if (rc) {
+		if (g)
+			cudaGraphDestroy(g);
+		return rc;
+	}
+	if (e != cudaSuccess)
+		return cuda_fail(c, e, "cudaStreamEndCapture");
+	e = cudaGraphInstantiate(&c->graph, g, 0);
+	cudaGraphDestroy(g);
+	if (e != cudaSuccess) {
+		c->graph = nullptr;
+		return cuda_fail(c, e, "cudaGraphInstantiate");
+	}
+	c->graph_launches = c->st.launches;
+	c->graph_trace_launches = c->st.trace_launches;
+	return 0;
+}
+
+bool use_graph(const Ctx *c)
+{
+	return c->cfg.mode != RENDGPU_MODE_NRC &&
+	  (c->batch || (c->cfg.flags & RENDGPU_FLAG_GRAPH));
+}
+
+int render_frame(Ctx *c)
+{
+	int rc = ready(c, true);
+	if (rc)
+		return rc;
+	bool nrc = c->cfg.mode == RENDGPU_MODE_NRC;
+	if (nrc) {
+		rc = nrc_frame_buffers(c);
+		if (rc)
+			return rc;
+	}
+	FrameArgs A;
+	rc = frame_params(c, nrc, &A);
+	if (rc)
+		return rc;
+	if (nrc)
+		c->nrc_frames++;
+	FrameDev F = frame_of(c);
+	c->nev = 0;
+	FrameEvents E;
+	bool graph = use_graph(c);
+	if (graph) {
+		if (!c->graph) {
+			rc = capture_frame(c, F, A);
+			if (rc)
+				return rc;
+		}
+		ev_record(c);
+		NB_CK(c, cudaGraphLaunch(c->graph, c->stream));
+		ev_record(c);
+		c->st.launches = c->graph_launches;
+		c->st.trace_launches = c->graph_trace_launches;
+	} else {
+		rc = enqueue_frame(c, F, A, nrc, &E);
+		if (rc)
+			return rc;
+	}
 	unsigned long long hr[4];
 	uint32_t hc[64];
+	size_t ns = c->sc.size();
+	c->scn_host.assign(2 * ns, 0ull);
 	NB_CK(c, cudaMemcpyAsync(hr, c->rays.p, sizeof(hr),
 	  cudaMemcpyDeviceToHost, c->stream));
 	NB_CK(c, cudaMemcpyAsync(hc, c->cnt.p, sizeof(hc),
 	  cudaMemcpyDeviceToHost, c->stream));
+	if (ns > 1)
+		NB_CK(c, cudaMemcpyAsync(c->scn_host.data(), c->scn.p, 2 * ns *
+		  sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
 	NB_CK(c, cudaStreamSynchronize(c->stream));
 	c->st.closest_rays = hr[0];
 	c->st.node_visits = hr[2];
@@ -678,6 +878,10 @@ int render_frame(Ctx *c)
 	c->st.shadow_rays = hr[1];
 	c->st.rays = hr[0] + hr[1];
 	c->st.device_errors = hc[3];
+	if (ns == 1) {
+		c->scn_host[0] = hr[0];
+		c->scn_host[1] = hr[1];
+	}
 	if (nrc) {
 		// loss of the last Adam step (partials of its CTAs)
 		float lp[1024];
@@ -696,20 +900,20 @@ int render_frame(Ctx *c)
 		c->st.bounce_closest[k] = hc[8 + k];
 		c->st.bounce_shadow[k] = hc[24 + k];
 	}
-	c->st.max_stack = need_stack(c);
+	c->st.max_stack = (uint32_t)stack_of(c);
 	if (c->cfg.flags & RENDGPU_FLAG_TIMING) {
 		c->st.ms_frame = ev_ms(c, 0, c->nev - 1);
 		float tr = 0.0f, sh = 0.0f;
-		for (int e : trace_ev)
+		for (int e : E.trace)
 			tr += ev_ms(c, e, e + 1);
-		for (int e : shadow_ev)
+		for (int e : E.shadow)
 			sh += ev_ms(c, e, e + 1);
 		c->st.ms_trace = tr;
 		c->st.ms_shadow = sh;
-		c->st.ms_nrc = nrc ? ev_ms(c, nrc_ev, nrc_ev + 1) +
-		  ev_ms(c, train_ev, train_ev + 1) : 0.0f;
-		c->st.ms_shade = c->st.ms_frame - tr - sh - c->st.ms_nrc;
-		(void)acc_ev;
+		c->st.ms_nrc = nrc ? ev_ms(c, E.nrc, E.nrc + 1) +
+		  ev_ms(c, E.train, E.train + 1) : 0.0f;
+		c->st.ms_shade = graph ? 0.0f :
+		  c->st.ms_frame - tr - sh - c->st.ms_nrc;
 	}
 	if (hc[3])
 		return fail(c, RENDGPU_EDEVICE, "rays abandoned on the device "
@@ -719,8 +923,9 @@ int render_frame(Ctx *c)
 
 void free_ctx(Ctx *c)
 {
+	drop_graph(c);
 	DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs, &c->insts,
-	  &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits, &c->shadow,
+	  &c->nrms, &c->mtls, &c->lights, &c->sp, &c->scn, &c->q0, &c->q1, &c->hits, &c->shadow,
 	  &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
 	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_wf,
 	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
@@ -728,7 +933,7 @@ void free_ctx(Ctx *c)
 	  &c->rtgt};
 	for (DevBuf *b : bufs)
 		b->release();
-	for (int i = 0; i < 64; i++)
+	for (int i = 0; i < kMaxEvents; i++)
 		if (c->ev[i])
 			cudaEventDestroy(c->ev[i]);
 	if (c->stream)
@@ -739,7 +944,7 @@ void free_ctx(Ctx *c)
 uint64_t held_bytes(const Ctx *c)
 {
 	const DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs,
-	  &c->insts, &c->nrms, &c->mtls, &c->lights, &c->q0, &c->q1, &c->hits,
+	  &c->insts, &c->nrms, &c->mtls, &c->lights, &c->sp, &c->scn, &c->q0, &c->q1, &c->hits,
 	  &c->shadow, &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf,
 	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
 	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
@@ -749,6 +954,467 @@ uint64_t held_bytes(const Ctx *c)
 	for (const DevBuf *b : bufs)
 		s += b->cap;
 	return s;
+}
+
+// A context over n scenes (n = 1 for the rdata API); max_depth[i] (or
+// cfg->max_depth when null) bounds scene i's paths.
+int new_ctx(nb_rdata *const *rds, uint32_t n, const uint32_t *max_depth,
+            const rendgpu_cfg *cfg, Ctx **out)
+{
+	if (!rds || n == 0 || n > kMaxScenes || !cfg ||
+	  cfg->size < sizeof(rendgpu_cfg) - 8 * sizeof(uint32_t))
+		return RENDGPU_EINVAL;
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+		return RENDGPU_ENODEV;
+	if (cfg->device < 0 || cfg->device >= ndev)
+		return RENDGPU_EINVAL;
+	if (cfg->mode > RENDGPU_MODE_NRC || cfg->max_depth < 1 ||
+	  cfg->max_depth > 1024 || cfg->sched > 3)
+		return RENDGPU_EINVAL;
+	for (uint32_t i = 0; i < n; i++) {
+		if (!rds[i])
+			return RENDGPU_EINVAL;
+		if (max_depth && (max_depth[i] < 1 || max_depth[i] > 1024))
+			return RENDGPU_EINVAL;
+	}
+	Ctx *c = new Ctx;
+	c->rd = rds[0];
+	c->sc.resize(n);
+	for (uint32_t i = 0; i < n; i++) {
+		c->sc[i].rd = rds[i];
+		c->sc[i].depth = max_depth ? max_depth[i] : cfg->max_depth;
+	}
+	c->cfg = *cfg;
+	c->tune.block = cfg->block;
+	c->device = cfg->device;
+	if (cudaSetDevice(c->device) != cudaSuccess ||
+	  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount,
+	  c->device) != cudaSuccess ||
+	  cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) !=
+	  cudaSuccess) {
+		free_ctx(c);
+		return RENDGPU_ECUDA;
+	}
+	if (c->cnt.ensure(64 * sizeof(uint32_t)) != cudaSuccess ||
+	  c->rays.ensure(4 * sizeof(unsigned long long)) != cudaSuccess ||
+	  c->berr.ensure(16) != cudaSuccess ||
+	  c->sp.ensure(n * sizeof(ScenePar)) != cudaSuccess ||
+	  c->scn.ensure(n * 16) != cudaSuccess) {
+		free_ctx(c);
+		return RENDGPU_ENOMEM;
+	}
+	*out = c;
+	return 0;
+}
+
+// ------------------------------------------------------------- uploads --
+
+// BLAS of every scene (rend_prepstatic output) into the shared node and
+// triangle arrays; normals and materials of all scenes back to back, with
+// each scene's material ids offset by its material base.
+int upload_static_all(Ctx *c)
+{
+	NB_CK(c, cudaSetDevice(c->device));
+	std::vector<nb_qnode> nodes;
+	std::vector<nb_gtri> tris;
+	uint32_t nrm_base = 0, mtl_base = 0;
+	c->blas_depth = 0;
+	for (SceneHost &h : c->sc) {
+		nb_rdata *rd = h.rd;
+		if (!rd->bnodes || !rd->tris || !rd->nrms || !rd->mtls ||
+		  !rd->insts)
+			return fail(c, RENDGPU_EINVAL, "render data not initialised");
+		if (rd->instcnt == 0 || rd->instcnt > (1u << NB_INST_ID_BITS))
+			return fail(c, RENDGPU_ELIMIT, "instance count outside "
+			  "1..4096 (INST_ID_BITS = 12, rend.c:24)");
+		h.root_of.clear();
+		h.blas_depth = 0;
+		uint32_t maxtri = 0, maxmtl = 0;
+		for (uint32_t i = 0; i < rd->instcnt; i++) {
+			const nb_rinst &ri = rd->insts[i];
+			if (ri.tricnt == 0)
+				return fail(c, RENDGPU_EINVAL, "instance without "
+				  "triangles");
+			if (ri.tricnt > (1u << (32 - NB_INST_ID_BITS)))
+				return fail(c, RENDGPU_ELIMIT, "mesh above 2^20 "
+				  "triangles");
+			maxtri = std::max(maxtri, ri.triofs + ri.tricnt);
+			if (h.root_of.count(ri.triofs))
+				continue;
+			uint32_t root = 0;
+			bvh_stats bs;
+			std::string err;
+			if (!convert_blas(rd, ri.triofs, nodes, tris, &root, &bs, &err))
+				return fail(c, RENDGPU_EINVAL, "BLAS of triofs " +
+				  std::to_string(ri.triofs) + ": " + err);
+			h.root_of[ri.triofs] = root;
+			h.blas_depth = std::max(h.blas_depth, bs.depth);
+		}
+		for (uint32_t t = 0; t < maxtri; t++)
+			maxmtl = std::max(maxmtl, rd->nrms[t].mtlid + 1u);
+		h.nrm_base = nrm_base;
+		h.mtl_base = mtl_base;
+		h.ntri = maxtri;
+		h.nmtl = maxmtl;
+		if ((uint64_t)nrm_base + maxtri > 0xffffffffull)
+			return fail(c, RENDGPU_ELIMIT, "more than 2^32 triangles");
+		nrm_base += maxtri;
+		mtl_base += maxmtl;
+		c->blas_depth = std::max(c->blas_depth, h.blas_depth);
+	}
+	NB_CK(c, c->blas.ensure(nodes.size() * sizeof(nb_qnode)));
+	NB_CK(c, c->tris.ensure(tris.size() * sizeof(nb_gtri)));
+	NB_CK(c, c->nrms.ensure((size_t)nrm_base * sizeof(nb_rnrm)));
+	NB_CK(c, c->mtls.ensure((size_t)mtl_base * sizeof(nb_rmtl)));
+	NB_CK(c, cudaMemcpyAsync(c->blas.p, nodes.data(), nodes.size() *
+	  sizeof(nb_qnode), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemcpyAsync(c->tris.p, tris.data(), tris.size() *
+	  sizeof(nb_gtri), cudaMemcpyHostToDevice, c->stream));
+	std::vector<nb_rnrm> nr;
+	for (const SceneHost &h : c->sc) {
+		nb_rnrm *dst = c->nrms.as<nb_rnrm>() + h.nrm_base;
+		const nb_rnrm *src = h.rd->nrms;
+		if (h.mtl_base) {
+			nr.assign(src, src + h.ntri);
+			for (nb_rnrm &n : nr)
+				n.mtlid += h.mtl_base;
+			src = nr.data();
+		}
+		NB_CK(c, cudaMemcpyAsync(dst, src, (size_t)h.ntri *
+		  sizeof(nb_rnrm), cudaMemcpyHostToDevice, c->stream));
+		// (a copy from pageable memory returns once the source has been
+		// read, so `nr` may be refilled for the next scene)
+		NB_CK(c, cudaMemcpyAsync(c->mtls.as<nb_rmtl>() + h.mtl_base,
+		  h.rd->mtls, (size_t)h.nmtl * sizeof(nb_rmtl),
+		  cudaMemcpyHostToDevice, c->stream));
+	}
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	c->ntris = (uint32_t)tris.size();
+	c->nnodes = (uint32_t)nodes.size();
+	drop_graph(c);
+	c->have_static = true;
+	c->have_dynamic = false;
+	return 0;
+}
+
+// TLAS, instances and lights of every scene (rend_prepdynamic output).
+// Instance references are global, so hit ids carry the instance's index
+// among all scenes' instances (at most 4096 in total).
+int upload_dynamic_all(Ctx *c)
+{
+	if (!c->have_static)
+		return fail(c, RENDGPU_ESTATE, "upload_static must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	std::vector<nb_qnode> nodes;
+	std::vector<uint32_t> irefs;
+	std::vector<nb_ginst> gi;
+	std::vector<nb_glight> lights;
+	c->tlas_depth = 0;
+	for (SceneHost &h : c->sc) {
+		nb_rdata *rd = h.rd;
+		h.inst_base = (uint32_t)gi.size();
+		if (gi.size() + rd->instcnt > (1u << NB_INST_ID_BITS))
+			return fail(c, RENDGPU_ELIMIT, "more than 4096 instances "
+			  "in the context (hit ids keep 12 instance bits, "
+			  "rend.c:24)");
+		bvh_stats bs;
+		std::string err;
+		if (!convert_tlas(rd, nodes, irefs, h.inst_base, &h.tlas_root, &bs,
+		  &err))
+			return fail(c, RENDGPU_EINVAL, "TLAS: " + err);
+		h.tlas_depth = bs.depth;
+		c->tlas_depth = std::max(c->tlas_depth, bs.depth);
+		for (uint32_t i = 0; i < rd->instcnt; i++) {
+			const nb_rinst &ri = rd->insts[i];
+			auto it = h.root_of.find(ri.triofs);
+			if (it == h.root_of.end())
+				return fail(c, RENDGPU_ESTATE, "instance mesh not "
+				  "uploaded by upload_static");
+			nb_ginst g;
+			std::memcpy(g.m, ri.globinv, sizeof(g.m));
+			g.root = it->second;
+			g.triofs = h.nrm_base + ri.triofs;
+			g.flags = ri.flags;
+			g.pad = 0;
+			gi.push_back(g);
+		}
+		h.light_area = build_lights(rd, h.lights);
+		h.light_off = (uint32_t)lights.size();
+		lights.insert(lights.end(), h.lights.begin(), h.lights.end());
+	}
+	{
+		// radiance-cache encoding box: the first scene's instance bounds
+		const nb_rdata *rd = c->sc[0].rd;
+		float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+		float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+		for (uint32_t i = 0; i < rd->instcnt; i++) {
+			const nb_aabb &b = rd->aabbs[i];
+			float bl[3] = {b.min.x, b.min.y, b.min.z};
+			float bh[3] = {b.max.x, b.max.y, b.max.z};
+			for (int a = 0; a < 3; a++) {
+				lo[a] = std::min(lo[a], bl[a]);
+				hi[a] = std::max(hi[a], bh[a]);
+			}
+		}
+		for (int a = 0; a < 3; a++) {
+			c->box.lo[a] = lo[a];
+			c->box.inv[a] = hi[a] > lo[a] ? 1.0f / (hi[a] - lo[a]) : 1.0f;
+		}
+	}
+	c->ninst = (uint32_t)gi.size();
+	NB_CK(c, c->tlas.ensure(nodes.size() * sizeof(nb_qnode)));
+	NB_CK(c, c->irefs.ensure(irefs.size() * sizeof(uint32_t)));
+	NB_CK(c, c->insts.ensure(gi.size() * sizeof(nb_ginst)));
+	NB_CK(c, c->lights.ensure(lights.size() * sizeof(nb_glight)));
+	NB_CK(c, c->sp.ensure(c->sc.size() * sizeof(ScenePar)));
+	NB_CK(c, cudaMemcpyAsync(c->tlas.p, nodes.data(), nodes.size() *
+	  sizeof(nb_qnode), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemcpyAsync(c->irefs.p, irefs.data(), irefs.size() *
+	  sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemcpyAsync(c->insts.p, gi.data(), gi.size() *
+	  sizeof(nb_ginst), cudaMemcpyHostToDevice, c->stream));
+	if (!lights.empty())
+		NB_CK(c, cudaMemcpyAsync(c->lights.p, lights.data(),
+		  lights.size() * sizeof(nb_glight), cudaMemcpyHostToDevice,
+		  c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	c->st.h2d_bytes = nodes.size() * sizeof(nb_qnode) + irefs.size() *
+	  sizeof(uint32_t) + gi.size() * sizeof(nb_ginst) +
+	  lights.size() * sizeof(nb_glight);
+	drop_graph(c);
+	c->have_dynamic = true;
+	if (!stack_of(c))
+		return too_deep(c);
+	return 0;
+}
+
+// Frame buffers for every scene's width, height and spp: per-path state
+// for all paths, ray queues for one wave of tune.queue camera slots (all
+// slots when 0); accumulation cleared.
+int alloc_frame(Ctx *c)
+{
+	NB_CK(c, cudaSetDevice(c->device));
+	uint64_t np = 0, npix = 0, nslots = 0;
+	for (SceneHost &h : c->sc) {
+		const nb_rdata *rd = h.rd;
+		uint32_t spp = rd->spp ? rd->spp : 1u;
+		uint64_t p = (uint64_t)rd->width * rd->height * spp;
+		if (p == 0)
+			return fail(c, RENDGPU_ELIMIT, "empty image");
+		h.W = rd->width;
+		h.H = rd->height;
+		h.spp = spp;
+		h.path_base = (uint32_t)np;
+		h.pix_base = (uint32_t)npix;
+		h.slot_base = (uint32_t)nslots;
+		h.nslots = ((h.W + 7u) >> 3) * ((h.H + 3u) >> 2) * 32u * spp;
+		np += p;
+		npix += (uint64_t)rd->width * rd->height;
+		nslots += h.nslots;
+		if (nslots > 0x7fffffffull)
+			return fail(c, RENDGPU_ELIMIT, "width*height*spp over all "
+			  "scenes outside 1..2^31-1");
+	}
+	uint64_t q = c->tune.queue ? std::min<uint64_t>(c->tune.queue, nslots) :
+	  nslots;
+	q = std::max<uint64_t>(q, 1);
+	NB_CK(c, c->q0.ensure(q * 32));
+	NB_CK(c, c->q1.ensure(q * 32));
+	NB_CK(c, c->hits.ensure(q * 16));
+	NB_CK(c, c->shadow.ensure(q * 32));
+	NB_CK(c, c->scol.ensure(q * 16));
+	NB_CK(c, c->pT.ensure(np * 16));
+	NB_CK(c, c->pL.ensure(np * 16));
+	NB_CK(c, c->rng.ensure(np * 8));
+	NB_CK(c, c->acc.ensure(npix * 12));
+	NB_CK(c, c->buf.ensure(npix * 4));
+	NB_CK(c, c->scn.ensure(c->sc.size() * 16));
+	NB_CK(c, c->sp.ensure(c->sc.size() * sizeof(ScenePar)));
+	c->npaths = (uint32_t)np;
+	c->npix = (uint32_t)npix;
+	c->nslots = (uint32_t)nslots;
+	c->qcap = (uint32_t)q;
+	c->have_frame = true;
+	drop_graph(c);
+	NB_CK(c, cudaMemsetAsync(c->acc.p, 0, npix * 12, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->buf.p, 0, npix * 4, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	return 0;
+}
+
+// Copy accumulation (which & 1) and/or ARGB8 (which & 2) of every scene
+// into its rd->acc / rd->buf.
+int readback_all(Ctx *c, int which)
+{
+	if (!c->have_frame)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_resaccum must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	c->st.d2h_bytes = 0;
+	for (const SceneHost &h : c->sc) {
+		size_t npix = (size_t)h.W * h.H;
+		if ((which & 1) && h.rd->acc) {
+			NB_CK(c, cudaMemcpyAsync(h.rd->acc, c->acc.as<float>() +
+			  3 * (size_t)h.pix_base, npix * 12, cudaMemcpyDeviceToHost,
+			  c->stream));
+			c->st.d2h_bytes += npix * 12;
+		}
+		if ((which & 2) && h.rd->buf) {
+			NB_CK(c, cudaMemcpyAsync(h.rd->buf, c->buf.as<uint32_t>() +
+			  h.pix_base, npix * 4, cudaMemcpyDeviceToHost, c->stream));
+			c->st.d2h_bytes += npix * 4;
+		}
+	}
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	return 0;
+}
+
+// ------------------------------------------------------------- tuning --
+
+bool tune_valid(const rendgpu_tune *t)
+{
+	return t && (t->block == 0 || t->block == 64 || t->block == 128 ||
+	  t->block == 256) && (t->stack == 0 || t->stack == 24 ||
+	  t->stack == 32 || t->stack == 48) && t->sched <= 3;
+}
+
+// Apply launch parameters; a new queue capacity re-sizes the queues (and
+// so clears the accumulator).
+int set_tune(Ctx *c, const rendgpu_tune *t)
+{
+	if (!tune_valid(t))
+		return fail(c, RENDGPU_EINVAL, "tune: block 0/64/128/256, stack "
+		  "0/24/32/48, sched 0..3");
+	bool requeue = t->queue != c->tune.queue;
+	c->tune.block = t->block;
+	c->tune.stack = t->stack;
+	c->tune.queue = t->queue;
+	c->tune.sched = t->sched;
+	drop_graph(c);
+	if (requeue && c->have_frame)
+		return alloc_frame(c);
+	return 0;
+}
+
+// The settings in effect (defaults resolved).
+rendgpu_tune effective_tune(const Ctx *c)
+{
+	rendgpu_tune t{};
+	t.block = (uint32_t)block_of(c);
+	t.stack = c->have_dynamic ? (uint32_t)stack_of(c) : c->tune.stack;
+	t.queue = c->tune.queue;
+	int sc = sched_of(c);
+	t.sched = sc == kSchedStep ? 1u : sc == kSchedPhase ? 2u : 3u;
+	return t;
+}
+
+// Median device time of `frames` frames with setting t (after one untimed
+// frame that also captures the graph).
+int tune_measure(Ctx *c, const rendgpu_tune &t, uint32_t frames, float *ms)
+{
+	int rc = set_tune(c, &t);
+	if (rc)
+		return rc;
+	rc = render_frame(c);
+	if (rc)
+		return rc;
+	std::vector<float> v;
+	for (uint32_t f = 0; f < frames; f++) {
+		rc = render_frame(c);
+		if (rc)
+			return rc;
+		v.push_back(c->st.ms_frame);
+	}
+	std::sort(v.begin(), v.end());
+	*ms = v[v.size() / 2];
+	return 0;
+}
+
+// Coordinate-descent autotuner over the traversal schedule, the trace
+// block size, the stack depth and the queue capacity: each knob in turn
+// takes the value with the lowest measured frame time, the others held at
+// the best so far.  Frames re-render the current sample index (rd->samples
+// is not advanced); the accumulator is cleared afterwards.
+int autotune(Ctx *c, uint32_t frames, rendgpu_tune *best_out,
+             rendgpu_tune *log, uint32_t cap, uint32_t *nlog)
+{
+	int rc = ready(c, true);
+	if (rc)
+		return rc;
+	if (c->cfg.mode == RENDGPU_MODE_NRC)
+		return fail(c, RENDGPU_EINVAL, "autotune: frames of the radiance "
+		  "cache train it; tune in PATH mode");
+	frames = std::max(frames, 1u);
+	uint32_t flags = c->cfg.flags;
+	c->cfg.flags = (flags | RENDGPU_FLAG_TIMING) & ~RENDGPU_FLAG_COUNT;
+	uint32_t nl = 0;
+	auto run = [&](rendgpu_tune t, float *ms) {
+		int r = tune_measure(c, t, frames, ms);
+		if (!r && log && nl < cap) {
+			log[nl] = t;
+			log[nl].ms = *ms;
+		}
+		if (!r)
+			nl++;
+		return r;
+	};
+	rendgpu_tune best = effective_tune(c);
+	best.ms = 0.0f;
+	float best_ms = 0.0f;
+	rc = run(best, &best_ms);
+	std::vector<uint32_t> queues;
+	for (uint32_t d : {2u, 4u, 8u}) {
+		uint32_t q = ((c->nslots / d + 1023u) / 1024u) * 1024u;
+		if (q >= 65536u && q < c->nslots)
+			queues.push_back(q);
+	}
+	for (int knob = 0; knob < 4 && !rc; knob++) {
+		std::vector<uint32_t> vals;
+		if (knob == 0)
+			vals = {3u, 1u};
+		else if (knob == 1)
+			vals = {64u, 128u, 256u};
+		else if (knob == 2) {
+			for (int st : kStacks)
+				if (need_stack(c) <= (uint32_t)st)
+					vals.push_back((uint32_t)st);
+		} else {
+			vals = queues;
+			vals.push_back(0u);
+		}
+		rendgpu_tune base = best;
+		for (uint32_t v : vals) {
+			rendgpu_tune t = base;
+			uint32_t *field = knob == 0 ? &t.sched : knob == 1 ? &t.block :
+			  knob == 2 ? &t.stack : &t.queue;
+			if (*field == v)
+				continue;
+			*field = v;
+			float ms = 0.0f;
+			rc = run(t, &ms);
+			if (rc)
+				break;
+			if (ms < best_ms) {
+				best_ms = ms;
+				best = t;
+			}
+		}
+	}
+	c->cfg.flags = flags;
+	if (nlog)
+		*nlog = nl;
+	if (rc)
+		return rc;
+	best.ms = best_ms;
+	rc = set_tune(c, &best);
+	if (rc)
+		return rc;
+	NB_CK(c, cudaMemsetAsync(c->acc.p, 0, (size_t)c->npix * 12, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->buf.p, 0, (size_t)c->npix * 4, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	if (best_out)
+		*best_out = best;
+	return 0;
 }
 
 // ------------------------------------------------ allocation-free tracing --
@@ -808,36 +1474,15 @@ extern "C" {
 
 int rendgpu_init(struct rdata *rdp, const struct rendgpu_cfg *cfg)
 {
-	if (!rdp || !cfg || cfg->size < sizeof(rendgpu_cfg) - 8 * sizeof(uint32_t))
+	if (!rdp)
 		return RENDGPU_EINVAL;
 	if (find_ctx(rdp))
 		return RENDGPU_ESTATE;
-	int ndev = 0;
-	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
-		return RENDGPU_ENODEV;
-	if (cfg->device < 0 || cfg->device >= ndev)
-		return RENDGPU_EINVAL;
-	if (cfg->mode > RENDGPU_MODE_NRC || cfg->max_depth < 1 ||
-	  cfg->max_depth > 1024 || cfg->sched > 3)
-		return RENDGPU_EINVAL;
-	Ctx *c = new Ctx;
-	c->rd = reinterpret_cast<nb_rdata *>(rdp);
-	c->cfg = *cfg;
-	c->device = cfg->device;
-	if (cudaSetDevice(c->device) != cudaSuccess ||
-	  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount,
-	  c->device) != cudaSuccess ||
-	  cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) !=
-	  cudaSuccess) {
-		free_ctx(c);
-		return RENDGPU_ECUDA;
-	}
-	if (c->cnt.ensure(64 * sizeof(uint32_t)) != cudaSuccess ||
-	  c->rays.ensure(4 * sizeof(unsigned long long)) != cudaSuccess ||
-	  c->berr.ensure(16) != cudaSuccess) {
-		free_ctx(c);
-		return RENDGPU_ENOMEM;
-	}
+	Ctx *c = nullptr;
+	nb_rdata *rd = reinterpret_cast<nb_rdata *>(rdp);
+	int rc = new_ctx(&rd, 1, nullptr, cfg, &c);
+	if (rc)
+		return rc;
 	std::lock_guard<std::mutex> lk(g_mu);
 	g_ctx[rdp] = c;
 	return 0;
@@ -865,58 +1510,7 @@ int rendgpu_upload_static(struct rdata *rdp)
 	Ctx *c = find_ctx(rdp);
 	if (!c)
 		return RENDGPU_EINVAL;
-	NB_CK(c, cudaSetDevice(c->device));
-	nb_rdata *rd = c->rd;
-	if (!rd->bnodes || !rd->tris || !rd->nrms || !rd->mtls || !rd->insts)
-		return fail(c, RENDGPU_EINVAL, "render data not initialised");
-	if (rd->instcnt == 0 || rd->instcnt > (1u << NB_INST_ID_BITS))
-		return fail(c, RENDGPU_ELIMIT, "instance count outside 1..4096 "
-		  "(INST_ID_BITS = 12, rend.c:24)");
-	std::vector<nb_qnode> nodes;
-	std::vector<nb_gtri> tris;
-	c->root_of.clear();
-	c->depth_of.clear();
-	c->blas_depth = 0;
-	uint32_t maxtri = 0, maxmtl = 0;
-	for (uint32_t i = 0; i < rd->instcnt; i++) {
-		const nb_rinst &ri = rd->insts[i];
-		if (ri.tricnt == 0)
-			return fail(c, RENDGPU_EINVAL, "instance without triangles");
-		if (ri.tricnt > (1u << (32 - NB_INST_ID_BITS)))
-			return fail(c, RENDGPU_ELIMIT, "mesh above 2^20 triangles");
-		maxtri = std::max(maxtri, ri.triofs + ri.tricnt);
-		if (c->root_of.count(ri.triofs))
-			continue;
-		uint32_t root = 0;
-		bvh_stats bs;
-		std::string err;
-		if (!convert_blas(rd, ri.triofs, nodes, tris, &root, &bs, &err))
-			return fail(c, RENDGPU_EINVAL, "BLAS of triofs " +
-			  std::to_string(ri.triofs) + ": " + err);
-		c->root_of[ri.triofs] = root;
-		c->depth_of[ri.triofs] = bs.depth;
-		c->blas_depth = std::max(c->blas_depth, bs.depth);
-	}
-	for (uint32_t t = 0; t < maxtri; t++)
-		maxmtl = std::max(maxmtl, rd->nrms[t].mtlid + 1u);
-	NB_CK(c, c->blas.ensure(nodes.size() * sizeof(nb_qnode)));
-	NB_CK(c, c->tris.ensure(tris.size() * sizeof(nb_gtri)));
-	NB_CK(c, c->nrms.ensure((size_t)maxtri * sizeof(nb_rnrm)));
-	NB_CK(c, c->mtls.ensure((size_t)maxmtl * sizeof(nb_rmtl)));
-	NB_CK(c, cudaMemcpyAsync(c->blas.p, nodes.data(), nodes.size() *
-	  sizeof(nb_qnode), cudaMemcpyHostToDevice, c->stream));
-	NB_CK(c, cudaMemcpyAsync(c->tris.p, tris.data(), tris.size() *
-	  sizeof(nb_gtri), cudaMemcpyHostToDevice, c->stream));
-	NB_CK(c, cudaMemcpyAsync(c->nrms.p, rd->nrms, (size_t)maxtri *
-	  sizeof(nb_rnrm), cudaMemcpyHostToDevice, c->stream));
-	NB_CK(c, cudaMemcpyAsync(c->mtls.p, rd->mtls, (size_t)maxmtl *
-	  sizeof(nb_rmtl), cudaMemcpyHostToDevice, c->stream));
-	NB_CK(c, cudaStreamSynchronize(c->stream));
-	c->ntris = (uint32_t)tris.size();
-	c->nnodes = (uint32_t)nodes.size();
-	c->have_static = true;
-	c->have_dynamic = false;
-	return 0;
+	return upload_static_all(c);
 }
 
 int rendgpu_upload_dynamic(struct rdata *rdp)
@@ -924,71 +1518,7 @@ int rendgpu_upload_dynamic(struct rdata *rdp)
 	Ctx *c = find_ctx(rdp);
 	if (!c)
 		return RENDGPU_EINVAL;
-	if (!c->have_static)
-		return fail(c, RENDGPU_ESTATE, "upload_static must come first");
-	NB_CK(c, cudaSetDevice(c->device));
-	nb_rdata *rd = c->rd;
-	std::vector<nb_qnode> nodes;
-	std::vector<uint32_t> irefs;
-	bvh_stats bs;
-	std::string err;
-	if (!convert_tlas(rd, nodes, irefs, &bs, &err))
-		return fail(c, RENDGPU_EINVAL, "TLAS: " + err);
-	c->tlas_depth = bs.depth;
-	std::vector<nb_ginst> gi(rd->instcnt);
-	for (uint32_t i = 0; i < rd->instcnt; i++) {
-		const nb_rinst &ri = rd->insts[i];
-		auto it = c->root_of.find(ri.triofs);
-		if (it == c->root_of.end())
-			return fail(c, RENDGPU_ESTATE, "instance mesh not uploaded "
-			  "by upload_static");
-		std::memcpy(gi[i].m, ri.globinv, sizeof(gi[i].m));
-		gi[i].root = it->second;
-		gi[i].triofs = ri.triofs;
-		gi[i].flags = ri.flags;
-		gi[i].pad = 0;
-	}
-	c->light_area = build_lights(rd, c->host_lights);
-	{
-		float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
-		float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-		for (uint32_t i = 0; i < rd->instcnt; i++) {
-			const nb_aabb &b = rd->aabbs[i];
-			float bl[3] = {b.min.x, b.min.y, b.min.z};
-			float bh[3] = {b.max.x, b.max.y, b.max.z};
-			for (int a = 0; a < 3; a++) {
-				lo[a] = std::min(lo[a], bl[a]);
-				hi[a] = std::max(hi[a], bh[a]);
-			}
-		}
-		for (int a = 0; a < 3; a++) {
-			c->box.lo[a] = lo[a];
-			c->box.inv[a] = hi[a] > lo[a] ? 1.0f / (hi[a] - lo[a]) : 1.0f;
-		}
-	}
-	NB_CK(c, c->tlas.ensure(nodes.size() * sizeof(nb_qnode)));
-	NB_CK(c, c->irefs.ensure(irefs.size() * sizeof(uint32_t)));
-	NB_CK(c, c->insts.ensure(gi.size() * sizeof(nb_ginst)));
-	NB_CK(c, c->lights.ensure(c->host_lights.size() * sizeof(nb_glight)));
-	NB_CK(c, cudaMemcpyAsync(c->tlas.p, nodes.data(), nodes.size() *
-	  sizeof(nb_qnode), cudaMemcpyHostToDevice, c->stream));
-	NB_CK(c, cudaMemcpyAsync(c->irefs.p, irefs.data(), irefs.size() *
-	  sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
-	NB_CK(c, cudaMemcpyAsync(c->insts.p, gi.data(), gi.size() *
-	  sizeof(nb_ginst), cudaMemcpyHostToDevice, c->stream));
-	if (!c->host_lights.empty())
-		NB_CK(c, cudaMemcpyAsync(c->lights.p, c->host_lights.data(),
-		  c->host_lights.size() * sizeof(nb_glight),
-		  cudaMemcpyHostToDevice, c->stream));
-	NB_CK(c, cudaStreamSynchronize(c->stream));
-	c->st.h2d_bytes = nodes.size() * sizeof(nb_qnode) + irefs.size() *
-	  sizeof(uint32_t) + gi.size() * sizeof(nb_ginst) +
-	  c->host_lights.size() * sizeof(nb_glight);
-	c->have_dynamic = true;
-	if (need_stack(c) > (uint32_t)kStackLarge)
-		return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal "
-		  "stack");
-	return 0;
+	return upload_dynamic_all(c);
 }
 
 int rendgpu_resaccum(struct rdata *rdp)
@@ -996,32 +1526,7 @@ int rendgpu_resaccum(struct rdata *rdp)
 	Ctx *c = find_ctx(rdp);
 	if (!c)
 		return RENDGPU_EINVAL;
-	NB_CK(c, cudaSetDevice(c->device));
-	nb_rdata *rd = c->rd;
-	uint64_t np = (uint64_t)rd->width * rd->height * (rd->spp ? rd->spp : 1);
-	if (np == 0 || np > 0x7fffffffull)
-		return fail(c, RENDGPU_ELIMIT, "width*height*spp outside "
-		  "1..2^31-1");
-	uint64_t npix = (uint64_t)rd->width * rd->height;
-	NB_CK(c, c->q0.ensure(np * 32));
-	NB_CK(c, c->q1.ensure(np * 32));
-	NB_CK(c, c->hits.ensure(np * 16));
-	NB_CK(c, c->shadow.ensure(np * 32));
-	NB_CK(c, c->scol.ensure(np * 16));
-	NB_CK(c, c->pT.ensure(np * 16));
-	NB_CK(c, c->pL.ensure(np * 16));
-	NB_CK(c, c->rng.ensure(np * 8));
-	NB_CK(c, c->acc.ensure(npix * 12));
-	NB_CK(c, c->buf.ensure(npix * 4));
-	c->W = rd->width;
-	c->H = rd->height;
-	c->spp = rd->spp ? rd->spp : 1;
-	c->npaths = (uint32_t)np;
-	c->have_frame = true;
-	NB_CK(c, cudaMemsetAsync(c->acc.p, 0, npix * 12, c->stream));
-	NB_CK(c, cudaMemsetAsync(c->buf.p, 0, npix * 4, c->stream));
-	NB_CK(c, cudaStreamSynchronize(c->stream));
-	return 0;
+	return alloc_frame(c);
 }
 
 int rendgpu_clraccum(struct rdata *rdp)
@@ -1032,8 +1537,7 @@ int rendgpu_clraccum(struct rdata *rdp)
 	if (!c->have_frame)
 		return fail(c, RENDGPU_ESTATE, "rendgpu_resaccum must come first");
 	NB_CK(c, cudaSetDevice(c->device));
-	NB_CK(c, cudaMemsetAsync(c->acc.p, 0, (size_t)c->W * c->H * 12,
-	  c->stream));
+	NB_CK(c, cudaMemsetAsync(c->acc.p, 0, (size_t)c->npix * 12, c->stream));
 	return 0;
 }
 
@@ -1067,24 +1571,7 @@ int rendgpu_readback(struct rdata *rdp, int which)
 	Ctx *c = find_ctx(rdp);
 	if (!c)
 		return RENDGPU_EINVAL;
-	if (!c->have_frame)
-		return fail(c, RENDGPU_ESTATE, "rendgpu_resaccum must come first");
-	NB_CK(c, cudaSetDevice(c->device));
-	nb_rdata *rd = c->rd;
-	size_t npix = (size_t)c->W * c->H;
-	c->st.d2h_bytes = 0;
-	if ((which & 1) && rd->acc) {
-		NB_CK(c, cudaMemcpyAsync(rd->acc, c->acc.p, npix * 12,
-		  cudaMemcpyDeviceToHost, c->stream));
-		c->st.d2h_bytes += npix * 12;
-	}
-	if ((which & 2) && rd->buf) {
-		NB_CK(c, cudaMemcpyAsync(rd->buf, c->buf.p, npix * 4,
-		  cudaMemcpyDeviceToHost, c->stream));
-		c->st.d2h_bytes += npix * 4;
-	}
-	NB_CK(c, cudaStreamSynchronize(c->stream));
-	return 0;
+	return readback_all(c, which);
 }
 
 int rendgpu_trace_rays_device(struct rdata *rdp, const void *rays,
@@ -1311,7 +1798,7 @@ int rendgpu_relmse_device(struct rdata *rdp, const float *ref, double *out)
 	if (!c->have_frame)
 		return fail(c, RENDGPU_ESTATE, "rendgpu_resaccum must come first");
 	NB_CK(c, cudaSetDevice(c->device));
-	uint32_t n = c->W * c->H * 3u;
+	uint32_t n = c->sc[0].W * c->sc[0].H * 3u;
 	NB_CK(c, c->mlp_loss.ensure(1024 * sizeof(float)));
 	double *d = reinterpret_cast<double *>(c->mlp_loss.p);
 	NB_CK(c, cudaMemsetAsync(d, 0, sizeof(double), c->stream));
@@ -1365,14 +1852,15 @@ int rendgpu_get_lights(struct rdata *rdp, float *out, uint32_t cap,
 		return RENDGPU_EINVAL;
 	if (!c->have_dynamic)
 		return fail(c, RENDGPU_ESTATE, "upload_dynamic must come first");
-	uint32_t n = (uint32_t)c->host_lights.size();
+	const SceneHost &h = c->sc[0];
+	uint32_t n = (uint32_t)h.lights.size();
 	if (out) {
 		uint32_t m = n < cap ? n : cap;
-		std::memcpy(out, c->host_lights.data(), (size_t)m *
+		std::memcpy(out, h.lights.data(), (size_t)m *
 		  sizeof(nb_glight));
 	}
 	if (total_area)
-		*total_area = c->light_area;
+		*total_area = h.light_area;
 	return (int)n;
 }
 
@@ -1386,6 +1874,198 @@ const char *rendgpu_strerror(struct rdata *rdp)
 {
 	Ctx *c = find_ctx(rdp);
 	return c ? c->msg.c_str() : "no GPU context for this rdata";
+}
+
+int rendgpu_set_tune(struct rdata *rdp, const struct rendgpu_tune *t)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	return set_tune(c, t);
+}
+
+int rendgpu_get_tune(struct rdata *rdp, struct rendgpu_tune *t)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c || !t)
+		return RENDGPU_EINVAL;
+	*t = effective_tune(c);
+	return 0;
+}
+
+int rendgpu_autotune(struct rdata *rdp, uint32_t frames,
+                     struct rendgpu_tune *best, struct rendgpu_tune *log,
+                     uint32_t cap, uint32_t *nlog)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	return autotune(c, frames, best, log, cap, nlog);
+}
+
+int rendgpu_batch_init(struct rdata *const *rds, uint32_t n,
+                       const uint32_t *max_depth,
+                       const struct rendgpu_cfg *cfg,
+                       struct rendgpu_batch **out)
+{
+	if (!out || !cfg || cfg->mode == RENDGPU_MODE_NRC)
+		return RENDGPU_EINVAL;
+	Ctx *c = nullptr;
+	int rc = new_ctx(reinterpret_cast<nb_rdata *const *>(rds), n, max_depth,
+	  cfg, &c);
+	if (rc)
+		return rc;
+	c->batch = true;
+	rendgpu_batch *b = reinterpret_cast<rendgpu_batch *>(c);
+	std::lock_guard<std::mutex> lk(g_mu);
+	g_batches.insert(b);
+	*out = b;
+	return 0;
+}
+
+int rendgpu_batch_release(struct rendgpu_batch *b)
+{
+	Ctx *c = find_batch(b);
+	if (!c)
+		return RENDGPU_EINVAL;
+	{
+		std::lock_guard<std::mutex> lk(g_mu);
+		g_batches.erase(b);
+	}
+	cudaSetDevice(c->device);
+	cudaStreamSynchronize(c->stream);
+	free_ctx(c);
+	return 0;
+}
+
+int rendgpu_batch_upload_static(struct rendgpu_batch *b)
+{
+	Ctx *c = find_batch(b);
+	return c ? upload_static_all(c) : RENDGPU_EINVAL;
+}
+
+int rendgpu_batch_upload_dynamic(struct rendgpu_batch *b)
+{
+	Ctx *c = find_batch(b);
+	return c ? upload_dynamic_all(c) : RENDGPU_EINVAL;
+}
+
+int rendgpu_batch_resaccum(struct rendgpu_batch *b)
+{
+	Ctx *c = find_batch(b);
+	return c ? alloc_frame(c) : RENDGPU_EINVAL;
+}
+
+int rendgpu_batch_clraccum(struct rendgpu_batch *b)
+{
+	Ctx *c = find_batch(b);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->have_frame)
+		return fail(c, RENDGPU_ESTATE, "resaccum must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	NB_CK(c, cudaMemsetAsync(c->acc.p, 0, (size_t)c->npix * 12, c->stream));
+	return 0;
+}
+
+int rendgpu_batch_render(struct rendgpu_batch *b)
+{
+	Ctx *c = find_batch(b);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	c->last = 0;
+	int rc = render_frame(c);
+	if (rc)
+		return rc;
+	for (size_t i = 0; i < c->sc.size(); i++)
+		__atomic_fetch_add(&c->sc[i].rd->rays, (unsigned int)(
+		  c->scn_host[2 * i] + c->scn_host[2 * i + 1]), __ATOMIC_SEQ_CST);
+	return 0;
+}
+
+int rendgpu_batch_readback(struct rendgpu_batch *b, int which)
+{
+	Ctx *c = find_batch(b);
+	return c ? readback_all(c, which) : RENDGPU_EINVAL;
+}
+
+int rendgpu_batch_get_stats(struct rendgpu_batch *b,
+                            struct rendgpu_stats *total,
+                            struct rendgpu_scene_stats *per, uint32_t n)
+{
+	Ctx *c = find_batch(b);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (total) {
+		c->st.device_bytes = held_bytes(c);
+		c->st.max_stack = need_stack(c);
+		*total = c->st;
+	}
+	for (uint32_t i = 0; per && i < n && i < c->sc.size(); i++) {
+		const SceneHost &h = c->sc[i];
+		per[i].closest_rays = i < c->scn_host.size() / 2 ?
+		  c->scn_host[2 * i] : 0;
+		per[i].shadow_rays = i < c->scn_host.size() / 2 ?
+		  c->scn_host[2 * i + 1] : 0;
+		per[i].paths = (uint64_t)h.W * h.H * h.spp;
+		per[i].pixels = (uint64_t)h.W * h.H;
+	}
+	return 0;
+}
+
+int rendgpu_batch_set_tune(struct rendgpu_batch *b,
+                           const struct rendgpu_tune *t)
+{
+	Ctx *c = find_batch(b);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	return set_tune(c, t);
+}
+
+int rendgpu_batch_get_tune(struct rendgpu_batch *b, struct rendgpu_tune *t)
+{
+	Ctx *c = find_batch(b);
+	if (!c || !t)
+		return RENDGPU_EINVAL;
+	*t = effective_tune(c);
+	return 0;
+}
+
+int rendgpu_batch_autotune(struct rendgpu_batch *b, uint32_t frames,
+                           struct rendgpu_tune *best,
+                           struct rendgpu_tune *log, uint32_t cap,
+                           uint32_t *nlog)
+{
+	Ctx *c = find_batch(b);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	return autotune(c, frames, best, log, cap, nlog);
+}
+
+int rendgpu_batch_get_stream(struct rendgpu_batch *b, void **stream)
+{
+	Ctx *c = find_batch(b);
+	if (!c || !stream)
+		return RENDGPU_EINVAL;
+	*stream = (void *)c->stream;
+	return 0;
+}
+
+int rendgpu_batch_last_error(struct rendgpu_batch *b)
+{
+	Ctx *c = find_batch(b);
+	return c ? c->last : RENDGPU_EINVAL;
+}
+
+const char *rendgpu_batch_strerror(struct rendgpu_batch *b)
+{
+	Ctx *c = find_batch(b);
+	return c ? c->msg.c_str() : "not a live batch handle";
 }
 
 } // extern "C"

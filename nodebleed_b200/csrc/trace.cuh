@@ -28,6 +28,25 @@ namespace nb {
 
 constexpr float kWiden = 1.00000095367431640625f; // 1 + 2^-20
 
+// Per-scene parameters of a frame (one entry per scene of a batch; a
+// single-scene context is a batch of one).  A scene's paths, pixels and
+// camera-ray slots are consecutive ranges starting at its bases; its PCG32
+// streams and pixel order are those of the scene rendered alone.
+struct ScenePar {
+	uint32_t tlas_root, light_off, light_cnt, depth;
+	uint32_t W, H, spp, frame;             // frame: rd->samples
+	uint32_t path_base, pix_base, slot_base, nrc_stride;
+	uint32_t nrc_offset, pad0[3];
+	float    light_area, inv, pad1[2];     // inv: 1 / (samples + spp)
+	float    bg[3], tanfangle;
+	float    eye[3], rw;
+	float    ri[3], rh;
+	float    up[3], fovfdist;
+	float    fwd[3], aspect;
+	float    fdist, focrad, pad2[2];
+	uint64_t seed, pad3;
+};
+
 struct DScene {
 	const nb_qnode *blas;
 	const float4   *tris;   // nb_gtri as 3 float4
@@ -37,10 +56,33 @@ struct DScene {
 	const nb_rnrm  *nrms;
 	const nb_rmtl  *mtls;
 	const float4   *lights; // nb_glight as 5 float4
-	uint32_t        nlights;
-	float           light_area;
-	float           bg[3];
+	const ScenePar *sp;
+	uint32_t        nscenes;
 };
+
+// Scene owning global index `key` in the range that starts at field
+// `base` of each entry: the last scene whose base <= key (bases ascend).
+template <class Base>
+__device__ __forceinline__ uint32_t scene_search(const DScene &S,
+                                                 uint32_t key, Base base)
+{
+	uint32_t lo = 0, hi = S.nscenes - 1u;
+	while (lo < hi) {
+		uint32_t mid = (lo + hi + 1u) >> 1;
+		if (base(S.sp + mid) <= key)
+			lo = mid;
+		else
+			hi = mid - 1u;
+	}
+	return lo;
+}
+
+__device__ __forceinline__ uint32_t scene_of_path(const DScene &S,
+                                                  uint32_t path)
+{
+	return scene_search(S, path, [](const ScenePar *p) {
+		return __ldg(&p->path_base); });
+}
 
 // Ray state in the space being traversed.
 struct TRay {
@@ -529,8 +571,10 @@ __device__ __forceinline__ void trace_step(const DScene &S,
 				if (my < n) {
 					ridx = my;
 					err = 0;
-					trav_start(T, rays[2u * my], rays[2u * my + 1u]);
-					vnode = 0u;
+					float4 rb = rays[2u * my + 1u];
+					trav_start(T, rays[2u * my], rb);
+					vnode = S.nscenes > 1u ? __ldg(&S.sp[scene_of_path(S,
+					  __float_as_uint(rb.w))].tlas_root) : 0u;
 					active = true;
 				}
 			}
@@ -609,8 +653,10 @@ __device__ __forceinline__ void trace_phase(const DScene &S,
 				if (my < n) {
 					ridx = my;
 					err = 0;
-					trav_start(T, rays[2u * my], rays[2u * my + 1u]);
-					vnode = 0u;
+					float4 rb = rays[2u * my + 1u];
+					trav_start(T, rays[2u * my], rb);
+					vnode = S.nscenes > 1u ? __ldg(&S.sp[scene_of_path(S,
+					  __float_as_uint(rb.w))].tlas_root) : 0u;
 					active = true;
 				}
 			}
@@ -711,8 +757,10 @@ __device__ __forceinline__ void trace_ylitie(const DScene &S,
 				if (my < n) {
 					ridx = my;
 					err = 0;
-					trav_start(T, rays[2u * my], rays[2u * my + 1u]);
-					vnode = 0u;
+					float4 rb = rays[2u * my + 1u];
+					trav_start(T, rays[2u * my], rb);
+					vnode = S.nscenes > 1u ? __ldg(&S.sp[scene_of_path(S,
+					  __float_as_uint(rb.w))].tlas_root) : 0u;
 					active = true;
 				}
 			}

@@ -1,0 +1,126 @@
+"""Batched multi-scene frames (rendgpu_batch_*): every scene of a batch
+renders bit-identical to the same scene rendered alone; waves, block sizes,
+stack depths and graph replay change no bits; the autotuner returns a
+setting it measured."""
+
+import numpy as np
+import pytest
+
+from nodebleed_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+# (family, scene seed, width, height, spp, max depth): uneven sizes,
+# sample counts and depths, as a batch of the 16-scene workload has
+SCENES = [(api.SCENE_TINY, 1, 64, 48, 1, 3),
+          (api.SCENE_SMALL, 1, 160, 90, 4, 5),
+          (api.SCENE_TINY, 2, 96, 72, 2, 8),
+          (api.SCENE_SMALL, 3, 120, 68, 1, 12)]
+
+
+def _rdatas(scenes=SCENES):
+    out = []
+    for fam, seed, w, h, spp, _ in scenes:
+        sc = api.Scene(fam, seed)
+        out.append(api.RenderData(sc, w, h, spp))
+    return out
+
+
+def _alone(seed=7, frames=2, scenes=SCENES, **kw):
+    imgs, rays = [], []
+    for rd, (_, _, _, _, _, depth) in zip(_rdatas(scenes), scenes):
+        gr = api.GpuRenderer(rd, max_depth=depth, seed=seed, **kw).upload()
+        r = []
+        for _ in range(frames):
+            gr.frame()
+            st = gr.stats()
+            r.append((st["closest_rays"], st["shadow_rays"]))
+        gr.readback(1)
+        imgs.append(rd.acc().copy())
+        rays.append(r)
+        gr.close()
+    return imgs, rays
+
+
+def _batch(seed=7, frames=2, scenes=SCENES, tune=None):
+    rds = _rdatas(scenes)
+    b = api.BatchRenderer(rds, max_depth=[s[5] for s in scenes],
+                          seed=seed).upload()
+    if tune:
+        b.set_tune(**tune)
+    rays = []
+    for _ in range(frames):
+        b.frame()
+        tot, per = b.stats()
+        assert tot["device_errors"] == 0
+        rays.append([(p["closest_rays"], p["shadow_rays"]) for p in per])
+    b.readback(1)
+    imgs = [rd.acc().copy() for rd in rds]
+    b.close()
+    return imgs, rays
+
+
+@pytest.fixture(scope="module")
+def alone(gpu):
+    return _alone()
+
+
+@pytest.fixture(scope="module")
+def batched(gpu):
+    return _batch()
+
+
+def test_batch_images_match_scenes_rendered_alone(alone, batched):
+    for i, (a, b) in enumerate(zip(alone[0], batched[0])):
+        assert a.shape == b.shape
+        assert np.array_equal(a, b), (i, np.abs(a - b).max())
+        assert a.max() > 0
+
+
+def test_batch_per_scene_ray_counts(alone, batched):
+    for f in range(2):
+        for i in range(len(SCENES)):
+            assert tuple(batched[1][f][i]) == tuple(alone[1][i][f])
+
+
+@pytest.mark.parametrize("tune", [
+    {"queue": 4096}, {"queue": 20000}, {"block": 64}, {"block": 256},
+    {"stack": 32}, {"stack": 48}])
+def test_tuning_changes_no_bits(batched, tune):
+    imgs, rays = _batch(tune=tune)
+    for a, b in zip(batched[0], imgs):
+        assert np.array_equal(a, b), tune
+    assert rays == batched[1]
+
+
+def test_graph_replay_matches_direct_launches(gpu):
+    scenes = SCENES[1:2]
+    direct, _ = _alone(frames=3, scenes=scenes)
+    graph, _ = _alone(frames=3, scenes=scenes, graph=True)
+    assert np.array_equal(direct[0], graph[0])
+
+
+def test_autotune_returns_a_measured_setting(gpu):
+    rds = _rdatas(SCENES[:2])
+    b = api.BatchRenderer(rds, max_depth=[3, 5], timing=True).upload()
+    best, log = b.autotune(frames=1)
+    assert len(log) >= 6
+    assert best["ms"] > 0 and best["ms"] == min(x["ms"] for x in log)
+    assert any(all(x[k] == best[k] for k in ("block", "stack", "queue",
+                                             "sched")) for x in log)
+    got = b.get_tune()
+    assert all(got[k] == best[k] for k in ("block", "stack", "queue",
+                                           "sched"))
+    # the accumulator is cleared; frames render normally afterwards
+    b.readback(1)
+    assert all(rd.acc().max() == 0 for rd in rds)
+    b.frame()
+    b.readback(1)
+    assert all(rd.acc().max() > 0 for rd in rds)
+    b.close()
+
+
+def test_batch_rejects_radiance_cache_mode(gpu):
+    rds = _rdatas(SCENES[:1])
+    with pytest.raises(api.RendgpuError):
+        api.BatchRenderer(rds, mode=api.MODE_NRC)
