@@ -64,6 +64,9 @@ def parse():
                         "for 4096; 1024 keeps the default run short)")
     p.add_argument("--cpu-seconds", type=float, default=15.0,
                    help="target CPU time of the bounded CPU sample")
+    p.add_argument("--no-batch", action="store_true",
+                   help="skip the 16-scene batched workload")
+    p.add_argument("--batch-frames", type=int, default=3)
     return p.parse_args()
 
 
@@ -224,6 +227,94 @@ def cpu_baseline(a, rd, lights, area, budget_s):
             "_counts": (cnt.nodes, cnt.leaves, cnt.insts, crays)}
 
 
+def _elapsed(ev):
+    return sum(s.elapsed_time(e) for s, e in ev)
+
+
+def batch_eval(a, dev, flush):
+    """The batched uneven workload: 16 seeded scenes of the small family
+    (one icosphere BLAS of 1k-1M triangles log-uniform x4 + ground + quad
+    light; resolution, spp and depth drawn per scene) rendered as one
+    batch (one captured launch sequence per frame over shared queues,
+    launch parameters autotuned), then each scene alone."""
+    import torch
+    from nodebleed_b200 import api
+    t0 = time.perf_counter()
+    scenes = [api.Scene(api.SCENE_BATCH, 1, i) for i in range(16)]
+    rds = [api.RenderData(sc) for sc in scenes]
+    depths = [sc.settings()["depth"] for sc in scenes]
+    host_s = time.perf_counter() - t0
+    b = api.BatchRenderer(rds, max_depth=depths, seed=1, timing=True,
+                          device=dev).upload()
+    t0 = time.perf_counter()
+    best, log = b.autotune(frames=1)
+    tune_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+    b.frame()
+    torch.cuda.synchronize()
+    ev, per_rays, tot_rays, launches = [], [0] * 16, 0, 0
+    for _ in range(a.batch_frames):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), \
+                torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+        tot_rays += b.frame()
+        with torch.cuda.stream(stream):
+            e.record(stream)
+        ev.append((s, e))
+        tot, per = b.stats()
+        launches = tot["launches"]
+        for i, p in enumerate(per):
+            per_rays[i] += p["closest_rays"] + p["shadow_rays"]
+    torch.cuda.synchronize()
+    ms = _elapsed(ev)
+    b.close()
+    rows, alone_ms = [], 0.0
+    for i, (sc, rd) in enumerate(zip(scenes, rds)):
+        gr = api.GpuRenderer(rd, max_depth=depths[i], seed=1, timing=True,
+                             device=dev, graph=True).upload()
+        st_ = torch.cuda.ExternalStream(gr.stream(), device=dev)
+        gr.frame()
+        ev1, r1 = [], 0
+        for _ in range(a.batch_frames):
+            with torch.cuda.stream(st_):
+                flush.zero_()
+                s, e = torch.cuda.Event(enable_timing=True), \
+                    torch.cuda.Event(enable_timing=True)
+                s.record(st_)
+            r1 += gr.frame()
+            with torch.cuda.stream(st_):
+                e.record(st_)
+            ev1.append((s, e))
+        torch.cuda.synchronize()
+        m1 = _elapsed(ev1)
+        alone_ms += m1
+        gr.close()
+        cfg = sc.settings()
+        rows.append({"scene": i, "tris": sc.tris,
+                     "res": [cfg["width"], cfg["height"]],
+                     "spp": cfg["spp"], "depth": cfg["depth"],
+                     "rays_per_frame": per_rays[i] / a.batch_frames,
+                     "mrays_s_share_in_batch": per_rays[i] / ms / 1e3,
+                     "mrays_s_alone": r1 / m1 / 1e3,
+                     "ms_alone": m1 / a.batch_frames})
+    return {"workload": "16 scenes of the small family (seed 1, scene "
+                        "index 0..15): 1k-1M tris log-uniform, resolutions "
+                        "320x180..1920x1080, spp {1,4,16}, depth {4,8,12}",
+            "frames": a.batch_frames,
+            "aggregate_mrays_s": tot_rays / ms / 1e3,
+            "ms_per_frame": ms / a.batch_frames,
+            "alone_ms_per_frame_sum": alone_ms / a.batch_frames,
+            "speedup_vs_alone": alone_ms / ms,
+            "gpu_launches_per_frame": launches,
+            "tuned": best, "autotune_log": log, "autotune_s": tune_s,
+            "host_build_s": host_s, "scenes": rows,
+            "paths_per_frame": sum(r["spp"] * r["res"][0] * r["res"][1]
+                                   for r in rows),
+            "unique_tris": sum(r["tris"] for r in rows)}
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -336,6 +427,11 @@ def run_ours(a):
                          "adam_lr": 1e-2}
         nrc["wall_s"] = time.perf_counter() - t0
 
+    batch = None
+    if rank == 0 and world == 1 and not a.no_batch:
+        gr.close()
+        batch = batch_eval(a, dev, flush)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(a, rd, lights, area, a.cpu_seconds)
@@ -379,7 +475,7 @@ def run_ours(a):
                "ms_trace_per_frame": trace_ms / a.steps,
                "ms_shadow_per_frame": shadow_ms / a.steps,
                "gpu_launches": launches, "e2e": e2e, "roofline": roof,
-               "gpu_visits": visits, "nrc": nrc,
+               "gpu_visits": visits, "nrc": nrc, "batch": batch,
                "cpu_baseline": cpu, "clocks": cl,
                "scene": {"unique_tris": scene.tris,
                          "instanced_tris": scene.inst_tris,
