@@ -67,6 +67,13 @@ def parse():
     p.add_argument("--no-batch", action="store_true",
                    help="skip the 16-scene batched workload")
     p.add_argument("--batch-frames", type=int, default=3)
+    p.add_argument("--no-stress", action="store_true",
+                   help="skip the 3840x2160 depth-16 stress workload")
+    p.add_argument("--stress-frames", type=int, default=2)
+    p.add_argument("--stress-eval-width", type=int, default=960)
+    p.add_argument("--stress-eval-height", type=int, default=540)
+    p.add_argument("--stress-ref-spp", type=int, default=256)
+    p.add_argument("--stress-nrc-frames", type=int, default=32)
     return p.parse_args()
 
 
@@ -315,6 +322,92 @@ def batch_eval(a, dev, flush):
             "unique_tris": sum(r["tris"] for r in rows)}
 
 
+def stress_eval(a, dev, flush):
+    """The stress workload: 128 BLAS of 1k-200k triangles, 4096 instances
+    (the reference's cap), Lambertian / GGX (roughness U[0.05,0.5]) /
+    mirror thirds, 8 quad lights, 3840x2160, 1 spp, depth 16.  Plain
+    wavefront throughput at full size; the reference traversal in the CPU
+    path tracer on a band of rows; radiance cache against plain at equal
+    device time on a reduced image (relMSE against a high-spp plain
+    reference)."""
+    import torch
+    from nodebleed_b200 import api, nrc_eval
+    t0 = time.perf_counter()
+    scene = api.Scene(api.SCENE_STRESS, 1)
+    rd = api.RenderData(scene)
+    host_s = time.perf_counter() - t0
+    cfg = scene.settings()
+    W, H, depth = cfg["width"], cfg["height"], cfg["depth"]
+    gr = api.GpuRenderer(rd, max_depth=depth, seed=1, timing=True,
+                         device=dev, graph=True).upload()
+    stream = torch.cuda.ExternalStream(gr.stream(), device=dev)
+    gr.frame()
+    ev, rays = [], 0
+    for _ in range(a.stress_frames):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), \
+                torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+        rays += gr.frame()
+        with torch.cuda.stream(stream):
+            e.record(stream)
+        ev.append((s, e))
+    torch.cuda.synchronize()
+    ms = _elapsed(ev)
+    st = gr.stats()
+    lights, area = gr.lights()
+    gr.close()
+    out = {"workload": "stress: 128 BLAS (1k-200k tris log-uniform), 4096 "
+                       "instances, Lambertian/GGX/mirror thirds, 8 quad "
+                       "lights; %dx%d, 1 spp, max depth %d" % (W, H, depth),
+           "unique_tris": scene.tris, "instanced_tris": scene.inst_tris,
+           "instances": scene.insts, "host_build_s": host_s,
+           "mrays_s": rays / ms / 1e3,
+           "samples_s": W * H * a.stress_frames / (ms / 1e3),
+           "ms_per_frame": ms / a.stress_frames,
+           "rays_per_frame": rays / a.stress_frames,
+           "max_stack": st["max_stack"]}
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as ol
+        use_ref = ol.ref() is not None
+        t0 = time.perf_counter()
+        _, r0 = ol.orc_render(rd, lights, area, depth, seed=1,
+                              window=(0, H // 2, W, H // 2 + 2),
+                              use_ref=use_ref)
+        dt = time.perf_counter() - t0
+        rows = max(2, min(H, int(2 * 10.0 / max(dt, 1e-3))))
+        y0 = max(0, H // 2 - rows // 2)
+        t0 = time.perf_counter()
+        _, n = ol.orc_render(rd, lights, area, depth, seed=1,
+                             window=(0, y0, W, y0 + rows), use_ref=use_ref)
+        dt = time.perf_counter() - t0
+        out["cpu_reference"] = {
+            "mrays_s": n / dt / 1e6, "cores": ol.ncpu(),
+            "kind": "reference" if use_ref else "port",
+            "sample": "rows %d..%d (%d rays in %.1f s)" % (y0, y0 + rows,
+                                                          n, dt)}
+        out["gpu_over_cpu"] = out["mrays_s"] / out["cpu_reference"]["mrays_s"]
+    t0 = time.perf_counter()
+    ref = nrc_eval.reference(scene, a.stress_eval_width,
+                             a.stress_eval_height, depth, a.stress_ref_spp)
+    ev_ = nrc_eval.equal_time(scene, a.stress_eval_width,
+                              a.stress_eval_height, depth,
+                              a.stress_nrc_frames, ref)
+    out["equal_time"] = {"width": a.stress_eval_width,
+                         "height": a.stress_eval_height,
+                         "reference_spp": a.stress_ref_spp,
+                         "nrc": {k: ev_["nrc"][k] for k in
+                                 ("frames", "ms", "relmse", "rays")},
+                         "plain": ev_["plain"],
+                         "ratio_plain_over_nrc":
+                             ev_["ratio_plain_over_nrc"],
+                         "wall_s": time.perf_counter() - t0}
+    rd.close()
+    return out
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -378,13 +471,21 @@ def run_ours(a):
         e2e_rays = 0
         barrier()
         torch.cuda.synchronize()
+        parts = [0.0, 0.0, 0.0]
         t0 = time.perf_counter()
         for _ in range(a.steps):
+            t1 = time.perf_counter()
             gr.upload_dynamic()
             h2d += gr.stats()["h2d_bytes"]
+            t2 = time.perf_counter()
             e2e_rays += gr.frame()
+            t3 = time.perf_counter()
             gr.readback(2)
             d2h += gr.stats()["d2h_bytes"]
+            t4 = time.perf_counter()
+            parts[0] += t2 - t1
+            parts[1] += t3 - t2
+            parts[2] += t4 - t3
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         dt_max = allreduce(dt, torch.distributed.ReduceOp.MAX) \
@@ -395,7 +496,9 @@ def run_ours(a):
                "h2d_bytes_per_step": h2d // a.steps,
                "d2h_bytes_per_step": d2h // a.steps,
                "timing": "wall clock around upload_dynamic + render + "
-                         "readback of the ARGB8 image (pinned host)"}
+                         "readback of the ARGB8 image (pinned host)",
+               "ms_upload_render_readback": [1e3 * x / a.steps
+                                             for x in parts]}
 
     visits = None
     if a.count:
@@ -431,6 +534,11 @@ def run_ours(a):
     if rank == 0 and world == 1 and not a.no_batch:
         gr.close()
         batch = batch_eval(a, dev, flush)
+
+    stress = None
+    if rank == 0 and world == 1 and not a.no_stress:
+        gr.close()
+        stress = stress_eval(a, dev, flush)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -476,6 +584,7 @@ def run_ours(a):
                "ms_shadow_per_frame": shadow_ms / a.steps,
                "gpu_launches": launches, "e2e": e2e, "roofline": roof,
                "gpu_visits": visits, "nrc": nrc, "batch": batch,
+               "stress": stress,
                "cpu_baseline": cpu, "clocks": cl,
                "scene": {"unique_tris": scene.tris,
                          "instanced_tris": scene.inst_tris,

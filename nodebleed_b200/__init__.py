@@ -16,5 +16,5 @@ from .api import (  # noqa: F401
     HostLib, GpuLib, Scene, RenderData, GpuRenderer, BatchRenderer,
     RendgpuError,
     RAY_DTYPE, HIT_DTYPE, host_lib, gpu_lib, SCENE_SMALL, SCENE_SCALE,
-    SCENE_BATCH, SCENE_STRESS, SCENE_TINY, MODE_PATH, MODE_PRIMARY, MODE_NRC,
+    SCENE_BATCH, SCENE_STRESS, SCENE_TINY, SCENE_GLOSSY, MODE_PATH, MODE_PRIMARY, MODE_NRC,
 )

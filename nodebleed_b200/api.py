@@ -8,6 +8,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 SCENE_SMALL, SCENE_SCALE, SCENE_BATCH, SCENE_STRESS, SCENE_TINY = 1, 2, 3, 5, 9
+SCENE_GLOSSY = 6
 MODE_PATH, MODE_PRIMARY, MODE_NRC = 0, 1, 2
 FLAG_TIMING, FLAG_COUNT, FLAG_GRAPH = 1, 2, 4
 

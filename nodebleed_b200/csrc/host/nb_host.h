@@ -71,12 +71,13 @@ enum {
 	NBH_SCENE_SCALE = 2,   // 64 BLAS (displaced spheres / soups), 1024 inst
 	NBH_SCENE_BATCH = 3,   // one scene of the 16-scene batch (small family)
 	NBH_SCENE_STRESS = 5,  // 128 BLAS, 4096 inst, GGX/mirror, 8 lights
+	NBH_SCENE_GLOSSY = 6,  // the stress mix at test size: 6 BLAS, 40 inst
 	NBH_SCENE_TINY = 9     // few hundred tris, for fast parity tests
 };
 
 // Generate a seeded scene.  `param` tunes the family: for BATCH it is the
 // scene index 0..15; for SMALL/TINY it scales the triangle budget (0 =
-// default); for SCALE/STRESS it is the BLAS count (0 = default).
+// default); for SCALE/STRESS/GLOSSY it is the BLAS count (0 = default).
 int  nbh_scene_gen(struct nbh_scene *s, int family, uint64_t seed,
                    unsigned int param);
 void nbh_scene_free(struct nbh_scene *s);

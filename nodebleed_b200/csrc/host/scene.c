@@ -644,8 +644,14 @@ int nbh_scene_gen(struct nbh_scene *s, int family, uint64_t seed,
 		  1024, 1, 0.2, 0.0, 1920, 1080, 4, 8, 25.0);
 		break;
 	case NBH_SCENE_STRESS:
+		// 4087 random instances + ground + 8 lights = 4096, the
+		// reference's instance cap (INST_ID_BITS = 12, rend.c:24)
 		rc = scene_field(&b, &r, param ? param : 128, 1000.0, 200000.0,
-		  4096, 8, 1.0 / 3.0, 1.0 / 3.0, 3840, 2160, 1, 16, 50.0);
+		  4087, 8, 1.0 / 3.0, 1.0 / 3.0, 3840, 2160, 1, 16, 50.0);
+		break;
+	case NBH_SCENE_GLOSSY:
+		rc = scene_field(&b, &r, param ? param : 6, 200.0, 3000.0, 40, 8,
+		  1.0 / 3.0, 1.0 / 3.0, 160, 96, 1, 8, 8.0);
 		break;
 	default:
 		rc = -1;

@@ -115,6 +115,47 @@ __device__ __forceinline__ void sincos2pi(float u, float *s, float *c)
 	}
 }
 
+// GGX (Trowbridge-Reitz) microfacet conductor, alpha = roughness (Walter et
+// al. 2007): Smith G1 for GGX and Schlick's Fresnel with F0 = albedo.  Same
+// operation order as the CPU oracle.
+__device__ __forceinline__ float ggx_g1(float a2, float nv)
+{
+	return __fdiv_rn(__fmul_rn(2.0f, nv), __fadd_rn(nv, __fsqrt_rn(
+	  __fadd_rn(a2, __fmul_rn(__fsub_rn(1.0f, a2), __fmul_rn(nv, nv))))));
+}
+
+__device__ __forceinline__ void schlick(const float f0[3], float c,
+                                        float out[3])
+{
+	float m = __fsub_rn(1.0f, c);
+	float m2 = __fmul_rn(m, m);
+	float m5 = __fmul_rn(__fmul_rn(m2, m2), m);
+	for (int a = 0; a < 3; a++)
+		out[a] = __fadd_rn(f0[a], __fmul_rn(__fsub_rn(1.0f, f0[a]), m5));
+}
+
+__device__ __forceinline__ float dot3(const float a[3], const float b[3])
+{
+	return __fadd_rn(__fadd_rn(__fmul_rn(a[0], b[0]), __fmul_rn(a[1], b[1])),
+	  __fmul_rn(a[2], b[2]));
+}
+
+// Orthonormal basis around n (rend.c:3126-3133).
+__device__ __forceinline__ void onb(const float n[3], float ta[3],
+                                    float tb[3])
+{
+	float sgn = copysignf(1.0f, n[2]);
+	float oa = __fdiv_rn(-1.0f, __fadd_rn(sgn, n[2]));
+	float ob = __fmul_rn(__fmul_rn(n[0], n[1]), oa);
+	ta[0] = __fadd_rn(1.0f, __fmul_rn(__fmul_rn(__fmul_rn(sgn, n[0]), n[0]),
+	  oa));
+	ta[1] = __fmul_rn(sgn, ob);
+	ta[2] = __fmul_rn(-sgn, n[0]);
+	tb[0] = ob;
+	tb[1] = __fadd_rn(sgn, __fmul_rn(__fmul_rn(n[1], n[1]), oa));
+	tb[2] = -n[1];
+}
+
 // Warp-aggregated append: returns this lane's slot in the queue.
 __device__ __forceinline__ uint32_t append(uint32_t *counter, bool want)
 {
@@ -449,7 +490,8 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 					bool spec = (pflags & kPathSpec) != 0u;
 					bool train = (pflags & kPathTrain) != 0u;
 					bool emissive = (mflags & NB_FLAG_EMISSIVE) != 0u;
-					bool mirror = mc.w >= 0.5f;
+					bool glossy = mc.w >= 0.5f && mf.x > 0.0f;
+					bool mirror = mc.w >= 0.5f && !glossy;
 					bool queried = false;
 					if (A.mode == 2u && k >= 1u && !emissive) {
 						if (!train && !mirror) {
@@ -508,7 +550,13 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 						want_ray = k + 1u < depth;
 					} else {
 						T.w = __uint_as_float(pflags & ~kPathSpec);
+						float wo[3] = {__fmul_rn(d[0], -1.0f),
+						  __fmul_rn(d[1], -1.0f), __fmul_rn(d[2], -1.0f)};
+						float nwo = dot3(n, wo);
+						float a2 = __fmul_rn(mf.x, mf.x);
 						uint32_t nl = __ldg(&P->light_cnt);
+						if (glossy && !(nwo > 0.0f))
+							nl = 0u; // the path ends here
 						if (nl) {
 							// pick an emitting triangle by area
 							const float4 *lt = S.lights +
@@ -561,15 +609,45 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 							tfar = __fsub_rn(ldist, __fmul_rn(2.0f, kEps2));
 							if (ndotl > 0.0f && cosl > 0.0f &&
 							    tfar > 0.0f) {
-								float wgt = __fmul_rn(ndotl, cosl);
-								wgt = __fmul_rn(wgt, __fmul_rn(kInvPi,
-								  __ldg(&P->light_area)));
-								wgt = __fdiv_rn(wgt, l2s);
 								float em[3] = {l3.x, l3.y, l3.z};
 								float tc[3] = {T.x, T.y, T.z};
+								float fr[3] = {col[0], col[1], col[2]};
+								float wgt;
+								if (glossy) {
+									// F D G / (4 n.wo n.l) n.l cosl
+									// area / l^2
+									float hv[3] = {__fadd_rn(wo[0], ld[0]),
+									  __fadd_rn(wo[1], ld[1]),
+									  __fadd_rn(wo[2], ld[2])};
+									float hil = __fdiv_rn(1.0f,
+									  __fsqrt_rn(dot3(hv, hv)));
+									for (int a = 0; a < 3; a++)
+										hv[a] = __fmul_rn(hv[a], hil);
+									float nh = dot3(n, hv);
+									float lh = dot3(ld, hv);
+									float dd = __fadd_rn(__fmul_rn(
+									  __fmul_rn(nh, nh),
+									  __fsub_rn(a2, 1.0f)), 1.0f);
+									float Dm = __fdiv_rn(__fmul_rn(a2,
+									  kInvPi), __fmul_rn(dd, dd));
+									float G = __fmul_rn(ggx_g1(a2, nwo),
+									  ggx_g1(a2, ndotl));
+									wgt = __fmul_rn(__fdiv_rn(
+									  __fmul_rn(Dm, G),
+									  __fmul_rn(4.0f, nwo)), cosl);
+									wgt = __fmul_rn(wgt,
+									  __ldg(&P->light_area));
+									wgt = __fdiv_rn(wgt, l2s);
+									schlick(col, lh, fr);
+								} else {
+									wgt = __fmul_rn(ndotl, cosl);
+									wgt = __fmul_rn(wgt, __fmul_rn(
+									  kInvPi, __ldg(&P->light_area)));
+									wgt = __fdiv_rn(wgt, l2s);
+								}
 								for (int a = 0; a < 3; a++) {
 									sc[a] = __fmul_rn(__fmul_rn(
-									  __fmul_rn(tc[a], col[a]), em[a]),
+									  __fmul_rn(tc[a], fr[a]), em[a]),
 									  wgt);
 									so[a] = __fmaf_rn(ld[a], kEps2,
 									  pos[a]);
@@ -578,7 +656,47 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 								want_shadow = true;
 							}
 						}
-						if (k + 1u < depth) {
+						if (glossy && k + 1u < depth && nwo > 0.0f) {
+							// microfacet normal from D(m) (m.n), reflect
+							// wo; weight F G1(wo) G1(wi) (wo.m) /
+							// ((n.wo) (n.m))
+							float ct2 = __fdiv_rn(__fsub_rn(1.0f, r1),
+							  __fadd_rn(1.0f, __fmul_rn(__fsub_rn(a2, 1.0f),
+							  r1)));
+							float ct = __fsqrt_rn(ct2);
+							float s2 = __fsub_rn(1.0f, ct2);
+							float st = __fsqrt_rn(s2 > 0.0f ? s2 : 0.0f);
+							float sn, cs;
+							sincos2pi(r0, &sn, &cs);
+							float ta[3], tb[3], m[3];
+							onb(n, ta, tb);
+							float mx = __fmul_rn(st, cs);
+							float my = __fmul_rn(st, sn);
+							for (int a = 0; a < 3; a++)
+								m[a] = __fadd_rn(__fadd_rn(
+								  __fmul_rn(ta[a], mx),
+								  __fmul_rn(tb[a], my)),
+								  __fmul_rn(n[a], ct));
+							float wom = dot3(wo, m);
+							float s2w = __fmul_rn(2.0f, wom);
+							for (int a = 0; a < 3; a++)
+								nd[a] = __fsub_rn(__fmul_rn(m[a], s2w),
+								  wo[a]);
+							float nwi = dot3(n, nd);
+							if (wom > 0.0f && nwi > 0.0f) {
+								float w = __fdiv_rn(__fmul_rn(__fmul_rn(
+								  ggx_g1(a2, nwo), ggx_g1(a2, nwi)), wom),
+								  __fmul_rn(nwo, ct));
+								float F[3];
+								schlick(col, wom, F);
+								T.x = __fmul_rn(__fmul_rn(T.x, F[0]), w);
+								T.y = __fmul_rn(__fmul_rn(T.y, F[1]), w);
+								T.z = __fmul_rn(__fmul_rn(T.z, F[2]), w);
+								for (int a = 0; a < 3; a++)
+									no[a] = __fmaf_rn(nd[a], kEps2, pos[a]);
+								want_ray = true;
+							}
+						} else if (!glossy && k + 1u < depth) {
 							float sn, cs;
 							sincos2pi(r0, &sn, &cs);
 							float s1 = __fsqrt_rn(r1);

@@ -316,7 +316,26 @@ bool convert_tlas(const nb_rdata *rd, std::vector<nb_qnode> &nodes,
 	return ok;
 }
 
-float build_lights(const nb_rdata *rd, std::vector<nb_glight> &lights)
+void find_emitters(const nb_rdata *rd,
+                   std::unordered_map<uint32_t, std::vector<uint32_t>> &out)
+{
+	out.clear();
+	for (uint32_t i = 0; i < rd->instcnt; i++) {
+		const nb_rinst *ri = &rd->insts[i];
+		if (out.count(ri->triofs))
+			continue;
+		std::vector<uint32_t> &e = out[ri->triofs];
+		for (uint32_t t = 0; t < ri->tricnt; t++) {
+			const nb_rnrm *rn = &rd->nrms[ri->triofs + t];
+			if (rd->mtls[rn->mtlid].flags & NB_FLAG_EMISSIVE)
+				e.push_back(t);
+		}
+	}
+}
+
+float build_lights(const nb_rdata *rd, std::vector<nb_glight> &lights,
+                   const std::unordered_map<uint32_t,
+                   std::vector<uint32_t>> *emitters)
 {
 	lights.clear();
 	double total = 0.0;
@@ -338,7 +357,16 @@ float build_lights(const nb_rdata *rd, std::vector<nb_glight> &lights)
 		  (A[0] * A[8] - A[2] * A[6]) / det, (A[2] * A[3] - A[0] * A[5]) / det,
 		  (A[3] * A[7] - A[4] * A[6]) / det, (A[1] * A[6] - A[0] * A[7]) / det,
 		  (A[0] * A[4] - A[1] * A[3]) / det};
-		for (uint32_t t = 0; t < ri->tricnt; t++) {
+		const std::vector<uint32_t> *em = nullptr;
+		if (emitters) {
+			auto it = emitters->find(ri->triofs);
+			if (it == emitters->end() || it->second.empty())
+				continue;
+			em = &it->second;
+		}
+		uint32_t cnt = em ? (uint32_t)em->size() : ri->tricnt;
+		for (uint32_t k = 0; k < cnt; k++) {
+			uint32_t t = em ? (*em)[k] : k;
 			const nb_rnrm *rn = &rd->nrms[ri->triofs + t];
 			const nb_rmtl *m = &rd->mtls[rn->mtlid];
 			if (!(m->flags & NB_FLAG_EMISSIVE))

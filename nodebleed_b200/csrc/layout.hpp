@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "gpulayout.h"
@@ -32,9 +33,19 @@ bool convert_tlas(const nb_rdata *rd, std::vector<nb_qnode> &nodes,
                   std::vector<uint32_t> &irefs, uint32_t inst_base,
                   uint32_t *root, bvh_stats *st, std::string *err);
 
+// Mesh-local ids of the EMISSIVE triangles of every mesh (keyed by its
+// triofs) that an instance of rd uses: the per-mesh scan build_lights
+// needs, done once per static upload.
+void find_emitters(const nb_rdata *rd,
+                   std::unordered_map<uint32_t, std::vector<uint32_t>> &out);
+
 // World-space emitting triangles of instances whose material is EMISSIVE,
-// with an area CDF; returns the total area.
-float build_lights(const nb_rdata *rd, std::vector<nb_glight> &lights);
+// with an area CDF; returns the total area.  `emitters` (from
+// find_emitters) limits the scan to emissive triangles; null scans every
+// triangle of every instance.
+float build_lights(const nb_rdata *rd, std::vector<nb_glight> &lights,
+                   const std::unordered_map<uint32_t,
+                   std::vector<uint32_t>> *emitters = nullptr);
 
 // Quantise one node: child boxes (min/max per slot; empty slots have
 // min > max) into n (origin, exponents, qlo/qhi).  Exposed for tests.

@@ -70,6 +70,8 @@ struct DevBuf {
 struct SceneHost {
 	nb_rdata *rd = nullptr;
 	std::unordered_map<uint32_t, uint32_t> root_of; // triofs -> BLAS root
+	// triofs -> mesh-local ids of its emissive triangles
+	std::unordered_map<uint32_t, std::vector<uint32_t>> emitters;
 	uint32_t nrm_base = 0, mtl_base = 0, inst_base = 0, ntri = 0, nmtl = 0;
 	uint32_t blas_depth = 0, tlas_depth = 0, tlas_root = 0;
 	uint32_t depth = 1;   // max path depth of this scene
@@ -1053,6 +1055,7 @@ int upload_static_all(Ctx *c)
 		}
 		for (uint32_t t = 0; t < maxtri; t++)
 			maxmtl = std::max(maxmtl, rd->nrms[t].mtlid + 1u);
+		find_emitters(rd, h.emitters);
 		h.nrm_base = nrm_base;
 		h.mtl_base = mtl_base;
 		h.ntri = maxtri;
@@ -1139,7 +1142,7 @@ int upload_dynamic_all(Ctx *c)
 			g.pad = 0;
 			gi.push_back(g);
 		}
-		h.light_area = build_lights(rd, h.lights);
+		h.light_area = build_lights(rd, h.lights, &h.emitters);
 		h.light_off = (uint32_t)lights.size();
 		lights.insert(lights.end(), h.lights.begin(), h.lights.end());
 	}

@@ -978,6 +978,25 @@ static uint32_t pick_light(const float *lights, uint32_t n, float r)
 
 struct shadow { struct v3 o, d, c; float tfar; int live; };
 
+// GGX (Trowbridge-Reitz) microfacet conductor with alpha = roughness
+// (Walter, Marschner, Li, Torrance 2007): Smith's separable masking term
+// for GGX, G1(v) = 2 n.v / (n.v + sqrt(a^2 + (1 - a^2) (n.v)^2)), and
+// Schlick's Fresnel with F0 = the albedo.  The reference carries metallic
+// and roughness in rmtl (rend.h:54-61) but never shades with them.
+static float ggx_g1(float a2, float nv)
+{
+	return (2.0f * nv) / (nv + sqrtf(a2 + (1.0f - a2) * (nv * nv)));
+}
+
+static struct v3 schlick(struct v3 f0, float c)
+{
+	float m = 1.0f - c;
+	float m2 = m * m;
+	float m5 = (m2 * m2) * m;
+	return v3(f0.x + (1.0f - f0.x) * m5, f0.y + (1.0f - f0.y) * m5,
+	  f0.z + (1.0f - f0.z) * m5);
+}
+
 // Radiance of one path (the GPU wavefront kernels follow the same steps,
 // bounce by bounce).
 static struct v3 path_radiance(const struct nb_rdata *rd,
@@ -1029,7 +1048,8 @@ static struct v3 path_radiance(const struct nb_rdata *rd,
 				L = vadd(L, vmul(T, col));
 			break;
 		}
-		if (mt->metallic >= 0.5f) { // perfect mirror
+		int glossy = mt->metallic >= 0.5f && mt->roughness > 0.0f;
+		if (mt->metallic >= 0.5f && !glossy) { // perfect mirror
 			float dn = vdot(d, n);
 			d = vsub(d, vscale(n, 2.0f * dn));
 			T = vmul(T, col);
@@ -1038,6 +1058,11 @@ static struct v3 path_radiance(const struct nb_rdata *rd,
 			continue;
 		}
 		spec = 0;
+		struct v3 wo = vscale(d, -1.0f);
+		float nwo = vdot(n, wo);
+		float a2 = mt->roughness * mt->roughness;
+		if (glossy && !(nwo > 0.0f))
+			break;
 		// next-event estimation to one point on the emitters
 		// (rend.c:3243-3267)
 		if (cfg->nlights) {
@@ -1056,11 +1081,27 @@ static struct v3 path_radiance(const struct nb_rdata *rd,
 			float cosl = -vdot(v3(lt[9], lt[10], lt[11]), ld);
 			float tfar = ldist - 2.0f * EPS2F;
 			if (ndotl > 0.0f && cosl > 0.0f && tfar > 0.0f) {
-				float wgt = ndotl * cosl;
-				wgt = wgt * (INV_PI_F * cfg->light_area);
-				wgt = wgt / l2;
-				struct v3 c = vscale(vmul(vmul(T, col),
-				  v3(lt[12], lt[13], lt[14])), wgt);
+				struct v3 c;
+				if (glossy) {
+					// f = F D G / (4 n.wo n.l); times n.l cosl
+					// area / l^2
+					struct v3 h = vunit(vadd(wo, ld));
+					float nh = vdot(n, h), lh = vdot(ld, h);
+					float dd = (nh * nh) * (a2 - 1.0f) + 1.0f;
+					float D = (a2 * INV_PI_F) / (dd * dd);
+					float G = ggx_g1(a2, nwo) * ggx_g1(a2, ndotl);
+					float wgt = ((D * G) / (4.0f * nwo)) * cosl;
+					wgt = wgt * cfg->light_area;
+					wgt = wgt / l2;
+					c = vscale(vmul(vmul(T, schlick(col, lh)),
+					  v3(lt[12], lt[13], lt[14])), wgt);
+				} else {
+					float wgt = ndotl * cosl;
+					wgt = wgt * (INV_PI_F * cfg->light_area);
+					wgt = wgt / l2;
+					c = vscale(vmul(vmul(T, col),
+					  v3(lt[12], lt[13], lt[14])), wgt);
+				}
 				struct v3 so = vfma(ld, EPS2F, pos);
 				(*rays)++;
 				if (!any(tfar, so.x, so.y, so.z, ld.x, ld.y,
@@ -1070,6 +1111,32 @@ static struct v3 path_radiance(const struct nb_rdata *rd,
 		}
 		if (k + 1 >= cfg->depth)
 			break;
+		if (glossy) {
+			// microfacet normal from D(m) (m.n): cos^2 = (1 - r1) /
+			// (1 + (a^2 - 1) r1); reflect wo; weight F G1(wo) G1(wi)
+			// (wo.m) / ((n.wo) (n.m))
+			float ct2 = (1.0f - r1) / (1.0f + (a2 - 1.0f) * r1);
+			float ct = sqrtf(ct2);
+			float s2 = 1.0f - ct2;
+			float st = sqrtf(s2 > 0.0f ? s2 : 0.0f);
+			float sn, cs;
+			orc_sincos2pi(r0, &sn, &cs);
+			struct v3 ta, bta;
+			onb(n, &ta, &bta);
+			struct v3 m = vadd(vadd(vscale(ta, st * cs),
+			  vscale(bta, st * sn)), vscale(n, ct));
+			float wom = vdot(wo, m);
+			struct v3 wi = vsub(vscale(m, 2.0f * wom), wo);
+			float nwi = vdot(n, wi);
+			if (!(wom > 0.0f) || !(nwi > 0.0f))
+				break;
+			float w = ((ggx_g1(a2, nwo) * ggx_g1(a2, nwi)) * wom) /
+			  (nwo * ct);
+			T = vscale(vmul(T, schlick(col, wom)), w);
+			d = wi;
+			o = vfma(d, EPS2F, pos);
+			continue;
+		}
 		// cosine-weighted bounce (rend.c:3135-3140, 3270-3288)
 		float sn, cs;
 		orc_sincos2pi(r0, &sn, &cs);
@@ -1083,6 +1150,56 @@ static struct v3 path_radiance(const struct nb_rdata *rd,
 		o = vfma(d, EPS2F, pos);
 	}
 	return L;
+}
+
+int orc_ggx_sample(const float nn[3], const float wwo[3], float alpha,
+                   const float f0[3], float r0, float r1, float wi[3],
+                   float w[3])
+{
+	struct v3 n = v3(nn[0], nn[1], nn[2]), wo = v3(wwo[0], wwo[1], wwo[2]);
+	float a2 = alpha * alpha, nwo = vdot(n, wo);
+	float ct2 = (1.0f - r1) / (1.0f + (a2 - 1.0f) * r1);
+	float ct = sqrtf(ct2);
+	float s2 = 1.0f - ct2;
+	float st = sqrtf(s2 > 0.0f ? s2 : 0.0f);
+	float sn, cs;
+	orc_sincos2pi(r0, &sn, &cs);
+	struct v3 ta, bta;
+	onb(n, &ta, &bta);
+	struct v3 m = vadd(vadd(vscale(ta, st * cs), vscale(bta, st * sn)),
+	  vscale(n, ct));
+	float wom = vdot(wo, m);
+	struct v3 d = vsub(vscale(m, 2.0f * wom), wo);
+	float nwi = vdot(n, d);
+	wi[0] = d.x;
+	wi[1] = d.y;
+	wi[2] = d.z;
+	if (!(wom > 0.0f) || !(nwi > 0.0f) || !(nwo > 0.0f))
+		return 0;
+	float g = ((ggx_g1(a2, nwo) * ggx_g1(a2, nwi)) * wom) / (nwo * ct);
+	struct v3 F = schlick(v3(f0[0], f0[1], f0[2]), wom);
+	w[0] = F.x * g;
+	w[1] = F.y * g;
+	w[2] = F.z * g;
+	return 1;
+}
+
+void orc_ggx_eval(const float nn[3], const float wwo[3], const float wwi[3],
+                  float alpha, const float f0[3], float f[3])
+{
+	struct v3 n = v3(nn[0], nn[1], nn[2]), wo = v3(wwo[0], wwo[1], wwo[2]);
+	struct v3 ld = v3(wwi[0], wwi[1], wwi[2]);
+	float a2 = alpha * alpha, nwo = vdot(n, wo), ndotl = vdot(n, ld);
+	struct v3 h = vunit(vadd(wo, ld));
+	float nh = vdot(n, h), lh = vdot(ld, h);
+	float dd = (nh * nh) * (a2 - 1.0f) + 1.0f;
+	float D = (a2 * INV_PI_F) / (dd * dd);
+	float G = ggx_g1(a2, nwo) * ggx_g1(a2, ndotl);
+	float k = (D * G) / ((4.0f * nwo) * ndotl);
+	struct v3 F = schlick(v3(f0[0], f0[1], f0[2]), lh);
+	f[0] = F.x * k;
+	f[1] = F.y * k;
+	f[2] = F.z * k;
 }
 
 struct rbatch {

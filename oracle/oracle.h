@@ -126,6 +126,18 @@ uint32_t orc_pcg_first(uint64_t seed, uint32_t frame, uint64_t path,
                        uint32_t count, uint32_t *out);
 void     orc_sincos2pi(float u, float *s, float *c);
 
+// GGX conductor of the path tracer, exported for unit tests: for shading
+// normal n, outgoing direction wo (both unit, n.wo > 0), roughness alpha
+// and uniforms r0, r1, the sampled direction wi and the sample weight
+// F G1(wo) G1(wi) (wo.m) / ((n.wo) (n.m)) with F0 = f0 (w[3]); returns 0
+// when the sample leaves the hemisphere.  orc_ggx_eval gives f(wo, wi)
+// (the BRDF, per channel).
+int  orc_ggx_sample(const float n[3], const float wo[3], float alpha,
+                    const float f0[3], float r0, float r1, float wi[3],
+                    float w[3]);
+void orc_ggx_eval(const float n[3], const float wo[3], const float wi[3],
+                  float alpha, const float f0[3], float f[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -56,6 +56,10 @@ def oracle():
         L.orc_sincos2pi.argtypes = [C.c_float, vp, vp]
         L.orc_mt_bounds.argtypes = [vp, vp, vp, u32, vp]
         L.orc_bruteforce_f64.argtypes = [vp, vp, u32, vp, vp]
+        L.orc_ggx_sample.argtypes = [vp, vp, C.c_float, vp, C.c_float,
+                                     C.c_float, vp, vp]
+        L.orc_ggx_sample.restype = C.c_int
+        L.orc_ggx_eval.argtypes = [vp, vp, vp, C.c_float, vp, vp]
         _ORC = L
     return _ORC
 
@@ -81,6 +85,26 @@ def ref():
         L.rend_staticinit(16, 8)
         _REF = L
     return _REF
+
+
+def ggx_sample(n, wo, alpha, f0, r0, r1):
+    """(ok, wi, weight) of the oracle's GGX sampling step."""
+    f = lambda v: np.ascontiguousarray(v, np.float32)
+    n, wo, f0 = f(n), f(wo), f(f0)
+    wi, w = np.zeros(3, np.float32), np.zeros(3, np.float32)
+    ok = oracle().orc_ggx_sample(n.ctypes.data, wo.ctypes.data, alpha,
+                                 f0.ctypes.data, r0, r1, wi.ctypes.data,
+                                 w.ctypes.data)
+    return ok, wi, w
+
+
+def ggx_eval(n, wo, wi, alpha, f0):
+    f = lambda v: np.ascontiguousarray(v, np.float32)
+    n, wo, wi, f0 = f(n), f(wo), f(wi), f(f0)
+    out = np.zeros(3, np.float32)
+    oracle().orc_ggx_eval(n.ctypes.data, wo.ctypes.data, wi.ctypes.data,
+                          alpha, f0.ctypes.data, out.ctypes.data)
+    return out
 
 
 def fn_addr(lib, name):

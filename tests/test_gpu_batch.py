@@ -15,7 +15,8 @@ pytestmark = pytest.mark.gpu
 SCENES = [(api.SCENE_TINY, 1, 64, 48, 1, 3),
           (api.SCENE_SMALL, 1, 160, 90, 4, 5),
           (api.SCENE_TINY, 2, 96, 72, 2, 8),
-          (api.SCENE_SMALL, 3, 120, 68, 1, 12)]
+          (api.SCENE_SMALL, 3, 120, 68, 1, 12),
+          (api.SCENE_GLOSSY, 1, 80, 48, 2, 6)]
 
 
 def _rdatas(scenes=SCENES):

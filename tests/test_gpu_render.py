@@ -29,7 +29,8 @@ def _gpu_frame(rd, depth, mode, seed):
 
 
 @pytest.mark.parametrize("fam,seed,depth", [
-    (api.SCENE_TINY, 1, 3), (api.SCENE_TINY, 2, 5), (api.SCENE_SMALL, 1, 2)])
+    (api.SCENE_TINY, 1, 3), (api.SCENE_TINY, 2, 5), (api.SCENE_SMALL, 1, 2),
+    (api.SCENE_GLOSSY, 1, 6), (api.SCENE_GLOSSY, 2, 8)])
 def test_path_frame_matches_oracle(gpu, fam, seed, depth):
     scene = api.Scene(fam, seed)
     rd = api.RenderData(scene)
