@@ -49,6 +49,10 @@ def parse():
                    help="BLAS count (0 = the workload's 64)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--sort", type=int, default=0,
+                   help="1: reorder each bounce's rays before tracing")
+    p.add_argument("--block", type=int, default=0,
+                   help="trace block size (0 = library default)")
     p.add_argument("--sched", type=int, default=0,
                    help="traversal schedule (0 = library default)")
     p.add_argument("--count", action="store_true",
@@ -420,6 +424,8 @@ def run_ours(a):
     rd = api.RenderData(scene, a.width, a.height, a.spp)
     gr = api.GpuRenderer(rd, max_depth=a.depth, seed=1 + rank, timing=True,
                          device=dev, sched=a.sched).upload()
+    if a.sort or a.block:
+        gr.set_tune(sort=a.sort, block=a.block)
     stream = torch.cuda.ExternalStream(gr.stream(), device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     lights, area = gr.lights()

@@ -126,7 +126,10 @@ struct rendgpu_tune {
 	                    (0 = one wave of all paths) */
 	uint32_t sched;  /* traversal schedule as rendgpu_cfg.sched (0 = cfg's) */
 	float    ms;     /* autotune: median device ms per frame measured */
-	uint32_t reserved[3];
+	uint32_t sort;   /* 1: reorder each bounce's rays by direction octant
+	                    and origin cell before tracing (single-scene
+	                    PATH/PRIMARY contexts); 0: queue order */
+	uint32_t reserved[2];
 };
 
 /* Per-scene counts of a batch frame. */

@@ -93,16 +93,19 @@ class RendgpuStats(C.Structure):
 class RendgpuTune(C.Structure):
     _fields_ = [("block", C.c_uint32), ("stack", C.c_uint32),
                 ("queue", C.c_uint32), ("sched", C.c_uint32),
-                ("ms", C.c_float), ("reserved", C.c_uint32 * 3)]
+                ("ms", C.c_float), ("sort", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
     def as_dict(self):
         return {"block": self.block, "stack": self.stack,
-                "queue": self.queue, "sched": self.sched, "ms": self.ms}
+                "queue": self.queue, "sched": self.sched, "ms": self.ms,
+                "sort": self.sort}
 
     @classmethod
-    def make(cls, block=0, stack=0, queue=0, sched=0):
+    def make(cls, block=0, stack=0, queue=0, sched=0, sort=0):
         t = cls()
         t.block, t.stack, t.queue, t.sched = block, stack, queue, sched
+        t.sort = sort
         return t
 
 

@@ -749,6 +749,116 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 	}
 }
 
+// ---------------------------------------------------------- reordering --
+//
+// Counting sort of a ray queue by a 12-bit key: direction octant (3 bits)
+// over a 3-bit-per-axis cell of the origin in the scene box, so rays of a
+// warp share their child order and nearby geometry.  Order within a key is
+// arbitrary; every path's result is independent of queue order.
+
+constexpr uint32_t kSortKeys = 4096;
+
+__device__ __forceinline__ uint32_t ray_key(float4 a, float4 b,
+                                            const NrcBox &B)
+{
+	uint32_t oct = (b.x < 0.0f ? 1u : 0u) | (b.y < 0.0f ? 2u : 0u) |
+	  (b.z < 0.0f ? 4u : 0u);
+	float p[3] = {a.x, a.y, a.z};
+	uint32_t cell = 0;
+	for (int k = 0; k < 3; k++) {
+		float u = (p[k] - B.lo[k]) * B.inv[k] * 8.0f;
+		int c = (int)fminf(fmaxf(u, 0.0f), 7.0f);
+		cell |= (uint32_t)c << (3 * k);
+	}
+	return (oct << 9) | cell;
+}
+
+// Histogram of the keys of queue `q` (count *n) into hist (kSortKeys).
+__global__ void __launch_bounds__(256) k_sort_hist(const float4 *q,
+                                                   const uint32_t *n,
+                                                   NrcBox B, uint32_t *hist)
+{
+	__shared__ uint32_t h[kSortKeys];
+	for (uint32_t i = threadIdx.x; i < kSortKeys; i += blockDim.x)
+		h[i] = 0u;
+	__syncthreads();
+	uint32_t cnt = *n;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
+	     i += gridDim.x * blockDim.x)
+		atomicAdd(&h[ray_key(q[2u * i], q[2u * i + 1u], B)], 1u);
+	__syncthreads();
+	for (uint32_t i = threadIdx.x; i < kSortKeys; i += blockDim.x)
+		if (h[i])
+			atomicAdd(&hist[i], h[i]);
+}
+
+// Exclusive scan of hist into offs; hist cleared for the next use
+// (one block of 1024 threads, 4 keys each).
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t *hist,
+                                                    uint32_t *offs)
+{
+	__shared__ uint32_t part[1024];
+	uint32_t t = threadIdx.x;
+	uint32_t v[4], s = 0;
+	for (int k = 0; k < 4; k++) {
+		v[k] = hist[4u * t + k];
+		hist[4u * t + k] = 0u;
+		s += v[k];
+	}
+	part[t] = s;
+	__syncthreads();
+	for (uint32_t d = 1; d < 1024u; d <<= 1) {
+		uint32_t x = t >= d ? part[t - d] : 0u;
+		__syncthreads();
+		part[t] += x;
+		__syncthreads();
+	}
+	uint32_t base = part[t] - s;
+	for (int k = 0; k < 4; k++) {
+		offs[4u * t + k] = base;
+		base += v[k];
+	}
+}
+
+// Scatter queue `src` (count *n) to `dst` in key order; *ndst = *n.
+__global__ void __launch_bounds__(256) k_sort_scatter(const float4 *src,
+                                                      const uint32_t *n,
+                                                      NrcBox B,
+                                                      uint32_t *offs,
+                                                      float4 *dst,
+                                                      uint32_t *ndst)
+{
+	uint32_t cnt = *n;
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		*ndst = cnt;
+	for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < cnt;
+	     i0 += gridDim.x * blockDim.x) {
+		uint32_t i = i0 + threadIdx.x;
+		bool live = i < cnt;
+		float4 a = make_float4(0, 0, 0, 0), b = a;
+		uint32_t key = 0xffffffffu;
+		if (live) {
+			a = src[2u * i];
+			b = src[2u * i + 1u];
+			key = ray_key(a, b, B);
+		}
+		// one atomic per run of equal keys in the warp
+		uint32_t act = __ballot_sync(0xffffffffu, live);
+		if (live) {
+			uint32_t peers = __match_any_sync(act, key);
+			uint32_t leader = __ffs(peers) - 1;
+			uint32_t lane = threadIdx.x & 31u;
+			uint32_t base = 0;
+			if (lane == leader)
+				base = atomicAdd(&offs[key], (uint32_t)__popc(peers));
+			base = __shfl_sync(peers, base, leader);
+			uint32_t pos = base + __popc(peers & ((1u << lane) - 1u));
+			dst[2u * pos] = a;
+			dst[2u * pos + 1u] = b;
+		}
+	}
+}
+
 // relMSE of the accumulated image (acc / samples) against a reference
 // image: mean over pixels and channels of (x - r)^2 / (r^2 + 0.01),
 // accumulated in FP64 (the only double-precision arithmetic on the device).

@@ -101,6 +101,7 @@ struct Ctx {
 	std::vector<ScenePar> par;  // host copy of the table
 	// frame: queues (capacity qcap entries), per-path state (npaths)
 	DevBuf q0, q1, hits, shadow, scol, pT, pL, rng, acc, buf, cnt, rays, scn;
+	DevBuf sortbuf; // ray reordering: key histogram and offsets
 	uint32_t npaths = 0, npix = 0, nslots = 0, qcap = 0;
 	bool     have_frame = false;
 	// captured frame (RENDGPU_FLAG_GRAPH and batches)
@@ -385,6 +386,14 @@ int launch_occluded(Ctx *c, const float4 *rays, const uint32_t *count,
 	}
 	NB_CK(c, cudaGetLastError());
 	return 0;
+}
+
+// Ray reordering applies to single-scene frames without the cache (whose
+// query and record order would change with it).
+bool sorts(const Ctx *c)
+{
+	return c->tune.sort && c->sc.size() == 1 &&
+	  c->cfg.mode != RENDGPU_MODE_NRC;
 }
 
 FrameDev frame_of(Ctx *c)
@@ -701,6 +710,10 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 {
 	DScene S = scene_of(c);
 	int rc = 0;
+	// reordering: rays are traced and shaded from q[0]; shading appends
+	// to q[1], which is sorted back into q[0]
+	bool sorting = sorts(c);
+	uint32_t *hist = c->sortbuf.as<uint32_t>();
 	c->st.launches = 0;
 	c->st.trace_launches = 0;
 	NB_CK(c, cudaMemsetAsync(c->cnt.p, 0, 64 * sizeof(uint32_t), c->stream));
@@ -717,7 +730,7 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		NB_CK(c, cudaGetLastError());
 		c->st.launches++;
 		for (uint32_t k = 0; k < A.depth; k++) {
-			uint32_t cur = k & 1u;
+			uint32_t cur = sorting ? 0u : (k & 1u);
 			E->trace.push_back(c->nev);
 			ev_record(c);
 			rc = launch_trace(c, F.q[cur], F.cnt + cur, F.cnt + 4, F.hits,
@@ -743,6 +756,17 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 					return rc;
 				ev_record(c);
 				c->st.launches++;
+			}
+			if (sorting && k + 1u < A.depth) {
+				int g = grid_for(c, hi - lo, 256);
+				k_sort_hist<<<g, 256, 0, c->stream>>>(F.q[1], F.cnt + 1,
+				  c->box, hist);
+				k_sort_scan<<<1, 1024, 0, c->stream>>>(hist,
+				  hist + kSortKeys);
+				k_sort_scatter<<<g, 256, 0, c->stream>>>(F.q[1], F.cnt + 1,
+				  c->box, hist + kSortKeys, F.q[0], F.cnt);
+				NB_CK(c, cudaGetLastError());
+				c->st.launches += 3;
 			}
 		}
 	}
@@ -927,7 +951,7 @@ void free_ctx(Ctx *c)
 {
 	drop_graph(c);
 	DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs, &c->insts,
-	  &c->nrms, &c->mtls, &c->lights, &c->sp, &c->scn, &c->q0, &c->q1, &c->hits, &c->shadow,
+	  &c->nrms, &c->mtls, &c->lights, &c->sp, &c->scn, &c->sortbuf, &c->q0, &c->q1, &c->hits, &c->shadow,
 	  &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
 	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_wf,
 	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
@@ -946,7 +970,8 @@ void free_ctx(Ctx *c)
 uint64_t held_bytes(const Ctx *c)
 {
 	const DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs,
-	  &c->insts, &c->nrms, &c->mtls, &c->lights, &c->sp, &c->scn, &c->q0, &c->q1, &c->hits,
+	  &c->insts, &c->nrms, &c->mtls, &c->lights, &c->sp, &c->scn,
+	  &c->sortbuf, &c->q0, &c->q1, &c->hits,
 	  &c->shadow, &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf,
 	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
 	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
@@ -1234,6 +1259,9 @@ int alloc_frame(Ctx *c)
 	NB_CK(c, c->buf.ensure(npix * 4));
 	NB_CK(c, c->scn.ensure(c->sc.size() * 16));
 	NB_CK(c, c->sp.ensure(c->sc.size() * sizeof(ScenePar)));
+	NB_CK(c, c->sortbuf.ensure(2 * kSortKeys * sizeof(uint32_t)));
+	NB_CK(c, cudaMemsetAsync(c->sortbuf.p, 0, 2 * kSortKeys *
+	  sizeof(uint32_t), c->stream));
 	c->npaths = (uint32_t)np;
 	c->npix = (uint32_t)npix;
 	c->nslots = (uint32_t)nslots;
@@ -1278,7 +1306,7 @@ bool tune_valid(const rendgpu_tune *t)
 {
 	return t && (t->block == 0 || t->block == 64 || t->block == 128 ||
 	  t->block == 256) && (t->stack == 0 || t->stack == 24 ||
-	  t->stack == 32 || t->stack == 48) && t->sched <= 3;
+	  t->stack == 32 || t->stack == 48) && t->sched <= 3 && t->sort <= 1;
 }
 
 // Apply launch parameters; a new queue capacity re-sizes the queues (and
@@ -1293,6 +1321,7 @@ int set_tune(Ctx *c, const rendgpu_tune *t)
 	c->tune.stack = t->stack;
 	c->tune.queue = t->queue;
 	c->tune.sched = t->sched;
+	c->tune.sort = t->sort;
 	drop_graph(c);
 	if (requeue && c->have_frame)
 		return alloc_frame(c);
@@ -1308,6 +1337,7 @@ rendgpu_tune effective_tune(const Ctx *c)
 	t.queue = c->tune.queue;
 	int sc = sched_of(c);
 	t.sched = sc == kSchedStep ? 1u : sc == kSchedPhase ? 2u : 3u;
+	t.sort = sorts(c) ? 1u : 0u;
 	return t;
 }
 
@@ -1334,7 +1364,8 @@ int tune_measure(Ctx *c, const rendgpu_tune &t, uint32_t frames, float *ms)
 }
 
 // Coordinate-descent autotuner over the traversal schedule, the trace
-// block size, the stack depth and the queue capacity: each knob in turn
+// block size, the stack depth, the queue capacity and (single-scene path
+// frames) ray reordering: each knob in turn
 // takes the value with the lowest measured frame time, the others held at
 // the best so far.  Frames re-render the current sample index (rd->samples
 // is not advanced); the accumulator is cleared afterwards.
@@ -1371,7 +1402,7 @@ int autotune(Ctx *c, uint32_t frames, rendgpu_tune *best_out,
 		if (q >= 65536u && q < c->nslots)
 			queues.push_back(q);
 	}
-	for (int knob = 0; knob < 4 && !rc; knob++) {
+	for (int knob = 0; knob < 5 && !rc; knob++) {
 		std::vector<uint32_t> vals;
 		if (knob == 0)
 			vals = {3u, 1u};
@@ -1381,15 +1412,17 @@ int autotune(Ctx *c, uint32_t frames, rendgpu_tune *best_out,
 			for (int st : kStacks)
 				if (need_stack(c) <= (uint32_t)st)
 					vals.push_back((uint32_t)st);
-		} else {
+		} else if (knob == 3) {
 			vals = queues;
 			vals.push_back(0u);
+		} else if (c->sc.size() == 1 && c->cfg.mode != RENDGPU_MODE_NRC) {
+			vals = {0u, 1u};
 		}
 		rendgpu_tune base = best;
 		for (uint32_t v : vals) {
 			rendgpu_tune t = base;
 			uint32_t *field = knob == 0 ? &t.sched : knob == 1 ? &t.block :
-			  knob == 2 ? &t.stack : &t.queue;
+			  knob == 2 ? &t.stack : knob == 3 ? &t.queue : &t.sort;
 			if (*field == v)
 				continue;
 			*field = v;

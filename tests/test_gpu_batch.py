@@ -125,3 +125,24 @@ def test_batch_rejects_radiance_cache_mode(gpu):
     rds = _rdatas(SCENES[:1])
     with pytest.raises(api.RendgpuError):
         api.BatchRenderer(rds, mode=api.MODE_NRC)
+
+
+@pytest.mark.parametrize("tune", [{"sort": 1}, {"sort": 1, "queue": 9000}])
+def test_ray_reordering_changes_no_bits(gpu, tune):
+    """Reordering each bounce's rays (single-scene contexts) leaves every
+    path's result unchanged."""
+    scenes = [SCENES[1]]
+    base, rays0 = _alone(frames=2, scenes=scenes)
+    rd = _rdatas(scenes)[0]
+    gr = api.GpuRenderer(rd, max_depth=scenes[0][5], seed=7).upload()
+    gr.set_tune(**tune)
+    assert gr.get_tune()["sort"] == 1
+    rays = []
+    for _ in range(2):
+        gr.frame()
+        st = gr.stats()
+        rays.append((st["closest_rays"], st["shadow_rays"]))
+    gr.readback(1)
+    assert np.array_equal(rd.acc(), base[0])
+    assert rays == rays0[0]
+    gr.close()
