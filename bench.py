@@ -107,6 +107,18 @@ def allreduce(x, op):
     return float(t.item())
 
 
+def job_rate(units, ms, world):
+    """Whole-job rate of N replicas: all ranks' units over the slowest
+    rank's device time (units per ms; collective on every rank).  Returns
+    (rate, slowest ms, all units)."""
+    import torch
+    ms_max = allreduce(ms, torch.distributed.ReduceOp.MAX) if world > 1 \
+        else ms
+    units_all = allreduce(units, torch.distributed.ReduceOp.SUM) \
+        if world > 1 else units
+    return units_all / ms_max, ms_max, units_all
+
+
 def barrier():
     import torch.distributed as dist
     if dist.is_available() and dist.is_initialized():
@@ -460,11 +472,9 @@ def run_ours(a):
     cl = clocks.stop()
     barrier()
     ms = sum(s.elapsed_time(e) for s, e in ev)
-    ms_max = allreduce(ms, torch.distributed.ReduceOp.MAX) if world > 1 else ms
-    rays_all = allreduce(rays, torch.distributed.ReduceOp.SUM) \
-        if world > 1 else rays
+    rate, ms_max, rays_all = job_rate(rays, ms, world)
     samples_all = a.width * a.height * a.spp * a.steps * world
-    value = rays_all / (ms_max / 1e3) / 1e6
+    value = rate / 1e3  # rays per ms -> Mrays/s
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -494,11 +504,8 @@ def run_ours(a):
             parts[2] += t4 - t3
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        dt_max = allreduce(dt, torch.distributed.ReduceOp.MAX) \
-            if world > 1 else dt
-        e2e_all = allreduce(e2e_rays, torch.distributed.ReduceOp.SUM) \
-            if world > 1 else e2e_rays
-        e2e = {"value": e2e_all / dt_max / 1e6, "unit": "Mrays/s",
+        e2e_rate, _, _ = job_rate(e2e_rays, dt, world)
+        e2e = {"value": e2e_rate / 1e6, "unit": "Mrays/s",
                "h2d_bytes_per_step": h2d // a.steps,
                "d2h_bytes_per_step": d2h // a.steps,
                "timing": "wall clock around upload_dynamic + render + "
