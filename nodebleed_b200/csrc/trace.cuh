@@ -98,6 +98,18 @@ __device__ __forceinline__ float sel3(float x, float y, float z, uint32_t k)
 	return k == 0 ? x : (k == 1 ? y : z);
 }
 
+// Hardware reciprocal (relative error below 2^-22; 0 -> inf with the sign
+// kept).  Slab distances computed with it carry that relative error on
+// every axis alike within 2 ulp, which the far-plane widening 1 + 2^-20
+// covers, so no box the ray enters is culled: node pruning only, hits are
+// decided by the triangle test.
+__device__ __forceinline__ float rcp_approx(float x)
+{
+	float r;
+	asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+	return r;
+}
+
 __device__ __forceinline__ void tray_slab(TRay &r, float ox, float oy,
                                           float oz, float dx, float dy,
                                           float dz)
@@ -108,9 +120,9 @@ __device__ __forceinline__ void tray_slab(TRay &r, float ox, float oy,
 	r.dx = dx;
 	r.dy = dy;
 	r.dz = dz;
-	r.ix = 1.0f / dx;
-	r.iy = 1.0f / dy;
-	r.iz = 1.0f / dz;
+	r.ix = rcp_approx(dx);
+	r.iy = rcp_approx(dy);
+	r.iz = rcp_approx(dz);
 	r.oct = (signbit(r.ix) ? 1u : 0u) | (signbit(r.iy) ? 2u : 0u) |
 	  (signbit(r.iz) ? 4u : 0u);
 }
@@ -130,9 +142,12 @@ __device__ __forceinline__ void tray_watertight(TRay &r)
 	r.kx = kx;
 	r.ky = ky;
 	r.kz = kz;
-	r.sx = sel3(r.dx, r.dy, r.dz, kx) / dkz;
-	r.sy = sel3(r.dx, r.dy, r.dz, ky) / dkz;
-	r.sz = 1.0f / dkz;
+	// any per-ray constants keep the test watertight (shared vertices
+	// project identically); one rounded reciprocal and two products are
+	// cheaper than two divisions
+	r.sz = __frcp_rn(dkz);
+	r.sx = sel3(r.dx, r.dy, r.dz, kx) * r.sz;
+	r.sy = sel3(r.dx, r.dy, r.dz, ky) * r.sz;
 }
 
 __device__ __forceinline__ uint32_t qb(uint32_t w, int k)
