@@ -67,7 +67,7 @@ struct rendgpu_cfg {
 	uint64_t seed;       /* PCG32 seed of the path streams */
 	int32_t  device;     /* CUDA device ordinal */
 	uint32_t block;      /* threads per block of the trace kernels: 64,
-	                        128 or 256 (0 = 128); see rendgpu_tune */
+	                        128 or 256 (0 = 256); see rendgpu_tune */
 	uint32_t sched;      /* traversal schedule: 0 = default, 1 = step,
 	                        2 = phase, 3 = ylitie (see trace.cuh) */
 	uint32_t reserved[7]; /* [0]: float bits of the cache's Adam learning
@@ -117,7 +117,7 @@ struct rendgpu_stats {
  * Zero fields take the defaults. */
 struct rendgpu_tune {
 	uint32_t block;  /* threads per block of the trace kernels: 64, 128
-	                    (default) or 256 */
+	                    or 256 (default) */
 	uint32_t stack;  /* traversal stack entries per thread in shared memory:
 	                    24, 32 or 48; a depth below the scene's need (TLAS +
 	                    BLAS depth + 2) gives the smallest that fits */
