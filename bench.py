@@ -38,7 +38,7 @@ L2_BYTES = 126 * 1024 * 1024
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--width", type=int, default=WORKLOAD["width"])
@@ -162,8 +162,11 @@ def traffic_from_profile():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi sampling (every 100 ms, timestamped) started before the
+    warm-up, so that it runs through the timed region; stop() keeps the
+    samples taken between mark_start() and mark_end()."""
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,"
+         "clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,"
@@ -172,15 +175,25 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.p = None
+        self.t0 = self.t1 = None
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", "-i", str(index), "--query-gpu=" + self.Q,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
 
+    def mark_start(self):
+        import datetime
+        self.t0 = datetime.datetime.now()
+
+    def mark_end(self):
+        import datetime
+        self.t1 = datetime.datetime.now()
+
     def stop(self):
+        import datetime
         if not self.p:
             return None
         self.p.terminate()
@@ -189,25 +202,40 @@ class Clocks:
         except Exception:
             self.p.kill()
             out = ""
-        sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
                  "sw_power_cap"]
+        rows = []
         for line in out.splitlines():
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
+                rows.append((ts, float(f[2]), float(f[3]), f[6:10]))
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
+        if not rows:
+            return None
+        inside = [r for r in rows if self.t0 and self.t1 and
+                  self.t0 <= r[0] <= self.t1]
+        scope = "timed region"
+        if not inside:
+            # a timed region shorter than the sampling period: the samples
+            # nearest to it
+            mid = self.t0 + (self.t1 - self.t0) / 2 if self.t0 and self.t1 \
+                else rows[-1][0]
+            inside = sorted(rows, key=lambda r: abs((r[0] - mid)
+                                                   .total_seconds()))[:2]
+            scope = "nearest to the timed region"
+        reasons = set()
+        for r in inside:
+            for n, v in zip(names, r[3]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(r[1] for r in inside),
+                "sm_max_mhz": max(r[2] for r in inside),
+                "reasons": sorted(reasons), "samples": len(inside),
+                "scope": scope}
 
 
 def cpu_baseline(a, rd, lights, area, budget_s):
@@ -442,11 +470,12 @@ def run_ours(a):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     lights, area = gr.lights()
 
+    clocks = Clocks(dev)
     for _ in range(a.warmup):
         gr.frame()
     barrier()
     torch.cuda.synchronize()
-    clocks = Clocks(dev)
+    clocks.mark_start()
     ev = []
     rays = closest = 0
     trace_ms = shadow_ms = 0.0
@@ -469,6 +498,7 @@ def run_ours(a):
         trace_launches += st["trace_launches"]
         ev.append((s, e))
     torch.cuda.synchronize()
+    clocks.mark_end()
     cl = clocks.stop()
     barrier()
     ms = sum(s.elapsed_time(e) for s, e in ev)
