@@ -51,6 +51,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--sort", type=int, default=0,
                    help="1: reorder each bounce's rays before tracing")
+    p.add_argument("--fuse", type=int, default=0,
+                   help="1: shadow rays traced with the next bounce's "
+                        "closest hits, 2: separate launches, 0: default")
     p.add_argument("--block", type=int, default=0,
                    help="trace block size (0 = library default)")
     p.add_argument("--sched", type=int, default=0,
@@ -464,8 +467,8 @@ def run_ours(a):
     rd = api.RenderData(scene, a.width, a.height, a.spp)
     gr = api.GpuRenderer(rd, max_depth=a.depth, seed=1 + rank, timing=True,
                          device=dev, sched=a.sched).upload()
-    if a.sort or a.block:
-        gr.set_tune(sort=a.sort, block=a.block)
+    if a.sort or a.block or a.fuse:
+        gr.set_tune(sort=a.sort, block=a.block, fuse=a.fuse)
     stream = torch.cuda.ExternalStream(gr.stream(), device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     lights, area = gr.lights()
@@ -543,6 +546,25 @@ def run_ours(a):
                "ms_upload_render_readback": [1e3 * x / a.steps
                                              for x in parts]}
 
+    # the roofline's kernel alone: closest-hit launches timed in frames
+    # whose shadow rays go to separate launches
+    sep_trace_ms = sep_closest = sep_launches = 0
+    if rank == 0 and world == 1:
+        tune = gr.get_tune()
+        gr.set_tune(**{k: tune[k] for k in ("block", "stack", "queue",
+                                             "sched", "sort")}, fuse=2)
+        gr.frame()
+        for _ in range(2):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            gr.frame()
+            st2 = gr.stats()
+            sep_trace_ms += st2["ms_trace"]
+            sep_closest += st2["closest_rays"]
+            sep_launches += st2["trace_launches"]
+        gr.set_tune(**{k: tune[k] for k in ("block", "stack", "queue",
+                                             "sched", "sort", "fuse")})
+
     visits = None
     if a.count:
         # one context per rdata: the counting context replaces the timed one
@@ -569,7 +591,8 @@ def run_ours(a):
         nrc["config"] = {"width": a.nrc_width, "height": a.nrc_height,
                          "spp_per_frame": 1, "depth": a.depth,
                          "reference_spp": a.nrc_ref_spp,
-                         "warmup_frames": 8, "train_paths_per_frame": 65536,
+                         "warmup_frames": 4, "self_train_bounce": 3,
+                         "train_paths_per_frame": 65536,
                          "adam_lr": 1e-2}
         nrc["wall_s"] = time.perf_counter() - t0
 
@@ -599,14 +622,15 @@ def run_ours(a):
             csample = max(crays * share, 1.0)
             b_ray = (256.0 * nodes + 192.0 * leaves + 64.0 * insts) / \
                 csample + 48.0
-            per_launch_rays = closest / max(trace_launches, 1)
-            launch_ms = trace_ms / max(trace_launches, 1)
+            per_launch_rays = sep_closest / max(sep_launches, 1)
+            launch_ms = sep_trace_ms / max(sep_launches, 1)
             achieved = per_launch_rays * b_ray / (launch_ms / 1e3) / 1e9
             traffic = traffic_from_profile()
             roof = {"bound": "hbm", "achieved": achieved, "peak": peak,
                     "unit": "GB/s", "frac": achieved / peak,
                     "peak_source": peak_kind,
-                    "kernel": "k_trace (closest hit)",
+                    "kernel": "k_trace (closest hit; timed in frames "
+                              "with separate shadow launches)",
                     "bytes_per_ray": b_ray,
                     "visits_per_ray": [nodes / csample, leaves / csample,
                                        insts / csample],

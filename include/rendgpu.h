@@ -45,7 +45,10 @@ enum rendgpu_mode {
 	RENDGPU_MODE_PRIMARY = 1, /* reference live shading: (n+1)/2 * albedo */
 	RENDGPU_MODE_NRC = 2      /* path tracing ended by the radiance cache at
 	                             the first diffuse vertex after the primary
-	                             hit; 2^16 unbiased paths per frame train it */
+	                             hit; 2^16 training paths per frame, unbiased
+	                             up to bounce reserved[2] (default 3) where
+	                             the cache ends them too (self-training),
+	                             train it */
 };
 
 enum rendgpu_flags {
@@ -72,7 +75,9 @@ struct rendgpu_cfg {
 	                        2 = phase, 3 = ylitie (see trace.cuh) */
 	uint32_t reserved[7]; /* [0]: float bits of the cache's Adam learning
 	                         rate (0 = 1e-2); [1]: radiance-cache warm-up
-	                         frames of unbiased tracing (0 = 8) */
+	                         frames of unbiased tracing (0 = 4); [2]: bounce
+	                         at which training paths end in the cache after
+	                         the warm-up (0 = 3) */
 };
 
 /* A ray for the batch calls: origin, tmax, direction (32 bytes). */
@@ -95,8 +100,10 @@ struct rendgpu_stats {
 	uint32_t trace_launches; /* closest-hit trace launches of the frame */
 	uint32_t launches;       /* all kernel launches of the frame */
 	float    ms_frame;       /* device time of the frame (TIMING flag) */
-	float    ms_trace;       /* sum over closest-hit trace launches */
-	float    ms_shadow;      /* sum over shadow (any-hit) launches */
+	float    ms_trace;       /* sum over closest-hit trace launches (fused
+	                            launches also trace the previous bounce's
+	                            shadow rays; see rendgpu_tune.fuse) */
+	float    ms_shadow;      /* sum over separate shadow (any-hit) launches */
 	float    ms_shade;       /* gen + shade + accumulate */
 	uint32_t device_errors;  /* rays abandoned by a device error */
 	uint32_t max_stack;      /* traversal stack entries the scene needs */
@@ -129,7 +136,11 @@ struct rendgpu_tune {
 	uint32_t sort;   /* 1: reorder each bounce's rays by direction octant
 	                    and origin cell before tracing (single-scene
 	                    PATH/PRIMARY contexts); 0: queue order */
-	uint32_t reserved[2];
+	uint32_t fuse;   /* 1: trace each bounce's shadow rays in the launch of
+	                    the next bounce's closest hits (2 launches per
+	                    bounce instead of 3); 2: separate launches;
+	                    0: the default (fused) */
+	uint32_t reserved[1];
 };
 
 /* Per-scene counts of a batch frame. */

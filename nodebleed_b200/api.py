@@ -94,18 +94,18 @@ class RendgpuTune(C.Structure):
     _fields_ = [("block", C.c_uint32), ("stack", C.c_uint32),
                 ("queue", C.c_uint32), ("sched", C.c_uint32),
                 ("ms", C.c_float), ("sort", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("fuse", C.c_uint32), ("reserved", C.c_uint32 * 1)]
 
     def as_dict(self):
         return {"block": self.block, "stack": self.stack,
                 "queue": self.queue, "sched": self.sched, "ms": self.ms,
-                "sort": self.sort}
+                "sort": self.sort, "fuse": self.fuse}
 
     @classmethod
-    def make(cls, block=0, stack=0, queue=0, sched=0, sort=0):
+    def make(cls, block=0, stack=0, queue=0, sched=0, sort=0, fuse=0):
         t = cls()
         t.block, t.stack, t.queue, t.sched = block, stack, queue, sched
-        t.sort = sort
+        t.sort, t.fuse = sort, fuse
         return t
 
 
@@ -342,7 +342,8 @@ class GpuRenderer:
 
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
                  timing=False, device=0, count=False, sched=0,
-                 nrc_warmup=0, nrc_lr=0.0, graph=False, block=0):
+                 nrc_warmup=0, nrc_lr=0.0, graph=False, block=0,
+                 nrc_end=0):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -351,6 +352,7 @@ class GpuRenderer:
         cfg.reserved[0] = C.c_uint32.from_buffer_copy(
             C.c_float(nrc_lr)).value
         cfg.reserved[1] = nrc_warmup
+        cfg.reserved[2] = nrc_end
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
         if rc != 0:
             raise RendgpuError(rc, "rendgpu_init")

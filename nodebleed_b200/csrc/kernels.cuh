@@ -57,6 +57,9 @@ constexpr uint32_t kPathTrain = 2u;  // unbiased cache-training path
 struct FrameArgs {
 	uint32_t depth;   // bounces of the launch sequence: max over scenes
 	uint32_t mode;    // 0 path, 1 primary, 2 path with radiance cache
+	uint32_t nrc_end; // mode 2: from this bounce on, training paths and
+	                  // mirror chains end in the cache too (self-training);
+	                  // 0xffffffff: never (warm-up frames)
 };
 
 // ------------------------------------------------------------- sampling --
@@ -357,6 +360,32 @@ __global__ void __launch_bounds__(256, 4) k_shadow(DScene S, FrameDev F,
 	  sstk + threadIdx.x, blockDim.x, sink);
 }
 
+// Closest-hit trace of queue `rays` (bounce k) and, in the same launch and
+// the same persistent loop, the shadow rays of bounce ks = k - 1: lanes take
+// shadow rays once the closest-hit queue is drained, so the two queues'
+// last, slowest rays overlap instead of ending two launches.  The shadow
+// rays' contributions land in pL before bounce k is shaded, as with
+// separate launches.  Ylitie schedule only.
+template <int STACK, bool COUNT>
+__global__ void __launch_bounds__(256, 4) k_trace_fused(DScene S, FrameDev F,
+                                                     const float4 *rays,
+                                                     const uint32_t *count,
+                                                     uint32_t ks)
+{
+	extern __shared__ uint2 sstk[];
+	uint32_t n = *count, ns = F.cnt[2];
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		atomicAdd(&F.rays[0], (unsigned long long)n);
+		atomicAdd(&F.rays[1], (unsigned long long)ns);
+		if (ks < 16u)
+			atomicAdd(&F.cnt[24u + ks], ns); // shadow rays of bounce ks
+	}
+	SinkRaw sink{F.hits, &F.cnt[3], COUNT ? F.rays + 2 : nullptr};
+	SinkShadow ss{F.shadow, F.scol, F.pL, &F.cnt[3]};
+	trace_two<STACK, COUNT>(S, rays, n, F.shadow, ns, &F.cnt[4],
+	  sstk + threadIdx.x, blockDim.x, sink, ss);
+}
+
 // Raw hits -> the reference's hit record (t, u, v, tri << 12 | inst).
 __global__ void __launch_bounds__(256) k_refine(DScene S, const float4 *rays,
                                                 const uint32_t *count,
@@ -494,7 +523,12 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 					bool mirror = mc.w >= 0.5f && !glossy;
 					bool queried = false;
 					if (A.mode == 2u && k >= 1u && !emissive) {
-						if (!train && !mirror) {
+						// rendering paths end at their first diffuse
+						// vertex after the primary hit; training paths
+						// (and mirror chains) at bounce nrc_end, where
+						// the cache supplies their remaining radiance
+						bool end = k >= A.nrc_end || (!train && !mirror);
+						if (end) {
 							// radiance cache query: the path ends here
 							uint32_t qi = atomicAdd(&F.cnt[40], 1u);
 							if (qi < F.nq_cap) {
@@ -508,7 +542,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 							}
 							queried = true;
 						}
-						if (train) {
+						if (train && !end) {
 							uint32_t ri = atomicAdd(&F.cnt[41], 1u);
 							if (ri < F.nrec_cap) {
 								float4 *q = F.nrec + 6u * ri;

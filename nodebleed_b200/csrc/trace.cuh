@@ -745,12 +745,20 @@ __device__ __forceinline__ void trace_phase(const DScene &S,
 // them one per inner iteration, unless fewer than a fifth of the active lanes
 // hold any: then those that still have nodes to visit push their triangles
 // and the warp goes back to visiting nodes.
-template <bool ANY, int STACK, bool COUNT, class Sink>
+template <bool ANY, int STACK, bool COUNT, class Sink, bool TWO = false,
+          class Sink2 = Sink>
 __device__ __forceinline__ void trace_ylitie(const DScene &S,
                                              const float4 *rays, uint32_t n,
                                              uint32_t *work, uint2 *stk,
-                                             uint32_t stride, Sink &sink)
+                                             uint32_t stride, Sink &sink,
+                                             const float4 *rays2 = nullptr,
+                                             uint32_t n2 = 0u,
+                                             Sink2 *sink2 = nullptr)
 {
+	// TWO: work items n .. n + n2 - 1 are any-hit rays of a second queue
+	// (rays2, reported to sink2), taken once the first queue is drained
+	const uint32_t ntot = TWO ? n + n2 : n;
+	bool second = false;
 	const uint32_t lane = threadIdx.x & 31u;
 	bool active = false, exhausted = false;
 	uint32_t ridx = 0, err = 0;
@@ -765,15 +773,17 @@ __device__ __forceinline__ void trace_ylitie(const DScene &S,
 			if (lane == leader)
 				base = atomicAdd(work, cnt);
 			base = __shfl_sync(kFull, base, leader);
-			if (base + cnt >= n)
+			if (base + cnt >= ntot)
 				exhausted = true;
 			if (!active) {
 				uint32_t my = base + __popc(idle & ((1u << lane) - 1u));
-				if (my < n) {
-					ridx = my;
+				if (my < ntot) {
+					second = TWO && my >= n;
+					ridx = second ? my - n : my;
 					err = 0;
-					float4 rb = rays[2u * my + 1u];
-					trav_start(T, rays[2u * my], rb);
+					const float4 *rq = second ? rays2 : rays;
+					float4 rb = rq[2u * ridx + 1u];
+					trav_start(T, rq[2u * ridx], rb);
 					vnode = S.nscenes > 1u ? __ldg(&S.sp[scene_of_path(S,
 					  __float_as_uint(rb.w))].tlas_root) : 0u;
 					active = true;
@@ -787,9 +797,12 @@ __device__ __forceinline__ void trace_ylitie(const DScene &S,
 		}
 		bool holding = active && T.level == 1u && T.tg.y != 0u;
 		if (active && !holding && vnode == kNone) {
-			if (node_step<STACK>(T, S, rays, ridx, stk, stride, err,
-			  &vnode)) {
-				sink(ridx, T, err);
+			if (node_step<STACK>(T, S, TWO && second ? rays2 : rays, ridx,
+			  stk, stride, err, &vnode)) {
+				if (TWO && second)
+					(*sink2)(ridx, T, err);
+				else
+					sink(ridx, T, err);
 				active = false;
 			}
 		}
@@ -825,6 +838,9 @@ __device__ __forceinline__ void trace_ylitie(const DScene &S,
 					if (ANY) {
 						sink(ridx, T, err);
 						active = false;
+					} else if (TWO && second) {
+						(*sink2)(ridx, T, err);
+						active = false;
 					}
 				}
 			}
@@ -849,6 +865,20 @@ __device__ __forceinline__ void trace_persistent(const DScene &S,
 	else
 		trace_ylitie<ANY, STACK, COUNT>(S, rays, n, work, stk, stride,
 		  sink);
+}
+
+// Closest hits of one queue, then any hits of a second queue, in one
+// persistent loop (Ylitie schedule).
+template <int STACK, bool COUNT, class Sink, class Sink2>
+__device__ __forceinline__ void trace_two(const DScene &S,
+                                          const float4 *rays, uint32_t n,
+                                          const float4 *rays2, uint32_t n2,
+                                          uint32_t *work, uint2 *stk,
+                                          uint32_t stride, Sink &sink,
+                                          Sink2 &sink2)
+{
+	trace_ylitie<false, STACK, COUNT, Sink, true, Sink2>(S, rays, n, work,
+	  stk, stride, sink, rays2, n2, &sink2);
 }
 
 // --------------------------------------------------------------- sinks --

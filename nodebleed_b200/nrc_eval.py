@@ -20,15 +20,16 @@ def reference(scene, w, h, depth, spp, seed=99, spp_per_frame=16):
     return img.astype(np.float32)
 
 
-def equal_time(scene, w, h, depth, frames, ref, seed=1):
+def equal_time(scene, w, h, depth, frames, ref, seed=1, **nrc_kw):
     """NRC for `frames` frames of 1 spp, then plain 1-spp frames until the
-    same device time; relMSE of both accumulated images against `ref`."""
+    same device time; relMSE of both accumulated images against `ref`.
+    nrc_kw go to the cache renderer (nrc_warmup, nrc_end, nrc_lr)."""
     import torch
     ref_dev = torch.from_numpy(np.ascontiguousarray(ref, np.float32)).cuda()
     out = {}
     rd = api.RenderData(scene, w, h, 1)
     gn = api.GpuRenderer(rd, max_depth=depth, mode=api.MODE_NRC, seed=seed,
-                         timing=True).upload()
+                         timing=True, **nrc_kw).upload()
     t_nrc, rays_nrc, curve = 0.0, 0, []
     for f in range(frames):
         rays_nrc += gn.frame()
