@@ -10,9 +10,11 @@
 // Forward: a warp owns 16 rows; the FP32 C fragments of two adjacent
 // 8-column tiles repack into the BF16 A fragment of the next layer's 16-wide
 // k tile in registers (thread layout of m16n8k16), so activations never leave
-// the register file.  Training additionally keeps each layer's input in shared
-// memory for the weight gradients, which use ldmatrix.trans to form the
-// transposed operands.
+// the register file.  Training runs forward and backward per tile, keeping
+// each layer's input in shared memory for the ReLU derivative and writing
+// inputs and output gradients to global memory; the weight gradients are
+// then split-K GEMMs over the batch (ldmatrix.trans forms the transposed
+// operands).
 
 #ifndef NB_NRC_CUH
 #define NB_NRC_CUH
@@ -34,6 +36,21 @@ constexpr int kMlpParams = kMlpSquare * kMlpSq + kMlpOutPad * kMlpHidden;
 // transposed BF16 copy: 5 square + [64][16]
 constexpr int kMlpParamsT = kMlpSquare * kMlpSq + kMlpHidden * kMlpOutPadT;
 constexpr int kMlpRowPad = 72;             // smem row stride (bf16), no bank conflicts
+constexpr int kMlpWRows = kMlpSquare * 64 + kMlpOutPad; // weight rows
+// forward weights in shared memory: rows of 64 padded to kMlpRowPad
+constexpr int kMlpWSmem = kMlpWRows * kMlpRowPad;
+
+// Copy the forward BF16 weights [rows][64] to shared memory with padded
+// rows (all threads of the block).
+__device__ __forceinline__ void load_w_smem(__nv_bfloat16 *w,
+                                            const __nv_bfloat16 *g)
+{
+	for (int i = threadIdx.x; i < kMlpWRows * 8; i += blockDim.x) {
+		int r = i >> 3, q = i & 7;
+		*reinterpret_cast<uint4 *>(w + r * kMlpRowPad + q * 8) =
+		  __ldg(reinterpret_cast<const uint4 *>(g + r * 64) + q);
+	}
+}
 
 // ------------------------------------------------------------ mma helpers --
 
@@ -150,7 +167,8 @@ __device__ __forceinline__ void lda_global(uint32_t a[4][4],
 	}
 }
 
-// One square layer: c = a x W^T (W [64][64] bf16 in shared memory).
+// One square layer: c = a x W^T (W [64][64] bf16 in shared memory with
+// padded rows).
 __device__ __forceinline__ void layer_sq(float c[8][4], const uint32_t a[4][4],
                                          const __nv_bfloat16 *w, int lane)
 {
@@ -160,7 +178,7 @@ __device__ __forceinline__ void layer_sq(float c[8][4], const uint32_t a[4][4],
 #pragma unroll
 		for (int kt = 0; kt < 4; kt++) {
 			uint32_t b[2];
-			ldb_w(b, w, 64, nt, kt, lane);
+			ldb_w(b, w, kMlpRowPad, nt, kt, lane);
 			mma16816(c[nt], a[kt], b[0], b[1]);
 		}
 	}
@@ -174,7 +192,7 @@ __device__ __forceinline__ void layer_out(float c[4], const uint32_t a[4][4],
 #pragma unroll
 	for (int kt = 0; kt < 4; kt++) {
 		uint32_t b[2];
-		ldb_w(b, w5, 64, 0, kt, lane);
+		ldb_w(b, w5, kMlpRowPad, 0, kt, lane);
 		mma16816(c, a[kt], b[0], b[1]);
 	}
 }
@@ -192,9 +210,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const __nv_bfloat16 *wbf,
 		n = min(*ncount, n); // count produced on the device
 	extern __shared__ __align__(16) unsigned char mlp_smem[];
 	__nv_bfloat16 *w = reinterpret_cast<__nv_bfloat16 *>(mlp_smem);
-	for (int i = threadIdx.x; i < kMlpParams / 8; i += blockDim.x)
-		reinterpret_cast<uint4 *>(w)[i] =
-		  __ldg(reinterpret_cast<const uint4 *>(wbf) + i);
+	load_w_smem(w, wbf);
 	__syncthreads();
 	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	uint32_t tiles = (n + 15u) / 16u;
@@ -205,11 +221,11 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const __nv_bfloat16 *wbf,
 		lda_global(a, feats, t * 16u, n, lane);
 #pragma unroll 1
 		for (int l = 0; l < kMlpSquare; l++) {
-			layer_sq(c, a, w + l * kMlpSq, lane);
+			layer_sq(c, a, w + l * 64 * kMlpRowPad, lane);
 			c_to_a(c, a, true);
 		}
 		float o[4];
-		layer_out(o, a, w + kMlpSquare * kMlpSq, lane);
+		layer_out(o, a, w + kMlpSquare * 64 * kMlpRowPad, lane);
 		// thread holds rows lane/4 (cols 2q, 2q+1) and lane/4+8
 		int q = lane & 3;
 		uint32_t r0 = t * 16u + (lane >> 2), r1 = r0 + 8u;
@@ -228,29 +244,51 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(const __nv_bfloat16 *wbf,
 
 // --------------------------------------------------------------- training --
 
-// Shared memory of the training kernel (per CTA of 4 warps).
+// Shared memory of the forward/backward pass of training (per CTA of 4
+// warps): the forward weights, each warp's layer inputs (for the ReLU
+// derivative) and its current output gradient.
 struct MlpTrainSmem {
-	__nv_bfloat16 w[kMlpParams];         // forward copy [out][in]
+	__nv_bfloat16 w[kMlpWSmem];          // forward copy [out][in], padded
 	__nv_bfloat16 act[4][6][16 * kMlpRowPad]; // inputs of layers 0..5
 	__nv_bfloat16 dz[4][16 * kMlpRowPad]; // gradient of one layer's output
-	float dw[kMlpParams];                // weight-gradient accumulators
 	float loss;
 };
 
+// Store one warp's 16 x 64 bf16 tile (padded shared-memory rows) to global
+// rows [row0, row0 + 16) of a [rows][64] array.
+__device__ __forceinline__ void st_tile_global(__nv_bfloat16 *g,
+                                               const __nv_bfloat16 *t,
+                                               uint32_t row0, int lane)
+{
+	// 16 rows x 128 bytes = 128 16-byte chunks, 4 per lane
+#pragma unroll
+	for (int k = 0; k < 4; k++) {
+		int c = lane + 32 * k, r = c >> 3, q = c & 7;
+		*reinterpret_cast<uint4 *>(g + (size_t)(row0 + r) * 64 + q * 8) =
+		  *reinterpret_cast<const uint4 *>(t + r * kMlpRowPad + q * 8);
+	}
+}
+
+// Training, pass 1: forward and backward of 16-row tiles.  Writes every
+// layer's BF16 input (act, [6][npad][64]) and the gradient of every
+// layer's output (dz, [6][npad][64]; the output layer's in columns 0..15)
+// for the weight-gradient GEMMs of pass 2, and per-CTA loss partials.
 // Relative L2 loss mean((y - t)^2 / (y^2 + 0.01)) over the batch and three
-// channels (y detached in the denominator); gradients of a batch of n
-// samples into this CTA's partial gradient slice grad[blockIdx.x].
-// With ncount set, the batch is samples [off, off + n) of the
-// min(*ncount, cap) produced on the device, off = offset mod that count.
-__global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16 *wbf,
-                                                  const __nv_bfloat16 *wbt,
-                                                  const __nv_bfloat16 *feats,
-                                                  const float4 *targets,
-                                                  uint32_t n, float *grad,
-                                                  float *loss,
-                                                  const uint32_t *ncount,
-                                                  uint32_t offset,
-                                                  uint32_t cap)
+// channels (y detached in the denominator).  With ncount set, the batch is
+// samples [off, off + n) of the min(*ncount, cap) produced on the device,
+// off = offset mod that count; rows past the batch are zero and add
+// nothing.
+__global__ void __launch_bounds__(128) k_mlp_fb(const __nv_bfloat16 *wbf,
+                                                const __nv_bfloat16 *wbt,
+                                                const __nv_bfloat16 *feats,
+                                                const float4 *targets,
+                                                uint32_t n, uint32_t npad,
+                                                __nv_bfloat16 *gact,
+                                                __nv_bfloat16 *gdz,
+                                                float *loss,
+                                                const uint32_t *ncount,
+                                                uint32_t offset,
+                                                uint32_t cap)
 {
 	if (ncount) {
 		uint32_t total = min(*ncount, cap);
@@ -262,17 +300,13 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16 *wbf,
 	}
 	extern __shared__ __align__(16) unsigned char mlp_smem[];
 	MlpTrainSmem &S = *reinterpret_cast<MlpTrainSmem *>(mlp_smem);
-	for (int i = threadIdx.x; i < kMlpParams / 8; i += blockDim.x)
-		reinterpret_cast<uint4 *>(S.w)[i] =
-		  __ldg(reinterpret_cast<const uint4 *>(wbf) + i);
-	for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x)
-		S.dw[i] = 0.0f;
+	load_w_smem(S.w, wbf);
 	if (threadIdx.x == 0)
 		S.loss = 0.0f;
 	__syncthreads();
 	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const float inv = n ? 1.0f / (3.0f * (float)n) : 0.0f;
-	uint32_t tiles = (n + 15u) / 16u;
+	uint32_t tiles = npad / 16u;
 	float lsum = 0.0f;
 	for (uint32_t t = blockIdx.x * 4u + warp; t < tiles;
 	     t += gridDim.x * 4u) {
@@ -281,12 +315,16 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16 *wbf,
 		lda_global(a, feats, t * 16u, n, lane);
 		st_a(S.act[warp][0], a, lane);
 		for (int l = 0; l < kMlpSquare; l++) {
-			layer_sq(c, a, S.w + l * kMlpSq, lane);
+			layer_sq(c, a, S.w + l * 64 * kMlpRowPad, lane);
 			c_to_a(c, a, true);
 			st_a(S.act[warp][l + 1], a, lane);
 		}
+		__syncwarp();
+		for (int l = 0; l <= kMlpSquare; l++)
+			st_tile_global(gact + (size_t)l * npad * 64, S.act[warp][l],
+			  t * 16u, lane);
 		float o[4];
-		layer_out(o, a, S.w + kMlpSquare * kMlpSq, lane);
+		layer_out(o, a, S.w + kMlpSquare * 64 * kMlpRowPad, lane);
 		// output gradient: thread holds rows r0 (cols 2q, 2q+1), r1
 		int q = lane & 3;
 		uint32_t r0 = t * 16u + (lane >> 2), r1 = r0 + 8u;
@@ -303,7 +341,8 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16 *wbf,
 				g[i] = 2.0f * d / den * inv;
 			}
 		}
-		// dz of the output layer as bf16, padded to 16 columns
+		// dz of the output layer as bf16, padded to 16 columns (64 in
+		// the global copy, zero past 8)
 		__nv_bfloat16 *dz = S.dz[warp];
 		{
 			int r = lane >> 2, cc = 2 * q;
@@ -311,54 +350,25 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16 *wbf,
 			  pack_bf16(g[0], g[1]);
 			*reinterpret_cast<uint32_t *>(dz + (r + 8) * kMlpRowPad + cc) =
 			  pack_bf16(g[2], g[3]);
-			*reinterpret_cast<uint32_t *>(dz + r * kMlpRowPad + cc + 8) = 0u;
-			*reinterpret_cast<uint32_t *>(dz + (r + 8) * kMlpRowPad + cc + 8) =
-			  0u;
+#pragma unroll
+			for (int z = 8; z < 64; z += 8) {
+				*reinterpret_cast<uint32_t *>(dz + r * kMlpRowPad + cc + z) =
+				  0u;
+				*reinterpret_cast<uint32_t *>(dz + (r + 8) * kMlpRowPad +
+				  cc + z) = 0u;
+			}
 		}
 		__syncwarp();
 		// backward through the 6 layers
 		for (int l = kMlpSquare; l >= 0; l--) {
-			int nout = l == kMlpSquare ? 8 : 64;
-			const __nv_bfloat16 *act = S.act[warp][l];
-			float *dw = S.dw + l * kMlpSq;
-			// dW[out][in] += sum_rows dz[row][out] * act[row][in]:
-			// M = out, N = in, K = 16 rows
-			for (int mt = 0; mt < nout / 16 + (nout == 8); mt++) {
-				uint32_t af[4];
-				// A = dz^T (m = out, k = row): ldmatrix.trans of dz
-				// blocks (rows 0-7 | 8-15) x (out mt*16 + 0-7 | 8-15)
-				{
-					int blk = lane >> 3, rr = lane & 7;
-					int row = (blk >> 1) * 8 + rr;
-					int col = mt * 16 + (blk & 1) * 8;
-					ldsm_x4_trans(af, dz + row * kMlpRowPad + col);
-				}
-#pragma unroll
-				for (int nt = 0; nt < 8; nt++) {
-					// B = act (k = row, n = in): ldmatrix.trans
-					uint32_t bf[2];
-					int blk = (lane >> 3) & 1, rr = lane & 7;
-					ldsm_x2_trans(bf, act + (blk * 8 + rr) * kMlpRowPad +
-					  nt * 8);
-					float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-					mma16816(acc, af, bf[0], bf[1]);
-					int m0 = mt * 16 + (lane >> 2), nn = nt * 8 + 2 * q;
-					if (m0 < nout) {
-						atomicAdd(dw + m0 * 64 + nn, acc[0]);
-						atomicAdd(dw + m0 * 64 + nn + 1, acc[1]);
-					}
-					if (m0 + 8 < nout) {
-						atomicAdd(dw + (m0 + 8) * 64 + nn, acc[2]);
-						atomicAdd(dw + (m0 + 8) * 64 + nn + 1, acc[3]);
-					}
-				}
-			}
+			st_tile_global(gdz + (size_t)l * npad * 64, dz, t * 16u, lane);
 			if (l == 0)
 				break;
+			const __nv_bfloat16 *act = S.act[warp][l];
 			// dA[row][in] = sum_out dz[row][out] * W[out][in]:
 			// M = 16 rows, N = 64 in, K = out (16 padded for the
 			// output layer); B from the transposed copy [in][out],
-			// read through L1 (it does not fit in shared memory too)
+			// read through L1
 			int kts = l == kMlpSquare ? 1 : 4;
 			int K = l == kMlpSquare ? kMlpOutPadT : 64;
 			const __nv_bfloat16 *wt = wbt + l * kMlpSq;
@@ -395,11 +405,89 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16 *wbf,
 	}
 	atomicAdd(&S.loss, lsum);
 	__syncthreads();
-	float *gp = grad + (size_t)blockIdx.x * kMlpParams;
-	for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x)
-		gp[i] = S.dw[i];
 	if (threadIdx.x == 0)
 		loss[blockIdx.x] = S.loss;
+}
+
+// Training, pass 2: weight gradients dW_l[out][in] = sum_rows dz_l[row][out]
+// act_l[row][in] as split-K tensor-core GEMMs.  CTA (l = blockIdx.y, split
+// blockIdx.x) sums rows [split * rows_per, ...) of layer l in chunks of 64
+// rows staged in shared memory; warp w owns outputs 16w..16w+15 (the output
+// layer: warp 0, 8 rows).  The partial goes to part[split][layer l slice];
+// the Adam kernel sums the splits.
+constexpr int kDwChunk = 64;
+__global__ void __launch_bounds__(128) k_mlp_dw(const __nv_bfloat16 *gact,
+                                                const __nv_bfloat16 *gdz,
+                                                uint32_t npad,
+                                                uint32_t rows_per,
+                                                float *part)
+{
+	__shared__ __align__(16) __nv_bfloat16 sdz[kDwChunk * kMlpRowPad];
+	__shared__ __align__(16) __nv_bfloat16 sact[kDwChunk * kMlpRowPad];
+	int l = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	int nout = l == kMlpSquare ? kMlpOutPad : 64;
+	const __nv_bfloat16 *act = gact + (size_t)l * npad * 64;
+	const __nv_bfloat16 *dzp = gdz + (size_t)l * npad * 64;
+	uint32_t r0 = blockIdx.x * rows_per;
+	uint32_t r1 = min(npad, r0 + rows_per);
+	bool busy = warp * 16 < nout;
+	float acc[8][4];
+#pragma unroll
+	for (int nt = 0; nt < 8; nt++)
+		acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
+	for (uint32_t c0 = r0; c0 < r1; c0 += kDwChunk) {
+		uint32_t rows = min((uint32_t)kDwChunk, r1 - c0); // multiple of 16
+		__syncthreads();
+		for (uint32_t i = threadIdx.x; i < rows * 8u; i += blockDim.x) {
+			uint32_t r = i >> 3, q = i & 7u;
+			*reinterpret_cast<uint4 *>(sdz + r * kMlpRowPad + q * 8) =
+			  __ldg(reinterpret_cast<const uint4 *>(dzp +
+			  (size_t)(c0 + r) * 64) + q);
+			*reinterpret_cast<uint4 *>(sact + r * kMlpRowPad + q * 8) =
+			  __ldg(reinterpret_cast<const uint4 *>(act +
+			  (size_t)(c0 + r) * 64) + q);
+		}
+		__syncthreads();
+		if (!busy)
+			continue;
+		for (uint32_t kb = 0; kb < rows; kb += 16) {
+			// A = dz^T (m = out, k = row): ldmatrix.trans of the dz
+			// blocks (rows kb+0-7 | 8-15) x (out 16w + 0-7 | 8-15)
+			uint32_t af[4];
+			{
+				int blk = lane >> 3, rr = lane & 7;
+				int row = kb + (blk >> 1) * 8 + rr;
+				int col = warp * 16 + (blk & 1) * 8;
+				ldsm_x4_trans(af, sdz + row * kMlpRowPad + col);
+			}
+#pragma unroll
+			for (int nt = 0; nt < 8; nt++) {
+				// B = act (k = row, n = in): ldmatrix.trans
+				uint32_t bf[2];
+				int blk = (lane >> 3) & 1, rr = lane & 7;
+				ldsm_x2_trans(bf, sact + (kb + blk * 8 + rr) * kMlpRowPad +
+				  nt * 8);
+				mma16816(acc[nt], af, bf[0], bf[1]);
+			}
+		}
+	}
+	// write this split's slice of layer l (every element, zeros included)
+	float *gp = part + (size_t)blockIdx.x * kMlpParams + (size_t)l * kMlpSq;
+	int q = lane & 3;
+	if (busy) {
+#pragma unroll
+		for (int nt = 0; nt < 8; nt++) {
+			int m0 = warp * 16 + (lane >> 2), nn = nt * 8 + 2 * q;
+			if (m0 < nout) {
+				gp[m0 * 64 + nn] = acc[nt][0];
+				gp[m0 * 64 + nn + 1] = acc[nt][1];
+			}
+			if (m0 + 8 < nout) {
+				gp[(m0 + 8) * 64 + nn] = acc[nt][2];
+				gp[(m0 + 8) * 64 + nn + 1] = acc[nt][3];
+			}
+		}
+	}
 }
 
 // Sum the per-CTA partial gradients; optionally write the sum (g_out) and

@@ -114,6 +114,7 @@ struct Ctx {
 	// neural radiance cache: FP32 master weights, Adam moments, BF16
 	// forward / transposed copies, per-CTA gradient partials and losses
 	DevBuf mlp_wf, mlp_m, mlp_v, mlp_wbf, mlp_wbt, mlp_part, mlp_loss;
+	DevBuf mlp_act, mlp_dz; // training: layer inputs and output gradients
 	uint32_t mlp_step = 0;
 	bool     mlp_ready = false;
 	NrcBox   box{};
@@ -616,7 +617,7 @@ int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out,
 	if (n == 0)
 		return 0;
 	int per_sm = 0;
-	size_t smem = kMlpParams * sizeof(__nv_bfloat16);
+	size_t smem = kMlpWSmem * sizeof(__nv_bfloat16); // 46 KB: no opt-in
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_fwd, 128,
 	  smem);
 	uint32_t tiles = (n + 15u) / 16u;
@@ -638,23 +639,33 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 {
 	if (n == 0)
 		return 0;
-	static bool attr = false;
 	size_t smem = sizeof(MlpTrainSmem);
-	if (!attr) {
-		NB_CK(c, cudaFuncSetAttribute(k_mlp_grad,
-		  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-		attr = true;
-	}
-	uint32_t tiles = (n + 15u) / 16u;
-	uint32_t grid = std::min<uint32_t>((tiles + 15u) / 16u,
-	  (uint32_t)c->nsm);
+	NB_CK(c, cudaFuncSetAttribute(k_mlp_fb,
+	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	// pass 1: forward + backward of 16-row tiles, 4 per CTA
+	uint32_t npad = (n + 15u) / 16u * 16u;
+	uint32_t tiles = npad / 16u;
+	uint32_t grid = std::min<uint32_t>((tiles + 3u) / 4u,
+	  std::min<uint32_t>(2u * (uint32_t)c->nsm, 1024u));
 	grid = std::max(grid, 1u);
-	NB_CK(c, c->mlp_part.ensure((size_t)grid * kMlpParams * sizeof(float)));
+	NB_CK(c, c->mlp_act.ensure((size_t)6 * npad * 64 * 2));
+	NB_CK(c, c->mlp_dz.ensure((size_t)6 * npad * 64 * 2));
 	c->train_grid = grid;
-	k_mlp_grad<<<grid, 128, smem, c->stream>>>(c->mlp_wbf.as<__nv_bfloat16>(),
+	k_mlp_fb<<<grid, 128, smem, c->stream>>>(c->mlp_wbf.as<__nv_bfloat16>(),
 	  c->mlp_wbt.as<__nv_bfloat16>(), static_cast<const __nv_bfloat16 *>(feats),
-	  targets, n, c->mlp_part.as<float>(), c->mlp_loss.as<float>(), ncount,
-	  offset, cap);
+	  targets, n, npad, c->mlp_act.as<__nv_bfloat16>(),
+	  c->mlp_dz.as<__nv_bfloat16>(), c->mlp_loss.as<float>(), ncount, offset,
+	  cap);
+	NB_CK(c, cudaGetLastError());
+	// pass 2: split-K weight-gradient GEMMs, (splits x 6 layers) CTAs
+	uint32_t chunks = (npad + (uint32_t)kDwChunk - 1u) / (uint32_t)kDwChunk;
+	uint32_t splits = std::min<uint32_t>(32u, chunks);
+	uint32_t rows_per = (chunks + splits - 1u) / splits * (uint32_t)kDwChunk;
+	splits = (npad + rows_per - 1u) / rows_per;
+	NB_CK(c, c->mlp_part.ensure((size_t)splits * kMlpParams * sizeof(float)));
+	k_mlp_dw<<<dim3(splits, kMlpSquare + 1), 128, 0, c->stream>>>(
+	  c->mlp_act.as<__nv_bfloat16>(), c->mlp_dz.as<__nv_bfloat16>(), npad,
+	  rows_per, c->mlp_part.as<float>());
 	NB_CK(c, cudaGetLastError());
 	if (update)
 		c->mlp_step++;
@@ -662,7 +673,7 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 	float bc2 = 1.0f - std::pow(kAdamBeta2, (float)std::max(c->mlp_step, 1u));
 	k_mlp_adam<<<grid_for(c, kMlpParams, 256), 256, 0, c->stream>>>(
 	  c->mlp_wf.as<float>(), c->mlp_m.as<float>(), c->mlp_v.as<float>(),
-	  c->mlp_part.as<float>(), (int)grid, g_out, update, nrc_lr(c),
+	  c->mlp_part.as<float>(), (int)splits, g_out, update, nrc_lr(c),
 	  kAdamBeta1, kAdamBeta2, kAdamEps, bc1, bc2,
 	  c->mlp_wbf.as<__nv_bfloat16>(), c->mlp_wbt.as<__nv_bfloat16>());
 	NB_CK(c, cudaGetLastError());
@@ -1018,7 +1029,8 @@ void free_ctx(Ctx *c)
 	DevBuf *bufs[] = {&c->blas, &c->tris, &c->tlas, &c->irefs, &c->insts,
 	  &c->nrms, &c->mtls, &c->lights, &c->sp, &c->scn, &c->sortbuf, &c->q0, &c->q1, &c->hits, &c->shadow,
 	  &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
-	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_wf,
+	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_act,
+	  &c->mlp_dz, &c->mlp_wf,
 	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
 	  &c->mlp_loss, &c->nq, &c->nfeat, &c->npred, &c->nrec, &c->rfeat,
 	  &c->rtgt};
@@ -1039,6 +1051,7 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->sortbuf, &c->q0, &c->q1, &c->hits,
 	  &c->shadow, &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf,
 	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
+	  &c->mlp_act, &c->mlp_dz,
 	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
 	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nfeat, &c->npred, &c->nrec,
 	  &c->rfeat, &c->rtgt};
