@@ -77,7 +77,8 @@ struct rendgpu_cfg {
 	                         rate (0 = 1e-2); [1]: radiance-cache warm-up
 	                         frames of unbiased tracing (0 = 4); [2]: bounce
 	                         at which training paths end in the cache after
-	                         the warm-up (0 = 3) */
+	                         the warm-up (0 = 3); [3]: cache training steps
+	                         of 16384 samples per frame (0 = 4) */
 };
 
 /* A ray for the batch calls: origin, tmax, direction (32 bytes). */

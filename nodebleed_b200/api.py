@@ -343,7 +343,7 @@ class GpuRenderer:
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
                  timing=False, device=0, count=False, sched=0,
                  nrc_warmup=0, nrc_lr=0.0, graph=False, block=0,
-                 nrc_end=0):
+                 nrc_end=0, nrc_steps=0):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -353,6 +353,7 @@ class GpuRenderer:
             C.c_float(nrc_lr)).value
         cfg.reserved[1] = nrc_warmup
         cfg.reserved[2] = nrc_end
+        cfg.reserved[3] = nrc_steps
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
         if rc != 0:
             raise RendgpuError(rc, "rendgpu_init")

@@ -579,7 +579,11 @@ uint32_t nrc_train_end(const Ctx *c)
 }
 
 constexpr uint32_t kNrcBatch = 16384;    // training samples per Adam step
-constexpr uint32_t kNrcSteps = 4;        // Adam steps per frame
+// Adam steps per frame (cfg.reserved[3]; 0 = 4)
+uint32_t nrc_steps(const Ctx *c)
+{
+	return c->cfg.reserved[3] ? std::min(c->cfg.reserved[3], 64u) : 4u;
+}
 constexpr uint32_t kNrcTrainPaths = 65536; // training paths per frame (2^16)
 
 // Radiance-cache buffers of a frame: queries and their features/outputs
@@ -600,7 +604,7 @@ int nrc_frame_buffers(Ctx *c)
 	// vertices beyond the steady-state need
 	uint32_t ntrain = np / c->nrc_stride + 1;
 	c->nq_cap = np;
-	c->nrec_cap = std::max(ntrain * verts + 64, kNrcSteps * kNrcBatch);
+	c->nrec_cap = std::max(ntrain * verts + 64, nrc_steps(c) * kNrcBatch);
 	NB_CK(c, c->nq.ensure((size_t)np * 64));
 	NB_CK(c, c->nfeat.ensure((size_t)np * 128));
 	NB_CK(c, c->npred.ensure((size_t)np * 16));
@@ -868,7 +872,7 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 	c->st.launches++;
 	if (nrc) {
 		// train on this frame's records: targets from the finished paths,
-		// then kNrcSteps Adam steps of kNrcBatch samples each
+		// then nrc_steps Adam steps of kNrcBatch samples each
 		E->train = c->nev;
 		ev_record(c);
 		k_nrc_targets<<<grid_for(c, c->nrec_cap, 256), 256, 0, c->stream>>>(
@@ -877,13 +881,13 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		  c->stream>>>(F.nrec, 6u, F.cnt + 41, c->nrec_cap, c->box,
 		  c->rfeat.as<__nv_bfloat16>());
 		NB_CK(c, cudaGetLastError());
-		for (uint32_t s = 0; s < kNrcSteps; s++) {
+		for (uint32_t s = 0; s < nrc_steps(c); s++) {
 			rc = nrc_train(c, c->rfeat.p, c->rtgt.as<float4>(), kNrcBatch, 1,
 			  nullptr, nullptr, F.cnt + 41, s * kNrcBatch, c->nrec_cap);
 			if (rc)
 				return rc;
 		}
-		c->st.launches += 2 + 2 * kNrcSteps;
+		c->st.launches += 2 + 3 * nrc_steps(c);
 		ev_record(c);
 	}
 	ev_record(c); // last
