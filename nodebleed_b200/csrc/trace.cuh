@@ -84,6 +84,23 @@ __device__ __forceinline__ uint32_t scene_of_path(const DScene &S,
 		return __ldg(&p->path_base); });
 }
 
+// Position of the j-th (from 0) set bit of m (j < popc(m)).
+__device__ __forceinline__ uint32_t nth_bit(uint32_t m, uint32_t j)
+{
+	uint32_t pos = 0, c;
+	c = __popc(m & 0xffffu);
+	if (j >= c) { j -= c; pos += 16; m >>= 16; }
+	c = __popc(m & 0xffu);
+	if (j >= c) { j -= c; pos += 8; m >>= 8; }
+	c = __popc(m & 0xfu);
+	if (j >= c) { j -= c; pos += 4; m >>= 4; }
+	c = __popc(m & 0x3u);
+	if (j >= c) { j -= c; pos += 2; m >>= 2; }
+	c = m & 1u;
+	if (j >= c) pos += 1;
+	return pos;
+}
+
 // Ray state in the space being traversed.
 struct TRay {
 	float ox, oy, oz, dx, dy, dz;
@@ -824,23 +841,80 @@ __device__ __forceinline__ void trace_ylitie(const DScene &S,
 				}
 				break;
 			}
-			if (want) {
-				uint32_t i = __ffs(T.tg.y) - 1;
-				T.tg.y &= T.tg.y - 1u;
-				float t;
+			// One round of the triangle phase: the first 32 pending
+			// triangles of the warp (in lane order) are tested by all 32
+			// lanes, each with its owner's ray taken by shuffle; an
+			// owner keeps the nearest hit of its testers (lowest item on
+			// equal t, as sequential testing would).  Lanes that test
+			// their own triangles one by one leave about 3/4 of the warp
+			// idle (7.7 active lanes per iteration measured on the
+			// 1080p workload).
+			uint32_t k = want ? __popc(T.tg.y) : 0u;
+			uint32_t incl = k;
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				uint32_t x = __shfl_up_sync(kFull, incl, o);
+				if (lane >= (uint32_t)o)
+					incl += x;
+			}
+			uint32_t total = __shfl_sync(kFull, incl, 31);
+			uint32_t excl = incl - k;
+			// owner of work item `lane`: first lane whose prefix exceeds it
+			uint32_t owner = 0;
+#pragma unroll
+			for (int step = 16; step >= 1; step >>= 1) {
+				uint32_t v = __shfl_sync(kFull, incl, owner + step - 1);
+				if (v <= lane)
+					owner += step;
+			}
+			owner = min(owner, 31u);
+			bool has = lane < total;
+			uint32_t o_excl = __shfl_sync(kFull, excl, owner);
+			uint32_t o_tgy = __shfl_sync(kFull, T.tg.y, owner);
+			uint32_t o_tgx = __shfl_sync(kFull, T.tg.x, owner);
+			TRay rr;
+			rr.ox = __shfl_sync(kFull, T.r.ox, owner);
+			rr.oy = __shfl_sync(kFull, T.r.oy, owner);
+			rr.oz = __shfl_sync(kFull, T.r.oz, owner);
+			rr.sx = __shfl_sync(kFull, T.r.sx, owner);
+			rr.sy = __shfl_sync(kFull, T.r.sy, owner);
+			rr.sz = __shfl_sync(kFull, T.r.sz, owner);
+			uint32_t kk = __shfl_sync(kFull, T.r.kx | (T.r.ky << 2) |
+			  (T.r.kz << 4), owner);
+			rr.kx = kk & 3u;
+			rr.ky = (kk >> 2) & 3u;
+			rr.kz = (kk >> 4) & 3u;
+			float obt = __shfl_sync(kFull, T.bt, owner);
+			uint32_t item = has ? o_tgx + nth_bit(o_tgy, lane - o_excl) : 0u;
+			float t = 0.0f;
+			bool hit = has && tri_hit(S.tris, item, rr, obt, &t);
+			uint32_t grp = __match_any_sync(kFull, has ? owner : 32u);
+			uint32_t key = hit ? __float_as_uint(t) : 0x7f800000u;
+			uint32_t tmin = __reduce_min_sync(grp, key);
+			uint32_t imin = __reduce_min_sync(grp, (hit && key == tmin) ?
+			  item : kNone);
+			uint32_t src = (want && excl < 32u) ? excl : lane;
+			uint32_t got_t = __shfl_sync(kFull, tmin, src);
+			uint32_t got_i = __shfl_sync(kFull, imin, src);
+			if (want && excl < 32u) {
+				uint32_t ntest = min(k, 32u - excl);
 				if (COUNT)
-					T.ntest++;
-				if (tri_hit(S.tris, T.tg.x + i, T.r, T.bt, &t)) {
-					T.bt = t;
-					T.btri = T.tg.x + i;
+					T.ntest += ntest;
+				T.tg.y = ntest >= k ? 0u :
+				  (T.tg.y & ~((1u << nth_bit(T.tg.y, ntest)) - 1u));
+				if (got_i != kNone && __uint_as_float(got_t) < T.bt) {
+					T.bt = __uint_as_float(got_t);
+					T.btri = got_i;
 					T.binst = T.cinst;
 					T.found = true;
 					if (ANY) {
 						sink(ridx, T, err);
 						active = false;
+						T.tg.y = 0u;
 					} else if (TWO && second) {
 						(*sink2)(ridx, T, err);
 						active = false;
+						T.tg.y = 0u;
 					}
 				}
 			}
