@@ -29,16 +29,18 @@ def test_nrc_frames_produce_queries_and_records(gpu):
 
 
 def test_nrc_relmse_reduction_is_reported(gpu):
-    """Against a 1024-spp plain reference: the FP64 relMSE of both methods
-    at equal device time.  The trained cache must not be worse than the
-    plain tracer by more than 20 % on this small scene, and the evaluation
-    must be self-consistent."""
-    scene = api.Scene(api.SCENE_SMALL, 1)
-    w, h, depth = 160, 90, 8
-    ref = nrc_eval.reference(scene, w, h, depth, 1024)
-    res = nrc_eval.equal_time(scene, w, h, depth, 24, ref)
-    print(res)
+    """What the trained cache gains: against a 256-spp plain reference, the
+    FP64 relMSE of the cache renderer and of the plain tracer at equal
+    device time.  On the scale scene at 640x360 (frames large enough that
+    launch overhead does not decide the timing) the cache must be ahead,
+    and the evaluation must be self-consistent."""
+    scene = api.Scene(api.SCENE_SCALE, 1)
+    w, h, depth = 640, 360, 8
+    ref = nrc_eval.reference(scene, w, h, depth, 256)
+    res = nrc_eval.equal_time(scene, w, h, depth, 32, ref)
+    print({k: res[k] for k in ("ratio_plain_over_nrc",)}, res["nrc"]["ms"],
+          res["plain"]["frames"])
     assert np.isfinite(res["nrc"]["relmse"]) and res["nrc"]["relmse"] > 0
     assert np.isfinite(res["plain"]["relmse"]) and res["plain"]["relmse"] > 0
     assert res["plain"]["ms"] >= res["nrc"]["ms"] or res["plain"]["frames"] == 1
-    assert res["nrc"]["relmse"] < 1.2 * res["plain"]["relmse"], res
+    assert res["ratio_plain_over_nrc"] > 1.1, res
