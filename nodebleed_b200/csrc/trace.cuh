@@ -227,7 +227,7 @@ __device__ __forceinline__ void visit(const nb_qnode *__restrict__ nodes,
 	uint32_t fy0 = fy ? w2.z : w4.x, fy1 = fy ? w2.w : w4.y;
 	uint32_t nz0 = fz ? w4.z : w3.x, nz1 = fz ? w4.w : w3.y;
 	uint32_t fz0 = fz ? w3.x : w4.z, fz1 = fz ? w3.y : w4.w;
-	uint32_t hits = 0, tbits = 0;
+	uint32_t hits = 0, tbits = 0, lhit = 0;
 	float gmin = FLT_MAX;
 #pragma unroll
 	for (int s = 0; s < 8; s++) {
@@ -245,15 +245,28 @@ __device__ __forceinline__ void visit(const nb_qnode *__restrict__ nodes,
 		float tf = fmin3(tfx, tfy, fminf(tfz, tmax));
 		if (tn <= tf * kWiden) {
 			if ((imask >> s) & 1u) {
-				hits |= 1u << (s ^ r.oct);
+				hits |= 1u << s;
 				gmin = fminf(gmin, tn);
 			} else {
-				uint32_t m = qb(s < 4 ? w1.z : w1.w, b);
-				if (m & NB_META_LEAF) {
-					uint32_t cnt = ((m >> 5) & 3u) + 1u;
-					tbits |= ((1u << cnt) - 1u) << (m & 31u);
-				}
+				lhit |= 1u << s;
 			}
+		}
+	}
+	// inner hits by slot -> by key (slot ^ octant)
+	{
+		const uint32_t o = r.oct;
+		hits = (o & 1u) ? ((hits & 0x55u) << 1) | ((hits >> 1) & 0x55u) : hits;
+		hits = (o & 2u) ? ((hits & 0x33u) << 2) | ((hits >> 2) & 0x33u) : hits;
+		hits = (o & 4u) ? ((hits & 0x0fu) << 4) | ((hits >> 4) & 0x0fu) : hits;
+	}
+	// items of the hit leaf children (typically few)
+	while (lhit) {
+		uint32_t sl = __ffs(lhit) - 1;
+		lhit &= lhit - 1u;
+		uint32_t m = ((sl < 4u ? w1.z : w1.w) >> (8u * (sl & 3u))) & 0xffu;
+		if (m & NB_META_LEAF) {
+			uint32_t cnt = ((m >> 5) & 3u) + 1u;
+			tbits |= ((1u << cnt) - 1u) << (m & 31u);
 		}
 	}
 	// node group: first child, hit mask (24..31), entry distance lower
