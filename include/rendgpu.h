@@ -241,7 +241,9 @@ int rendgpu_nrc_weights(struct rdata *rd, float *host, int write);
  * box, encoded direction, normal, albedo, zero padding). */
 int rendgpu_nrc_encode_device(struct rdata *rd, const float *raw_device,
                               uint32_t n, void *feats_device);
-/* MLP outputs (r, g, b, 0) per query. */
+/* MLP outputs (r, g, b, 0) per query (tcgen05 tensor cores, TMEM
+ * accumulators).  The device buffers of the infer and train calls must be
+ * 16-byte aligned (RENDGPU_EINVAL otherwise). */
 int rendgpu_nrc_infer_device(struct rdata *rd, const void *feats_device,
                              uint32_t n, float *out_device);
 /* Gradient of the relative L2 loss mean((y-t)^2 / (y^2 + 0.01)) over a
@@ -258,7 +260,9 @@ int rendgpu_nrc_train_device(struct rdata *rd, const void *feats_device,
 int rendgpu_relmse_device(struct rdata *rd, const float *ref_device,
                           double *out);
 
-/* Wait for all work of the context. */
+/* Wait for all work of the context.  Returns RENDGPU_EDEVICE when one of
+ * the asynchronous _device calls since the last check met a device error
+ * (rays abandoned, or a tensor-core wait of the cache that timed out). */
 int rendgpu_sync(struct rdata *rd);
 
 /* The cudaStream_t every call of this context runs on (for callers that

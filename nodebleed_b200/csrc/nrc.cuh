@@ -7,12 +7,15 @@
 // backward pass reads a transposed copy [in][out].  The output layer has 3
 // outputs padded to 8 (forward) / 16 (transposed copy) with zero rows.
 //
-// Forward: a warp owns 16 rows; the FP32 C fragments of two adjacent
-// 8-column tiles repack into the BF16 A fragment of the next layer's 16-wide
-// k tile in registers (thread layout of m16n8k16), so activations never leave
-// the register file.  Training runs forward and backward per tile, keeping
-// each layer's input in shared memory for the ReLU derivative and writing
-// inputs and output gradients to global memory; the weight gradients are
+// Inference runs on the tcgen05 tensor cores: 128-row tiles in shared
+// memory, FP32 accumulators in TMEM, one thread issuing the UMMAs of a
+// layer while the other pipeline of the CTA runs its epilogue.
+//
+// Training runs forward and backward per 16-row warp tile with
+// mma.m16n8k16: the FP32 C fragments of two adjacent 8-column tiles repack
+// into the BF16 A fragment of the next layer's 16-wide k tile in registers,
+// each layer's input stays in shared memory for the ReLU derivative, and
+// inputs and output gradients go to global memory; the weight gradients are
 // then split-K GEMMs over the batch (ldmatrix.trans forms the transposed
 // operands).
 
@@ -197,49 +200,311 @@ __device__ __forceinline__ void layer_out(float c[4], const uint32_t a[4][4],
 	}
 }
 
-// ------------------------------------------------------------- inference --
+// -------------------------------------------- inference (tcgen05 / UMMA) --
+//
+// 128-row tiles.  Operands in shared memory in the K-major 128-byte
+// swizzled layout of the UMMA descriptors: a row of 64 BF16 is 128 bytes,
+// 8-row groups are 1024-byte atoms (stride byte offset) whose 16-byte
+// chunks are XOR-permuted by the row within the atom, so the tensor core
+// and the row-per-thread epilogue both read and write without bank
+// conflicts; a K-step of 16 advances the descriptor by 32 bytes.  One
+// thread issues tcgen05.mma (kind::f16, BF16 in, FP32 accumulate, M = 128,
+// N = 64, 4 K-steps of 16) into a 64-column TMEM accumulator and commits to
+// an mbarrier; the 4 warps read their 32 TMEM lanes (one row per thread),
+// apply ReLU, round to BF16 and write the next layer's A tile.  Every wait
+// on the mbarrier is bounded: on a timeout the kernel raises *err, stops
+// issuing and still frees its TMEM.
 
-// out[i] = (r, g, b, 0) = MLP(feats[i]) for i < n.  Persistent CTAs of 4
-// warps; the forward BF16 weights (41 KB) are staged in shared memory once.
-__global__ void __launch_bounds__(128) k_mlp_fwd(const __nv_bfloat16 *wbf,
-                                                 const __nv_bfloat16 *feats,
-                                                 uint32_t n, float4 *out,
-                                                 const uint32_t *ncount)
+constexpr int kTcRows = 128;                 // rows per tile (UMMA M)
+constexpr int kTcTile = kTcRows * 64;        // bf16 elements of a tile
+constexpr int kTcW = 5 * 64 * 64 + 16 * 64;  // weights, output layer as 16 rows
+constexpr uint32_t kTcSpin = 1u << 24;       // mbarrier poll limit
+constexpr int kTcGroups = 4;                 // tile pipelines per CTA
+constexpr int kTcThreads = 128 * kTcGroups;  // 4 warps per pipeline
+constexpr int kTcCols = 64 * kTcGroups;      // TMEM columns of a CTA
+
+// Byte offset of element (row, k) of a K-major [rows][64] bf16 operand in
+// the 128-byte swizzled layout (operand base 1024-byte aligned).
+__device__ __forceinline__ uint32_t tc_off(uint32_t row, uint32_t k)
+{
+	return (row >> 3) * 1024u + (row & 7u) * 128u +
+	  (((k >> 3) ^ row) & 7u) * 16u + (k & 7u) * 2u;
+}
+
+// Shared-memory matrix descriptor (sm_100 UMMA): start address, leading
+// byte offset (unused by swizzled K-major layouts, 16 bytes), stride byte
+// offset 1024 (16-byte units), version 1, layout type 2 (128-byte swizzle).
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr)
+{
+	uint64_t d = 0;
+	d |= (uint64_t)((saddr >> 4) & 0x3fffu);
+	d |= (uint64_t)1u << 16;
+	d |= (uint64_t)((1024u >> 4) & 0x3fffu) << 32;
+	d |= (uint64_t)1u << 46;
+	d |= (uint64_t)2u << 61;
+	return d;
+}
+
+// Instruction descriptor: F32 accumulate, BF16 A and B, both K-major,
+// N = n, M = 128.
+__device__ __forceinline__ uint32_t tc_idesc(uint32_t n)
+{
+	return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) |
+	  ((uint32_t)(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da,
+                                       uint64_t db, uint32_t idesc,
+                                       uint32_t accumulate)
+{
+	asm volatile(
+	  "{\n\t.reg .pred p;\n\t"
+	  "setp.ne.b32 p, %4, 0;\n\t"
+	  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+	  :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar)
+{
+	asm volatile(
+	  "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64"
+	  " [%0];" :: "r"(bar) : "memory");
+}
+
+// Wait for the mbarrier phase `parity` with at most kTcSpin polls; false
+// on a timeout.
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity)
+{
+	for (uint32_t i = 0; i < kTcSpin; i++) {
+		uint32_t done;
+		asm volatile(
+		  "{\n\t.reg .pred p;\n\t"
+		  "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		  "selp.u32 %0, 1, 0, p;\n\t}\n"
+		  : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+		if (done)
+			return true;
+	}
+	return false;
+}
+
+// 64 consecutive FP32 accumulator columns of this thread's TMEM lane
+// (raw bits); waits for the load.
+__device__ __forceinline__ void tc_ld64(uint32_t taddr, uint32_t *r)
+{
+	asm volatile(
+	  "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+	  "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+	  "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,"
+	  "%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,"
+	  "%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63},"
+	  " [%64];"
+	  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+	    "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]),
+	    "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+	    "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+	    "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+	    "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+	    "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]),
+	    "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]),
+	    "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]),
+	    "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]),
+	    "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+	    "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]),
+	    "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+	  : "r"(taddr));
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// 4 consecutive FP32 accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tc_ld4(uint32_t taddr, float *v)
+{
+	uint32_t r[4];
+	asm volatile(
+	  "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+	  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(taddr));
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+	for (int i = 0; i < 4; i++)
+		v[i] = __uint_as_float(r[i]);
+}
+
+// 16-byte global -> shared copy (cp.async, L2 only); src_bytes 0 fills
+// the 16 bytes with zeros.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src,
+                                           uint32_t src_bytes)
+{
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;"
+	  :: "r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
+struct MlpTcSmem {
+	__nv_bfloat16 w[kTcW];               // B operands, swizzled layout
+	__nv_bfloat16 a[kTcGroups][kTcTile]; // A operands of layers 1..5
+	__nv_bfloat16 f[kTcGroups][kTcTile]; // feature tile (layer 0's A)
+	uint64_t bar[kTcGroups];
+	uint32_t ok[kTcGroups];              // the issuer's wait result
+	uint32_t tmem;
+};
+// every operand starts on a 1024-byte swizzle atom
+static_assert(kTcW * 2 % 1024 == 0 && kTcTile * 2 % 1024 == 0,
+              "UMMA operands must stay 1024-byte aligned");
+
+// Barrier of the 128 threads of group g (named barrier 1 + g).
+__device__ __forceinline__ void tc_group_sync(uint32_t g)
+{
+	asm volatile("bar.sync %0, 128;" :: "r"(1u + g) : "memory");
+}
+
+// out[i] = (r, g, b, 0) = MLP(feats[i]) for i < n (n = min(*ncount, n)
+// with ncount set).  kTcGroups groups of 4 warps, each an independent
+// pipeline over 128-row tiles (its own TMEM accumulator of 64 columns,
+// feature and A buffers and mbarrier) sharing the weights: while the tensor
+// core works for one group, the others run their epilogues.  The next
+// tile's features stream into the feature buffer (cp.async) as soon as
+// layer 0 has read it.  One CTA per SM.
+__global__ void __launch_bounds__(kTcThreads, 1)
+k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
+             float4 *out, const uint32_t *ncount, uint32_t *err)
 {
 	if (ncount)
-		n = min(*ncount, n); // count produced on the device
-	extern __shared__ __align__(16) unsigned char mlp_smem[];
-	__nv_bfloat16 *w = reinterpret_cast<__nv_bfloat16 *>(mlp_smem);
-	load_w_smem(w, wbf);
-	__syncthreads();
-	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	uint32_t tiles = (n + 15u) / 16u;
-	for (uint32_t t = blockIdx.x * 4u + warp; t < tiles;
-	     t += gridDim.x * 4u) {
-		uint32_t a[4][4];
-		float c[8][4];
-		lda_global(a, feats, t * 16u, n, lane);
-#pragma unroll 1
-		for (int l = 0; l < kMlpSquare; l++) {
-			layer_sq(c, a, w + l * 64 * kMlpRowPad, lane);
-			c_to_a(c, a, true);
-		}
-		float o[4];
-		layer_out(o, a, w + kMlpSquare * 64 * kMlpRowPad, lane);
-		// thread holds rows lane/4 (cols 2q, 2q+1) and lane/4+8
-		int q = lane & 3;
-		uint32_t r0 = t * 16u + (lane >> 2), r1 = r0 + 8u;
-		// gather the 3 valid columns of each row into lanes with q == 0
-		float x1 = __shfl_down_sync(0xffffffffu, o[0], 1);
-		float x3 = __shfl_down_sync(0xffffffffu, o[2], 1);
-		if (q == 0) {
-			// cols 0,1 from this lane, col 2 from lane+1 (its col 2q = 2)
-			if (r0 < n)
-				out[r0] = make_float4(o[0], o[1], x1, 0.0f);
-			if (r1 < n)
-				out[r1] = make_float4(o[2], o[3], x3, 0.0f);
-		}
+		n = min(*ncount, n);
+	extern __shared__ __align__(1024) unsigned char tc_smem[];
+	// the swizzle pattern repeats every 1024 bytes of the shared-memory
+	// address: start the operands on such a boundary (the launch adds
+	// 1 KB of slack)
+	const uint32_t base = (uint32_t)__cvta_generic_to_shared(tc_smem);
+	MlpTcSmem &S = *reinterpret_cast<MlpTcSmem *>(tc_smem +
+	  ((1024u - (base & 1023u)) & 1023u));
+	const uint32_t tid = threadIdx.x, warp = tid >> 5;
+	const uint32_t g = tid >> 7, gt = tid & 127u; // group, thread in group
+	const uint32_t sw = (uint32_t)__cvta_generic_to_shared(S.w);
+	const uint32_t sa = (uint32_t)__cvta_generic_to_shared(S.a[g]);
+	const uint32_t sf = (uint32_t)__cvta_generic_to_shared(S.f[g]);
+	const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar[g]);
+	unsigned char *abytes = reinterpret_cast<unsigned char *>(S.a[g]);
+	uint32_t tiles = (n + kTcRows - 1u) / kTcRows;
+	const uint32_t tstep = gridDim.x * (uint32_t)kTcGroups;
+	// this thread's feature row of tile tt (zeros past n) into the group's
+	// feature buffer
+	auto fetch = [&](uint32_t tt) {
+		uint32_t rr = tt * kTcRows + gt;
+		bool in = rr < n;
+		const uint4 *src = reinterpret_cast<const uint4 *>(feats +
+		  (size_t)(in ? rr : 0u) * 64u);
+#pragma unroll
+		for (uint32_t kc = 0; kc < 8u; kc++)
+			cp_async16(sf + tc_off(gt, kc * 8u), src + kc, in ? 16u : 0u);
+		asm volatile("cp.async.commit_group;" ::: "memory");
+	};
+	const uint32_t t0 = blockIdx.x * (uint32_t)kTcGroups + g;
+	if (t0 < tiles)
+		fetch(t0);
+	// weights: layer l (rows 64, output layer 16 with rows 8..15 zero) in
+	// the swizzled layout, layer bases 8 KB apart
+	for (uint32_t i = tid; i < 5u * 64u * 8u + 16u * 8u;
+	     i += (uint32_t)kTcThreads) {
+		uint32_t row = i >> 3, kc = i & 7u; // row over all layers
+		uint32_t l = row >> 6, r = row & 63u;
+		uint4 v = make_uint4(0, 0, 0, 0);
+		if (l < 5u || r < (uint32_t)kMlpOutPad)
+			v = __ldg(reinterpret_cast<const uint4 *>(wbf + (size_t)row *
+			  64u) + kc);
+		*reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(S.w) +
+		  l * 8192u + tc_off(r, kc * 8u)) = v;
 	}
+	if (warp == 0) {
+		asm volatile(
+		  "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+		  :: "r"((uint32_t)__cvta_generic_to_shared(&S.tmem)),
+		  "n"(kTcCols));
+		asm volatile(
+		  "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+	}
+	if (tid < (uint32_t)kTcGroups) {
+		uint32_t b = (uint32_t)__cvta_generic_to_shared(&S.bar[tid]);
+		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(b));
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	const uint32_t tmem = S.tmem + g * 64u;
+	const uint32_t tlane = tmem + (((warp & 3u) * 32u) << 16);
+	uint32_t parity = 0;
+	bool ok = true;
+	for (uint32_t t = t0; t < tiles && ok; t += tstep) {
+		uint32_t row = t * kTcRows + gt;
+		// this thread's part of the feature tile has landed
+		asm volatile("cp.async.wait_all;" ::: "memory");
+		float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+		for (int l = 0; l <= kMlpSquare; l++) {
+			// generic-proxy / cp.async writes visible to the tensor core
+			asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+			asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+			tc_group_sync(g);
+			asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+			uint32_t nn = l == kMlpSquare ? 16u : 64u;
+			if (gt == 0) {
+				uint32_t idesc = tc_idesc(nn);
+				uint32_t src = l == 0 ? sf : sa;
+#pragma unroll
+				for (uint32_t ks = 0; ks < 4u; ks++)
+					tc_mma(tmem, tc_desc(src + ks * 32u),
+					  tc_desc(sw + (uint32_t)l * 8192u + ks * 32u), idesc,
+					  ks > 0u ? 1u : 0u);
+				tc_commit(bar);
+				// one thread polls (bounded); the group barrier hands
+				// the answer to the others
+				S.ok[g] = tc_wait(bar, parity) ? 1u : 0u;
+			}
+			parity ^= 1u;
+			tc_group_sync(g);
+			ok = S.ok[g] != 0u;
+			if (!ok)
+				break;
+			asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+			// layer 0 has read the feature tile: fetch the next one
+			if (l == 0 && t + tstep < tiles)
+				fetch(t + tstep);
+			if (l < kMlpSquare) {
+				// ReLU, BF16, next layer's A (this thread's row)
+				uint32_t v[64];
+				tc_ld64(tlane, v);
+#pragma unroll
+				for (uint32_t q = 0; q < 8u; q++) {
+					uint4 pk;
+					pk.x = pack_bf16(
+					  fmaxf(__uint_as_float(v[8 * q]), 0.0f),
+					  fmaxf(__uint_as_float(v[8 * q + 1]), 0.0f));
+					pk.y = pack_bf16(
+					  fmaxf(__uint_as_float(v[8 * q + 2]), 0.0f),
+					  fmaxf(__uint_as_float(v[8 * q + 3]), 0.0f));
+					pk.z = pack_bf16(
+					  fmaxf(__uint_as_float(v[8 * q + 4]), 0.0f),
+					  fmaxf(__uint_as_float(v[8 * q + 5]), 0.0f));
+					pk.w = pack_bf16(
+					  fmaxf(__uint_as_float(v[8 * q + 6]), 0.0f),
+					  fmaxf(__uint_as_float(v[8 * q + 7]), 0.0f));
+					*reinterpret_cast<uint4 *>(abytes + tc_off(gt, q * 8u)) =
+					  pk;
+				}
+			} else {
+				tc_ld4(tlane, o);
+			}
+		}
+		if (ok && row < n)
+			out[row] = make_float4(o[0], o[1], o[2], 0.0f);
+	}
+	asm volatile("cp.async.wait_all;" ::: "memory");
+	if (!ok && gt == 0)
+		atomicAdd(err, 1u);
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	if (warp == 0)
+		asm volatile(
+		  "tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(S.tmem),
+		  "n"(kTcCols));
 }
 
 // --------------------------------------------------------------- training --

@@ -614,21 +614,30 @@ int nrc_frame_buffers(Ctx *c)
 	return 0;
 }
 
-// Forward pass of n (or, with ncount, of min(*ncount, n)) queries.
+// Null or not 16-byte aligned (vector loads, cp.async and float4 stores
+// of the cache kernels need 16 bytes).
+inline bool misaligned16(const void *p)
+{
+	return !p || (reinterpret_cast<uintptr_t>(p) & 15u) != 0;
+}
+
+// Forward pass of n (or, with ncount, of min(*ncount, n)) queries on the
+// tcgen05 tensor cores; a timed-out wait on the device counts into *errs.
 int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out,
-              const uint32_t *ncount = nullptr)
+              const uint32_t *ncount = nullptr, uint32_t *errs = nullptr)
 {
 	if (n == 0)
 		return 0;
-	int per_sm = 0;
-	size_t smem = kMlpWSmem * sizeof(__nv_bfloat16); // 46 KB: no opt-in
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_fwd, 128,
-	  smem);
-	uint32_t tiles = (n + 15u) / 16u;
-	uint32_t grid = std::min<uint32_t>((tiles + 3u) / 4u,
-	  (uint32_t)std::max(per_sm, 1) * (uint32_t)c->nsm);
-	k_mlp_fwd<<<grid, 128, smem, c->stream>>>(c->mlp_wbf.as<__nv_bfloat16>(),
-	  static_cast<const __nv_bfloat16 *>(feats), n, out, ncount);
+	size_t smem = sizeof(MlpTcSmem) + 1024; // + alignment slack
+	NB_CK(c, cudaFuncSetAttribute(k_mlp_fwd_tc,
+	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	// one CTA of kTcGroups pipelines per SM (the whole register file)
+	uint32_t tiles = (n + (uint32_t)kTcRows - 1u) / (uint32_t)kTcRows;
+	uint32_t grid = std::min<uint32_t>((tiles + kTcGroups - 1u) / kTcGroups,
+	  (uint32_t)c->nsm);
+	k_mlp_fwd_tc<<<grid, kTcThreads, smem, c->stream>>>(
+	  c->mlp_wbf.as<__nv_bfloat16>(), static_cast<const __nv_bfloat16 *>(feats),
+	  n, out, ncount, errs ? errs : c->berr.as<uint32_t>() + 1);
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -858,7 +867,7 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		  c->stream>>>(F.nq, 4u, F.cnt + 40, c->nq_cap, c->box,
 		  c->nfeat.as<__nv_bfloat16>());
 		rc = nrc_infer(c, c->nfeat.p, c->nq_cap, c->npred.as<float4>(),
-		  F.cnt + 40);
+		  F.cnt + 40, F.cnt + 3);
 		if (rc)
 			return rc;
 		k_nrc_apply<<<grid_for(c, c->nq_cap, 256), 256, 0, c->stream>>>(
@@ -1022,8 +1031,8 @@ int render_frame(Ctx *c)
 		  c->st.ms_frame - tr - sh - c->st.ms_nrc;
 	}
 	if (hc[3])
-		return fail(c, RENDGPU_EDEVICE, "rays abandoned on the device "
-		  "(traversal stack overflow)");
+		return fail(c, RENDGPU_EDEVICE, "device error: rays abandoned "
+		  "(traversal stack overflow) or a tensor-core wait timed out");
 	return 0;
 }
 
@@ -1112,6 +1121,10 @@ int new_ctx(nb_rdata *const *rds, uint32_t n, const uint32_t *max_depth,
 	  c->scn.ensure(n * 16) != cudaSuccess) {
 		free_ctx(c);
 		return RENDGPU_ENOMEM;
+	}
+	if (cudaMemset(c->berr.p, 0, 16) != cudaSuccess) {
+		free_ctx(c);
+		return RENDGPU_ECUDA;
 	}
 	*out = c;
 	return 0;
@@ -1893,6 +1906,9 @@ int rendgpu_nrc_infer_device(struct rdata *rdp, const void *feats, uint32_t n,
 		return RENDGPU_EINVAL;
 	if (!c->mlp_ready)
 		return fail(c, RENDGPU_ESTATE, "rendgpu_nrc_reset must come first");
+	if (n && (misaligned16(feats) || misaligned16(out)))
+		return fail(c, RENDGPU_EINVAL,
+		  "feats and out must be non-null 16-byte aligned device pointers");
 	NB_CK(c, cudaSetDevice(c->device));
 	return nrc_infer(c, feats, n, reinterpret_cast<float4 *>(out));
 }
@@ -1906,6 +1922,9 @@ int rendgpu_nrc_train_device(struct rdata *rdp, const void *feats,
 		return RENDGPU_EINVAL;
 	if (!c->mlp_ready)
 		return fail(c, RENDGPU_ESTATE, "rendgpu_nrc_reset must come first");
+	if (n && (misaligned16(feats) || misaligned16(targets)))
+		return fail(c, RENDGPU_EINVAL,
+		  "feats and targets must be non-null 16-byte aligned device pointers");
 	NB_CK(c, cudaSetDevice(c->device));
 	return nrc_train(c, feats, reinterpret_cast<const float4 *>(targets), n,
 	  update, grad, loss);
@@ -1942,6 +1961,15 @@ int rendgpu_sync(struct rdata *rdp)
 		return RENDGPU_EINVAL;
 	NB_CK(c, cudaSetDevice(c->device));
 	NB_CK(c, cudaStreamSynchronize(c->stream));
+	// device errors of the asynchronous calls since the last check
+	uint32_t e = 0;
+	NB_CK(c, cudaMemcpy(&e, c->berr.as<uint32_t>() + 1, 4,
+	  cudaMemcpyDeviceToHost));
+	if (e) {
+		NB_CK(c, cudaMemset(c->berr.as<uint32_t>() + 1, 0, 4));
+		return fail(c, RENDGPU_EDEVICE, "device error in an asynchronous "
+		  "call (abandoned rays or a timed-out tensor-core wait)");
+	}
 	return 0;
 }
 

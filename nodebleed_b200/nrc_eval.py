@@ -75,3 +75,65 @@ def equal_time(scene, w, h, depth, frames, ref, seed=1, **nrc_kw):
     out["ratio_plain_over_nrc"] = out["plain"]["relmse"] / \
         max(out["nrc"]["relmse"], 1e-30)
     return out
+
+
+def kernel_times(n_query=700_000, n_train=16_384, reps=20, seed=3):
+    """Warm CUDA-event times (us per call) of the cache's two device entry
+    points on random BF16 feature rows: inference of n_query rows
+    (rendgpu_nrc_infer_device) and one Adam step of n_train rows
+    (rendgpu_nrc_train_device).  n_query = 700k is about the number of
+    queries of a 1080p radiance-cache frame."""
+    import torch
+    sc = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(sc)
+    gr = api.GpuRenderer(rd).upload()
+    gr.nrc_reset(seed)
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    f = torch.rand((n_train, 64), device="cuda",
+                   generator=gen).to(torch.bfloat16)
+    t = torch.rand((n_train, 4), device="cuda", generator=gen)
+    fq = torch.rand((n_query, 64), device="cuda",
+                    generator=gen).to(torch.bfloat16)
+    out = torch.zeros((n_query, 4), device="cuda")
+    s = torch.cuda.ExternalStream(gr.stream())
+    calls = {
+        "train": lambda: gr._ck(gr.g.rendgpu_nrc_train_device(
+            gr.ptr, f.data_ptr(), t.data_ptr(), n_train, 1, None, None),
+            "nrc_train_device"),
+        "infer": lambda: gr._ck(gr.g.rendgpu_nrc_infer_device(
+            gr.ptr, fq.data_ptr(), n_query, out.data_ptr()),
+            "nrc_infer_device")}
+    res = {"n_query": n_query, "n_train": n_train}
+    torch.cuda.synchronize()
+    for name, fn in calls.items():
+        for _ in range(3):
+            fn()
+        gr._ck(gr.g.rendgpu_sync(gr.ptr), "sync")
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        res[name + "_us"] = e0.elapsed_time(e1) / reps * 1e3
+    gr._ck(gr.g.rendgpu_sync(gr.ptr), "sync")
+    gr.close()
+    rd.close()
+    return res
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--kernels", action="store_true",
+                    help="time the cache's inference and training calls")
+    ap.add_argument("--queries", type=int, default=700_000)
+    ap.add_argument("--train-rows", type=int, default=16_384)
+    ap.add_argument("--reps", type=int, default=20)
+    a = ap.parse_args()
+    if a.kernels:
+        print(json.dumps(kernel_times(a.queries, a.train_rows, a.reps)))
+    else:
+        ap.print_help()

@@ -81,11 +81,14 @@ def test_encode_matches_oracle(gpu):
     gr.close()
 
 
-def test_forward_matches_oracle(gpu):
+@pytest.mark.parametrize("n", [1, 129, 3001, 200_003])
+def test_forward_matches_oracle(gpu, n):
+    """Ragged sizes: a single row, one row past a 128-row tile, and a batch
+    large enough that every tile pipeline of every CTA runs several tiles
+    (and prefetches the next one)."""
     import torch
     rd, gr = _setup()
     rng = np.random.default_rng(1)
-    n = 3001  # not a multiple of the 16-row tiles
     f, f64 = _feats_dev(rng.uniform(0, 1, (n, 64)))
     out = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
