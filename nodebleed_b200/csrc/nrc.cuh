@@ -2,22 +2,18 @@
 // ReLU units, 3 linear outputs, no biases; BF16 operands on the tensor cores
 // with FP32 accumulation, FP32 master weights updated by Adam.
 //
-// Weights of layer l are stored [out][in] (row-major), so a row of 8..64
-// outputs is the "col" B operand of mma.m16n8k16.row.col directly; the
-// backward pass reads a transposed copy [in][out].  The output layer has 3
-// outputs padded to 8 (forward) / 16 (transposed copy) with zero rows.
+// Weights of layer l are stored [out][in] (row-major); the backward pass
+// reads a transposed copy [in][out].  The output layer has 3 outputs padded
+// to 8 (forward) / 16 (transposed copy) with zero rows.
 //
-// Inference runs on the tcgen05 tensor cores: 128-row tiles in shared
-// memory, FP32 accumulators in TMEM, one thread issuing the UMMAs of a
-// layer while the other pipeline of the CTA runs its epilogue.
-//
-// Training runs forward and backward per 16-row warp tile with
-// mma.m16n8k16: the FP32 C fragments of two adjacent 8-column tiles repack
-// into the BF16 A fragment of the next layer's 16-wide k tile in registers,
-// each layer's input stays in shared memory for the ReLU derivative, and
-// inputs and output gradients go to global memory; the weight gradients are
-// then split-K GEMMs over the batch (ldmatrix.trans forms the transposed
-// operands).
+// Inference and the forward/backward pass of training run on the tcgen05
+// tensor cores: 128-row tiles in shared memory (128-byte swizzled K-major
+// operands), FP32 accumulators in TMEM; one thread issues a layer's UMMAs
+// and the tile's 128 threads (one row each) turn the accumulator into the
+// next layer's operand (in inference, four such tile pipelines per SM
+// overlap one another).  The weight gradients dW_l = dz_l^T act_l are
+// split-K GEMMs over the batch with mma.m16n8k16 (ldmatrix.trans forms the
+// transposed operands).
 
 #ifndef NB_NRC_CUH
 #define NB_NRC_CUH
@@ -38,22 +34,9 @@ constexpr int kMlpSq = kMlpHidden * kMlpHidden;
 constexpr int kMlpParams = kMlpSquare * kMlpSq + kMlpOutPad * kMlpHidden;
 // transposed BF16 copy: 5 square + [64][16]
 constexpr int kMlpParamsT = kMlpSquare * kMlpSq + kMlpHidden * kMlpOutPadT;
-constexpr int kMlpRowPad = 72;             // smem row stride (bf16), no bank conflicts
-constexpr int kMlpWRows = kMlpSquare * 64 + kMlpOutPad; // weight rows
-// forward weights in shared memory: rows of 64 padded to kMlpRowPad
-constexpr int kMlpWSmem = kMlpWRows * kMlpRowPad;
-
-// Copy the forward BF16 weights [rows][64] to shared memory with padded
-// rows (all threads of the block).
-__device__ __forceinline__ void load_w_smem(__nv_bfloat16 *w,
-                                            const __nv_bfloat16 *g)
-{
-	for (int i = threadIdx.x; i < kMlpWRows * 8; i += blockDim.x) {
-		int r = i >> 3, q = i & 7;
-		*reinterpret_cast<uint4 *>(w + r * kMlpRowPad + q * 8) =
-		  __ldg(reinterpret_cast<const uint4 *>(g + r * 64) + q);
-	}
-}
+// shared-memory row stride (bf16) of the weight-gradient staging tiles:
+// rows of 64 padded to 72 keep ldmatrix free of bank conflicts
+constexpr int kMlpRowPad = 72;
 
 // ------------------------------------------------------------ mma helpers --
 
@@ -89,116 +72,12 @@ __device__ __forceinline__ void ldsm_x2_trans(uint32_t *r, const void *p)
 	  : "=r"(r[0]), "=r"(r[1]) : "r"(a));
 }
 
-// A fragment (16 rows x 16 k) of a row-major bf16 tile in shared memory
-// with row stride kMlpRowPad.
-__device__ __forceinline__ void lda_smem(uint32_t *a, const __nv_bfloat16 *t,
-                                         int kt, int lane)
-{
-	int r = lane >> 2, c = (lane & 3) * 2 + kt * 16;
-	a[0] = *reinterpret_cast<const uint32_t *>(t + r * kMlpRowPad + c);
-	a[1] = *reinterpret_cast<const uint32_t *>(t + (r + 8) * kMlpRowPad + c);
-	a[2] = *reinterpret_cast<const uint32_t *>(t + r * kMlpRowPad + c + 8);
-	a[3] = *reinterpret_cast<const uint32_t *>(t + (r + 8) * kMlpRowPad + c +
-	  8);
-}
 
-// B fragment (16 k x 8 n) from weights stored [n][k] with row length K
-// (shared or global memory).
-__device__ __forceinline__ void ldb_w(uint32_t *b, const __nv_bfloat16 *w,
-                                      int K, int nt, int kt, int lane)
-{
-	int n = nt * 8 + (lane >> 2), k = kt * 16 + (lane & 3) * 2;
-	b[0] = *reinterpret_cast<const uint32_t *>(w + n * K + k);
-	b[1] = *reinterpret_cast<const uint32_t *>(w + n * K + k + 8);
-}
 
-// Repack 8 FP32 C tiles (16 x 64) into 4 BF16 A fragments (k tiles), with
-// ReLU when relu is set.
-__device__ __forceinline__ void c_to_a(const float c[8][4], uint32_t a[4][4],
-                                       bool relu)
-{
-#pragma unroll
-	for (int kt = 0; kt < 4; kt++) {
-		const float *lo = c[2 * kt], *hi = c[2 * kt + 1];
-		float v[8];
-#pragma unroll
-		for (int i = 0; i < 4; i++) {
-			v[i] = relu ? fmaxf(lo[i], 0.0f) : lo[i];
-			v[4 + i] = relu ? fmaxf(hi[i], 0.0f) : hi[i];
-		}
-		a[kt][0] = pack_bf16(v[0], v[1]);
-		a[kt][1] = pack_bf16(v[2], v[3]);
-		a[kt][2] = pack_bf16(v[4], v[5]);
-		a[kt][3] = pack_bf16(v[6], v[7]);
-	}
-}
 
-// Store 4 A fragments (16 x 64 bf16) to a padded shared-memory tile.
-__device__ __forceinline__ void st_a(__nv_bfloat16 *t, const uint32_t a[4][4],
-                                     int lane)
-{
-	int r = lane >> 2;
-#pragma unroll
-	for (int kt = 0; kt < 4; kt++) {
-		int c = (lane & 3) * 2 + kt * 16;
-		*reinterpret_cast<uint32_t *>(t + r * kMlpRowPad + c) = a[kt][0];
-		*reinterpret_cast<uint32_t *>(t + (r + 8) * kMlpRowPad + c) = a[kt][1];
-		*reinterpret_cast<uint32_t *>(t + r * kMlpRowPad + c + 8) = a[kt][2];
-		*reinterpret_cast<uint32_t *>(t + (r + 8) * kMlpRowPad + c + 8) =
-		  a[kt][3];
-	}
-}
 
-// A fragments of one 16-row tile of BF16 features [n][64] in global memory;
-// rows beyond n read as zero.
-__device__ __forceinline__ void lda_global(uint32_t a[4][4],
-                                           const __nv_bfloat16 *f,
-                                           uint32_t row0, uint32_t n, int lane)
-{
-	uint32_t r0 = row0 + (lane >> 2), r1 = r0 + 8;
-#pragma unroll
-	for (int kt = 0; kt < 4; kt++) {
-		int c = (lane & 3) * 2 + kt * 16;
-		a[kt][0] = r0 < n ? __ldg(reinterpret_cast<const uint32_t *>(
-		  f + (size_t)r0 * kMlpIn + c)) : 0u;
-		a[kt][1] = r1 < n ? __ldg(reinterpret_cast<const uint32_t *>(
-		  f + (size_t)r1 * kMlpIn + c)) : 0u;
-		a[kt][2] = r0 < n ? __ldg(reinterpret_cast<const uint32_t *>(
-		  f + (size_t)r0 * kMlpIn + c + 8)) : 0u;
-		a[kt][3] = r1 < n ? __ldg(reinterpret_cast<const uint32_t *>(
-		  f + (size_t)r1 * kMlpIn + c + 8)) : 0u;
-	}
-}
 
-// One square layer: c = a x W^T (W [64][64] bf16 in shared memory with
-// padded rows).
-__device__ __forceinline__ void layer_sq(float c[8][4], const uint32_t a[4][4],
-                                         const __nv_bfloat16 *w, int lane)
-{
-#pragma unroll
-	for (int nt = 0; nt < 8; nt++) {
-		c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0f;
-#pragma unroll
-		for (int kt = 0; kt < 4; kt++) {
-			uint32_t b[2];
-			ldb_w(b, w, kMlpRowPad, nt, kt, lane);
-			mma16816(c[nt], a[kt], b[0], b[1]);
-		}
-	}
-}
 
-// Output layer: c (16 x 8, first 3 columns valid) = a x W5^T.
-__device__ __forceinline__ void layer_out(float c[4], const uint32_t a[4][4],
-                                          const __nv_bfloat16 *w5, int lane)
-{
-	c[0] = c[1] = c[2] = c[3] = 0.0f;
-#pragma unroll
-	for (int kt = 0; kt < 4; kt++) {
-		uint32_t b[2];
-		ldb_w(b, w5, kMlpRowPad, 0, kt, lane);
-		mma16816(c, a[kt], b[0], b[1]);
-	}
-}
 
 // -------------------------------------------- inference (tcgen05 / UMMA) --
 //
@@ -509,51 +388,49 @@ k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
 
 // --------------------------------------------------------------- training --
 
-// Shared memory of the forward/backward pass of training (per CTA of 4
-// warps): the forward weights, each warp's layer inputs (for the ReLU
-// derivative) and its current output gradient.
-struct MlpTrainSmem {
-	__nv_bfloat16 w[kMlpWSmem];          // forward copy [out][in], padded
-	__nv_bfloat16 act[4][6][16 * kMlpRowPad]; // inputs of layers 0..5
-	__nv_bfloat16 dz[4][16 * kMlpRowPad]; // gradient of one layer's output
+// Training, pass 1 on tcgen05: forward and backward of 128-row tiles, one
+// tile pipeline (4 warps, one row per thread) per CTA.  UMMAs as in
+// inference (M = 128 rows, N = 64, K-steps of 16, FP32 accumulators in
+// TMEM, 128-byte swizzled K-major operands):
+//   forward  l = 0..5: z_l = act_l W_l^T, act_{l+1} = bf16(relu(z_l))
+//   backward l = 5..1: dA_l = dz_l W_l (B = the transposed copy [in][out],
+//            one K-step for the 16-wide output layer), dz_{l-1} =
+//            bf16(dA_l) where act_l > 0, else 0.
+// All six layer inputs stay in shared memory for the ReLU derivative.
+// Writes every layer's input (gact, [6][npad][64]), every layer's output
+// gradient (gdz, [6][npad][64], the output layer's in columns 0..15, zero
+// past 3) and a loss partial per CTA, exactly as k_mlp_fb; rows at or
+// past npad are not written.  Waits are bounded; a timeout counts into
+// *err and the CTA stops.
+constexpr int kFbRows = kTcRows;
+struct MlpFbSmem {
+	__nv_bfloat16 w[kTcW];             // forward weights, layers 0..5
+	__nv_bfloat16 wt[5 * 64 * 64];     // transposed weights, layers 1..5
+	__nv_bfloat16 act[6][kTcTile];     // inputs of layers 0..5
+	__nv_bfloat16 dz[kTcTile];         // output gradient of one layer
+	uint64_t bar;
+	uint32_t ok;
+	uint32_t tmem;
 	float loss;
 };
+static_assert(sizeof(__nv_bfloat16) * 5 * 64 * 64 % 1024 == 0,
+              "UMMA operands must stay 1024-byte aligned");
 
-// Store one warp's 16 x 64 bf16 tile (padded shared-memory rows) to global
-// rows [row0, row0 + 16) of a [rows][64] array.
-__device__ __forceinline__ void st_tile_global(__nv_bfloat16 *g,
-                                               const __nv_bfloat16 *t,
-                                               uint32_t row0, int lane)
+// Store 8 16-byte chunks (one 64-wide bf16 row) to a global row.
+__device__ __forceinline__ void st_row_global(__nv_bfloat16 *g,
+                                              const uint4 *v)
 {
-	// 16 rows x 128 bytes = 128 16-byte chunks, 4 per lane
 #pragma unroll
-	for (int k = 0; k < 4; k++) {
-		int c = lane + 32 * k, r = c >> 3, q = c & 7;
-		*reinterpret_cast<uint4 *>(g + (size_t)(row0 + r) * 64 + q * 8) =
-		  *reinterpret_cast<const uint4 *>(t + r * kMlpRowPad + q * 8);
-	}
+	for (int q = 0; q < 8; q++)
+		reinterpret_cast<uint4 *>(g)[q] = v[q];
 }
 
-// Training, pass 1: forward and backward of 16-row tiles.  Writes every
-// layer's BF16 input (act, [6][npad][64]) and the gradient of every
-// layer's output (dz, [6][npad][64]; the output layer's in columns 0..15)
-// for the weight-gradient GEMMs of pass 2, and per-CTA loss partials.
-// Relative L2 loss mean((y - t)^2 / (y^2 + 0.01)) over the batch and three
-// channels (y detached in the denominator).  With ncount set, the batch is
-// samples [off, off + n) of the min(*ncount, cap) produced on the device,
-// off = offset mod that count; rows past the batch are zero and add
-// nothing.
-__global__ void __launch_bounds__(128) k_mlp_fb(const __nv_bfloat16 *wbf,
-                                                const __nv_bfloat16 *wbt,
-                                                const __nv_bfloat16 *feats,
-                                                const float4 *targets,
-                                                uint32_t n, uint32_t npad,
-                                                __nv_bfloat16 *gact,
-                                                __nv_bfloat16 *gdz,
-                                                float *loss,
-                                                const uint32_t *ncount,
-                                                uint32_t offset,
-                                                uint32_t cap)
+__global__ void __launch_bounds__(kFbRows, 1)
+k_mlp_fb_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *wbt,
+            const __nv_bfloat16 *feats, const float4 *targets, uint32_t n,
+            uint32_t npad, __nv_bfloat16 *gact, __nv_bfloat16 *gdz,
+            float *loss, const uint32_t *ncount, uint32_t offset,
+            uint32_t cap, uint32_t *err)
 {
 	if (ncount) {
 		uint32_t total = min(*ncount, cap);
@@ -563,115 +440,209 @@ __global__ void __launch_bounds__(128) k_mlp_fb(const __nv_bfloat16 *wbf,
 		targets += off;
 		n = min(n, avail);
 	}
-	extern __shared__ __align__(16) unsigned char mlp_smem[];
-	MlpTrainSmem &S = *reinterpret_cast<MlpTrainSmem *>(mlp_smem);
-	load_w_smem(S.w, wbf);
-	if (threadIdx.x == 0)
+	extern __shared__ __align__(1024) unsigned char tc_smem[];
+	const uint32_t base = (uint32_t)__cvta_generic_to_shared(tc_smem);
+	MlpFbSmem &S = *reinterpret_cast<MlpFbSmem *>(tc_smem +
+	  ((1024u - (base & 1023u)) & 1023u));
+	const uint32_t tid = threadIdx.x, warp = tid >> 5;
+	const uint32_t sw = (uint32_t)__cvta_generic_to_shared(S.w);
+	const uint32_t swt = (uint32_t)__cvta_generic_to_shared(S.wt);
+	const uint32_t sdz = (uint32_t)__cvta_generic_to_shared(S.dz);
+	const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
+	unsigned char *dzb = reinterpret_cast<unsigned char *>(S.dz);
+	// forward weights: layer l at l * 8 KB, output layer 16 rows (8..15
+	// zero); transposed weights of layer l at (l - 1) * 8 KB, the output
+	// layer's 16 columns in K-chunks 0..1 (the rest zero).  cp.async keeps
+	// all of a thread's copies in flight at once.
+	for (uint32_t i = tid; i < 5u * 64u * 8u + 16u * 8u; i += kFbRows) {
+		uint32_t row = i >> 3, kc = i & 7u;
+		uint32_t l = row >> 6, r = row & 63u;
+		bool in = l < 5u || r < (uint32_t)kMlpOutPad;
+		cp_async16(sw + l * 8192u + tc_off(r, kc * 8u),
+		  wbf + (in ? (size_t)row * 64u + kc * 8u : 0u), in ? 16u : 0u);
+	}
+	asm volatile("cp.async.commit_group;" ::: "memory");
+	for (uint32_t i = tid; i < 5u * 64u * 8u; i += kFbRows) {
+		uint32_t sl = i >> 9, r = (i >> 3) & 63u, kc = i & 7u;
+		uint32_t l = sl + 1u;
+		bool in = l < 5u || kc < 2u;
+		size_t src = l < 5u ? (size_t)l * kMlpSq + r * 64u + kc * 8u :
+		  (size_t)l * kMlpSq + r * (uint32_t)kMlpOutPadT + kc * 8u;
+		cp_async16(swt + sl * 8192u + tc_off(r, kc * 8u),
+		  wbt + (in ? src : 0u), in ? 16u : 0u);
+	}
+	asm volatile("cp.async.commit_group;" ::: "memory");
+	// the forward weights have landed; the transposed ones may still be in
+	// flight until the first backward layer
+	asm volatile("cp.async.wait_group 1;" ::: "memory");
+	if (warp == 0) {
+		asm volatile(
+		  "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;"
+		  :: "r"((uint32_t)__cvta_generic_to_shared(&S.tmem)));
+		asm volatile(
+		  "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+	}
+	if (tid == 0) {
+		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar));
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 		S.loss = 0.0f;
+	}
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 	__syncthreads();
-	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	const uint32_t tmem = S.tmem;
+	const uint32_t tlane = tmem + ((warp * 32u) << 16);
 	const float inv = n ? 1.0f / (3.0f * (float)n) : 0.0f;
-	uint32_t tiles = npad / 16u;
+	const uint32_t tiles = (npad + kFbRows - 1u) / kFbRows;
+	uint32_t parity = 0;
+	bool ok = true;
 	float lsum = 0.0f;
-	for (uint32_t t = blockIdx.x * 4u + warp; t < tiles;
-	     t += gridDim.x * 4u) {
-		uint32_t a[4][4];
-		float c[8][4];
-		lda_global(a, feats, t * 16u, n, lane);
-		st_a(S.act[warp][0], a, lane);
-		for (int l = 0; l < kMlpSquare; l++) {
-			layer_sq(c, a, S.w + l * 64 * kMlpRowPad, lane);
-			c_to_a(c, a, true);
-			st_a(S.act[warp][l + 1], a, lane);
+	// one layer's UMMAs (ks K-steps of A x B^T into TMEM) by thread 0,
+	// then a bounded wait; every thread learns the outcome
+	auto run_layer = [&](uint32_t sa, uint32_t sb, uint32_t nn,
+	                     uint32_t ksteps) {
+		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+		asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+		__syncthreads();
+		asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+		if (tid == 0) {
+			uint32_t idesc = tc_idesc(nn);
+			for (uint32_t ks = 0; ks < ksteps; ks++)
+				tc_mma(tmem, tc_desc(sa + ks * 32u), tc_desc(sb + ks * 32u),
+				  idesc, ks > 0u ? 1u : 0u);
+			tc_commit(bar);
+			S.ok = tc_wait(bar, parity) ? 1u : 0u;
 		}
-		__syncwarp();
-		for (int l = 0; l <= kMlpSquare; l++)
-			st_tile_global(gact + (size_t)l * npad * 64, S.act[warp][l],
-			  t * 16u, lane);
-		float o[4];
-		layer_out(o, a, S.w + kMlpSquare * 64 * kMlpRowPad, lane);
-		// output gradient: thread holds rows r0 (cols 2q, 2q+1), r1
-		int q = lane & 3;
-		uint32_t r0 = t * 16u + (lane >> 2), r1 = r0 + 8u;
-		float g[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-		for (int i = 0; i < 4; i++) {
-			int col = 2 * q + (i & 1);
-			uint32_t row = i < 2 ? r0 : r1;
-			if (col < 3 && row < n) {
-				float4 tv = __ldg(targets + row);
-				float tt = col == 0 ? tv.x : (col == 1 ? tv.y : tv.z);
-				float y = o[i], d = y - tt, den = y * y + 0.01f;
-				lsum += d * d / den;
-				g[i] = 2.0f * d / den * inv;
-			}
-		}
-		// dz of the output layer as bf16, padded to 16 columns (64 in
-		// the global copy, zero past 8)
-		__nv_bfloat16 *dz = S.dz[warp];
+		parity ^= 1u;
+		__syncthreads();
+		asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+		return S.ok != 0u;
+	};
+	for (uint32_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+		const uint32_t rr = t * kFbRows + tid;
+		const bool live = rr < npad;
+		// act_0 = the features of this thread's row (zero past n)
 		{
-			int r = lane >> 2, cc = 2 * q;
-			*reinterpret_cast<uint32_t *>(dz + r * kMlpRowPad + cc) =
-			  pack_bf16(g[0], g[1]);
-			*reinterpret_cast<uint32_t *>(dz + (r + 8) * kMlpRowPad + cc) =
-			  pack_bf16(g[2], g[3]);
+			uint4 v[8];
 #pragma unroll
-			for (int z = 8; z < 64; z += 8) {
-				*reinterpret_cast<uint32_t *>(dz + r * kMlpRowPad + cc + z) =
-				  0u;
-				*reinterpret_cast<uint32_t *>(dz + (r + 8) * kMlpRowPad +
-				  cc + z) = 0u;
+			for (uint32_t kc = 0; kc < 8u; kc++) {
+				v[kc] = rr < n ? __ldg(reinterpret_cast<const uint4 *>(
+				  feats + (size_t)rr * 64u) + kc) : make_uint4(0, 0, 0, 0);
+				*reinterpret_cast<uint4 *>(reinterpret_cast<unsigned char *>(
+				  S.act[0]) + tc_off(tid, kc * 8u)) = v[kc];
+			}
+			if (live)
+				st_row_global(gact + (size_t)rr * 64u, v);
+		}
+		float y[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+		for (uint32_t l = 0; l <= (uint32_t)kMlpSquare; l++) {
+			ok = run_layer((uint32_t)__cvta_generic_to_shared(S.act[l]),
+			  sw + l * 8192u, l == (uint32_t)kMlpSquare ? 16u : 64u, 4u);
+			if (!ok)
+				break;
+			if (l < (uint32_t)kMlpSquare) {
+				uint32_t v[64];
+				tc_ld64(tlane, v);
+				uint4 pk[8];
+#pragma unroll
+				for (uint32_t q = 0; q < 8u; q++) {
+					pk[q].x = pack_bf16(
+					  fmaxf(__uint_as_float(v[8 * q]), 0.0f),
+					  fmaxf(__uint_as_float(v[8 * q + 1]), 0.0f));
+					pk[q].y = pack_bf16(
+					  fmaxf(__uint_as_float(v[8 * q + 2]), 0.0f),
+					  fmaxf(__uint_as_float(v[8 * q + 3]), 0.0f));
+					pk[q].z = pack_bf16(
+					  fmaxf(__uint_as_float(v[8 * q + 4]), 0.0f),
+					  fmaxf(__uint_as_float(v[8 * q + 5]), 0.0f));
+					pk[q].w = pack_bf16(
+					  fmaxf(__uint_as_float(v[8 * q + 6]), 0.0f),
+					  fmaxf(__uint_as_float(v[8 * q + 7]), 0.0f));
+					*reinterpret_cast<uint4 *>(
+					  reinterpret_cast<unsigned char *>(S.act[l + 1u]) +
+					  tc_off(tid, q * 8u)) = pk[q];
+				}
+				if (live)
+					st_row_global(gact + ((size_t)(l + 1u) * npad + rr) *
+					  64u, pk);
+			} else {
+				tc_ld4(tlane, y);
 			}
 		}
-		__syncwarp();
-		// backward through the 6 layers
-		for (int l = kMlpSquare; l >= 0; l--) {
-			st_tile_global(gdz + (size_t)l * npad * 64, dz, t * 16u, lane);
-			if (l == 0)
+		if (!ok)
+			break;
+		// relative L2 loss and the output layer's gradient (this row)
+		float g[3] = {0.0f, 0.0f, 0.0f};
+		if (rr < n) {
+			float4 tv = __ldg(targets + rr);
+			float tt[3] = {tv.x, tv.y, tv.z};
+#pragma unroll
+			for (int c = 0; c < 3; c++) {
+				float d = y[c] - tt[c], den = y[c] * y[c] + 0.01f;
+				lsum += d * d / den;
+				g[c] = 2.0f * d / den * inv;
+			}
+		}
+		{
+			uint4 pk[8];
+			pk[0] = make_uint4(pack_bf16(g[0], g[1]), pack_bf16(g[2], 0.0f),
+			  0u, 0u);
+#pragma unroll
+			for (int q = 1; q < 8; q++)
+				pk[q] = make_uint4(0, 0, 0, 0);
+			*reinterpret_cast<uint4 *>(dzb + tc_off(tid, 0u)) = pk[0];
+			*reinterpret_cast<uint4 *>(dzb + tc_off(tid, 8u)) = pk[1];
+			if (live)
+				st_row_global(gdz + ((size_t)kMlpSquare * npad + rr) * 64u,
+				  pk);
+		}
+		// backward: dz_{l-1} = (dz_l W_l) where act_l > 0
+		asm volatile("cp.async.wait_all;" ::: "memory");
+		for (uint32_t l = (uint32_t)kMlpSquare; l >= 1u; l--) {
+			ok = run_layer(sdz, swt + (l - 1u) * 8192u, 64u,
+			  l == (uint32_t)kMlpSquare ? 1u : 4u);
+			if (!ok)
 				break;
-			const __nv_bfloat16 *act = S.act[warp][l];
-			// dA[row][in] = sum_out dz[row][out] * W[out][in]:
-			// M = 16 rows, N = 64 in, K = out (16 padded for the
-			// output layer); B from the transposed copy [in][out],
-			// read through L1
-			int kts = l == kMlpSquare ? 1 : 4;
-			int K = l == kMlpSquare ? kMlpOutPadT : 64;
-			const __nv_bfloat16 *wt = wbt + l * kMlpSq;
-			uint32_t dzf[4][4];
-			for (int kt = 0; kt < kts; kt++)
-				lda_smem(dzf[kt], dz, kt, lane);
+			uint32_t v[64];
+			tc_ld64(tlane, v);
+			const unsigned char *ab =
+			  reinterpret_cast<const unsigned char *>(S.act[l]);
+			uint4 pk[8];
 #pragma unroll
-			for (int nt = 0; nt < 8; nt++) {
-				c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0f;
-				for (int kt = 0; kt < kts; kt++) {
-					uint32_t b[2];
-					ldb_w(b, wt, K, nt, kt, lane);
-					mma16816(c[nt], dzf[kt], b[0], b[1]);
+			for (uint32_t q = 0; q < 8u; q++) {
+				uint4 a = *reinterpret_cast<const uint4 *>(ab +
+				  tc_off(tid, q * 8u));
+				uint32_t aw[4] = {a.x, a.y, a.z, a.w};
+				uint32_t o[4];
+#pragma unroll
+				for (int h = 0; h < 4; h++) {
+					// relu'(z) from the stored input act_l = relu(z)
+					bool p0 = (int16_t)(aw[h] & 0xffffu) > 0;
+					bool p1 = (int16_t)(aw[h] >> 16) > 0;
+					o[h] = pack_bf16(
+					  p0 ? __uint_as_float(v[8 * q + 2 * h]) : 0.0f,
+					  p1 ? __uint_as_float(v[8 * q + 2 * h + 1]) : 0.0f);
 				}
+				pk[q] = make_uint4(o[0], o[1], o[2], o[3]);
+				if (l > 1u)
+					*reinterpret_cast<uint4 *>(dzb + tc_off(tid, q * 8u)) =
+					  pk[q];
 			}
-			// dz of layer l-1 = dA * relu'(act_l), act_l = relu(z_{l-1})
-			__syncwarp();
-#pragma unroll
-			for (int nt = 0; nt < 8; nt++) {
-				int r = lane >> 2, cc = nt * 8 + 2 * q;
-				const __nv_bfloat16 *ap = act + r * kMlpRowPad + cc;
-				const __nv_bfloat16 *ap8 = act + (r + 8) * kMlpRowPad + cc;
-				float v0 = __bfloat162float(ap[0]) > 0.0f ? c[nt][0] : 0.0f;
-				float v1 = __bfloat162float(ap[1]) > 0.0f ? c[nt][1] : 0.0f;
-				float v2 = __bfloat162float(ap8[0]) > 0.0f ? c[nt][2] : 0.0f;
-				float v3 = __bfloat162float(ap8[1]) > 0.0f ? c[nt][3] : 0.0f;
-				*reinterpret_cast<uint32_t *>(dz + r * kMlpRowPad + cc) =
-				  pack_bf16(v0, v1);
-				*reinterpret_cast<uint32_t *>(dz + (r + 8) * kMlpRowPad +
-				  cc) = pack_bf16(v2, v3);
-			}
-			__syncwarp();
+			if (live)
+				st_row_global(gdz + ((size_t)(l - 1u) * npad + rr) * 64u,
+				  pk);
 		}
 	}
+	if (!ok && tid == 0)
+		atomicAdd(err, 1u);
 	atomicAdd(&S.loss, lsum);
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 	__syncthreads();
-	if (threadIdx.x == 0)
+	if (tid == 0)
 		loss[blockIdx.x] = S.loss;
+	if (warp == 0)
+		asm volatile(
+		  "tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" :: "r"(S.tmem));
 }
 
 // Training, pass 2: weight gradients dW_l[out][in] = sum_rows dz_l[row][out]

@@ -652,23 +652,23 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 {
 	if (n == 0)
 		return 0;
-	size_t smem = sizeof(MlpTrainSmem);
-	NB_CK(c, cudaFuncSetAttribute(k_mlp_fb,
+	size_t smem = sizeof(MlpFbSmem) + 1024; // + alignment slack
+	NB_CK(c, cudaFuncSetAttribute(k_mlp_fb_tc,
 	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-	// pass 1: forward + backward of 16-row tiles, 4 per CTA
+	// pass 1: forward + backward of 128-row tiles on tcgen05, one tile
+	// pipeline per CTA, one CTA per SM
 	uint32_t npad = (n + 15u) / 16u * 16u;
-	uint32_t tiles = npad / 16u;
-	uint32_t grid = std::min<uint32_t>((tiles + 3u) / 4u,
-	  std::min<uint32_t>(2u * (uint32_t)c->nsm, 1024u));
-	grid = std::max(grid, 1u);
+	uint32_t tiles = (npad + (uint32_t)kFbRows - 1u) / (uint32_t)kFbRows;
+	uint32_t grid = std::max(std::min<uint32_t>(tiles, (uint32_t)c->nsm), 1u);
 	NB_CK(c, c->mlp_act.ensure((size_t)6 * npad * 64 * 2));
 	NB_CK(c, c->mlp_dz.ensure((size_t)6 * npad * 64 * 2));
 	c->train_grid = grid;
-	k_mlp_fb<<<grid, 128, smem, c->stream>>>(c->mlp_wbf.as<__nv_bfloat16>(),
-	  c->mlp_wbt.as<__nv_bfloat16>(), static_cast<const __nv_bfloat16 *>(feats),
-	  targets, n, npad, c->mlp_act.as<__nv_bfloat16>(),
-	  c->mlp_dz.as<__nv_bfloat16>(), c->mlp_loss.as<float>(), ncount, offset,
-	  cap);
+	k_mlp_fb_tc<<<grid, kFbRows, smem, c->stream>>>(
+	  c->mlp_wbf.as<__nv_bfloat16>(), c->mlp_wbt.as<__nv_bfloat16>(),
+	  static_cast<const __nv_bfloat16 *>(feats), targets, n, npad,
+	  c->mlp_act.as<__nv_bfloat16>(), c->mlp_dz.as<__nv_bfloat16>(),
+	  c->mlp_loss.as<float>(), ncount, offset, cap,
+	  c->berr.as<uint32_t>() + 1);
 	NB_CK(c, cudaGetLastError());
 	// pass 2: split-K weight-gradient GEMMs, (splits x 6 layers) CTAs
 	uint32_t chunks = (npad + (uint32_t)kDwChunk - 1u) / (uint32_t)kDwChunk;
