@@ -12,8 +12,8 @@
 // and the tile's 128 threads (one row each) turn the accumulator into the
 // next layer's operand (in inference, four such tile pipelines per SM
 // overlap one another).  The weight gradients dW_l = dz_l^T act_l are
-// split-K GEMMs over the batch with mma.m16n8k16 (ldmatrix.trans forms the
-// transposed operands).
+// split-K UMMAs over the batch (M = N = 64, the batch rows as K, both
+// operands MN-major).
 
 #ifndef NB_NRC_CUH
 #define NB_NRC_CUH
@@ -34,21 +34,9 @@ constexpr int kMlpSq = kMlpHidden * kMlpHidden;
 constexpr int kMlpParams = kMlpSquare * kMlpSq + kMlpOutPad * kMlpHidden;
 // transposed BF16 copy: 5 square + [64][16]
 constexpr int kMlpParamsT = kMlpSquare * kMlpSq + kMlpHidden * kMlpOutPadT;
-// shared-memory row stride (bf16) of the weight-gradient staging tiles:
-// rows of 64 padded to 72 keep ldmatrix free of bank conflicts
-constexpr int kMlpRowPad = 72;
 
-// ------------------------------------------------------------ mma helpers --
+// --------------------------------------------------------------- helpers --
 
-__device__ __forceinline__ void mma16816(float *c, const uint32_t *a,
-                                         uint32_t b0, uint32_t b1)
-{
-	asm volatile(
-	  "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-	  "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-	  : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-	  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 {
@@ -56,21 +44,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 	return *reinterpret_cast<uint32_t *>(&v);
 }
 
-__device__ __forceinline__ void ldsm_x4_trans(uint32_t *r, const void *p)
-{
-	uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-	asm volatile(
-	  "ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-	  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
-}
 
-__device__ __forceinline__ void ldsm_x2_trans(uint32_t *r, const void *p)
-{
-	uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
-	asm volatile(
-	  "ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
-	  : "=r"(r[0]), "=r"(r[1]) : "r"(a));
-}
 
 
 
@@ -646,84 +620,153 @@ k_mlp_fb_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *wbt,
 }
 
 // Training, pass 2: weight gradients dW_l[out][in] = sum_rows dz_l[row][out]
-// act_l[row][in] as split-K tensor-core GEMMs.  CTA (l = blockIdx.y, split
-// blockIdx.x) sums rows [split * rows_per, ...) of layer l in chunks of 64
-// rows staged in shared memory; warp w owns outputs 16w..16w+15 (the output
-// layer: warp 0, 8 rows).  The partial goes to part[split][layer l slice];
-// the Adam kernel sums the splits.
-constexpr int kDwChunk = 64;
-__global__ void __launch_bounds__(128) k_mlp_dw(const __nv_bfloat16 *gact,
-                                                const __nv_bfloat16 *gdz,
-                                                uint32_t npad,
-                                                uint32_t rows_per,
-                                                float *part)
+// act_l[row][in] as split-K UMMAs.  CTA (l = blockIdx.y, split blockIdx.x)
+// sums rows [split * rows_per, ...) of layer l: chunks of 128 rows of dz_l
+// and act_l stream into shared memory (cp.async, two stages) in the
+// 128-byte swizzled layout, which read with the rows as K is the MN-major
+// operand layout of both (A = dz^T: M = 64 outputs, B = act^T: N = 64
+// inputs); one thread issues M64 N64 K16 UMMAs, 8 per chunk, into a
+// 64-column TMEM accumulator.  An M = 64 accumulator puts output row i in
+// TMEM lane (i mod 16) + 32 (i / 16): warp w's lanes 0..15 hold outputs
+// 16w..16w+15.  The partial goes to part[split][layer l slice] (rows
+// 0..7 of the output layer); the Adam kernel sums the splits.  Waits are
+// bounded; a timeout counts into *err.
+constexpr int kDwChunk = 128;
+struct MlpDwSmem {
+	__nv_bfloat16 dz[2][kDwChunk * 64];
+	__nv_bfloat16 act[2][kDwChunk * 64];
+	// slack behind the last operand: no descriptor stride can reach past
+	// the allocation
+	unsigned char guard[2048];
+	uint64_t bar;
+	uint32_t ok;
+	uint32_t tmem;
+};
+
+// MN-major operand descriptor: 128-byte swizzle, 8-row K blocks 1024
+// bytes apart; the one 64-wide MN block makes the leading offset unused
+// (1024, inside the chunk).
+__device__ __forceinline__ uint64_t tc_desc_mn(uint32_t saddr)
 {
-	__shared__ __align__(16) __nv_bfloat16 sdz[kDwChunk * kMlpRowPad];
-	__shared__ __align__(16) __nv_bfloat16 sact[kDwChunk * kMlpRowPad];
-	int l = blockIdx.y, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	int nout = l == kMlpSquare ? kMlpOutPad : 64;
+	uint64_t d = 0;
+	d |= (uint64_t)((saddr >> 4) & 0x3fffu);
+	d |= (uint64_t)((1024u >> 4) & 0x3fffu) << 16;
+	d |= (uint64_t)((1024u >> 4) & 0x3fffu) << 32;
+	d |= (uint64_t)1u << 46;
+	d |= (uint64_t)2u << 61;
+	return d;
+}
+
+__global__ void __launch_bounds__(128) k_mlp_dw_tc(const __nv_bfloat16 *gact,
+                                                   const __nv_bfloat16 *gdz,
+                                                   uint32_t npad,
+                                                   uint32_t rows_per,
+                                                   float *part,
+                                                   uint32_t *err)
+{
+	extern __shared__ __align__(1024) unsigned char tc_smem[];
+	const uint32_t base = (uint32_t)__cvta_generic_to_shared(tc_smem);
+	MlpDwSmem &S = *reinterpret_cast<MlpDwSmem *>(tc_smem +
+	  ((1024u - (base & 1023u)) & 1023u));
+	const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+	const uint32_t l = blockIdx.y;
+	const uint32_t nout = l == (uint32_t)kMlpSquare ? (uint32_t)kMlpOutPad : 64u;
 	const __nv_bfloat16 *act = gact + (size_t)l * npad * 64;
 	const __nv_bfloat16 *dzp = gdz + (size_t)l * npad * 64;
-	uint32_t r0 = blockIdx.x * rows_per;
-	uint32_t r1 = min(npad, r0 + rows_per);
-	bool busy = warp * 16 < nout;
-	float acc[8][4];
-#pragma unroll
-	for (int nt = 0; nt < 8; nt++)
-		acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.0f;
-	for (uint32_t c0 = r0; c0 < r1; c0 += kDwChunk) {
-		uint32_t rows = min((uint32_t)kDwChunk, r1 - c0); // multiple of 16
-		__syncthreads();
-		for (uint32_t i = threadIdx.x; i < rows * 8u; i += blockDim.x) {
+	const uint32_t r0 = blockIdx.x * rows_per;
+	const uint32_t r1 = min(npad, r0 + rows_per);
+	const uint32_t nch = r1 > r0 ? (r1 - r0 + kDwChunk - 1u) / kDwChunk : 0u;
+	const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
+	// rows [c0, c0 + rows) of dz_l and act_l into stage st
+	auto fetch = [&](uint32_t c, uint32_t st) {
+		uint32_t c0 = r0 + c * kDwChunk;
+		uint32_t rows = min((uint32_t)kDwChunk, r1 - c0);
+		uint32_t sd = (uint32_t)__cvta_generic_to_shared(S.dz[st]);
+		uint32_t sa = (uint32_t)__cvta_generic_to_shared(S.act[st]);
+		for (uint32_t i = tid; i < rows * 8u; i += 128u) {
 			uint32_t r = i >> 3, q = i & 7u;
-			*reinterpret_cast<uint4 *>(sdz + r * kMlpRowPad + q * 8) =
-			  __ldg(reinterpret_cast<const uint4 *>(dzp +
-			  (size_t)(c0 + r) * 64) + q);
-			*reinterpret_cast<uint4 *>(sact + r * kMlpRowPad + q * 8) =
-			  __ldg(reinterpret_cast<const uint4 *>(act +
-			  (size_t)(c0 + r) * 64) + q);
+			cp_async16(sd + tc_off(r, q * 8u), dzp + (size_t)(c0 + r) * 64u +
+			  q * 8u, 16u);
+			cp_async16(sa + tc_off(r, q * 8u), act + (size_t)(c0 + r) * 64u +
+			  q * 8u, 16u);
 		}
+		asm volatile("cp.async.commit_group;" ::: "memory");
+	};
+	if (warp == 0) {
+		asm volatile(
+		  "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;"
+		  :: "r"((uint32_t)__cvta_generic_to_shared(&S.tmem)));
+		asm volatile(
+		  "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+	}
+	if (tid == 0) {
+		asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar));
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if (nch > 0u)
+		fetch(0u, 0u);
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	const uint32_t tmem = S.tmem;
+	// F32 accumulate, BF16 A and B, both MN-major, N = 64, M = 64
+	const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) |
+	  (1u << 16) | ((64u >> 3) << 17) | ((64u >> 4) << 24);
+	uint32_t parity = 0;
+	bool ok = true;
+	for (uint32_t c = 0; c < nch && ok; c++) {
+		const uint32_t st = c & 1u;
+		// the stage being refilled was read by chunk c - 1's UMMAs, which
+		// completed before this iteration
+		if (c + 1u < nch) {
+			fetch(c + 1u, st ^ 1u);
+			asm volatile("cp.async.wait_group 1;" ::: "memory");
+		} else {
+			asm volatile("cp.async.wait_all;" ::: "memory");
+		}
+		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+		asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 		__syncthreads();
-		if (!busy)
-			continue;
-		for (uint32_t kb = 0; kb < rows; kb += 16) {
-			// A = dz^T (m = out, k = row): ldmatrix.trans of the dz
-			// blocks (rows kb+0-7 | 8-15) x (out 16w + 0-7 | 8-15)
-			uint32_t af[4];
-			{
-				int blk = lane >> 3, rr = lane & 7;
-				int row = kb + (blk >> 1) * 8 + rr;
-				int col = warp * 16 + (blk & 1) * 8;
-				ldsm_x4_trans(af, sdz + row * kMlpRowPad + col);
-			}
-#pragma unroll
-			for (int nt = 0; nt < 8; nt++) {
-				// B = act (k = row, n = in): ldmatrix.trans
-				uint32_t bf[2];
-				int blk = (lane >> 3) & 1, rr = lane & 7;
-				ldsm_x2_trans(bf, sact + (kb + blk * 8 + rr) * kMlpRowPad +
-				  nt * 8);
-				mma16816(acc[nt], af, bf[0], bf[1]);
-			}
+		asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+		if (tid == 0) {
+			uint32_t rows = min((uint32_t)kDwChunk, r1 - (r0 + c * kDwChunk));
+			uint32_t sd = (uint32_t)__cvta_generic_to_shared(S.dz[st]);
+			uint32_t sa = (uint32_t)__cvta_generic_to_shared(S.act[st]);
+			for (uint32_t ks = 0; ks < rows / 16u; ks++)
+				tc_mma(tmem, tc_desc_mn(sd + ks * 2048u),
+				  tc_desc_mn(sa + ks * 2048u), idesc,
+				  (c > 0u || ks > 0u) ? 1u : 0u);
+			tc_commit(bar);
+			S.ok = tc_wait(bar, parity) ? 1u : 0u;
 		}
+		parity ^= 1u;
+		__syncthreads();
+		ok = S.ok != 0u;
 	}
-	// write this split's slice of layer l (every element, zeros included)
-	float *gp = part + (size_t)blockIdx.x * kMlpParams + (size_t)l * kMlpSq;
-	int q = lane & 3;
-	if (busy) {
+	asm volatile("cp.async.wait_all;" ::: "memory");
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	// this split's slice of layer l (every element, zeros included)
+	uint32_t v[64];
+	tc_ld64(tmem + ((warp * 32u) << 16), v);
+	const uint32_t o = warp * 16u + lane;
+	if (lane < 16u && o < nout) {
+		float *gp = part + (size_t)blockIdx.x * kMlpParams +
+		  (size_t)l * kMlpSq + (size_t)o * 64u;
+		bool any = nch > 0u && ok;
 #pragma unroll
-		for (int nt = 0; nt < 8; nt++) {
-			int m0 = warp * 16 + (lane >> 2), nn = nt * 8 + 2 * q;
-			if (m0 < nout) {
-				gp[m0 * 64 + nn] = acc[nt][0];
-				gp[m0 * 64 + nn + 1] = acc[nt][1];
-			}
-			if (m0 + 8 < nout) {
-				gp[(m0 + 8) * 64 + nn] = acc[nt][2];
-				gp[(m0 + 8) * 64 + nn + 1] = acc[nt][3];
-			}
-		}
+		for (uint32_t j = 0; j < 64u; j += 4u)
+			*reinterpret_cast<float4 *>(gp + j) = any ? make_float4(
+			  __uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+			  __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3])) :
+			  make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 	}
+	if (!ok && tid == 0)
+		atomicAdd(err, 1u);
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	if (warp == 0)
+		asm volatile(
+		  "tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" :: "r"(S.tmem));
 }
 
 // Sum the per-CTA partial gradients; optionally write the sum (g_out) and

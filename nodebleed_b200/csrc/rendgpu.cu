@@ -670,15 +670,18 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 	  c->mlp_loss.as<float>(), ncount, offset, cap,
 	  c->berr.as<uint32_t>() + 1);
 	NB_CK(c, cudaGetLastError());
-	// pass 2: split-K weight-gradient GEMMs, (splits x 6 layers) CTAs
+	// pass 2: split-K weight-gradient UMMAs, (splits x 6 layers) CTAs
 	uint32_t chunks = (npad + (uint32_t)kDwChunk - 1u) / (uint32_t)kDwChunk;
 	uint32_t splits = std::min<uint32_t>(32u, chunks);
 	uint32_t rows_per = (chunks + splits - 1u) / splits * (uint32_t)kDwChunk;
 	splits = (npad + rows_per - 1u) / rows_per;
 	NB_CK(c, c->mlp_part.ensure((size_t)splits * kMlpParams * sizeof(float)));
-	k_mlp_dw<<<dim3(splits, kMlpSquare + 1), 128, 0, c->stream>>>(
+	size_t dsmem = sizeof(MlpDwSmem) + 1024; // + alignment slack
+	NB_CK(c, cudaFuncSetAttribute(k_mlp_dw_tc,
+	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
+	k_mlp_dw_tc<<<dim3(splits, kMlpSquare + 1), 128, dsmem, c->stream>>>(
 	  c->mlp_act.as<__nv_bfloat16>(), c->mlp_dz.as<__nv_bfloat16>(), npad,
-	  rows_per, c->mlp_part.as<float>());
+	  rows_per, c->mlp_part.as<float>(), c->berr.as<uint32_t>() + 1);
 	NB_CK(c, cudaGetLastError());
 	if (update)
 		c->mlp_step++;
