@@ -593,7 +593,7 @@ def run_ours(a):
                          "reference_spp": a.nrc_ref_spp,
                          "warmup_frames": 4, "self_train_bounce": 3,
                          "train_paths_per_frame": 65536,
-                         "adam_lr": 1e-2}
+                         "adam_steps_per_frame": 6, "adam_lr": 1e-2}
         nrc["wall_s"] = time.perf_counter() - t0
 
     batch = None

@@ -78,7 +78,7 @@ struct rendgpu_cfg {
 	                         frames of unbiased tracing (0 = 4); [2]: bounce
 	                         at which training paths end in the cache after
 	                         the warm-up (0 = 3); [3]: cache training steps
-	                         of 16384 samples per frame (0 = 4) */
+	                         of 16384 samples per frame (0 = 6) */
 };
 
 /* A ray for the batch calls: origin, tmax, direction (32 bytes). */
