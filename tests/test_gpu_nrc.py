@@ -104,11 +104,15 @@ def test_forward_matches_oracle(gpu, n):
     gr.close()
 
 
-def test_gradients_match_oracle(gpu):
+@pytest.mark.parametrize("n", [2048, 1000, 40_000])
+def test_gradients_match_oracle(gpu, n):
+    """Per-layer gradients and the loss against the FP64 oracle.  1000 rows
+    leave a partial 112-row chunk in the weight-gradient pass; 40,000 rows
+    are 313 tiles of 128, so every CTA of the forward/backward pass runs
+    several tiles."""
     import torch
     rd, gr = _setup(11)
     rng = np.random.default_rng(2)
-    n = 2048
     f, f64 = _feats_dev(rng.uniform(0, 1, (n, 64)))
     t = rng.uniform(0, 2, (n, 4)).astype(np.float32)
     d_t = _dev(t)
