@@ -246,6 +246,18 @@ int rendgpu_nrc_encode_device(struct rdata *rd, const float *raw_device,
  * 16-byte aligned (RENDGPU_EINVAL otherwise). */
 int rendgpu_nrc_infer_device(struct rdata *rd, const void *feats_device,
                              uint32_t n, float *out_device);
+/* The frame's cache lookup in one pass: for each of n queries, 4 float4 at
+ * entries_device + 16 i hold (position, path index as uint32 bits),
+ * (outgoing direction, throughput r), (normal, throughput g), (albedo,
+ * throughput b); the query is encoded as rendgpu_nrc_encode_device does,
+ * run through the MLP as rendgpu_nrc_infer_device does, and
+ * radiance_device[4 path .. + 2] += throughput * max(output, 0).  Queries
+ * whose path index is npath or more are skipped; two queries of one path
+ * in a call race.  Device buffers 16-byte aligned (RENDGPU_EINVAL
+ * otherwise); needs rendgpu_upload_dynamic (the encoding's scene box). */
+int rendgpu_nrc_query_device(struct rdata *rd, const float *entries_device,
+                             uint32_t n, float *radiance_device,
+                             uint32_t npath);
 /* Gradient of the relative L2 loss mean((y-t)^2 / (y^2 + 0.01)) over a
  * batch (targets: 4 floats per query, the 4th unused); update = 1 takes
  * one Adam step.  grad_device (RENDGPU_NRC_PARAMS floats) and loss_host

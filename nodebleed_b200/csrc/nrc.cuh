@@ -53,6 +53,67 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 
 
 
+// ------------------------------------------------------------- encoding --
+
+// Raw cache inputs (12 floats: world position, outgoing direction, shading
+// normal, albedo) -> 64 BF16 features:
+//   0..35  position in the scene box, per axis sin/cos(2^k pi x), k = 0..5
+//   36..43 direction (theta/pi, phi/2pi), sin/cos(2^k pi u), k = 0..1
+//   44..46 (normal + 1) / 2,  47..49 albedo,  50..63 zero
+struct NrcBox {
+	float lo[3], inv[3]; // position -> [0,1]^3
+};
+
+__device__ __forceinline__ void nrc_encode(const float *in, const NrcBox &B,
+                                           uint4 *out)
+{
+	float f[64];
+#pragma unroll
+	for (int i = 0; i < 64; i++)
+		f[i] = 0.0f;
+#pragma unroll
+	for (int a = 0; a < 3; a++) {
+		float x = fminf(fmaxf((in[a] - B.lo[a]) * B.inv[a], 0.0f), 1.0f);
+#pragma unroll
+		for (int k = 0; k < 6; k++) {
+			float s, c;
+			// sin/cos(2^k pi x) = sin/cos(2 pi * frac(x 2^(k-1)))
+			float u = x * ldexpf(1.0f, k - 1);
+			u = u - floorf(u);
+			sincospif(2.0f * u, &s, &c);
+			f[a * 12 + 2 * k] = s;
+			f[a * 12 + 2 * k + 1] = c;
+		}
+	}
+	float dz = fminf(fmaxf(in[5], -1.0f), 1.0f);
+	float th = acosf(dz) * 0.318309886f;
+	float ph = atan2f(in[4], in[3]) * 0.159154943f + 0.5f;
+	float ang[2] = {th, ph};
+#pragma unroll
+	for (int j = 0; j < 2; j++)
+#pragma unroll
+		for (int k = 0; k < 2; k++) {
+			float s, c;
+			sincospif(ldexpf(1.0f, k) * ang[j], &s, &c);
+			f[36 + j * 4 + 2 * k] = s;
+			f[36 + j * 4 + 2 * k + 1] = c;
+		}
+#pragma unroll
+	for (int a = 0; a < 3; a++) {
+		f[44 + a] = 0.5f * (in[6 + a] + 1.0f);
+		f[47 + a] = in[9 + a];
+	}
+#pragma unroll
+	for (int i = 0; i < 64; i += 8) {
+		uint4 v;
+		v.x = pack_bf16(f[i], f[i + 1]);
+		v.y = pack_bf16(f[i + 2], f[i + 3]);
+		v.z = pack_bf16(f[i + 4], f[i + 5]);
+		v.w = pack_bf16(f[i + 6], f[i + 7]);
+		out[i / 8] = v;
+	}
+}
+
 // -------------------------------------------- inference (tcgen05 / UMMA) --
 //
 // 128-row tiles.  Operands in shared memory in the K-major 128-byte
@@ -209,16 +270,23 @@ __device__ __forceinline__ void tc_group_sync(uint32_t g)
 	asm volatile("bar.sync %0, 128;" :: "r"(1u + g) : "memory");
 }
 
-// out[i] = (r, g, b, 0) = MLP(feats[i]) for i < n (n = min(*ncount, n)
-// with ncount set).  kTcGroups groups of 4 warps, each an independent
-// pipeline over 128-row tiles (its own TMEM accumulator of 64 columns,
-// feature and A buffers and mbarrier) sharing the weights: while the tensor
-// core works for one group, the others run their epilogues.  The next
-// tile's features stream into the feature buffer (cp.async) as soon as
-// layer 0 has read it.  One CTA per SM.
+// Q = false: out[i] = (r, g, b, 0) = MLP(feats[i]) for i < n.
+// Q = true (the frame's cache queries): query i is the entry qe[4i..4i+3]
+// (position, direction, normal, albedo in .xyz; path index bits and the
+// throughput in .w), encoded in registers straight into the feature tile;
+// its output is added to the path's radiance, L[path] += T * max(y, 0)
+// (entries whose path index is npath or more are skipped).
+// n = min(*ncount, n) with ncount set.  kTcGroups groups of 4 warps, each an
+// independent pipeline over 128-row tiles (its own TMEM accumulator of 64
+// columns, feature and A buffers and mbarrier) sharing the weights: while
+// the tensor core works for one group, the others run their epilogues.  The
+// next tile's features go into the feature buffer as soon as layer 0 has
+// read it.  One CTA per SM.
+template <bool Q>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
-             float4 *out, const uint32_t *ncount, uint32_t *err)
+             float4 *out, const uint32_t *ncount, uint32_t *err,
+             const float4 *qe, NrcBox box, float4 *pL, uint32_t npath)
 {
 	if (ncount)
 		n = min(*ncount, n);
@@ -238,17 +306,42 @@ k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
 	unsigned char *abytes = reinterpret_cast<unsigned char *>(S.a[g]);
 	uint32_t tiles = (n + kTcRows - 1u) / kTcRows;
 	const uint32_t tstep = gridDim.x * (uint32_t)kTcGroups;
+	unsigned char *fbytes = reinterpret_cast<unsigned char *>(S.f[g]);
+	// path index bits and throughput of this thread's query in the next
+	// tile and in the current one (Q)
+	float4 meta_next = make_float4(0.0f, 0.0f, 0.0f, 0.0f), meta = meta_next;
 	// this thread's feature row of tile tt (zeros past n) into the group's
 	// feature buffer
 	auto fetch = [&](uint32_t tt) {
 		uint32_t rr = tt * kTcRows + gt;
 		bool in = rr < n;
-		const uint4 *src = reinterpret_cast<const uint4 *>(feats +
-		  (size_t)(in ? rr : 0u) * 64u);
+		if constexpr (Q) {
+			uint4 pk[8];
+			if (in) {
+				const float4 *e = qe + 4ull * rr;
+				float4 a = __ldg(e), b = __ldg(e + 1), c = __ldg(e + 2),
+				  d = __ldg(e + 3);
+				float raw[12] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z,
+				  d.x, d.y, d.z};
+				nrc_encode(raw, box, pk);
+				meta_next = make_float4(a.w, b.w, c.w, d.w);
+			} else {
 #pragma unroll
-		for (uint32_t kc = 0; kc < 8u; kc++)
-			cp_async16(sf + tc_off(gt, kc * 8u), src + kc, in ? 16u : 0u);
-		asm volatile("cp.async.commit_group;" ::: "memory");
+				for (int q = 0; q < 8; q++)
+					pk[q] = make_uint4(0, 0, 0, 0);
+			}
+#pragma unroll
+			for (uint32_t q = 0; q < 8u; q++)
+				*reinterpret_cast<uint4 *>(fbytes + tc_off(gt, q * 8u)) =
+				  pk[q];
+		} else {
+			const uint4 *src = reinterpret_cast<const uint4 *>(feats +
+			  (size_t)(in ? rr : 0u) * 64u);
+#pragma unroll
+			for (uint32_t kc = 0; kc < 8u; kc++)
+				cp_async16(sf + tc_off(gt, kc * 8u), src + kc, in ? 16u : 0u);
+			asm volatile("cp.async.commit_group;" ::: "memory");
+		}
 	};
 	const uint32_t t0 = blockIdx.x * (uint32_t)kTcGroups + g;
 	if (t0 < tiles)
@@ -290,6 +383,7 @@ k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
 		uint32_t row = t * kTcRows + gt;
 		// this thread's part of the feature tile has landed
 		asm volatile("cp.async.wait_all;" ::: "memory");
+		meta = meta_next;
 		float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 		for (int l = 0; l <= kMlpSquare; l++) {
 			// generic-proxy / cp.async writes visible to the tensor core
@@ -346,8 +440,20 @@ k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
 				tc_ld4(tlane, o);
 			}
 		}
-		if (ok && row < n)
-			out[row] = make_float4(o[0], o[1], o[2], 0.0f);
+		if (ok && row < n) {
+			if constexpr (Q) {
+				uint32_t path = __float_as_uint(meta.x);
+				if (path < npath) {
+					float4 L = pL[path];
+					L.x += meta.y * fmaxf(o[0], 0.0f);
+					L.y += meta.z * fmaxf(o[1], 0.0f);
+					L.z += meta.w * fmaxf(o[2], 0.0f);
+					pL[path] = L;
+				}
+			} else {
+				out[row] = make_float4(o[0], o[1], o[2], 0.0f);
+			}
+		}
 	}
 	asm volatile("cp.async.wait_all;" ::: "memory");
 	if (!ok && gt == 0)
@@ -807,73 +913,15 @@ __global__ void k_mlp_adam(float *wf, float *m, float *v, const float *part,
 	}
 }
 
-// ------------------------------------------------------------- encoding --
-
-// Raw cache inputs (12 floats: world position, outgoing direction, shading
-// normal, albedo) -> 64 BF16 features:
-//   0..35  position in the scene box, per axis sin/cos(2^k pi x), k = 0..5
-//   36..43 direction (theta/pi, phi/2pi), sin/cos(2^k pi u), k = 0..1
-//   44..46 (normal + 1) / 2,  47..49 albedo,  50..63 zero
-struct NrcBox {
-	float lo[3], inv[3]; // position -> [0,1]^3
-};
-
-__device__ __forceinline__ void nrc_encode(const float *in, const NrcBox &B,
-                                           __nv_bfloat16 *out)
-{
-	float f[64];
-#pragma unroll
-	for (int i = 0; i < 64; i++)
-		f[i] = 0.0f;
-#pragma unroll
-	for (int a = 0; a < 3; a++) {
-		float x = fminf(fmaxf((in[a] - B.lo[a]) * B.inv[a], 0.0f), 1.0f);
-#pragma unroll
-		for (int k = 0; k < 6; k++) {
-			float s, c;
-			// sin/cos(2^k pi x) = sin/cos(2 pi * frac(x 2^(k-1)))
-			float u = x * ldexpf(1.0f, k - 1);
-			u = u - floorf(u);
-			sincospif(2.0f * u, &s, &c);
-			f[a * 12 + 2 * k] = s;
-			f[a * 12 + 2 * k + 1] = c;
-		}
-	}
-	float dz = fminf(fmaxf(in[5], -1.0f), 1.0f);
-	float th = acosf(dz) * 0.318309886f;
-	float ph = atan2f(in[4], in[3]) * 0.159154943f + 0.5f;
-	float ang[2] = {th, ph};
-#pragma unroll
-	for (int j = 0; j < 2; j++)
-#pragma unroll
-		for (int k = 0; k < 2; k++) {
-			float s, c;
-			sincospif(ldexpf(1.0f, k) * ang[j], &s, &c);
-			f[36 + j * 4 + 2 * k] = s;
-			f[36 + j * 4 + 2 * k + 1] = c;
-		}
-#pragma unroll
-	for (int a = 0; a < 3; a++) {
-		f[44 + a] = 0.5f * (in[6 + a] + 1.0f);
-		f[47 + a] = in[9 + a];
-	}
-#pragma unroll
-	for (int i = 0; i < 64; i += 8) {
-		uint4 v;
-		v.x = pack_bf16(f[i], f[i + 1]);
-		v.y = pack_bf16(f[i + 2], f[i + 3]);
-		v.z = pack_bf16(f[i + 4], f[i + 5]);
-		v.w = pack_bf16(f[i + 6], f[i + 7]);
-		*reinterpret_cast<uint4 *>(out + i) = v;
-	}
-}
+// --------------------------------------------- encoding and frame kernels --
 
 __global__ void k_nrc_encode(const float *raw, uint32_t n, NrcBox B,
                              __nv_bfloat16 *feats)
 {
 	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
 	     i += gridDim.x * blockDim.x)
-		nrc_encode(raw + 12ull * i, B, feats + 64ull * i);
+		nrc_encode(raw + 12ull * i, B,
+		  reinterpret_cast<uint4 *>(feats + 64ull * i));
 }
 
 // Features of cache queries / training records produced by k_shade: the
@@ -890,25 +938,7 @@ __global__ void k_nrc_encode_entries(const float4 *e, uint32_t stride,
 		float4 a = q[0], b = q[1], c = q[2], d = q[3];
 		float raw[12] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z,
 		  d.x, d.y, d.z};
-		nrc_encode(raw, B, feats + 64ull * i);
-	}
-}
-
-// L[path] += T * max(cache(x), 0) for every query.
-__global__ void k_nrc_apply(const float4 *q, const uint32_t *count,
-                            uint32_t cap, const float4 *pred, float4 *pL)
-{
-	uint32_t n = min(*count, cap);
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-	     i += gridDim.x * blockDim.x) {
-		const float4 *e = q + 4u * i;
-		uint32_t path = __float_as_uint(e[0].w);
-		float4 y = pred[i];
-		float4 L = pL[path];
-		L.x += e[1].w * fmaxf(y.x, 0.0f);
-		L.y += e[2].w * fmaxf(y.y, 0.0f);
-		L.z += e[3].w * fmaxf(y.z, 0.0f);
-		pL[path] = L;
+		nrc_encode(raw, B, reinterpret_cast<uint4 *>(feats + 64ull * i));
 	}
 }
 

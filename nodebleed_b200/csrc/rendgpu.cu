@@ -118,7 +118,7 @@ struct Ctx {
 	uint32_t mlp_step = 0;
 	bool     mlp_ready = false;
 	NrcBox   box{};
-	DevBuf   nq, nfeat, npred, nrec, rfeat, rtgt; // radiance-cache frame data
+	DevBuf   nq, nrec, rfeat, rtgt; // radiance-cache frame data
 	uint32_t nq_cap = 0, nrec_cap = 0, nrc_stride = 1;
 	uint32_t nrc_frames = 0; // radiance-cache frames rendered so far
 	uint32_t train_grid = 0; // CTAs of the last training step
@@ -608,8 +608,6 @@ int nrc_frame_buffers(Ctx *c)
 	c->nq_cap = np;
 	c->nrec_cap = std::max(ntrain * verts + 64, nrc_steps(c) * kNrcBatch);
 	NB_CK(c, c->nq.ensure((size_t)np * 64));
-	NB_CK(c, c->nfeat.ensure((size_t)np * 128));
-	NB_CK(c, c->npred.ensure((size_t)np * 16));
 	NB_CK(c, c->nrec.ensure((size_t)c->nrec_cap * 96));
 	NB_CK(c, c->rfeat.ensure((size_t)c->nrec_cap * 128));
 	NB_CK(c, c->rtgt.ensure((size_t)c->nrec_cap * 16));
@@ -623,23 +621,55 @@ inline bool misaligned16(const void *p)
 	return !p || (reinterpret_cast<uintptr_t>(p) & 15u) != 0;
 }
 
-// Forward pass of n (or, with ncount, of min(*ncount, n)) queries on the
-// tcgen05 tensor cores; a timed-out wait on the device counts into *errs.
-int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out,
-              const uint32_t *ncount = nullptr, uint32_t *errs = nullptr)
+// Inference kernel of one kind: dynamic shared memory set once, one CTA
+// of kTcGroups tile pipelines per SM (the whole register file).
+template <bool Q>
+int fwd_tc_setup(Ctx *c, uint32_t n, uint32_t *grid, size_t *smem)
+{
+	*smem = sizeof(MlpTcSmem) + 1024; // + alignment slack
+	NB_CK(c, cudaFuncSetAttribute(k_mlp_fwd_tc<Q>,
+	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+	uint32_t tiles = (n + (uint32_t)kTcRows - 1u) / (uint32_t)kTcRows;
+	*grid = std::max(std::min<uint32_t>((tiles + kTcGroups - 1u) / kTcGroups,
+	  (uint32_t)c->nsm), 1u);
+	return 0;
+}
+
+// Forward pass of n queries' features on the tcgen05 tensor cores; a
+// timed-out wait on the device counts into the device error word.
+int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out)
 {
 	if (n == 0)
 		return 0;
-	size_t smem = sizeof(MlpTcSmem) + 1024; // + alignment slack
-	NB_CK(c, cudaFuncSetAttribute(k_mlp_fwd_tc,
-	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-	// one CTA of kTcGroups pipelines per SM (the whole register file)
-	uint32_t tiles = (n + (uint32_t)kTcRows - 1u) / (uint32_t)kTcRows;
-	uint32_t grid = std::min<uint32_t>((tiles + kTcGroups - 1u) / kTcGroups,
-	  (uint32_t)c->nsm);
-	k_mlp_fwd_tc<<<grid, kTcThreads, smem, c->stream>>>(
+	uint32_t grid;
+	size_t smem;
+	int rc = fwd_tc_setup<false>(c, n, &grid, &smem);
+	if (rc)
+		return rc;
+	k_mlp_fwd_tc<false><<<grid, kTcThreads, smem, c->stream>>>(
 	  c->mlp_wbf.as<__nv_bfloat16>(), static_cast<const __nv_bfloat16 *>(feats),
-	  n, out, ncount, errs ? errs : c->berr.as<uint32_t>() + 1);
+	  n, out, nullptr, c->berr.as<uint32_t>() + 1, nullptr, c->box, nullptr,
+	  0u);
+	NB_CK(c, cudaGetLastError());
+	return 0;
+}
+
+// The frame's cache queries (min(*count, cap) entries of 4 float4, made on
+// the device): encode, infer and add each output to its path's radiance in
+// one kernel.
+int nrc_query(Ctx *c, const float4 *q, const uint32_t *count, uint32_t cap,
+              float4 *pL, uint32_t npath, uint32_t *errs)
+{
+	if (cap == 0)
+		return 0;
+	uint32_t grid;
+	size_t smem;
+	int rc = fwd_tc_setup<true>(c, cap, &grid, &smem);
+	if (rc)
+		return rc;
+	k_mlp_fwd_tc<true><<<grid, kTcThreads, smem, c->stream>>>(
+	  c->mlp_wbf.as<__nv_bfloat16>(), nullptr, cap, nullptr, count, errs, q,
+	  c->box, pL, npath);
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -868,17 +898,11 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		// cache inference for the queries of this frame
 		E->nrc = c->nev;
 		ev_record(c);
-		k_nrc_encode_entries<<<grid_for(c, c->nq_cap, 128), 128, 0,
-		  c->stream>>>(F.nq, 4u, F.cnt + 40, c->nq_cap, c->box,
-		  c->nfeat.as<__nv_bfloat16>());
-		rc = nrc_infer(c, c->nfeat.p, c->nq_cap, c->npred.as<float4>(),
-		  F.cnt + 40, F.cnt + 3);
+		rc = nrc_query(c, F.nq, F.cnt + 40, c->nq_cap, F.pL, c->npaths,
+		  F.cnt + 3);
 		if (rc)
 			return rc;
-		k_nrc_apply<<<grid_for(c, c->nq_cap, 256), 256, 0, c->stream>>>(
-		  F.nq, F.cnt + 40, c->nq_cap, c->npred.as<float4>(), F.pL);
-		NB_CK(c, cudaGetLastError());
-		c->st.launches += 3;
+		c->st.launches += 1;
 		ev_record(c);
 	}
 	k_accum<<<grid_for(c, c->npix, 256), 256, 0, c->stream>>>(S, F);
@@ -1050,7 +1074,7 @@ void free_ctx(Ctx *c)
 	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_act,
 	  &c->mlp_dz, &c->mlp_wf,
 	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
-	  &c->mlp_loss, &c->nq, &c->nfeat, &c->npred, &c->nrec, &c->rfeat,
+	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat,
 	  &c->rtgt};
 	for (DevBuf *b : bufs)
 		b->release();
@@ -1071,7 +1095,7 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
 	  &c->mlp_act, &c->mlp_dz,
 	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
-	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nfeat, &c->npred, &c->nrec,
+	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec,
 	  &c->rfeat, &c->rtgt};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
@@ -1916,6 +1940,26 @@ int rendgpu_nrc_infer_device(struct rdata *rdp, const void *feats, uint32_t n,
 		  "feats and out must be non-null 16-byte aligned device pointers");
 	NB_CK(c, cudaSetDevice(c->device));
 	return nrc_infer(c, feats, n, reinterpret_cast<float4 *>(out));
+}
+
+int rendgpu_nrc_query_device(struct rdata *rdp, const float *entries,
+                             uint32_t n, float *radiance, uint32_t npath)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->mlp_ready)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_nrc_reset must come first");
+	if (!c->have_dynamic)
+		return fail(c, RENDGPU_ESTATE, "upload_dynamic must come first");
+	if (n && (misaligned16(entries) || misaligned16(radiance)))
+		return fail(c, RENDGPU_EINVAL,
+		  "entries and radiance must be non-null 16-byte aligned device "
+		  "pointers");
+	NB_CK(c, cudaSetDevice(c->device));
+	return nrc_query(c, reinterpret_cast<const float4 *>(entries), nullptr, n,
+	  reinterpret_cast<float4 *>(radiance), npath,
+	  c->berr.as<uint32_t>() + 1);
 }
 
 int rendgpu_nrc_train_device(struct rdata *rdp, const void *feats,

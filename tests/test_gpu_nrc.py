@@ -104,6 +104,51 @@ def test_forward_matches_oracle(gpu, n):
     gr.close()
 
 
+def test_query_pass_matches_encode_infer_apply(gpu):
+    """rendgpu_nrc_query_device (encode, infer and add to the path's
+    radiance in one kernel, as cache frames do) against the separate encode
+    and infer calls and the same arithmetic in torch, bit for bit.  150,001
+    queries give every tile pipeline several tiles; queries whose path index
+    is out of range change nothing."""
+    import torch
+    rd, gr = _setup(13)
+    rng = np.random.default_rng(6)
+    n = 150_001
+    npath = n + 4000
+    raw = _random_raw(rd, n, seed=5)
+    paths = rng.permutation(npath)[:n].astype(np.uint32)
+    paths[::997] = npath + 3          # skipped
+    tput = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    e = np.zeros((n, 4, 4), np.float32)
+    for k in range(4):
+        e[:, k, :3] = raw[:, 3 * k:3 * k + 3]
+    e[:, 0, 3] = paths.view(np.float32)
+    e[:, 1:, 3] = tput
+    d_e = _dev(e)
+    rad = torch.from_numpy(rng.uniform(0, 1, (npath, 4)).astype(
+        np.float32)).cuda()
+    before = rad.clone()
+    d_raw = _dev(raw)
+    feats = torch.zeros((n, 64), dtype=torch.bfloat16, device="cuda")
+    y = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    gr._ck(gr.g.rendgpu_nrc_query_device(gr.ptr, d_e.data_ptr(), n,
+                                         rad.data_ptr(), npath), "query")
+    gr._ck(gr.g.rendgpu_nrc_encode_device(gr.ptr, d_raw.data_ptr(), n,
+                                          feats.data_ptr()), "encode")
+    gr._ck(gr.g.rendgpu_nrc_infer_device(gr.ptr, feats.data_ptr(), n,
+                                         y.data_ptr()), "infer")
+    assert gr.g.rendgpu_sync(gr.ptr) == 0
+    valid = torch.from_numpy(paths < npath).cuda()
+    idx = torch.from_numpy(paths.astype(np.int64)).cuda()[valid]
+    add = _dev(tput)[valid] * torch.clamp(y[valid, :3], min=0.0)
+    want = before.clone()
+    want[idx, :3] = before[idx, :3] + add
+    assert torch.equal(rad, want)
+    assert torch.count_nonzero(add).item() > n // 2
+    gr.close()
+
+
 @pytest.mark.parametrize("n", [2048, 1000, 40_000])
 def test_gradients_match_oracle(gpu, n):
     """Per-layer gradients and the loss against the FP64 oracle.  1000 rows
