@@ -246,6 +246,16 @@ int rendgpu_nrc_encode_device(struct rdata *rd, const float *raw_device,
  * 16-byte aligned (RENDGPU_EINVAL otherwise). */
 int rendgpu_nrc_infer_device(struct rdata *rd, const void *feats_device,
                              uint32_t n, float *out_device);
+/* Diagnostic of the device-side timeout (no counterpart in the reference).
+ * Every wait of the tensor-core kernels on their own UMMAs gives up after
+ * 2^31 SM clock cycles (about 1.1 s at 1965 MHz) and is then reported as
+ * RENDGPU_EDEVICE.  This call runs such a wait limited to `cycles`
+ * (1..2^31) on a barrier nothing completes, then on one that completes:
+ * out[0] = 1 if the first timed out, out[1] = 1 if the second succeeded,
+ * out[2] = clock cycles the timed-out wait took.  Synchronises; the
+ * context stays usable. */
+int rendgpu_check_bounded_wait(struct rdata *rd, uint32_t cycles,
+                               uint32_t *out);
 /* The frame's cache lookup in one pass: for each of n queries, 4 float4 at
  * entries_device + 16 i hold (position, path index as uint32 bits),
  * (outgoing direction, throughput r), (normal, throughput g), (albedo,

@@ -162,6 +162,7 @@ class GpuLib:
                 ("rendgpu_nrc_encode_device", [vp, vp, u32, vp]),
                 ("rendgpu_nrc_infer_device", [vp, vp, u32, vp]),
                 ("rendgpu_nrc_query_device", [vp, vp, u32, vp, u32]),
+                ("rendgpu_check_bounded_wait", [vp, u32, vp]),
                 ("rendgpu_nrc_train_device", [vp, vp, vp, u32, C.c_int, vp,
                                               vp]),
                 ("rendgpu_sync", [vp]), ("rendgpu_get_stats", [vp, vp]),

@@ -132,7 +132,10 @@ __device__ __forceinline__ void nrc_encode(const float *in, const NrcBox &B,
 constexpr int kTcRows = 128;                 // rows per tile (UMMA M)
 constexpr int kTcTile = kTcRows * 64;        // bf16 elements of a tile
 constexpr int kTcW = 5 * 64 * 64 + 16 * 64;  // weights, output layer as 16 rows
-constexpr uint32_t kTcSpin = 1u << 24;       // mbarrier poll limit
+// mbarrier wait limit in SM clock cycles (about 1.1 s at 1965 MHz): a poll
+// (mbarrier.try_wait) suspends the thread for about 7,800 cycles on B200,
+// so the limit is set in time, not in polls
+constexpr long long kTcWaitCycles = 1ll << 31;
 constexpr int kTcGroups = 4;                 // tile pipelines per CTA
 constexpr int kTcThreads = 128 * kTcGroups;  // 4 warps per pipeline
 constexpr int kTcCols = 64 * kTcGroups;      // TMEM columns of a CTA
@@ -185,11 +188,13 @@ __device__ __forceinline__ void tc_commit(uint32_t bar)
 	  " [%0];" :: "r"(bar) : "memory");
 }
 
-// Wait for the mbarrier phase `parity` with at most kTcSpin polls; false
-// on a timeout.
-__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity)
+// Wait for the mbarrier phase `parity` for at most `limit` SM clock cycles
+// (the kernels use kTcWaitCycles); false on a timeout.
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity,
+                                        long long limit = kTcWaitCycles)
 {
-	for (uint32_t i = 0; i < kTcSpin; i++) {
+	const long long t0 = clock64();
+	for (;;) {
 		uint32_t done;
 		asm volatile(
 		  "{\n\t.reg .pred p;\n\t"
@@ -198,8 +203,9 @@ __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity)
 		  : "=r"(done) : "r"(bar), "r"(parity) : "memory");
 		if (done)
 			return true;
+		if (clock64() - t0 > limit)
+			return false;
 	}
-	return false;
 }
 
 // 64 consecutive FP32 accumulator columns of this thread's TMEM lane
@@ -250,6 +256,30 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src,
 {
 	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;"
 	  :: "r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+
+// Check of the bounded wait on this device (one thread): a wait limited to
+// `cycles` on an mbarrier phase that nothing completes must time out
+// (out[0] = 1), and after one arrival the same wait must succeed
+// (out[1] = 1).  out[2] = clock cycles the timed-out wait took.
+__global__ void k_wait_check(uint32_t cycles, uint32_t *out)
+{
+	__shared__ __align__(8) uint64_t mb;
+	if (threadIdx.x != 0)
+		return;
+	uint32_t b = (uint32_t)__cvta_generic_to_shared(&mb);
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(b));
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	long long c0 = clock64();
+	bool early = tc_wait(b, 0u, (long long)cycles);
+	long long c1 = clock64();
+	uint64_t state;
+	asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];"
+	  : "=l"(state) : "r"(b) : "memory");
+	bool done = tc_wait(b, 0u, (long long)cycles);
+	out[0] = early ? 0u : 1u;
+	out[1] = done ? 1u : 0u;
+	out[2] = (uint32_t)min(c1 - c0, (long long)0xffffffff);
 }
 
 struct MlpTcSmem {

@@ -119,6 +119,7 @@ struct Ctx {
 	bool     mlp_ready = false;
 	NrcBox   box{};
 	DevBuf   nq, nrec, rfeat, rtgt; // radiance-cache frame data
+	DevBuf   waitchk;                // rendgpu_check_bounded_wait
 	uint32_t nq_cap = 0, nrec_cap = 0, nrc_stride = 1;
 	uint32_t nrc_frames = 0; // radiance-cache frames rendered so far
 	uint32_t train_grid = 0; // CTAs of the last training step
@@ -1074,7 +1075,7 @@ void free_ctx(Ctx *c)
 	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_act,
 	  &c->mlp_dz, &c->mlp_wf,
 	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
-	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat,
+	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat, &c->waitchk,
 	  &c->rtgt};
 	for (DevBuf *b : bufs)
 		b->release();
@@ -1095,7 +1096,7 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
 	  &c->mlp_act, &c->mlp_dz,
 	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
-	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec,
+	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec, &c->waitchk,
 	  &c->rfeat, &c->rtgt};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
@@ -1940,6 +1941,24 @@ int rendgpu_nrc_infer_device(struct rdata *rdp, const void *feats, uint32_t n,
 		  "feats and out must be non-null 16-byte aligned device pointers");
 	NB_CK(c, cudaSetDevice(c->device));
 	return nrc_infer(c, feats, n, reinterpret_cast<float4 *>(out));
+}
+
+int rendgpu_check_bounded_wait(struct rdata *rdp, uint32_t cycles,
+                               uint32_t *out)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c || !out)
+		return RENDGPU_EINVAL;
+	if (cycles == 0 || cycles > (1u << 31))
+		return fail(c, RENDGPU_EINVAL, "cycles must be in 1..2^31");
+	NB_CK(c, cudaSetDevice(c->device));
+	NB_CK(c, c->waitchk.ensure(4 * sizeof(uint32_t)));
+	k_wait_check<<<1, 32, 0, c->stream>>>(cycles, c->waitchk.as<uint32_t>());
+	NB_CK(c, cudaGetLastError());
+	NB_CK(c, cudaMemcpyAsync(out, c->waitchk.p, 3 * sizeof(uint32_t),
+	  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	return 0;
 }
 
 int rendgpu_nrc_query_device(struct rdata *rdp, const float *entries,

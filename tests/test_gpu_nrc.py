@@ -149,6 +149,35 @@ def test_query_pass_matches_encode_infer_apply(gpu):
     gr.close()
 
 
+@pytest.mark.parametrize("cycles", [1_000_000, 20_000_000])
+def test_bounded_wait_times_out_and_recovers(gpu, cycles):
+    """The tensor-core kernels' waits on their own UMMAs give up after a
+    bounded time, so a stuck wait becomes an error status rather than a
+    hang.  rendgpu_check_bounded_wait runs that wait on a barrier nothing
+    completes (it must time out after its cycle budget, within one poll of
+    it), then on one that completes (it must succeed); the context keeps
+    working afterwards."""
+    import time
+    import torch
+    rd, gr = _setup()
+    out = (C.c_uint32 * 3)()
+    t0 = time.perf_counter()
+    gr._ck(gr.g.rendgpu_check_bounded_wait(gr.ptr, cycles, out), "check")
+    dt = time.perf_counter() - t0
+    assert out[0] == 1, "a wait on an unfinished barrier did not time out"
+    assert out[1] == 1, "a wait on a finished barrier did not succeed"
+    # one try_wait poll suspends the thread for about 8k cycles
+    assert cycles <= out[2] < cycles + 200_000, out[2]
+    assert dt < 10.0
+    f = torch.zeros((256, 64), dtype=torch.bfloat16, device="cuda")
+    y = torch.ones((256, 4), dtype=torch.float32, device="cuda")
+    gr._ck(gr.g.rendgpu_nrc_infer_device(gr.ptr, f.data_ptr(), 256,
+                                         y.data_ptr()), "infer")
+    assert gr.g.rendgpu_sync(gr.ptr) == 0
+    assert torch.count_nonzero(y[:, :3]).item() == 0
+    gr.close()
+
+
 @pytest.mark.parametrize("n", [2048, 1000, 40_000])
 def test_gradients_match_oracle(gpu, n):
     """Per-layer gradients and the loss against the FP64 oracle.  1000 rows
