@@ -123,6 +123,23 @@ def kernel_times(n_query=700_000, n_train=16_384, reps=20, seed=3):
     return res
 
 
+def cache_frames(frames=8, w=1920, h=1080, depth=8):
+    """Render `frames` radiance-cache frames of the scale scene (1 spp);
+    device milliseconds per frame (for launch lists and timelines)."""
+    _load_cache_kernels(depth)
+    scene = api.Scene(api.SCENE_SCALE, 1)
+    rd = api.RenderData(scene, w, h, 1)
+    g = api.GpuRenderer(rd, max_depth=depth, mode=api.MODE_NRC,
+                        timing=True).upload()
+    ms = []
+    for _ in range(frames):
+        g.frame()
+        ms.append(g.stats()["ms_frame"])
+    g.close()
+    rd.close()
+    return ms
+
+
 if __name__ == "__main__":
     import argparse
     import json
@@ -132,8 +149,13 @@ if __name__ == "__main__":
     ap.add_argument("--queries", type=int, default=700_000)
     ap.add_argument("--train-rows", type=int, default=16_384)
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--frames", type=int, default=0,
+                    help="render this many 1080p radiance-cache frames of "
+                    "the scale scene and print their device times")
     a = ap.parse_args()
     if a.kernels:
         print(json.dumps(kernel_times(a.queries, a.train_rows, a.reps)))
+    elif a.frames:
+        print(json.dumps({"ms_per_frame": cache_frames(a.frames)}))
     else:
         ap.print_help()
