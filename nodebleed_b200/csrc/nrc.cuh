@@ -509,9 +509,12 @@ k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
 // All six layer inputs stay in shared memory for the ReLU derivative.
 // Writes every layer's input (gact, [6][npad][64]), every layer's output
 // gradient (gdz, [6][npad][64], the output layer's in columns 0..15, zero
-// past 3) and a loss partial per CTA, exactly as k_mlp_fb; rows at or
-// past npad are not written.  Waits are bounded; a timeout counts into
-// *err and the CTA stops.
+// past 3) for pass 2, and a loss partial per CTA (relative L2 loss
+// mean((y - t)^2 / (y^2 + 0.01)) over the batch and three channels, y
+// detached in the denominator); rows at or past npad are not written.
+// With ncount set, the batch is samples [off, off + n) of the
+// min(*ncount, cap) produced on the device, off = offset mod that count.
+// Waits are bounded; a timeout counts into *err and the CTA stops.
 constexpr int kFbRows = kTcRows;
 struct MlpFbSmem {
 	__nv_bfloat16 w[kTcW];             // forward weights, layers 0..5
