@@ -591,7 +591,7 @@ def run_ours(a):
         nrc["config"] = {"width": a.nrc_width, "height": a.nrc_height,
                          "spp_per_frame": 1, "depth": a.depth,
                          "reference_spp": a.nrc_ref_spp,
-                         "warmup_frames": 4, "self_train_bounce": 3,
+                         "warmup_frames": 1, "self_train_bounce": 3,
                          "train_paths_per_frame": 65536,
                          "adam_steps_per_frame": 6, "adam_lr": 1e-2}
         nrc["wall_s"] = time.perf_counter() - t0

@@ -75,7 +75,7 @@ struct rendgpu_cfg {
 	                        2 = phase, 3 = ylitie (see trace.cuh) */
 	uint32_t reserved[7]; /* [0]: float bits of the cache's Adam learning
 	                         rate (0 = 1e-2); [1]: radiance-cache warm-up
-	                         frames of unbiased tracing (0 = 4); [2]: bounce
+	                         frames of unbiased tracing (0 = 1); [2]: bounce
 	                         at which training paths end in the cache after
 	                         the warm-up (0 = 3); [3]: cache training steps
 	                         of 16384 samples per frame (0 = 6) */
