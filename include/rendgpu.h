@@ -44,7 +44,7 @@ enum rendgpu_mode {
 	RENDGPU_MODE_PATH = 0,    /* path tracing: NEE + cosine/mirror bounces */
 	RENDGPU_MODE_PRIMARY = 1, /* reference live shading: (n+1)/2 * albedo */
 	RENDGPU_MODE_NRC = 2      /* path tracing ended by the radiance cache at
-	                             the first diffuse vertex after the primary
+	                             vertex 2, the first vertex after the primary
 	                             hit; 2^16 training paths per frame, unbiased
 	                             up to bounce reserved[2] (default 3) where
 	                             the cache ends them too (self-training),

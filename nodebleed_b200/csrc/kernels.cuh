@@ -57,9 +57,9 @@ constexpr uint32_t kPathTrain = 2u;  // unbiased cache-training path
 struct FrameArgs {
 	uint32_t depth;   // bounces of the launch sequence: max over scenes
 	uint32_t mode;    // 0 path, 1 primary, 2 path with radiance cache
-	uint32_t nrc_end; // mode 2: from this bounce on, training paths and
-	                  // mirror chains end in the cache too (self-training);
-	                  // 0xffffffff: never (warm-up frames)
+	uint32_t nrc_end; // mode 2: from this bounce on, training paths end in
+	                  // the cache too (self-training); 0xffffffff: never
+	                  // (warm-up frames)
 };
 
 // ------------------------------------------------------------- sampling --
@@ -523,11 +523,11 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 					bool mirror = mc.w >= 0.5f && !glossy;
 					bool queried = false;
 					if (A.mode == 2u && k >= 1u && !emissive) {
-						// rendering paths end at their first diffuse
-						// vertex after the primary hit; training paths
-						// (and mirror chains) at bounce nrc_end, where
-						// the cache supplies their remaining radiance
-						bool end = k >= A.nrc_end || (!train && !mirror);
+						// rendering paths end at vertex 2 (the first
+						// vertex after the primary hit, mirrors
+						// included); training paths at bounce nrc_end.
+						// The cache supplies their remaining radiance.
+						bool end = k >= A.nrc_end || !train;
 						if (end) {
 							// radiance cache query: the path ends here
 							uint32_t qi = atomicAdd(&F.cnt[40], 1u);

@@ -273,9 +273,8 @@ __global__ void k_wait_check(uint32_t cycles, uint32_t *out)
 	long long c0 = clock64();
 	bool early = tc_wait(b, 0u, (long long)cycles);
 	long long c1 = clock64();
-	uint64_t state;
-	asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];"
-	  : "=l"(state) : "r"(b) : "memory");
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(b)
+	  : "memory");
 	bool done = tc_wait(b, 0u, (long long)cycles);
 	out[0] = early ? 0u : 1u;
 	out[1] = done ? 1u : 0u;
