@@ -793,11 +793,20 @@ __device__ __forceinline__ void trace_ylitie(const DScene &S,
 	bool active = false, exhausted = false;
 	uint32_t ridx = 0, err = 0;
 	Trav T;
+	// a warp keeps at most `share` rays in flight: 32 when the launch has
+	// at least 32 rays per resident warp; fewer in small launches, which
+	// then spread over every warp instead of filling a few (a warp runs
+	// until its slowest ray ends)
+	const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+	const uint32_t share = min(32u, max(1u, (ntot + nwarps - 1u) / nwarps));
+	const uint32_t need = min((uint32_t)kRefill, share);
 	for (;;) {
 		uint32_t vnode = kNone;
 		uint32_t idle = __ballot_sync(kFull, !active);
-		if (!exhausted && __popc(idle) >= kRefill) {
-			uint32_t cnt = __popc(idle);
+		uint32_t nidle = __popc(idle), nact = 32u - nidle;
+		uint32_t room = min(nidle, share > nact ? share - nact : 0u);
+		if (!exhausted && room >= need) {
+			uint32_t cnt = room;
 			uint32_t leader = __ffs(idle) - 1;
 			uint32_t base = 0;
 			if (lane == leader)
@@ -806,8 +815,9 @@ __device__ __forceinline__ void trace_ylitie(const DScene &S,
 			if (base + cnt >= ntot)
 				exhausted = true;
 			if (!active) {
-				uint32_t my = base + __popc(idle & ((1u << lane) - 1u));
-				if (my < ntot) {
+				uint32_t rank = __popc(idle & ((1u << lane) - 1u));
+				uint32_t my = base + rank;
+				if (rank < cnt && my < ntot) {
 					second = TWO && my >= n;
 					ridx = second ? my - n : my;
 					err = 0;
