@@ -796,9 +796,12 @@ __device__ __forceinline__ void trace_ylitie(const DScene &S,
 	// a warp keeps at most `share` rays in flight: 32 when the launch has
 	// at least 32 rays per resident warp; fewer in small launches, which
 	// then spread over every warp instead of filling a few (a warp runs
-	// until its slowest ray ends)
+	// until its slowest ray ends).  Only the launches that can be small
+	// (bounces: fused or any-hit) use it; the primary closest-hit launch
+	// keeps 32 and its register.
 	const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-	const uint32_t share = min(32u, max(1u, (ntot + nwarps - 1u) / nwarps));
+	const uint32_t share = (TWO || ANY) ?
+	  min(32u, max(1u, (ntot + nwarps - 1u) / nwarps)) : 32u;
 	const uint32_t need = min((uint32_t)kRefill, share);
 	for (;;) {
 		uint32_t vnode = kNone;
