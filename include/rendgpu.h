@@ -141,7 +141,11 @@ struct rendgpu_tune {
 	                    the next bounce's closest hits (2 launches per
 	                    bounce instead of 3); 2: separate launches;
 	                    0: the default (fused) */
-	uint32_t reserved[1];
+	uint32_t force;  /* 1: use `stack` as given even where the scene needs
+	                    more (8 is then accepted too, for the ray-batch calls
+	                    only): rays that overflow it are abandoned and
+	                    reported, which tests the overflow handling; 0: the
+	                    stack always fits (default) */
 };
 
 /* Per-scene counts of a batch frame. */
@@ -198,7 +202,11 @@ int rendgpu_occluded(struct rdata *rd, const struct rendgpu_ray *rays,
                      uint32_t n, uint8_t *occl);
 
 /* Device-pointer forms of the two calls above, on the context's stream;
- * return without synchronising. */
+ * return without synchronising.  A ray the device had to abandon (a
+ * traversal stack overflow; the upload's depth check makes this unreachable
+ * for trees it accepts) comes back as a miss from the closest-hit form and as
+ * occluded from the occlusion form, and counts into the context's
+ * device-error word, which rendgpu_sync reports and clears. */
 int rendgpu_trace_rays_device(struct rdata *rd, const void *rays_device,
                               uint32_t n, void *hits_device);
 int rendgpu_occluded_device(struct rdata *rd, const void *rays_device,
@@ -214,12 +222,15 @@ int rendgpu_occluded_device(struct rdata *rd, const void *rays_device,
  * of at most RENDGPU_NOALLOC_MAX_RAYS rays plus three counters, 4 MiB +
  * 256 B) is one static device array that every GPU loading the library keeps
  * until the process exits.  n above the maximum returns RENDGPU_ELIMIT.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The first call in each CUDA context of a device (after a device reset,
+ * again) looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.
  * All calls share the array: calls whose work overlaps on the GPU (two
  * contexts, two streams, or two host threads) race on it; calls on one
  * context are ordered by its stream.  Rays the device had to abandon come
- * back as misses.  Returns without synchronising. */
+ * back as misses and count into the context's device-error word (allocated
+ * with the context, not by this call), which rendgpu_sync reports as
+ * RENDGPU_EDEVICE.  Returns without synchronising. */
 #define RENDGPU_NOALLOC_MAX_RAYS (1u << 18)
 int rendgpu_trace_rays_device_noalloc(struct rdata *rd,
                                       const void *rays_device, uint32_t n,
@@ -283,8 +294,11 @@ int rendgpu_relmse_device(struct rdata *rd, const float *ref_device,
                           double *out);
 
 /* Wait for all work of the context.  Returns RENDGPU_EDEVICE when one of
- * the asynchronous _device calls since the last check met a device error
- * (rays abandoned, or a tensor-core wait of the cache that timed out). */
+ * the asynchronous _device calls since the last check (the no-alloc trace
+ * included) met a device error (rays abandoned, or a tensor-core wait of the
+ * cache that timed out); stats.device_errors then holds their number.  The
+ * check reads and clears the context's device-error word, as the
+ * host-pointer trace calls also do. */
 int rendgpu_sync(struct rdata *rd);
 
 /* The cudaStream_t every call of this context runs on (for callers that
@@ -299,6 +313,26 @@ int rendgpu_get_stats(struct rdata *rd, struct rendgpu_stats *st);
  * negative code.  `out` may be NULL to query the count. */
 int rendgpu_get_lights(struct rdata *rd, float *out, uint32_t cap,
                        float *total_area);
+
+/* Ray capture for parity checks (no counterpart in the reference, whose
+ * rays never leave the CPU; it lets a test re-trace the very rays a GPU frame
+ * traced with intersect_tlas / intersect_any_tlas, rend.c:1976/2883).  With
+ * bounce_mask != 0, every later frame records for each bounce k < 32 whose
+ * bit is set: an even sample (stride ceil(n / cap)) of at most `cap` of the
+ * closest-hit rays traced at bounce k, together with the hits the frame
+ * found for them (refined, as rendgpu_trace_rays returns them), and an even
+ * sample of at most `cap` of the shadow rays shading generated at bounce k.
+ * Only the first wave of camera slots is captured (rendgpu_tune.queue).
+ * Each captured bounce adds two small launches; bounce_mask = 0 stops it. */
+int rendgpu_capture(struct rdata *rd, uint32_t bounce_mask, uint32_t cap);
+/* The last frame's capture of bounce k.  rays / hits / shadow hold `cap`
+ * entries each (any may be NULL; a ray's pad word carries its path index);
+ * counts[0] = closest rays returned, [1] = closest rays traced at bounce k,
+ * [2] = shadow rays returned, [3] = shadow rays generated at bounce k.
+ * Synchronises. */
+int rendgpu_captured(struct rdata *rd, uint32_t bounce,
+                     struct rendgpu_ray *rays, struct rendgpu_hit *hits,
+                     struct rendgpu_ray *shadow, uint32_t counts[4]);
 
 /* Last error of any call on this thread's most recent context. */
 int         rendgpu_last_error(struct rdata *rd);

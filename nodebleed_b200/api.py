@@ -94,18 +94,19 @@ class RendgpuTune(C.Structure):
     _fields_ = [("block", C.c_uint32), ("stack", C.c_uint32),
                 ("queue", C.c_uint32), ("sched", C.c_uint32),
                 ("ms", C.c_float), ("sort", C.c_uint32),
-                ("fuse", C.c_uint32), ("reserved", C.c_uint32 * 1)]
+                ("fuse", C.c_uint32), ("force", C.c_uint32)]
 
     def as_dict(self):
         return {"block": self.block, "stack": self.stack,
                 "queue": self.queue, "sched": self.sched, "ms": self.ms,
-                "sort": self.sort, "fuse": self.fuse}
+                "sort": self.sort, "fuse": self.fuse, "force": self.force}
 
     @classmethod
-    def make(cls, block=0, stack=0, queue=0, sched=0, sort=0, fuse=0):
+    def make(cls, block=0, stack=0, queue=0, sched=0, sort=0, fuse=0,
+             force=0):
         t = cls()
         t.block, t.stack, t.queue, t.sched = block, stack, queue, sched
-        t.sort, t.fuse = sort, fuse
+        t.sort, t.fuse, t.force = sort, fuse, force
         return t
 
 
@@ -167,6 +168,8 @@ class GpuLib:
                                               vp]),
                 ("rendgpu_sync", [vp]), ("rendgpu_get_stats", [vp, vp]),
                 ("rendgpu_get_lights", [vp, vp, u32, vp]),
+                ("rendgpu_capture", [vp, u32, u32]),
+                ("rendgpu_captured", [vp, u32, vp, vp, vp, vp]),
                 ("rendgpu_get_stream", [vp, vp]),
                 ("rendgpu_set_tune", [vp, vp]),
                 ("rendgpu_get_tune", [vp, vp]),
@@ -467,6 +470,31 @@ class GpuRenderer:
         out = np.zeros((max(n, 1), 20), np.float32)
         self.g.rendgpu_get_lights(self.ptr, out.ctypes.data, n, C.byref(area))
         return out[:n], area.value
+
+    def capture(self, bounces, cap):
+        """Record, in every later frame, up to `cap` closest-hit rays (with
+        the frame's hits) and shadow rays of each bounce in `bounces`."""
+        mask = 0
+        for k in bounces:
+            mask |= 1 << k
+        self._ck(self.g.rendgpu_capture(self.ptr, mask, cap if mask else 0),
+                 "capture")
+        self.cap = cap
+
+    def captured(self, bounce):
+        """(rays, hits, shadow rays, counts) of the last frame's capture of
+        `bounce`; counts = (returned, traced, shadow returned, shadow
+        generated)."""
+        cap = self.cap
+        rays = np.zeros(cap, RAY_DTYPE)
+        hits = np.zeros(cap, HIT_DTYPE)
+        shadow = np.zeros(cap, RAY_DTYPE)
+        counts = (C.c_uint32 * 4)()
+        self._ck(self.g.rendgpu_captured(self.ptr, bounce, rays.ctypes.data,
+                                         hits.ctypes.data, shadow.ctypes.data,
+                                         counts), "captured")
+        n, ns = counts[0], counts[2]
+        return rays[:n], hits[:n], shadow[:ns], tuple(counts)
 
     def close(self):
         if self.live:

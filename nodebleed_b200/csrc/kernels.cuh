@@ -893,6 +893,39 @@ __global__ void __launch_bounds__(256) k_sort_scatter(const float4 *src,
 	}
 }
 
+// Parity capture: an even sample (stride ceil(n / cap)) of at most `cap`
+// entries of a queue whose count n is on the device.  With raw hits, each
+// sampled ray's closest hit is refined into the reference's record exactly
+// as k_shade refines it.  out_n[0] = entries written, out_n[1] = n.
+__global__ void __launch_bounds__(256) k_capture(DScene S, const float4 *rays,
+                                                 const uint32_t *count,
+                                                 const float4 *raw,
+                                                 uint32_t cap,
+                                                 float4 *out_rays,
+                                                 float4 *out_hits,
+                                                 uint32_t *out_n)
+{
+	uint32_t n = *count;
+	uint32_t stride = n > cap ? (n + cap - 1u) / cap : 1u;
+	uint32_t m = n ? (n - 1u) / stride + 1u : 0u;
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		out_n[0] = m;
+		out_n[1] = n;
+	}
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m;
+	     i += gridDim.x * blockDim.x) {
+		uint32_t j = i * stride;
+		float4 a = rays[2u * j], b = rays[2u * j + 1u];
+		out_rays[2u * i] = a;
+		out_rays[2u * i + 1u] = b;
+		if (out_hits) {
+			float4 h = raw[j];
+			THit th{h.x, __float_as_uint(h.y), __float_as_uint(h.z)};
+			out_hits[i] = finish_hit(S, a.x, a.y, a.z, b.x, b.y, b.z, th);
+		}
+	}
+}
+
 // relMSE of the accumulated image (acc / samples) against a reference
 // image: mean over pixels and channels of (x - r)^2 / (r^2 + 0.01),
 // accumulated in FP64 (the only double-precision arithmetic on the device).

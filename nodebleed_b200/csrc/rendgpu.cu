@@ -33,6 +33,10 @@ namespace {
 // bytes per thread in shared memory), and the default trace block size.
 constexpr int kStacks[3] = {24, 32, 48};
 constexpr int kStackMax = 48;
+// A deliberately small stack, compiled for the ray-batch calls only and used
+// only when rendgpu_tune.force asks for it: rays whose traversal needs more
+// entries are abandoned, which tests the device's overflow handling.
+constexpr int kStackForced = 8;
 constexpr int kTraceBlock = 256; // +0.6% over 128 on the 1080p workload
 constexpr uint32_t kMaxScenes = 4096;
 constexpr int kMaxEvents = 512;
@@ -123,6 +127,10 @@ struct Ctx {
 	uint32_t nq_cap = 0, nrec_cap = 0, nrc_stride = 1;
 	uint32_t nrc_frames = 0; // radiance-cache frames rendered so far
 	uint32_t train_grid = 0; // CTAs of the last training step
+	// parity capture (rendgpu_capture): per captured bounce, cap_n closest
+	// rays, their hits, cap_n shadow rays and 4 counts
+	DevBuf   capbuf;
+	uint32_t cap_mask = 0, cap_n = 0;
 	// stats / errors
 	rendgpu_stats st{};
 	int          last = 0;
@@ -181,6 +189,8 @@ uint32_t need_stack(const Ctx *c)
 // (0: none does).
 int stack_of(const Ctx *c)
 {
+	if (c->tune.force && c->tune.stack)
+		return (int)c->tune.stack; // tests of the overflow handling
 	uint32_t need = need_stack(c);
 	for (int st : kStacks)
 		if ((uint32_t)st == c->tune.stack && need <= (uint32_t)st)
@@ -286,6 +296,12 @@ void trace_kernel_s(Ctx *c, const float4 *rays, const uint32_t *count,
 	}
 }
 
+int forced_only(Ctx *c)
+{
+	return fail(c, RENDGPU_EINVAL, "a forced 8-entry traversal stack serves "
+	  "the ray-batch calls only");
+}
+
 int too_deep(Ctx *c)
 {
 	return fail(c, RENDGPU_ELIMIT, "BVH too deep for the traversal stack "
@@ -299,6 +315,10 @@ int launch_trace(Ctx *c, const float4 *rays, const uint32_t *count,
                  unsigned long long *nrays)
 {
 	switch (stack_of(c)) {
+	case kStackForced:
+		trace_kernel<kSchedYlitie, kStackForced, false>(c, rays, count, work,
+		  hits, errs, nrays);
+		break;
 	case 24:
 		trace_kernel_s<24>(c, rays, count, work, hits, errs, nrays);
 		break;
@@ -343,6 +363,8 @@ void shadow_kernel_s(Ctx *c, FrameDev &F, uint32_t k)
 int launch_shadow(Ctx *c, FrameDev &F, uint32_t k)
 {
 	switch (stack_of(c)) {
+	case kStackForced:
+		return forced_only(c);
 	case 24:
 		shadow_kernel_s<24>(c, F, k);
 		break;
@@ -386,6 +408,8 @@ int launch_fused(Ctx *c, FrameDev &F, const float4 *rays,
                  const uint32_t *count, uint32_t ks)
 {
 	switch (stack_of(c)) {
+	case kStackForced:
+		return forced_only(c);
 	case 24:
 		fused_kernel_s<24>(c, F, rays, count, ks);
 		break;
@@ -417,6 +441,9 @@ int launch_occluded(Ctx *c, const float4 *rays, const uint32_t *count,
                     uint32_t *work, uint8_t *occl, uint32_t *errs)
 {
 	switch (stack_of(c)) {
+	case kStackForced:
+		occl_kernel<kStackForced>(c, rays, count, work, occl, errs);
+		break;
 	case 24:
 		occl_kernel<24>(c, rays, count, work, occl, errs);
 		break;
@@ -814,6 +841,35 @@ void drop_graph(Ctx *c)
 	c->graph = nullptr;
 }
 
+// Where the capture of bounce k sits in capbuf: closest rays (cap_n x 32 B),
+// their hits (cap_n x 16 B), shadow rays (cap_n x 32 B), 4 counts.
+struct CapSlot {
+	float4   *rays, *hits, *shadow;
+	uint32_t *counts;
+};
+
+size_t cap_slot_bytes(uint32_t cap)
+{
+	return (size_t)cap * 80 + 16;
+}
+
+CapSlot cap_slot(const Ctx *c, uint32_t k)
+{
+	uint32_t s = (uint32_t)__builtin_popcount(c->cap_mask & ((1u << k) - 1u));
+	unsigned char *b = c->capbuf.as<unsigned char>() + s *
+	  cap_slot_bytes(c->cap_n);
+	size_t n = c->cap_n;
+	return CapSlot{reinterpret_cast<float4 *>(b),
+	  reinterpret_cast<float4 *>(b + n * 32),
+	  reinterpret_cast<float4 *>(b + n * 48),
+	  reinterpret_cast<uint32_t *>(b + n * 80)};
+}
+
+bool captures(const Ctx *c, uint32_t k)
+{
+	return c->cap_n && k < 32u && ((c->cap_mask >> k) & 1u);
+}
+
 // Event indices of the per-kernel timing of one directly launched frame.
 struct FrameEvents {
 	std::vector<int> trace, shadow;
@@ -866,6 +922,16 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 			ev_record(c);
 			c->st.launches++;
 			c->st.trace_launches++;
+			bool cap = lo == 0u && captures(c, k);
+			if (cap) {
+				// the frame's own closest hits of bounce k
+				CapSlot cs = cap_slot(c, k);
+				k_capture<<<grid_for(c, c->cap_n, 256), 256, 0,
+				  c->stream>>>(S, F.q[cur], F.cnt + cur, F.hits, c->cap_n,
+				  cs.rays, cs.hits, cs.counts);
+				NB_CK(c, cudaGetLastError());
+				c->st.launches++;
+			}
 			NB_CK(c, cudaMemsetAsync(F.cnt + (cur ^ 1u), 0,
 			  sizeof(uint32_t), c->stream));
 			NB_CK(c, cudaMemsetAsync(F.cnt + 2, 0, sizeof(uint32_t),
@@ -874,6 +940,15 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 			  A, cur, k);
 			NB_CK(c, cudaGetLastError());
 			c->st.launches++;
+			if (cap) {
+				// the shadow rays shading generated at bounce k
+				CapSlot cs = cap_slot(c, k);
+				k_capture<<<grid_for(c, c->cap_n, 256), 256, 0,
+				  c->stream>>>(S, F.shadow, F.cnt + 2, nullptr, c->cap_n,
+				  cs.shadow, nullptr, cs.counts + 2);
+				NB_CK(c, cudaGetLastError());
+				c->st.launches++;
+			}
 			if (A.mode != RENDGPU_MODE_PRIMARY &&
 			  (!fused || k + 1u == A.depth)) {
 				E->shadow.push_back(c->nev);
@@ -1078,7 +1153,7 @@ void free_ctx(Ctx *c)
 	  &c->mlp_dz, &c->mlp_wf,
 	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
 	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat, &c->waitchk,
-	  &c->rtgt};
+	  &c->rtgt, &c->capbuf};
 	for (DevBuf *b : bufs)
 		b->release();
 	for (int i = 0; i < kMaxEvents; i++)
@@ -1099,7 +1174,7 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->mlp_act, &c->mlp_dz,
 	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
 	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec, &c->waitchk,
-	  &c->rfeat, &c->rtgt};
+	  &c->rfeat, &c->rtgt, &c->capbuf};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
 		s += b->cap;
@@ -1433,8 +1508,9 @@ bool tune_valid(const rendgpu_tune *t)
 {
 	return t && (t->block == 0 || t->block == 64 || t->block == 128 ||
 	  t->block == 256) && (t->stack == 0 || t->stack == 24 ||
-	  t->stack == 32 || t->stack == 48) && t->sched <= 3 && t->sort <= 1 &&
-	  t->fuse <= 2;
+	  t->stack == 32 || t->stack == 48 ||
+	  (t->force && t->stack == (uint32_t)kStackForced)) && t->sched <= 3 &&
+	  t->sort <= 1 && t->fuse <= 2 && t->force <= 1;
 }
 
 // Apply launch parameters; a new queue capacity re-sizes the queues (and
@@ -1443,7 +1519,7 @@ int set_tune(Ctx *c, const rendgpu_tune *t)
 {
 	if (!tune_valid(t))
 		return fail(c, RENDGPU_EINVAL, "tune: block 0/64/128/256, stack "
-		  "0/24/32/48, sched 0..3");
+		  "0/24/32/48 (8 with force), sched 0..3, force 0/1");
 	bool requeue = t->queue != c->tune.queue;
 	c->tune.block = t->block;
 	c->tune.stack = t->stack;
@@ -1451,6 +1527,7 @@ int set_tune(Ctx *c, const rendgpu_tune *t)
 	c->tune.sched = t->sched;
 	c->tune.sort = t->sort;
 	c->tune.fuse = t->fuse;
+	c->tune.force = t->force;
 	drop_graph(c);
 	if (requeue && c->have_frame)
 		return alloc_frame(c);
@@ -1468,6 +1545,7 @@ rendgpu_tune effective_tune(const Ctx *c)
 	t.sched = sc == kSchedStep ? 1u : sc == kSchedPhase ? 2u : 3u;
 	t.sort = sorts(c) ? 1u : 0u;
 	t.fuse = c->tune.fuse == 2u ? 2u : 1u;
+	t.force = c->tune.force;
 	return t;
 }
 
@@ -1601,32 +1679,69 @@ static __device__ __align__(256) unsigned char
 
 std::mutex g_noalloc_mu;
 void *g_noalloc_addr[64];
+unsigned long long g_noalloc_ctx[64]; // context id the address belongs to
 
-// Device address of the scratch array on the current device `dev` (first
-// use on a device performs the lookup).
+// Id of the current CUDA context (cuCtxGetCurrent + cuCtxGetId, reached
+// through the runtime's driver entry points so the library needs no link
+// against libcuda).  A device reset ends the context; the next one has a new
+// id and loads the module, and with it the array, again, possibly at another
+// address.  0 when the id is not available.
+unsigned long long current_ctx_id()
+{
+	typedef int (*GetCurrent)(void **);
+	typedef int (*GetId)(void *, unsigned long long *);
+	static GetCurrent get_current = nullptr;
+	static GetId get_id = nullptr;
+	static bool tried = false;
+	if (!tried) {
+		tried = true;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuCtxGetCurrent",
+		  reinterpret_cast<void **>(&get_current), cudaEnableDefault, &q) !=
+		  cudaSuccess || q != cudaDriverEntryPointSuccess)
+			get_current = nullptr;
+		if (cudaGetDriverEntryPoint("cuCtxGetId",
+		  reinterpret_cast<void **>(&get_id), cudaEnableDefault, &q) !=
+		  cudaSuccess || q != cudaDriverEntryPointSuccess)
+			get_id = nullptr;
+	}
+	void *ctx = nullptr;
+	unsigned long long id = 0;
+	if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx ||
+	    get_id(ctx, &id) != 0)
+		return 0;
+	return id;
+}
+
+// Device address of the scratch array on the current device `dev`: looked
+// up on the first use in each CUDA context of the device (a device reset
+// makes a new context), cached otherwise.
 int noalloc_scratch(Ctx *c, int dev, unsigned char **base)
 {
 	if (dev < 0 || dev >= 64)
 		return fail(c, RENDGPU_EINVAL, "device ordinal above 63");
 	std::lock_guard<std::mutex> lk(g_noalloc_mu);
-	if (!g_noalloc_addr[dev]) {
+	unsigned long long id = current_ctx_id();
+	if (!g_noalloc_addr[dev] || id != g_noalloc_ctx[dev]) {
 		void *p = nullptr;
 		cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
 		if (e != cudaSuccess || !p)
 			return cuda_fail(c, e, "cudaGetSymbolAddress(scratch)");
 		g_noalloc_addr[dev] = p;
+		g_noalloc_ctx[dev] = id;
 	}
 	*base = static_cast<unsigned char *>(g_noalloc_addr[dev]);
 	return 0;
 }
 
-// Count, error and work counters of one call, written on the device so the
-// call needs no host-to-device copy.
-__global__ void k_noalloc_begin(uint32_t *hdr, uint32_t n)
+// Count and work counter of one ray-batch call (hdr[0], hdr[2]), written on
+// the device so the call needs no host-to-device copy.  hdr[1] is left
+// alone: in a context's berr it is the sticky device-error count that
+// rendgpu_sync and the host-pointer calls read and clear.
+__global__ void k_call_begin(uint32_t *hdr, uint32_t n)
 {
 	if (threadIdx.x == 0) {
 		hdr[0] = n;
-		hdr[1] = 0u;
 		hdr[2] = 0u;
 	}
 }
@@ -1751,11 +1866,10 @@ int rendgpu_trace_rays_device(struct rdata *rdp, const void *rays,
 		return 0;
 	NB_CK(c, cudaSetDevice(c->device));
 	NB_CK(c, c->braw.ensure((size_t)n * 16));
-	// berr: [0] count, [1] errors, [2] work counter
-	uint32_t hdr[3] = {n, 0u, 0u};
-	NB_CK(c, cudaMemcpyAsync(c->berr.p, hdr, sizeof(hdr),
-	  cudaMemcpyHostToDevice, c->stream));
+	// berr: [0] count, [1] device errors (sticky until read), [2] work
 	uint32_t *b = c->berr.as<uint32_t>();
+	k_call_begin<<<1, 32, 0, c->stream>>>(b, n);
+	NB_CK(c, cudaGetLastError());
 	const float4 *r4 = static_cast<const float4 *>(rays);
 	rc = launch_trace(c, r4, b, b + 2, c->braw.as<float4>(), b + 1, nullptr);
 	if (rc)
@@ -1776,10 +1890,9 @@ int rendgpu_occluded_device(struct rdata *rdp, const void *rays, uint32_t n,
 	if (n == 0)
 		return 0;
 	NB_CK(c, cudaSetDevice(c->device));
-	uint32_t hdr[3] = {n, 0u, 0u};
-	NB_CK(c, cudaMemcpyAsync(c->berr.p, hdr, sizeof(hdr),
-	  cudaMemcpyHostToDevice, c->stream));
 	uint32_t *b = c->berr.as<uint32_t>();
+	k_call_begin<<<1, 32, 0, c->stream>>>(b, n);
+	NB_CK(c, cudaGetLastError());
 	return launch_occluded(c, static_cast<const float4 *>(rays), b, b + 2,
 	  static_cast<uint8_t *>(occl), b + 1);
 }
@@ -1806,10 +1919,13 @@ int rendgpu_trace_rays_device_noalloc(struct rdata *rdp, const void *rays,
 		return rc;
 	uint32_t *hdr = reinterpret_cast<uint32_t *>(base);
 	float4 *raw = reinterpret_cast<float4 *>(base + kNoAllocHeader);
-	k_noalloc_begin<<<1, 32, 0, c->stream>>>(hdr, n);
+	k_call_begin<<<1, 32, 0, c->stream>>>(hdr, n);
 	NB_CK(c, cudaGetLastError());
 	const float4 *r4 = static_cast<const float4 *>(rays);
-	rc = launch_trace(c, r4, hdr, hdr + 2, raw, hdr + 1, nullptr);
+	// abandoned rays count into the context's device-error word (allocated
+	// with the context), which rendgpu_sync reports
+	rc = launch_trace(c, r4, hdr, hdr + 2, raw, c->berr.as<uint32_t>() + 1,
+	  nullptr);
 	if (rc)
 		return rc;
 	k_refine<<<grid_for(c, n, 256), 256, 0, c->stream>>>(scene_of(c), r4,
@@ -1818,12 +1934,26 @@ int rendgpu_trace_rays_device_noalloc(struct rdata *rdp, const void *rays,
 	return 0;
 }
 
+// Read and clear the context's device-error word (after the stream's work
+// so far); it counts every device error since the last read.
+static int take_device_errors(Ctx *c, uint32_t *e)
+{
+	*e = 0;
+	NB_CK(c, cudaMemcpyAsync(e, c->berr.as<uint32_t>() + 1, 4,
+	  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	if (*e)
+		NB_CK(c, cudaMemsetAsync(c->berr.as<uint32_t>() + 1, 0, 4,
+		  c->stream));
+	return 0;
+}
+
 static int batch_errors(Ctx *c)
 {
 	uint32_t e = 0;
-	NB_CK(c, cudaMemcpyAsync(&e, c->berr.as<uint32_t>() + 1, 4,
-	  cudaMemcpyDeviceToHost, c->stream));
-	NB_CK(c, cudaStreamSynchronize(c->stream));
+	int rc = take_device_errors(c, &e);
+	if (rc)
+		return rc;
 	c->st.device_errors = e;
 	if (e)
 		return fail(c, RENDGPU_EDEVICE, "rays abandoned on the device "
@@ -2030,16 +2160,16 @@ int rendgpu_sync(struct rdata *rdp)
 	if (!c)
 		return RENDGPU_EINVAL;
 	NB_CK(c, cudaSetDevice(c->device));
-	NB_CK(c, cudaStreamSynchronize(c->stream));
 	// device errors of the asynchronous calls since the last check
 	uint32_t e = 0;
-	NB_CK(c, cudaMemcpy(&e, c->berr.as<uint32_t>() + 1, 4,
-	  cudaMemcpyDeviceToHost));
-	if (e) {
-		NB_CK(c, cudaMemset(c->berr.as<uint32_t>() + 1, 0, 4));
+	int rc = take_device_errors(c, &e);
+	if (rc)
+		return rc;
+	c->st.device_errors = e;
+	if (e)
 		return fail(c, RENDGPU_EDEVICE, "device error in an asynchronous "
-		  "call (abandoned rays or a timed-out tensor-core wait)");
-	}
+		  "call (" + std::to_string(e) + " abandoned rays or timed-out "
+		  "tensor-core waits)");
 	return 0;
 }
 
@@ -2081,6 +2211,56 @@ int rendgpu_get_lights(struct rdata *rdp, float *out, uint32_t cap,
 	if (total_area)
 		*total_area = h.light_area;
 	return (int)n;
+}
+
+int rendgpu_capture(struct rdata *rdp, uint32_t bounce_mask, uint32_t cap)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (bounce_mask && (cap == 0u || cap > (1u << 24)))
+		return fail(c, RENDGPU_EINVAL, "capture: cap must be 1..2^24");
+	NB_CK(c, cudaSetDevice(c->device));
+	drop_graph(c); // the captured launch sequence changes
+	c->cap_mask = bounce_mask;
+	c->cap_n = bounce_mask ? cap : 0u;
+	if (!bounce_mask)
+		return 0;
+	size_t bytes = (size_t)__builtin_popcount(bounce_mask) *
+	  cap_slot_bytes(cap);
+	NB_CK(c, c->capbuf.ensure(bytes));
+	NB_CK(c, cudaMemsetAsync(c->capbuf.p, 0, bytes, c->stream));
+	return 0;
+}
+
+int rendgpu_captured(struct rdata *rdp, uint32_t bounce,
+                     struct rendgpu_ray *rays, struct rendgpu_hit *hits,
+                     struct rendgpu_ray *shadow, uint32_t counts[4])
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c || !counts)
+		return RENDGPU_EINVAL;
+	if (!captures(c, bounce))
+		return fail(c, RENDGPU_EINVAL, "bounce " + std::to_string(bounce) +
+		  " is not captured (rendgpu_capture)");
+	NB_CK(c, cudaSetDevice(c->device));
+	CapSlot cs = cap_slot(c, bounce);
+	NB_CK(c, cudaMemcpyAsync(counts, cs.counts, 4 * sizeof(uint32_t),
+	  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	uint32_t m = std::min(counts[0], c->cap_n);
+	uint32_t ms = std::min(counts[2], c->cap_n);
+	if (rays && m)
+		NB_CK(c, cudaMemcpyAsync(rays, cs.rays, (size_t)m * 32,
+		  cudaMemcpyDeviceToHost, c->stream));
+	if (hits && m)
+		NB_CK(c, cudaMemcpyAsync(hits, cs.hits, (size_t)m * 16,
+		  cudaMemcpyDeviceToHost, c->stream));
+	if (shadow && ms)
+		NB_CK(c, cudaMemcpyAsync(shadow, cs.shadow, (size_t)ms * 32,
+		  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	return 0;
 }
 
 int rendgpu_last_error(struct rdata *rdp)

@@ -1003,6 +1003,9 @@ struct SinkRaw {
 	}
 };
 
+// Occlusion answer; a ray abandoned by a device error reports occluded, the
+// conservative answer (no light leaks through), as SinkShadow adds no light
+// for it.
 struct SinkOccl {
 	uint8_t  *occl;
 	uint32_t *errs;
@@ -1010,7 +1013,7 @@ struct SinkOccl {
 	{
 		if (err)
 			atomicAdd(errs, 1u);
-		occl[i] = T.found ? 1 : 0;
+		occl[i] = (T.found || err) ? 1 : 0;
 	}
 };
 

@@ -26,9 +26,13 @@ def _ensure_built():
     orc = os.path.join(ROOT, "oracle")
     if not os.path.exists(os.path.join(orc, "liboracle.so")):
         subprocess.run(["make", "-C", orc, "liboracle.so"], check=True)
+    # the reference itself: built where its sources are named by
+    # NODEBLEED_REF; a checkout that travels prebuilt keeps oracle/_ref
+    ref_src = os.environ.get("NODEBLEED_REF", "")
     if not os.path.exists(os.path.join(orc, "_ref", "libnbref.so")) and \
-            os.path.exists("/root/reference/rend.c"):
-        subprocess.run(["make", "-C", orc, "ref"], check=True)
+            ref_src and os.path.exists(os.path.join(ref_src, "rend.c")):
+        subprocess.run(["make", "-C", orc, "ref", "REF=" + ref_src],
+                       check=True)
 
 
 _ensure_built()

@@ -323,3 +323,36 @@ def camera_rays(rd, n_side=None, seed=3):
     rays["d"] = d.astype(np.float32)
     rays["tmax"] = FLT_MAX
     return rays
+
+
+def classify_occlusion(rd_ptr, rays, occ_a, occ_b, blk_a, blk_b, eps_t,
+                       eps_b):
+    """Compare two occlusion answers on the same shadow rays.  blk_a / blk_b
+    are each side's closest hit within the ray's tmax (the blocker it sees;
+    t = FLT_MAX when none).  Returns (n_same, ties, bad).  A disagreement is a
+    tie when the blocker of the side that reports the ray occluded lies, by
+    an FP64 re-intersection with the FP32 object-space ray, within eps_b (plus
+    its Moeller-Trumbore bound) of an edge, or within eps_t relative (plus
+    the bound) of either end of the segment (0, tmax)."""
+    occ_a = np.asarray(occ_a).astype(bool)
+    occ_b = np.asarray(occ_b).astype(bool)
+    idx = np.nonzero(occ_a != occ_b)[0]
+    ties, bad = [], []
+    if len(idx):
+        r = rays[idx]
+        blk = np.where(occ_a[idx], blk_a["id"][idx], blk_b["id"][idx])
+        bt = np.where(occ_a[idx], blk_a["t"][idx], blk_b["t"][idx])
+        t64, b64 = reintersect(rd_ptr, r, blk)
+        e = mt_bounds(rd_ptr, r, blk)
+        for j, i in enumerate(idx):
+            if bt[j] == FLT_MAX:
+                bad.append(i)  # occluded, yet no blocker within tmax
+                continue
+            tmax = float(rays["tmax"][i])
+            near_edge = (b64[j][1] < eps_b + e[j][0] or
+                         b64[j][2] < eps_b + e[j][1] or
+                         b64[j][0] < eps_b + e[j][0] + e[j][1])
+            near_end = (abs(t64[j] - tmax) <= eps_t * tmax + e[j][2] or
+                        abs(t64[j]) <= eps_t * tmax + e[j][2])
+            (ties if near_edge or near_end else bad).append(i)
+    return int((occ_a == occ_b).sum()), ties, bad

@@ -1,0 +1,270 @@
+"""Parity on the benchmarked workloads themselves.
+
+* The scale scene the headline number is measured on (64 BLAS, 1024
+  instances, 1920x1080, 4 spp, depth 8): real bounce rays of a GPU frame
+  (rendgpu_capture) are re-traced by the compiled reference's
+  intersect_tlas (rend.c:1976) and by the oracle; the frame's own hits must
+  agree bit for bit in (instance, triangle) apart from classified ties, and
+  the frame's shadow rays are re-answered by intersect_any_tlas
+  (rend.c:2883).
+* The stress scene (4096 instances, GGX, mirrors, 8 lights, depth 16): the
+  same ray exchange, plus a reduced-resolution frame against the oracle's
+  path tracer.
+* The small scene at its stated 640x360, 1 spp, depth 5, and the scale scene
+  at reduced resolution, pixel for pixel against the oracle.
+* The device relMSE reduction against a host FP64 relMSE.
+* The traversal's stack-overflow handling, forced with an 8-entry stack:
+  rays are abandoned and reported, nothing faults, the context stays usable.
+
+Tie counts are reported in the assertion messages and printed (pytest -rP).
+"""
+
+import numpy as np
+import pytest
+
+from nodebleed_b200 import api
+import oracle_lib as ol
+from test_gpu_trace import (RCP_B, RCP_T, TIGHT_B, TIGHT_T,
+                            _check_against_oracle, _check_fp64)
+
+pytestmark = pytest.mark.gpu
+
+# Ties against the compiled reference (its rcpps 1/det, rend.c:872, and
+# rsqrt-free FP32 Moeller-Trumbore): at most 1 in 500 rays.
+REF_TIE_FRAC = 1.0 / 500
+# Occlusion disagreements with the reference that are not ties: none; ties
+# at most 1 in 500 shadow rays.
+OCCL_TIE_FRAC = 1.0 / 500
+
+
+def relmse(x, ref):
+    return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def _need_ref():
+    if ol.ref() is None:
+        pytest.fail("the compiled reference (oracle/_ref) is required")
+
+
+@pytest.fixture(scope="module")
+def scale_rd():
+    scene = api.Scene(api.SCENE_SCALE, 1)
+    rd = api.RenderData(scene)
+    yield rd
+    rd.close()
+    scene.close()
+
+
+@pytest.fixture(scope="module")
+def stress_rd():
+    scene = api.Scene(api.SCENE_STRESS, 1)
+    rd = api.RenderData(scene, 960, 540, 1)
+    yield rd
+    rd.close()
+    scene.close()
+
+
+def _frame_capture(rd, depth, bounces, cap, seed):
+    gr = api.GpuRenderer(rd, max_depth=depth, seed=seed).upload()
+    gr.capture(bounces, cap)
+    samples = rd.rd.samples
+    gr.frame()
+    rd.rd.samples = samples
+    out = {k: gr.captured(k) for k in bounces}
+    gr.close()
+    return out
+
+
+def _check_hits_vs_reference(rd, rays, hits, what):
+    _need_ref()
+    ref = ol.ref_trace(rd.ptr, rays)
+    same, ties, bad = ol.classify(rd.ptr, rays, hits, ref, RCP_T, RCP_B)
+    n = len(rays)
+    msg = (f"{what}: {n} rays, {same} same, {len(ties)} ties, {len(bad)} bad "
+           "against intersect_tlas")
+    print(msg)
+    assert not bad, msg + f", e.g. {bad[:5]}"
+    assert len(ties) <= max(3, int(n * REF_TIE_FRAC)), msg
+    return len(ties)
+
+
+def _check_occlusion(rd, gr, shadow, what):
+    """GPU any-hit answers against the reference's intersect_any_tlas and
+    the oracle's, disagreements classified by the blockers both sides see
+    (closest hits within the shadow ray's tmax)."""
+    _need_ref()
+    n = len(shadow)
+    occ = gr.occluded(shadow)
+    blk_gpu = gr.trace(shadow)
+    ref = ol.ref_occluded(rd.ptr, shadow)
+    blk_ref = ol.ref_trace(rd.ptr, shadow)
+    same, ties, bad = ol.classify_occlusion(rd.ptr, shadow, occ, ref,
+                                            blk_gpu, blk_ref, RCP_T, RCP_B)
+    msg = (f"{what}: {n} shadow rays, {len(ties)} ties, {len(bad)} bad "
+           "against intersect_any_tlas")
+    print(msg)
+    assert not bad, msg + f", e.g. {bad[:5]}"
+    assert len(ties) <= max(3, int(n * OCCL_TIE_FRAC)), msg
+    # the any-hit answer agrees with the closest hit within tmax
+    assert np.array_equal(occ.astype(bool), blk_gpu["t"] < ol.FLT_MAX)
+    orc = ol.orc_occluded(rd.ptr, shadow)
+    blk_orc = ol.orc_refine(rd.ptr, shadow, ol.orc_trace(rd.ptr, shadow))
+    same, ties, bad = ol.classify_occlusion(rd.ptr, shadow, occ, orc,
+                                            blk_gpu, blk_orc, TIGHT_T,
+                                            TIGHT_B)
+    assert not bad, f"{what}: {len(bad)} bad against the oracle"
+    assert len(ties) <= max(2, n // 2000)
+
+
+def test_scale_frame_rays_match_reference(gpu, scale_rd):
+    """Config 2 as benchmarked: bounces 1-3 of a 1920x1080 4 spp frame."""
+    rd = scale_rd
+    assert (rd.rd.width, rd.rd.height, rd.rd.spp) == (1920, 1080, 4)
+    cap = 100000
+    got = _frame_capture(rd, 8, [1, 2, 3], cap, seed=1)
+    rays = np.concatenate([got[k][0] for k in got])
+    hits = np.concatenate([got[k][1] for k in got])
+    shadow = np.concatenate([got[k][2] for k in got])
+    for k, (_, _, _, counts) in got.items():
+        stride = -(-counts[1] // cap)
+        assert counts[0] == (counts[1] - 1) // stride + 1
+        assert counts[1] > 10 * cap  # a sample of a full-size queue
+        assert counts[3] > cap       # and of its shadow queue
+    assert len(rays) >= 200000
+    _check_hits_vs_reference(rd, rays, hits, "scale bounces 1-3")
+    same, ties = _check_against_oracle(rd, rays, hits)
+    _check_fp64(rd, rays, hits)
+    gr = api.GpuRenderer(rd).upload()
+    # re-tracing the captured rays through the C ABI gives the frame's hits
+    again = gr.trace(rays)
+    assert np.array_equal(again.view(np.uint32), hits.view(np.uint32))
+    _check_occlusion(rd, gr, shadow, "scale shadow rays of bounces 1-3")
+    gr.close()
+
+
+def test_stress_rays_match_reference(gpu, stress_rd):
+    """Config 5's scene (4096 instances, the deepest stacks): bounce and
+    shadow rays of a 960x540 depth-16 frame, plus random and camera rays."""
+    rd = stress_rd
+    assert rd.rd.instcnt == 4096
+    got = _frame_capture(rd, 16, [1, 2, 3], 60000, seed=3)
+    rays = np.concatenate([got[k][0] for k in got] +
+                          [ol.random_rays(rd, 60000, seed=4, spread=20.0),
+                           ol.camera_rays(rd)[::9]])
+    gr = api.GpuRenderer(rd).upload()
+    st = gr.stats()
+    hits = gr.trace(rays)
+    _check_hits_vs_reference(rd, rays, hits, "stress rays")
+    _check_against_oracle(rd, rays, hits)
+    _check_fp64(rd, rays, hits)
+    shadow = np.concatenate([got[k][2] for k in got])
+    _check_occlusion(rd, gr, shadow, "stress shadow rays of bounces 1-3")
+    print(f"stress: traversal stack {st['max_stack']} entries")
+    gr.close()
+
+
+def _gpu_frame(rd, depth, seed, mode=api.MODE_PATH):
+    gr = api.GpuRenderer(rd, max_depth=depth, mode=mode, seed=seed).upload()
+    samples = rd.rd.samples
+    rays = gr.frame()
+    rd.rd.samples = samples
+    gr.readback(3)
+    acc = rd.acc().copy()
+    lights, area = gr.lights()
+    gr.close()
+    return acc, rays, lights, area
+
+
+@pytest.mark.parametrize("fam,w,h,spp,depth,seed", [
+    (api.SCENE_SMALL, 640, 360, 1, 5, 1),     # config 1 as stated
+    (api.SCENE_SCALE, 480, 270, 1, 8, 2),     # config 2's scene and depth
+    (api.SCENE_STRESS, 320, 180, 1, 16, 3)])  # config 5's scene and depth
+def test_config_frame_matches_oracle(gpu, fam, w, h, spp, depth, seed):
+    scene = api.Scene(fam, 1)
+    rd = api.RenderData(scene, w, h, spp)
+    acc, rays, lights, area = _gpu_frame(rd, depth, seed)
+    rad, orays = ol.orc_render(rd, lights, area, depth, seed=seed)
+    same = float(np.all(acc == rad, axis=2).mean())
+    print(f"family {fam} {w}x{h} depth {depth}: {same:.5f} of pixels "
+          f"bit-identical, relMSE {relmse(acc, rad):.2e}, rays {rays} vs "
+          f"{orays}")
+    assert same > 0.98, same
+    assert relmse(acc, rad) < 2e-3
+    assert abs(int(rays) - int(orays)) <= 0.01 * orays
+    rd.close()
+    scene.close()
+
+
+def test_relmse_matches_host_fp64(gpu):
+    import torch
+    scene = api.Scene(api.SCENE_TINY, 2)
+    rd = api.RenderData(scene, 96, 64, 2)
+    gr = api.GpuRenderer(rd, max_depth=3, seed=7).upload()
+    for _ in range(3):
+        gr.frame()
+    gr.readback(1)
+    acc = rd.acc().astype(np.float32).copy()
+    inv = np.float32(1.0) / np.float32(rd.rd.samples)
+    x = acc.astype(np.float64) * np.float64(inv)
+    rng = np.random.default_rng(3)
+    refs = [rng.random(acc.shape, dtype=np.float32) * 2.0,
+            np.ascontiguousarray((x * 1.1).astype(np.float32))]
+    for ref in refs:
+        d_ref = torch.from_numpy(ref.reshape(-1).copy()).cuda()
+        got = gr.relmse(d_ref.data_ptr())
+        r = ref.astype(np.float64)
+        want = float(np.mean((x - r) ** 2 / (r * r + 0.01)))
+        assert abs(got - want) <= 1e-12 * abs(want), (got, want)
+    gr.close()
+
+
+def test_stack_overflow_is_reported_not_faulted(gpu, scale_rd):
+    """An 8-entry stack (rendgpu_tune.force) is too small for the scale
+    scene: rays that need more are abandoned on the device, come back as
+    misses (closest hit) or occluded (any hit), and are reported as
+    RENDGPU_EDEVICE; afterwards the default stack gives the full answers."""
+    import torch
+    rd = scale_rd
+    gr = api.GpuRenderer(rd).upload()
+    g = gr.g
+    rays = np.concatenate([ol.random_rays(rd, 40000, seed=12),
+                           ol.camera_rays(rd)[::97]])
+    good = gr.trace(rays)
+    good_occ = gr.occluded(rays)
+    gr.set_tune(stack=8, force=1)
+    assert gr.get_tune()["stack"] == 8
+    with pytest.raises(api.RendgpuError) as e:
+        gr.trace(rays)
+    assert e.value.code == -6  # RENDGPU_EDEVICE
+    nerr = gr.stats()["device_errors"]
+    assert 0 < nerr < len(rays)
+    # device forms: answers on the device, the error through rendgpu_sync
+    n = len(rays)
+    d_rays = torch.from_numpy(rays.view(np.uint8).copy()).cuda()
+    d_hits = torch.zeros(n * 16, dtype=torch.uint8, device="cuda")
+    d_occ = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    assert g.rendgpu_trace_rays_device(gr.ptr, d_rays.data_ptr(), n,
+                                       d_hits.data_ptr()) == 0
+    assert g.rendgpu_occluded_device(gr.ptr, d_rays.data_ptr(), n,
+                                     d_occ.data_ptr()) == 0
+    assert g.rendgpu_sync(gr.ptr) == -6
+    assert gr.stats()["device_errors"] >= nerr
+    assert g.rendgpu_sync(gr.ptr) == 0  # read and cleared
+    hits = d_hits.cpu().numpy().view(api.HIT_DTYPE)
+    occ = d_occ.cpu().numpy()
+    lost = hits.view(np.uint32).reshape(-1, 4) != \
+        good.view(np.uint32).reshape(-1, 4)
+    lost = lost.any(axis=1)
+    assert lost.sum() > 0
+    assert (hits["t"][lost] == ol.FLT_MAX).all()  # abandoned: a miss
+    assert (occ[occ != good_occ] == 1).all()      # abandoned: occluded
+    # a frame needs the full stack
+    with pytest.raises(api.RendgpuError):
+        gr.frame()
+    rd.rd.blknum = 0
+    gr.set_tune()
+    again = gr.trace(rays)
+    assert np.array_equal(again.view(np.uint32), good.view(np.uint32))
+    assert g.rendgpu_sync(gr.ptr) == 0
+    gr.close()

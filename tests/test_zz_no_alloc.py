@@ -55,6 +55,36 @@ def test_noalloc_matches_device_entry_point(gpu):
     gr.close()
 
 
+def test_noalloc_full_array_and_error_report(gpu):
+    """A batch of exactly the maximum fills the array to its last hit
+    record; rays the device abandons (an 8-entry stack forced on a deep
+    scene) come back as misses and are reported by rendgpu_sync."""
+    scene = api.Scene(api.SCENE_SCALE, 3, 8)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd).upload()
+    g = gr.g
+    rays = ol.random_rays(rd, MAX_RAYS, seed=8)
+    d_rays = _device(rays)
+    ref = _trace(gr, g.rendgpu_trace_rays_device, d_rays, MAX_RAYS)
+    got = _trace(gr, g.rendgpu_trace_rays_device_noalloc, d_rays, MAX_RAYS)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    gr.set_tune(stack=8, force=1)
+    import torch
+    out = torch.zeros(MAX_RAYS * 16, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    assert g.rendgpu_trace_rays_device_noalloc(
+        gr.ptr, d_rays.data_ptr(), MAX_RAYS, out.data_ptr()) == 0
+    assert g.rendgpu_sync(gr.ptr) == -6  # RENDGPU_EDEVICE
+    assert gr.stats()["device_errors"] > 0
+    lost = out.cpu().numpy().view(api.HIT_DTYPE)
+    diff = lost.view(np.uint32).reshape(-1, 4) != \
+        ref.view(np.uint32).reshape(-1, 4)
+    assert (lost["t"][diff.any(axis=1)] == ol.FLT_MAX).all()
+    gr.set_tune()
+    assert g.rendgpu_sync(gr.ptr) == 0
+    gr.close()
+
+
 def test_noalloc_rejects_oversized_batch(gpu):
     scene = api.Scene(api.SCENE_TINY, 1)
     rd = api.RenderData(scene)
