@@ -314,6 +314,58 @@ int rendgpu_get_stats(struct rdata *rd, struct rendgpu_stats *st);
 int rendgpu_get_lights(struct rdata *rd, float *out, uint32_t cap,
                        float *total_area);
 
+/* Device-side scene update.  It replaces the host steps the reference's
+ * frame loop runs whenever a transform changed (main.c:257-264): upd_rinsts
+ * (main.c:117-157: each instance's world->object matrix as the inverse of
+ * its object->world matrix, mat4.c:299, and its world box from the 8
+ * transformed corners of its BLAS root box), rend_prepdynamic
+ * (rend.c:3073-3090: the TLAS build, build_bvh8 rend.c:458-709) and, for the
+ * path tracer, the world-space light table; the device does all three
+ * from the new matrices alone, so a moving scene never round-trips through
+ * host memory.  glob: n row-major 4x4 object->world matrices (tfmat.glob) in
+ * rd->insts order, n = rd->instcnt, 4-byte aligned; the _device form takes
+ * device memory, the other copies n * 64 bytes from host memory first.
+ * The world->object matrices and world boxes are bit-identical to the host
+ * bridge's.  The TLAS is this library's own device build (binned SAH, at
+ * most as deep as the TLAS rendgpu_upload_dynamic uploaded, so the
+ * traversal stack still fits); hits do not depend on its shape.  flags:
+ * RENDGPU_UPDATE_REFIT keeps the last device build's topology and only
+ * recomputes its boxes (faster, looser as instances move; the first update
+ * always builds).  Single-scene contexts; needs rendgpu_upload_dynamic once
+ * (which again makes the host-built TLAS current).  rd->insts and rd->aabbs
+ * on the host are not touched.  A singular matrix zeroes that instance (it
+ * is never hit) and counts into the device-error word (rendgpu_sync).  The
+ * radiance cache keeps the encoding box of the upload.  Returns without
+ * synchronising. */
+#define RENDGPU_UPDATE_REFIT 1u
+int rendgpu_update_instances_device(struct rdata *rd,
+                                    const float *glob_device, uint32_t n,
+                                    uint32_t flags);
+int rendgpu_update_instances(struct rdata *rd, const float *glob, uint32_t n,
+                             uint32_t flags);
+/* The device's instance records after the last upload or update (for
+ * checks): xf[12 i ..] = world->object 3x4 of instance i; wbox[6 i ..] =
+ * its world box (min xyz, max xyz) and info = (TLAS nodes, TLAS depth,
+ * build overflow flag) of the last device-side update, which must exist
+ * when wbox or info is asked for.  Any pointer may be NULL.  Returns the
+ * number of instances copied (<= cap).  Synchronises. */
+int rendgpu_get_instances(struct rdata *rd, float *xf, float *wbox,
+                          uint32_t cap, uint32_t info[3]);
+
+/* 8-bit resolve of the frame image (rd->buf through rendgpu_readback),
+ * done in the accumulation pass of every later frame.  The reference packs
+ * 255 * acc / samples per channel and lets values above 1 wrap
+ * (accum_pckt, rend.c:3574-3577); that stays the default.  The tonemapped
+ * forms (no counterpart in the reference) scale by `exposure`, apply
+ * Reinhard x / (1 + x) or the fitted ACES curve of Narkowicz (2015), then
+ * the sRGB transfer function, and round to the nearest 8-bit value. */
+enum rendgpu_resolve_op {
+	RENDGPU_RESOLVE_WRAP = 0,     /* the reference's wrapping pack */
+	RENDGPU_RESOLVE_REINHARD = 1,
+	RENDGPU_RESOLVE_ACES = 2
+};
+int rendgpu_set_resolve(struct rdata *rd, uint32_t op, float exposure);
+
 /* Ray capture for parity checks (no counterpart in the reference, whose
  * rays never leave the CPU; it lets a test re-trace the very rays a GPU frame
  * traced with intersect_tlas / intersect_any_tlas, rend.c:1976/2883).  With
@@ -388,6 +440,9 @@ int rendgpu_batch_autotune(struct rendgpu_batch *b, uint32_t frames,
                            struct rendgpu_tune *log, uint32_t cap,
                            uint32_t *nlog);
 int rendgpu_batch_get_stream(struct rendgpu_batch *b, void **stream);
+/* rendgpu_set_resolve for every scene of the batch. */
+int rendgpu_batch_set_resolve(struct rendgpu_batch *b, uint32_t op,
+                              float exposure);
 int         rendgpu_batch_last_error(struct rendgpu_batch *b);
 const char *rendgpu_batch_strerror(struct rendgpu_batch *b);
 

@@ -10,6 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SCENE_SMALL, SCENE_SCALE, SCENE_BATCH, SCENE_STRESS, SCENE_TINY = 1, 2, 3, 5, 9
 SCENE_GLOSSY = 6
 MODE_PATH, MODE_PRIMARY, MODE_NRC = 0, 1, 2
+RESOLVE_WRAP, RESOLVE_REINHARD, RESOLVE_ACES = 0, 1, 2
 FLAG_TIMING, FLAG_COUNT, FLAG_GRAPH = 1, 2, 4
 
 # struct rendgpu_ray / rendgpu_hit (32 / 16 bytes)
@@ -169,6 +170,11 @@ class GpuLib:
                 ("rendgpu_sync", [vp]), ("rendgpu_get_stats", [vp, vp]),
                 ("rendgpu_get_lights", [vp, vp, u32, vp]),
                 ("rendgpu_capture", [vp, u32, u32]),
+                ("rendgpu_update_instances_device", [vp, vp, u32, u32]),
+                ("rendgpu_update_instances", [vp, vp, u32, u32]),
+                ("rendgpu_get_instances", [vp, vp, vp, u32, vp]),
+                ("rendgpu_set_resolve", [vp, u32, C.c_float]),
+                ("rendgpu_batch_set_resolve", [vp, u32, C.c_float]),
                 ("rendgpu_captured", [vp, u32, vp, vp, vp, vp]),
                 ("rendgpu_get_stream", [vp, vp]),
                 ("rendgpu_set_tune", [vp, vp]),
@@ -244,6 +250,14 @@ class Scene:
     def inst_tris(self):
         return self.h.nbh_scene_insttris(self.ptr)
 
+    def globs(self):
+        """Writable (instances, 16) view of every instance's row-major
+        object->world matrix (nbh_inst.glob)."""
+        n = self.s.instcnt
+        raw = (C.c_ubyte * (72 * n)).from_address(self.s.insts)
+        return np.ctypeslib.as_array(raw).view(np.float32).reshape(n, 18)[
+            :, 2:]
+
     def settings(self):
         s = self.s
         return dict(width=s.width, height=s.height, spp=s.spp, depth=s.depth)
@@ -290,6 +304,28 @@ class RenderData:
         camp = C.addressof(self.scene.s) + SceneStruct.cam.offset
         self.h.nbh_upd_rcam(self.ptr, camp, float(w), float(h))
         self.attach_buf()
+
+    def update_host(self):
+        """The reference frame loop's host update after a transform change
+        (main.c:257-264): upd_rinsts, then the TLAS build (prepdynamic)."""
+        rc = self.h.nbh_upd_rinsts(self.ptr, self.scene.ptr)
+        if rc != 0:
+            raise RuntimeError("nbh_upd_rinsts: singular transform")
+        self.h.nbh_prepdynamic(self.ptr)
+
+    def globinv(self):
+        """(instances, 12) world->object 3x4 of rd->insts."""
+        n = self.rd.instcnt
+        raw = (C.c_ubyte * (64 * n)).from_address(self.rd.insts)
+        return np.ctypeslib.as_array(raw).view(np.float32).reshape(n, 16)[
+            :, :12].copy()
+
+    def aabbs(self):
+        """(instances, 6) world boxes of rd->aabbs (min xyz, max xyz)."""
+        n = self.rd.instcnt
+        raw = (C.c_ubyte * (32 * n)).from_address(self.rd.aabbs)
+        a = np.ctypeslib.as_array(raw).view(np.float32).reshape(n, 8)
+        return np.concatenate([a[:, 0:3], a[:, 4:7]], axis=1).copy()
 
     def attach_buf(self):
         n = self.rd.width * self.rd.height
@@ -470,6 +506,42 @@ class GpuRenderer:
         out = np.zeros((max(n, 1), 20), np.float32)
         self.g.rendgpu_get_lights(self.ptr, out.ctypes.data, n, C.byref(area))
         return out[:n], area.value
+
+    def set_resolve(self, op=0, exposure=1.0):
+        """8-bit resolve: 0 the reference's wrapping pack, 1 Reinhard,
+        2 ACES (with exposure and the sRGB transfer function)."""
+        self._ck(self.g.rendgpu_set_resolve(self.ptr, op, exposure),
+                 "set_resolve")
+
+    def update_instances(self, globs, refit=False):
+        """Device-side scene update from (instances, 16) object->world
+        matrices (host array: copied; else an integer device pointer)."""
+        n = self.rdata.rd.instcnt
+        flags = 1 if refit else 0
+        if isinstance(globs, int):
+            self._ck(self.g.rendgpu_update_instances_device(self.ptr, globs,
+                                                            n, flags),
+                     "update_instances_device")
+        else:
+            g = np.ascontiguousarray(globs, np.float32)
+            assert g.shape == (n, 16)
+            self._ck(self.g.rendgpu_update_instances(self.ptr,
+                                                     g.ctypes.data, n, flags),
+                     "update_instances")
+
+    def instances(self, boxes=True):
+        """(world->object 3x4 (n, 12), world boxes (n, 6) or None, TLAS
+        info (nodes, depth, overflow) or None) held by the device."""
+        n = self.rdata.rd.instcnt
+        xf = np.zeros((n, 12), np.float32)
+        wb = np.zeros((n, 6), np.float32) if boxes else None
+        info = (C.c_uint32 * 3)()
+        rc = self.g.rendgpu_get_instances(
+            self.ptr, xf.ctypes.data, wb.ctypes.data if boxes else None, n,
+            info if boxes else None)
+        if rc < 0:
+            self._ck(rc, "get_instances")
+        return xf, wb, (tuple(info) if boxes else None)
 
     def capture(self, bounces, cap):
         """Record, in every later frame, up to `cap` closest-hit rays (with

@@ -60,7 +60,8 @@ def build_gpu(force=False):
     cpp = os.path.join(CSRC, "layout.cpp")
     deps = [cu, cpp] + [os.path.join(CSRC, f) for f in
                         ("trace.cuh", "kernels.cuh", "nrc.cuh", "gpulayout.h",
-                         "layout.hpp", os.path.join("host", "nb_rdata.h"))]
+                         "layout.hpp", "qnode.h", "tlas_build.cuh",
+                         os.path.join("host", "nb_rdata.h"))]
     deps.append(os.path.join(ROOT, "include", "rendgpu.h"))
     if not force and _newer(out, deps):
         return out

@@ -954,7 +954,30 @@ __global__ void __launch_bounds__(256) k_relmse(const float *acc, float inv,
 	}
 }
 
-// acc += sum over the pixel's samples; ARGB8 resolve (rend.c:3565-3580).
+// Tonemapped 8-bit channel of a linear radiance value x (exposure applied):
+// op 1 = Reinhard x / (1 + x), op 2 = the fitted ACES curve of Narkowicz
+// (2015), x (2.51 x + 0.03) / (x (2.43 x + 0.59) + 0.14) clamped to [0, 1];
+// then the sRGB transfer function (IEC 61966-2-1) and rounding to the
+// nearest of 0..255.  Negative and NaN inputs give 0.
+__device__ __forceinline__ uint32_t tonemap8(float x, uint32_t op)
+{
+	float v = x > 0.0f ? x : 0.0f;
+	if (op == 1u) {
+		v = __fdiv_rn(v, __fadd_rn(1.0f, v));
+	} else {
+		float num = __fmul_rn(v, __fadd_rn(__fmul_rn(2.51f, v), 0.03f));
+		float den = __fadd_rn(__fmul_rn(v, __fadd_rn(__fmul_rn(2.43f, v),
+		  0.59f)), 0.14f);
+		v = fminf(__fdiv_rn(num, den), 1.0f);
+	}
+	float s = v <= 0.0031308f ? __fmul_rn(12.92f, v) :
+	  __fsub_rn(__fmul_rn(1.055f, powf(v, 1.0f / 2.4f)), 0.055f);
+	int q = __float2int_rn(__fmul_rn(s, 255.0f));
+	return (uint32_t)min(max(q, 0), 255);
+}
+
+// acc += sum over the pixel's samples; ARGB8 resolve (rend.c:3565-3580), or
+// a tonemapped resolve (rendgpu_set_resolve).
 // Pixels of all scenes: acc and buf hold the scenes' images back to back.
 __global__ void __launch_bounds__(256) k_accum(DScene S, FrameDev F)
 {
@@ -980,9 +1003,19 @@ __global__ void __launch_bounds__(256) k_accum(DScene S, FrameDev F)
 		F.acc[3u * p] = ax;
 		F.acc[3u * p + 1u] = ay;
 		F.acc[3u * p + 2u] = az;
-		uint32_t cx = (uint32_t)__fmul_rn(255.0f, __fmul_rn(ax, inv));
-		uint32_t cy = (uint32_t)__fmul_rn(255.0f, __fmul_rn(ay, inv));
-		uint32_t cz = (uint32_t)__fmul_rn(255.0f, __fmul_rn(az, inv));
+		uint32_t op = __ldg(&P->resolve);
+		uint32_t cx, cy, cz;
+		if (op == 0u) {
+			// the reference's pack: wraps instead of clamping
+			cx = (uint32_t)__fmul_rn(255.0f, __fmul_rn(ax, inv));
+			cy = (uint32_t)__fmul_rn(255.0f, __fmul_rn(ay, inv));
+			cz = (uint32_t)__fmul_rn(255.0f, __fmul_rn(az, inv));
+		} else {
+			float e = __fmul_rn(inv, __ldg(&P->exposure));
+			cx = tonemap8(__fmul_rn(ax, e), op);
+			cy = tonemap8(__fmul_rn(ay, e), op);
+			cz = tonemap8(__fmul_rn(az, e), op);
+		}
 		F.buf[p] = 0xff000000u | (cx & 0xffu) << 16 | (cy & 0xffu) << 8 |
 		  (cz & 0xffu);
 	}

@@ -9,6 +9,7 @@
 // only the encoding changes.
 
 #include "layout.hpp"
+#include "qnode.h"
 
 #include <cfloat>
 #include <cmath>
@@ -31,113 +32,12 @@ bool empty_child(const nb_bnode8 *n, int j)
 	  !(n->minz8[j] <= n->maxz8[j]);
 }
 
-// Greedy assignment of children to slots: slot s prefers children lying
-// towards (+/-x, +/-y, +/-z) by its bits, so that ascending slot ^ octant is
-// roughly near-to-far for rays of that octant.
-void assign_slots(int nchild, const float cen[8][3], const float nc[3],
-                  int slot_of[8])
-{
-	bool used_c[8] = {false}, used_s[8] = {false};
-	for (int i = 0; i < 8; i++)
-		slot_of[i] = -1;
-	for (int round = 0; round < nchild; round++) {
-		float best = -FLT_MAX;
-		int bc = -1, bs = -1;
-		for (int c = 0; c < nchild; c++) {
-			if (used_c[c])
-				continue;
-			for (int s = 0; s < 8; s++) {
-				if (used_s[s])
-					continue;
-				float sc = 0.0f;
-				for (int a = 0; a < 3; a++)
-					sc += (cen[c][a] - nc[a]) *
-					  ((s >> a) & 1 ? 1.0f : -1.0f);
-				if (sc > best) {
-					best = sc;
-					bc = c;
-					bs = s;
-				}
-			}
-		}
-		used_c[bc] = used_s[bs] = true;
-		slot_of[bc] = bs;
-	}
-}
-
-double pow2(int e) { return std::ldexp(1.0, e); }
-
 } // namespace
 
 void quantise_node(const float cmin[8][3], const float cmax[8][3],
                    nb_qnode *n)
 {
-	float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
-	float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-	bool any = false;
-	for (int s = 0; s < 8; s++) {
-		if (!(cmin[s][0] <= cmax[s][0] && cmin[s][1] <= cmax[s][1] &&
-		  cmin[s][2] <= cmax[s][2]))
-			continue;
-		any = true;
-		for (int a = 0; a < 3; a++) {
-			lo[a] = std::fmin(lo[a], cmin[s][a]);
-			hi[a] = std::fmax(hi[a], cmax[s][a]);
-		}
-	}
-	if (!any)
-		for (int a = 0; a < 3; a++)
-			lo[a] = hi[a] = 0.0f;
-	float p[3];
-	int ex[3];
-	for (int a = 0; a < 3; a++) {
-		double ext = (double)hi[a] - lo[a];
-		double floor_scale = std::fmax(std::fabs((double)lo[a]),
-		  std::fabs((double)hi[a])) * std::ldexp(1.0, -22);
-		double need = std::fmax(std::fmax(ext / 249.0, floor_scale),
-		  std::ldexp(1.0, -100));
-		int e = (int)std::ceil(std::log2(need));
-		for (;; e++) {
-			double sc = pow2(e);
-			// origin two quanta below lo, rounded down to a float
-			double want = (double)lo[a] - 2.0 * sc;
-			float pf = (float)want;
-			if ((double)pf > want)
-				pf = std::nextafter(pf, -FLT_MAX);
-			double top = ((double)hi[a] - pf) / sc;
-			if (top + 2.0 <= 255.0 && e + 127 >= 1 && e + 127 <= 254) {
-				p[a] = pf;
-				ex[a] = e;
-				break;
-			}
-		}
-	}
-	n->px = p[0];
-	n->py = p[1];
-	n->pz = p[2];
-	n->ex = (uint8_t)(ex[0] + 127);
-	n->ey = (uint8_t)(ex[1] + 127);
-	n->ez = (uint8_t)(ex[2] + 127);
-	uint8_t *qlo[3] = {n->qlox, n->qloy, n->qloz};
-	uint8_t *qhi[3] = {n->qhix, n->qhiy, n->qhiz};
-	for (int s = 0; s < 8; s++) {
-		bool valid = cmin[s][0] <= cmax[s][0] &&
-		  cmin[s][1] <= cmax[s][1] && cmin[s][2] <= cmax[s][2];
-		for (int a = 0; a < 3; a++) {
-			if (!valid) {
-				qlo[a][s] = 255;
-				qhi[a][s] = 0;
-				continue;
-			}
-			double sc = pow2(ex[a]);
-			double l = std::floor(((double)cmin[s][a] - p[a]) / sc) - 1.0;
-			double h = std::ceil(((double)cmax[s][a] - p[a]) / sc) + 1.0;
-			l = std::fmax(l, 0.0);
-			h = std::fmin(h, 255.0);
-			qlo[a][s] = (uint8_t)l;
-			qhi[a][s] = (uint8_t)h;
-		}
-	}
+	quantise_node_hd(cmin, cmax, n);
 }
 
 namespace {

@@ -1,0 +1,153 @@
+// Encoding of one 8-wide node in the GPU layout (gpulayout.h), shared by the
+// host conversion of the reference BVH8 (layout.cpp) and the device TLAS
+// build (tlas_build.cuh), so both produce the same bytes for the same child
+// boxes: the greedy slot assignment and the conservative 8-bit quantisation.
+// Every operation is an IEEE-754 operation with one rounding, with no fused
+// multiply-add (the host file is built without FMA, the device file with
+// -fmad=false), so host and device results are identical.
+
+#ifndef NB_QNODE_H
+#define NB_QNODE_H
+
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "gpulayout.h"
+
+#ifdef __CUDACC__
+#define NB_HD __host__ __device__
+#else
+#define NB_HD
+#endif
+
+namespace nb {
+
+// ceil(log2(x)) for a finite x > 0, exactly (frexp is exact: x = m 2^k with
+// m in [0.5, 1); x is a power of two iff m = 0.5).
+NB_HD inline int ceil_log2(double x)
+{
+	int k = 0;
+	double m = frexp(x, &k);
+	return m == 0.5 ? k - 1 : k;
+}
+
+// Greedy assignment of children to slots: slot s prefers children lying
+// towards (+/-x, +/-y, +/-z) by its bits, so that ascending slot ^ octant is
+// roughly near-to-far for rays of that octant (after Ylitie, Karras and
+// Laine 2017).  cen: child box centres, nc: node box centre.
+NB_HD inline void assign_slots(int nchild, const float cen[8][3],
+                               const float nc[3], int slot_of[8])
+{
+	bool used_c[8] = {false, false, false, false, false, false, false,
+	  false};
+	bool used_s[8] = {false, false, false, false, false, false, false,
+	  false};
+	for (int i = 0; i < 8; i++)
+		slot_of[i] = -1;
+	for (int round = 0; round < nchild; round++) {
+		float best = -FLT_MAX;
+		int bc = -1, bs = -1;
+		for (int c = 0; c < nchild; c++) {
+			if (used_c[c])
+				continue;
+			for (int s = 0; s < 8; s++) {
+				if (used_s[s])
+					continue;
+				float sc = 0.0f;
+				for (int a = 0; a < 3; a++)
+					sc += (cen[c][a] - nc[a]) *
+					  ((s >> a) & 1 ? 1.0f : -1.0f);
+				if (sc > best) {
+					best = sc;
+					bc = c;
+					bs = s;
+				}
+			}
+		}
+		used_c[bc] = used_s[bs] = true;
+		slot_of[bc] = bs;
+	}
+}
+
+// Quantise one node: child boxes (min/max per slot; empty slots have
+// min > max) into n's origin, exponents and qlo/qhi.  Per axis the scale is
+// the smallest power of two 2^e with the node box spanning at most 249
+// quanta (and at least 2^-22 of the coordinates' magnitude); the origin
+// lies two quanta below the box, rounded down to a float; child planes are
+// rounded outwards and padded by one more quantum.  Other fields of n are
+// left as they are.
+NB_HD inline void quantise_node_hd(const float cmin[8][3],
+                                   const float cmax[8][3], nb_qnode *n)
+{
+	float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+	float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+	bool any = false;
+	for (int s = 0; s < 8; s++) {
+		if (!(cmin[s][0] <= cmax[s][0] && cmin[s][1] <= cmax[s][1] &&
+		  cmin[s][2] <= cmax[s][2]))
+			continue;
+		any = true;
+		for (int a = 0; a < 3; a++) {
+			lo[a] = fminf(lo[a], cmin[s][a]);
+			hi[a] = fmaxf(hi[a], cmax[s][a]);
+		}
+	}
+	if (!any)
+		for (int a = 0; a < 3; a++)
+			lo[a] = hi[a] = 0.0f;
+	float p[3];
+	int ex[3];
+	for (int a = 0; a < 3; a++) {
+		double ext = (double)hi[a] - lo[a];
+		double floor_scale = fmax(fabs((double)lo[a]),
+		  fabs((double)hi[a])) * ldexp(1.0, -22);
+		double need = fmax(fmax(ext / 249.0, floor_scale), ldexp(1.0, -100));
+		int e = ceil_log2(need);
+		for (;; e++) {
+			double sc = ldexp(1.0, e);
+			// origin two quanta below lo, rounded down to a float
+			double want = (double)lo[a] - 2.0 * sc;
+			float pf = (float)want;
+			if ((double)pf > want)
+				pf = nextafterf(pf, -FLT_MAX);
+			double top = ((double)hi[a] - pf) / sc;
+			if (top + 2.0 <= 255.0 && e + 127 >= 1 && e + 127 <= 254) {
+				p[a] = pf;
+				ex[a] = e;
+				break;
+			}
+		}
+	}
+	n->px = p[0];
+	n->py = p[1];
+	n->pz = p[2];
+	n->ex = (uint8_t)(ex[0] + 127);
+	n->ey = (uint8_t)(ex[1] + 127);
+	n->ez = (uint8_t)(ex[2] + 127);
+	uint8_t *qlo[3] = {n->qlox, n->qloy, n->qloz};
+	uint8_t *qhi[3] = {n->qhix, n->qhiy, n->qhiz};
+	for (int s = 0; s < 8; s++) {
+		bool valid = cmin[s][0] <= cmax[s][0] &&
+		  cmin[s][1] <= cmax[s][1] && cmin[s][2] <= cmax[s][2];
+		for (int a = 0; a < 3; a++) {
+			if (!valid) {
+				qlo[a][s] = 255;
+				qhi[a][s] = 0;
+				continue;
+			}
+			double sc = ldexp(1.0, ex[a]);
+			double l = floor(((double)cmin[s][a] - p[a]) / sc) - 1.0;
+			double h = ceil(((double)cmax[s][a] - p[a]) / sc) + 1.0;
+			l = fmax(l, 0.0);
+			h = fmin(h, 255.0);
+			qlo[a][s] = (uint8_t)l;
+			qhi[a][s] = (uint8_t)h;
+		}
+	}
+}
+
+} // namespace nb
+
+#endif

@@ -25,6 +25,7 @@
 #include "kernels.cuh"
 #include "layout.hpp"
 #include "nrc.cuh"
+#include "tlas_build.cuh"
 
 namespace nb {
 namespace {
@@ -85,6 +86,9 @@ struct SceneHost {
 	// frame layout (rendgpu_resaccum)
 	uint32_t W = 0, H = 0, spp = 0;
 	uint32_t path_base = 0, pix_base = 0, slot_base = 0, nslots = 0;
+	// 8-bit resolve (rendgpu_set_resolve): 0 = the reference's pack
+	uint32_t resolve = 0;
+	float    exposure = 1.0f;
 };
 
 struct Ctx {
@@ -131,6 +135,14 @@ struct Ctx {
 	// rays, their hits, cap_n shadow rays and 4 counts
 	DevBuf   capbuf;
 	uint32_t cap_mask = 0, cap_n = 0;
+	// device-side scene update (rendgpu_update_instances*): per-instance
+	// BLAS root boxes, new matrices, world boxes, TLAS build queues, slot
+	// ranges and instance order (refit), build info, emitter sources, area
+	DevBuf   dyn_root, dyn_glob, dyn_wbox, dyn_q, dyn_ranges, dyn_order,
+	         dyn_info, dyn_emit, dyn_area;
+	uint32_t dyn_nemit = 0;
+	bool     dyn_built = false;  // a device TLAS build ran (refit possible)
+	bool     dyn_active = false; // the device holds the current instances
 	// stats / errors
 	rendgpu_stats st{};
 	int          last = 0;
@@ -812,6 +824,8 @@ int frame_params(Ctx *c, bool nrc, FrameArgs *A)
 		}
 		P.light_area = h.light_area;
 		P.inv = 1.0f / (float)(rd->samples + rd->spp);
+		P.resolve = h.resolve;
+		P.exposure = h.exposure;
 		P.bg[0] = rd->bgcol.x;
 		P.bg[1] = rd->bgcol.y;
 		P.bg[2] = rd->bgcol.z;
@@ -831,6 +845,11 @@ int frame_params(Ctx *c, bool nrc, FrameArgs *A)
 	}
 	NB_CK(c, cudaMemcpyAsync(c->sp.p, c->par.data(), n * sizeof(ScenePar),
 	  cudaMemcpyHostToDevice, c->stream));
+	if (c->dyn_active)
+		// the light area of the last device-side update
+		NB_CK(c, cudaMemcpyAsync(&c->sp.as<ScenePar>()[0].light_area,
+		  c->dyn_area.p, sizeof(float), cudaMemcpyDeviceToDevice,
+		  c->stream));
 	return 0;
 }
 
@@ -1153,7 +1172,9 @@ void free_ctx(Ctx *c)
 	  &c->mlp_dz, &c->mlp_wf,
 	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
 	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat, &c->waitchk,
-	  &c->rtgt, &c->capbuf};
+	  &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob, &c->dyn_wbox,
+	  &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info, &c->dyn_emit,
+	  &c->dyn_area};
 	for (DevBuf *b : bufs)
 		b->release();
 	for (int i = 0; i < kMaxEvents; i++)
@@ -1174,7 +1195,9 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->mlp_act, &c->mlp_dz,
 	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
 	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec, &c->waitchk,
-	  &c->rfeat, &c->rtgt, &c->capbuf};
+	  &c->rfeat, &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob,
+	  &c->dyn_wbox, &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info,
+	  &c->dyn_emit, &c->dyn_area};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
 		s += b->cap;
@@ -1328,6 +1351,157 @@ int upload_static_all(Ctx *c)
 	return 0;
 }
 
+// Inputs of device-side scene updates that an upload fixes (single-scene
+// contexts): each instance's BLAS root box as the host bridge forms it (the
+// union of the root's child boxes, main.c:133-140), the emitting triangles
+// in light-table order, and scratch of the TLAS build.
+int dyn_prepare(Ctx *c, uint64_t *bytes)
+{
+	SceneHost &h = c->sc[0];
+	const nb_rdata *rd = h.rd;
+	uint32_t n = rd->instcnt;
+	std::vector<float4> rb(2 * (size_t)n);
+	for (uint32_t i = 0; i < n; i++) {
+		const nb_bnode8 *b = &rd->bnodes[(size_t)rd->insts[i].triofs << 1];
+		float mi[3] = {b->minx8[0], b->miny8[0], b->minz8[0]};
+		float ma[3] = {b->maxx8[0], b->maxy8[0], b->maxz8[0]};
+		for (int k = 1; k < 8; k++) {
+			mi[0] = b->minx8[k] < mi[0] ? b->minx8[k] : mi[0];
+			mi[1] = b->miny8[k] < mi[1] ? b->miny8[k] : mi[1];
+			mi[2] = b->minz8[k] < mi[2] ? b->minz8[k] : mi[2];
+			ma[0] = b->maxx8[k] > ma[0] ? b->maxx8[k] : ma[0];
+			ma[1] = b->maxy8[k] > ma[1] ? b->maxy8[k] : ma[1];
+			ma[2] = b->maxz8[k] > ma[2] ? b->maxz8[k] : ma[2];
+		}
+		rb[2 * i] = make_float4(mi[0], mi[1], mi[2], 0.0f);
+		rb[2 * i + 1] = make_float4(ma[0], ma[1], ma[2], 0.0f);
+	}
+	std::vector<EmitSrc> es;
+	for (uint32_t i = 0; i < n; i++) {
+		const nb_rinst &ri = rd->insts[i];
+		auto it = h.emitters.find(ri.triofs);
+		if (it == h.emitters.end())
+			continue;
+		for (uint32_t t : it->second) {
+			const nb_rnrm *rn = &rd->nrms[ri.triofs + t];
+			const nb_rmtl *m = &rd->mtls[rn->mtlid];
+			if (!(m->flags & NB_FLAG_EMISSIVE))
+				continue;
+			const nb_rtri *tr = &rd->tris[ri.triofs + t];
+			EmitSrc e;
+			std::memset(&e, 0, sizeof(e));
+			e.inst = i;
+			const nb_vec3 *vv[3] = {&tr->v0, &tr->v1, &tr->v2};
+			const nb_vec3 *nn[3] = {&rn->n0, &rn->n1, &rn->n2};
+			for (int k = 0; k < 3; k++) {
+				e.v[k][0] = vv[k]->x;
+				e.v[k][1] = vv[k]->y;
+				e.v[k][2] = vv[k]->z;
+				e.n[k][0] = nn[k]->x;
+				e.n[k][1] = nn[k]->y;
+				e.n[k][2] = nn[k]->z;
+			}
+			e.emit[0] = m->col.x;
+			e.emit[1] = m->col.y;
+			e.emit[2] = m->col.z;
+			es.push_back(e);
+		}
+	}
+	// a degenerate emitter the host table skipped: device updates (which
+	// keep every entry) are then refused
+	c->dyn_nemit = es.size() == h.lights.size() ? (uint32_t)es.size() :
+	  0xffffffffu;
+	size_t nn = std::max(n, 1u);
+	NB_CK(c, c->dyn_root.ensure(nn * 32));
+	NB_CK(c, c->dyn_glob.ensure(nn * 64));
+	NB_CK(c, c->dyn_wbox.ensure(nn * 32));
+	NB_CK(c, c->dyn_q.ensure(2 * nn * sizeof(TbNode)));
+	NB_CK(c, c->dyn_ranges.ensure(nn * 8 * sizeof(uint2)));
+	NB_CK(c, c->dyn_order.ensure(nn * sizeof(uint32_t)));
+	NB_CK(c, c->dyn_info.ensure(4 * sizeof(uint32_t)));
+	NB_CK(c, c->dyn_emit.ensure(std::max<size_t>(es.size(), 1) *
+	  sizeof(EmitSrc)));
+	NB_CK(c, c->dyn_area.ensure(16));
+	NB_CK(c, cudaMemcpyAsync(c->dyn_root.p, rb.data(), rb.size() *
+	  sizeof(float4), cudaMemcpyHostToDevice, c->stream));
+	if (!es.empty())
+		NB_CK(c, cudaMemcpyAsync(c->dyn_emit.p, es.data(), es.size() *
+		  sizeof(EmitSrc), cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->dyn_info.p, 0, 4 * sizeof(uint32_t),
+	  c->stream));
+	// (pageable sources: the copies have read them when they return)
+	*bytes = rb.size() * sizeof(float4) + es.size() * sizeof(EmitSrc);
+	c->dyn_built = false;
+	c->dyn_active = false;
+	return 0;
+}
+
+// New object->world matrices (device, 16 floats each, rd->insts order) ->
+// instance records, world boxes, TLAS (built, or refitted when asked and a
+// device build exists) and light table, all on the context's stream.
+int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
+{
+	int rc = ready(c, false);
+	if (rc)
+		return rc;
+	if (c->batch)
+		return fail(c, RENDGPU_EINVAL, "device-side scene updates serve "
+		  "single-scene contexts");
+	SceneHost &h = c->sc[0];
+	if (n != h.rd->instcnt)
+		return fail(c, RENDGPU_EINVAL, "update: n must equal rd->instcnt");
+	if (!glob || (reinterpret_cast<uintptr_t>(glob) & 3u))
+		return fail(c, RENDGPU_EINVAL, "update: null or misaligned matrices");
+	if (c->dyn_nemit == 0xffffffffu)
+		return fail(c, RENDGPU_ESTATE, "update: the uploaded light table "
+		  "skipped a degenerate emitter; upload non-degenerate transforms "
+		  "first");
+	if (flags & ~(uint32_t)RENDGPU_UPDATE_REFIT)
+		return fail(c, RENDGPU_EINVAL, "update: unknown flags");
+	NB_CK(c, cudaSetDevice(c->device));
+	bool refit = (flags & RENDGPU_UPDATE_REFIT) && c->dyn_built;
+	uint32_t nn = std::max(n, 1u);
+	k_inst_update<<<(n + 127u) / 128u, 128, 0, c->stream>>>(glob, n,
+	  c->dyn_root.as<float4>(), c->insts.as<float4>(),
+	  c->dyn_wbox.as<float4>(), c->berr.as<uint32_t>() + 1);
+	NB_CK(c, cudaGetLastError());
+	if (!refit) {
+		TbArgs A;
+		A.wbox = c->dyn_wbox.as<float4>();
+		A.n = n;
+		A.inst_base = 0u;
+		A.nodes = c->tlas.as<nb_qnode>();
+		A.node_cap = nn;
+		A.irefs = c->irefs.as<uint32_t>();
+		A.qa = c->dyn_q.as<TbNode>();
+		A.qb = c->dyn_q.as<TbNode>() + nn;
+		A.ranges = c->dyn_ranges.as<uint2>();
+		A.order = c->dyn_order.as<uint32_t>();
+		A.info = c->dyn_info.as<uint32_t>();
+		// the host-converted TLAS sized the traversal stack; the device
+		// tree stays within its depth (at least a balanced tree's)
+		A.depth_limit = h.tlas_depth;
+		k_tlas_build<<<1, kTbWarps * 32, 0, c->stream>>>(A);
+	} else {
+		k_tlas_refit<<<grid_for(c, nn * 32u, 256), 256, 0, c->stream>>>(
+		  c->dyn_wbox.as<float4>(), c->dyn_order.as<uint32_t>(),
+		  c->dyn_ranges.as<uint2>(), c->dyn_info.as<uint32_t>(),
+		  c->tlas.as<nb_qnode>());
+	}
+	NB_CK(c, cudaGetLastError());
+	if (c->dyn_nemit) {
+		k_light_update<<<1, 32, 0, c->stream>>>(c->dyn_emit.as<EmitSrc>(),
+		  c->dyn_nemit, c->insts.as<float4>(),
+		  c->lights.as<float4>() + 5u * h.light_off, c->dyn_area.as<float>());
+		NB_CK(c, cudaGetLastError());
+	}
+	h.tlas_root = 0u;
+	c->dyn_built = true;
+	c->dyn_active = true;
+	c->st.h2d_bytes = 0;
+	return 0;
+}
+
 // TLAS, instances and lights of every scene (rend_prepdynamic output).
 // Instance references are global, so hit ids carry the instance's index
 // among all scenes' instances (at most 4096 in total).
@@ -1393,7 +1567,12 @@ int upload_dynamic_all(Ctx *c)
 		}
 	}
 	c->ninst = (uint32_t)gi.size();
-	NB_CK(c, c->tlas.ensure(nodes.size() * sizeof(nb_qnode)));
+	// device-side updates (single-scene contexts) rebuild the TLAS in place:
+	// room for max(instances, 1) nodes
+	size_t tlas_nodes = nodes.size();
+	if (!c->batch)
+		tlas_nodes = std::max(tlas_nodes, (size_t)std::max(c->ninst, 1u));
+	NB_CK(c, c->tlas.ensure(tlas_nodes * sizeof(nb_qnode)));
 	NB_CK(c, c->irefs.ensure(irefs.size() * sizeof(uint32_t)));
 	NB_CK(c, c->insts.ensure(gi.size() * sizeof(nb_ginst)));
 	NB_CK(c, c->lights.ensure(lights.size() * sizeof(nb_glight)));
@@ -1408,10 +1587,16 @@ int upload_dynamic_all(Ctx *c)
 		NB_CK(c, cudaMemcpyAsync(c->lights.p, lights.data(),
 		  lights.size() * sizeof(nb_glight), cudaMemcpyHostToDevice,
 		  c->stream));
+	uint64_t dyn_bytes = 0;
+	if (!c->batch) {
+		int rc = dyn_prepare(c, &dyn_bytes);
+		if (rc)
+			return rc;
+	}
 	NB_CK(c, cudaStreamSynchronize(c->stream));
 	c->st.h2d_bytes = nodes.size() * sizeof(nb_qnode) + irefs.size() *
 	  sizeof(uint32_t) + gi.size() * sizeof(nb_ginst) +
-	  lights.size() * sizeof(nb_glight);
+	  lights.size() * sizeof(nb_glight) + dyn_bytes;
 	drop_graph(c);
 	c->have_dynamic = true;
 	if (!stack_of(c))
@@ -2203,6 +2388,22 @@ int rendgpu_get_lights(struct rdata *rdp, float *out, uint32_t cap,
 		return fail(c, RENDGPU_ESTATE, "upload_dynamic must come first");
 	const SceneHost &h = c->sc[0];
 	uint32_t n = (uint32_t)h.lights.size();
+	if (c->dyn_active) {
+		// the table of the last device-side update
+		NB_CK(c, cudaSetDevice(c->device));
+		uint32_t m = out ? std::min(n, cap) : 0u;
+		if (m)
+			NB_CK(c, cudaMemcpyAsync(out, c->lights.as<nb_glight>() +
+			  h.light_off, (size_t)m * sizeof(nb_glight),
+			  cudaMemcpyDeviceToHost, c->stream));
+		float area = 0.0f;
+		NB_CK(c, cudaMemcpyAsync(&area, c->dyn_area.p, sizeof(float),
+		  cudaMemcpyDeviceToHost, c->stream));
+		NB_CK(c, cudaStreamSynchronize(c->stream));
+		if (total_area)
+			*total_area = area;
+		return (int)n;
+	}
 	if (out) {
 		uint32_t m = n < cap ? n : cap;
 		std::memcpy(out, h.lights.data(), (size_t)m *
@@ -2211,6 +2412,97 @@ int rendgpu_get_lights(struct rdata *rdp, float *out, uint32_t cap,
 	if (total_area)
 		*total_area = h.light_area;
 	return (int)n;
+}
+
+int rendgpu_update_instances_device(struct rdata *rdp,
+                                    const float *glob_device, uint32_t n,
+                                    uint32_t flags)
+{
+	return update_instances(find_ctx(rdp), glob_device, n, flags);
+}
+
+int rendgpu_update_instances(struct rdata *rdp, const float *glob,
+                             uint32_t n, uint32_t flags)
+{
+	Ctx *c = find_ctx(rdp);
+	int rc = ready(c, false);
+	if (rc)
+		return rc;
+	if (!glob || n != c->sc[0].rd->instcnt || c->batch)
+		return fail(c, RENDGPU_EINVAL, "update: n must equal rd->instcnt "
+		  "of a single-scene context");
+	NB_CK(c, cudaSetDevice(c->device));
+	NB_CK(c, cudaMemcpyAsync(c->dyn_glob.p, glob, (size_t)n * 64,
+	  cudaMemcpyHostToDevice, c->stream));
+	rc = update_instances(c, c->dyn_glob.as<float>(), n, flags);
+	c->st.h2d_bytes = (uint64_t)n * 64;
+	return rc;
+}
+
+int rendgpu_get_instances(struct rdata *rdp, float *xf, float *wbox,
+                          uint32_t cap, uint32_t info[3])
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->have_dynamic || c->batch)
+		return fail(c, RENDGPU_ESTATE, "upload_dynamic of a single-scene "
+		  "context must come first");
+	if ((wbox || info) && !c->dyn_active)
+		return fail(c, RENDGPU_ESTATE, "world boxes and build info exist "
+		  "after a device-side update");
+	NB_CK(c, cudaSetDevice(c->device));
+	uint32_t n = std::min(cap, c->sc[0].rd->instcnt);
+	std::vector<float4> gi(4 * (size_t)n), wb(2 * (size_t)n);
+	if (xf && n)
+		NB_CK(c, cudaMemcpyAsync(gi.data(), c->insts.p, (size_t)n * 64,
+		  cudaMemcpyDeviceToHost, c->stream));
+	if (wbox && n)
+		NB_CK(c, cudaMemcpyAsync(wb.data(), c->dyn_wbox.p, (size_t)n * 32,
+		  cudaMemcpyDeviceToHost, c->stream));
+	if (info)
+		NB_CK(c, cudaMemcpyAsync(info, c->dyn_info.p, 3 * sizeof(uint32_t),
+		  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	for (uint32_t i = 0; i < n; i++) {
+		if (xf)
+			std::memcpy(xf + 12 * (size_t)i, &gi[4 * (size_t)i], 48);
+		if (wbox) {
+			const float4 &l = wb[2 * (size_t)i], &h = wb[2 * (size_t)i + 1];
+			float v[6] = {l.x, l.y, l.z, h.x, h.y, h.z};
+			std::memcpy(wbox + 6 * (size_t)i, v, sizeof(v));
+		}
+	}
+	return (int)n;
+}
+
+static int set_resolve(Ctx *c, uint32_t op, float exposure)
+{
+	if (op > RENDGPU_RESOLVE_ACES || !(exposure > 0.0f) ||
+	    !(exposure < FLT_MAX))
+		return fail(c, RENDGPU_EINVAL, "resolve: op 0..2, exposure > 0");
+	for (SceneHost &h : c->sc) {
+		h.resolve = op;
+		h.exposure = exposure;
+	}
+	return 0;
+}
+
+int rendgpu_set_resolve(struct rdata *rdp, uint32_t op, float exposure)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	return set_resolve(c, op, exposure);
+}
+
+int rendgpu_batch_set_resolve(struct rendgpu_batch *b, uint32_t op,
+                              float exposure)
+{
+	Ctx *c = find_batch(b);
+	if (!c)
+		return RENDGPU_EINVAL;
+	return set_resolve(c, op, exposure);
 }
 
 int rendgpu_capture(struct rdata *rdp, uint32_t bounce_mask, uint32_t cap)

@@ -36,8 +36,8 @@ struct ScenePar {
 	uint32_t tlas_root, light_off, light_cnt, depth;
 	uint32_t W, H, spp, frame;             // frame: rd->samples
 	uint32_t path_base, pix_base, slot_base, nrc_stride;
-	uint32_t nrc_offset, pad0[3];
-	float    light_area, inv, pad1[2];     // inv: 1 / (samples + spp)
+	uint32_t nrc_offset, resolve, pad0[2]; // resolve: rendgpu_set_resolve op
+	float    light_area, inv, exposure, pad1; // inv: 1 / (samples + spp)
 	float    bg[3], tanfangle;
 	float    eye[3], rw;
 	float    ri[3], rh;

@@ -101,3 +101,52 @@ def test_frame_claim_and_ray_count(gpu):
     g.rendgpu_render(rd.ptr)  # same frame: no second render
     assert rd.rd.rays == rays1 and rd.rd.blknum == 2
     gr.close()
+
+
+def _tonemap_fp64(acc, samples, op, exposure):
+    """The tonemapped 8-bit resolve restated in FP64 after the FP32
+    exposure product: Reinhard (op 1) or Narkowicz's ACES fit (op 2), the
+    sRGB transfer function, round to nearest, clamp to 0..255."""
+    inv = np.float32(1.0) / np.float32(samples)
+    e = np.float32(inv * np.float32(exposure))
+    v = np.maximum((acc.astype(np.float32) * e).astype(np.float64), 0.0)
+    if op == 1:
+        v = v / (1.0 + v)
+    else:
+        v = np.minimum(v * (2.51 * v + 0.03) / (v * (2.43 * v + 0.59) + 0.14),
+                       1.0)
+    s = np.where(v <= 0.0031308, 12.92 * v, 1.055 * v ** (1 / 2.4) - 0.055)
+    return np.clip(np.rint(s * 255.0), 0, 255).astype(np.int64)
+
+
+@pytest.mark.parametrize("op", [api.RESOLVE_REINHARD, api.RESOLVE_ACES])
+def test_tonemapped_resolve(gpu, op):
+    scene = api.Scene(api.SCENE_TINY, 3)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd, max_depth=3, seed=2).upload()
+    gr.set_resolve(op, 1.5)
+    for _ in range(2):
+        gr.frame()
+    gr.readback(3)
+    acc, buf = rd.acc(), rd.buf.reshape(rd.rd.height, rd.rd.width)
+    want = _tonemap_fp64(acc, rd.rd.samples, op, 1.5)
+    got = np.stack([(buf >> 16) & 255, (buf >> 8) & 255, buf & 255],
+                   axis=2).astype(np.int64)
+    assert ((buf >> 24) == 255).all()
+    diff = np.abs(got - want)
+    # powf on the device against FP64 pow: at most one 8-bit step apart
+    assert diff.max() <= 1, diff.max()
+    assert (diff == 0).mean() > 0.99
+    assert want.max() > 128  # the image is not black
+    # back to the reference's wrapping pack (rend.c:3574-3577)
+    gr.set_resolve(api.RESOLVE_WRAP)
+    gr.frame()
+    gr.readback(3)
+    acc, buf = rd.acc(), rd.buf.reshape(rd.rd.height, rd.rd.width)
+    inv = np.float32(1.0) / np.float32(rd.rd.samples)
+    wrap = ((np.float32(255.0) * (acc * inv)).astype(np.uint32) & 255)
+    got = np.stack([(buf >> 16) & 255, (buf >> 8) & 255, buf & 255], axis=2)
+    assert np.array_equal(got, wrap)
+    with pytest.raises(api.RendgpuError):
+        gr.set_resolve(3)
+    gr.close()
