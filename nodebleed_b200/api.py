@@ -140,6 +140,8 @@ class HostLib:
         L.nbh_prepstatic.argtypes = [vp]
         L.nbh_prepdynamic.argtypes = [vp]
         L.nbh_rdata_from_scene.argtypes = [vp, vp]
+        L.nbh_scene_load_gltf.argtypes = [vp, C.c_char_p, u32]
+        L.nbh_scene_save_gltf.argtypes = [vp, C.c_char_p]
         self.L = L
 
 
@@ -224,15 +226,35 @@ def gpu_lib():
 
 
 class Scene:
-    """A seeded synthetic scene (nbh_scene_gen)."""
+    """A seeded synthetic scene (nbh_scene_gen), or one loaded from glTF
+    (Scene.load_gltf)."""
 
     def __init__(self, family, seed=1, param=0):
         self.h = host_lib().L
         self.s = SceneStruct()
+        if family is None:  # filled by load_gltf
+            self.family = self.seed = self.param = None
+            return
         rc = self.h.nbh_scene_gen(C.byref(self.s), family, seed, param)
         if rc != 0:
             raise RuntimeError(f"nbh_scene_gen({family}, {seed}) = {rc}")
         self.family, self.seed, self.param = family, seed, param
+
+    @classmethod
+    def load_gltf(cls, path, extras=True):
+        """nbh_scene_load_gltf; extras=False reads the file as nodebleed's
+        importer would (no exact-transform extras)."""
+        sc = cls(None)
+        rc = sc.h.nbh_scene_load_gltf(C.byref(sc.s), os.fsencode(path),
+                                      0 if extras else 1)
+        if rc != 0:
+            raise RuntimeError(f"nbh_scene_load_gltf({path}) = {rc}")
+        return sc
+
+    def save_gltf(self, path):
+        rc = self.h.nbh_scene_save_gltf(self.ptr, os.fsencode(path))
+        if rc != 0:
+            raise RuntimeError(f"nbh_scene_save_gltf({path}) = {rc}")
 
     @property
     def ptr(self):

@@ -39,8 +39,9 @@ def build_host(force=False):
     out = os.path.join(HERE, "libnbhost.so")
     scene = os.path.join(CSRC, "host", "scene.c")
     bvh = os.path.join(CSRC, "host", "bvh8.c")
+    gltf = os.path.join(CSRC, "host", "nb_gltf.c")
     hdrs = [os.path.join(CSRC, "host", h) for h in ("nb_host.h", "nb_rdata.h")]
-    if not force and _newer(out, [scene, bvh] + hdrs):
+    if not force and _newer(out, [scene, bvh, gltf] + hdrs):
         return out
     tmp = os.path.join(HERE, "_build")
     os.makedirs(tmp, exist_ok=True)
@@ -50,7 +51,10 @@ def build_host(force=False):
           "-c", scene, "-o", o1])
     _run(["gcc", "-std=gnu11", "-O3", "-mavx2", "-mfma", "-ffast-math",
           "-fPIC", "-Wall", "-Wextra", "-c", bvh, "-o", o2])
-    _run(["gcc", "-shared", "-o", out, o1, o2, "-lm"])
+    o3 = os.path.join(tmp, "nb_gltf.o")
+    _run(["gcc", "-std=gnu11", "-O2", "-fPIC", "-Wall", "-Wextra",
+          "-c", gltf, "-o", o3])
+    _run(["gcc", "-shared", "-o", out, o1, o2, o3, "-lm"])
     return out
 
 

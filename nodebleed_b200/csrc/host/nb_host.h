@@ -21,8 +21,10 @@ extern "C" {
 
 // ---------------------------------------------------------------- scenes --
 
-// One triangle mesh with a single material (scene.h:34 holds a list of
-// material runs per mesh; the synthetic scenes use one run).
+// One triangle mesh.  scene.h:34 keeps a list of material runs per mesh;
+// here tmtl holds each triangle's material (glTF meshes of several
+// primitives), or is NULL and every triangle has mtlid (the synthetic
+// scenes).
 struct nbh_mesh {
 	unsigned int vcnt;
 	float        *vrts; // vcnt * 3
@@ -30,6 +32,7 @@ struct nbh_mesh {
 	unsigned int icnt;
 	unsigned int *inds; // icnt, 3 per triangle
 	unsigned int mtlid;
+	unsigned int *tmtl; // icnt / 3 material ids, or NULL
 };
 
 // A mesh node: mesh id + object->world 4x4 row-major (tfmat.glob,
@@ -85,6 +88,23 @@ void nbh_scene_free(struct nbh_scene *s);
 unsigned int nbh_scene_tricnt(const struct nbh_scene *s);   // unique tris
 unsigned int nbh_scene_instcnt(const struct nbh_scene *s);  // mesh nodes
 double       nbh_scene_insttris(const struct nbh_scene *s); // instanced tris
+
+// glTF 2.0 (nb_gltf.c).  Load the subset nodebleed's importer reads
+// (gltf.h:4-11, gltfimp.c): one external .bin buffer, float VEC3 POSITION and
+// NORMAL, u8/u16/u32 indices, PBR base colour / metallic / roughness,
+// emissive factor x KHR_materials_emissive_strength, node TRS (or matrix)
+// hierarchies, the first perspective camera.  The resolution, spp and depth
+// fields get 640x360, 1, 5.  NBH_GLTF_NO_EXTRAS ignores the exact
+// transforms this library's writer stores in node extras (so the scene is
+// read as nodebleed would read it).  Returns 0, or -1 on any error (the
+// scene is then empty).  The writer emits one mesh per nbh_mesh (a single
+// material run each), one node per instance (TRS plus the exact matrix in
+// extras) and a camera node; the .bin goes beside the .gltf with the same
+// basename, as nodebleed's importer expects (gltfimp.c:420-428).
+#define NBH_GLTF_NO_EXTRAS 1u
+int nbh_scene_load_gltf(struct nbh_scene *s, const char *path,
+                        unsigned int flags);
+int nbh_scene_save_gltf(const struct nbh_scene *s, const char *path);
 
 // ------------------------------------------------------------ render data --
 

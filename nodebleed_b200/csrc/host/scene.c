@@ -394,6 +394,7 @@ static int add_mesh(struct sbuild *b, struct mbuf *m, unsigned int mtl)
 	o->icnt = m->icnt;
 	o->inds = m->i;
 	o->mtlid = mtl;
+	o->tmtl = NULL;
 	memset(m, 0, sizeof(*m));
 	return (int)s->meshcnt++;
 }
@@ -667,6 +668,7 @@ void nbh_scene_free(struct nbh_scene *s)
 		free(s->meshes[i].vrts);
 		free(s->meshes[i].nrms);
 		free(s->meshes[i].inds);
+		free(s->meshes[i].tmtl);
 	}
 	free(s->meshes);
 	free(s->mtls);
@@ -717,7 +719,7 @@ int nbh_cpy_rdata(struct nb_rdata *rd, const struct nbh_scene *s)
 			memcpy(&rn->n0, &m->nrms[3 * ip[0]], 12);
 			memcpy(&rn->n1, &m->nrms[3 * ip[1]], 12);
 			memcpy(&rn->n2, &m->nrms[3 * ip[2]], 12);
-			rn->mtlid = m->mtlid;
+			rn->mtlid = m->tmtl ? m->tmtl[t] : m->mtlid;
 		}
 		triofs[k] = ofs;
 		ofs += m->icnt / 3;

@@ -304,3 +304,86 @@ void refh_camrays(struct rdata *rd, unsigned int x, unsigned int y,
 		}
 	}
 }
+
+// Import a glTF file with nodebleed's own importer (imp_gltf_f,
+// gltfimp.c:415) and report what the render-data bridge would take from it
+// (cpy_rdata main.c:53, upd_rinsts main.c:117, the camera of
+// scene_updcams scene.c:411).  counts: [0] meshes, [1] vertices, [2]
+// indices, [3] materials, [4] mesh nodes.  With non-NULL buffers it also
+// copies, mesh after mesh: vertices and normals (3 floats each), indices
+// (mesh-local), the material of each triangle; per material col, metallic,
+// roughness, ior and the flags as a float's bits (7 floats); per mesh node
+// its mesh and its world matrix (16 floats); the camera's eye, fwd, ri, up
+// and vfov (13 floats).  Buffers must hold the counts of a first call.
+#include "scene.h"
+#include "gltfimp.h"
+#include "types.h"
+
+int refh_gltf_import(const char *path, unsigned int *counts, float *vrts,
+                     float *nrms, unsigned int *inds, unsigned int *trimtl,
+                     float *mtls, unsigned int *node_mesh, float *globs,
+                     float *cam)
+{
+	struct scene s;
+	memset(&s, 0, sizeof(s));
+	char name[4096];
+	size_t n = strlen(path);
+	if (n >= sizeof(name))
+		return -1;
+	memcpy(name, path, n + 1);
+	imp_gltf_f(&s, name);
+	scene_updtransforms(&s);
+	scene_updcams(&s);
+	unsigned int nv = 0, ni = 0, nn = 0;
+	for (unsigned int k = 0; k < s.meshcnt; k++) {
+		nv += s.meshes[k].vcnt;
+		ni += s.meshes[k].icnt;
+	}
+	for (unsigned int i = 0; i < s.nodecnt; i++)
+		if (s.objs[i].flags & MESH)
+			nn++;
+	counts[0] = s.meshcnt;
+	counts[1] = nv;
+	counts[2] = ni;
+	counts[3] = s.mtlcnt;
+	counts[4] = nn;
+	if (vrts) {
+		unsigned int v = 0, ix = 0, t = 0;
+		for (unsigned int k = 0; k < s.meshcnt; k++) {
+			struct mesh *m = &s.meshes[k];
+			memcpy(vrts + 3ull * v, m->vrts, 12ull * m->vcnt);
+			memcpy(nrms + 3ull * v, m->nrms, 12ull * m->vcnt);
+			memcpy(inds + ix, m->inds, 4ull * m->icnt);
+			for (unsigned int j = 0; j < m->mcnt; j++)
+				for (unsigned int q = 0; q < m->mtls[j].tricnt; q++)
+					trimtl[t++] = m->mtls[j].mtlid;
+			v += m->vcnt;
+			ix += m->icnt;
+		}
+		for (unsigned int i = 0; i < s.mtlcnt; i++) {
+			struct mtl *m = &s.mtls[i];
+			float *o = mtls + 7ull * i;
+			o[0] = m->col.x;
+			o[1] = m->col.y;
+			o[2] = m->col.z;
+			o[3] = m->metallic;
+			o[4] = m->roughness;
+			o[5] = m->ior;
+			memcpy(&o[6], &m->flags, 4);
+		}
+		unsigned int q = 0;
+		for (unsigned int i = 0; i < s.nodecnt; i++)
+			if (s.objs[i].flags & MESH) {
+				node_mesh[q] = (unsigned int)s.objs[i].objid;
+				memcpy(globs + 16ull * q, s.tfmats[i].glob, 64);
+				q++;
+			}
+		struct cam *c = &s.cams[s.currcam];
+		float cv[13] = {c->eye.x, c->eye.y, c->eye.z, c->fwd.x, c->fwd.y,
+		  c->fwd.z, c->ri.x, c->ri.y, c->ri.z, c->up.x, c->up.y, c->up.z,
+		  c->vfov};
+		memcpy(cam, cv, sizeof(cv));
+	}
+	scene_release(&s);
+	return 0;
+}
