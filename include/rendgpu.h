@@ -403,6 +403,17 @@ int rendgpu_get_tune(struct rdata *rd, struct rendgpu_tune *t);
 int rendgpu_autotune(struct rdata *rd, uint32_t frames,
                      struct rendgpu_tune *best, struct rendgpu_tune *log,
                      uint32_t cap, uint32_t *nlog);
+/* Tuned settings kept across runs (the reference fixes its variants at
+ * compile time, rend.c:3597-3599).  tune_save stores the settings in effect
+ * (and the last autotune's ms) in a text file under this GPU model (name, SM
+ * count, compute capability) and this context's scene signature (a hash of
+ * the mode and of every scene's triangle and instance counts, BVH depths,
+ * image size, spp and path depth), replacing an older line of the same key.
+ * tune_load applies the stored line of the same key and returns 1, or
+ * returns 0 when the file or the line does not exist.  Both need
+ * rendgpu_resaccum first. */
+int rendgpu_tune_save(struct rdata *rd, const char *path);
+int rendgpu_tune_load(struct rdata *rd, const char *path);
 
 /* Batches (no counterpart in the reference, which renders one rdata per
  * rend_render): n scenes of uneven triangle counts, resolutions, spp and
@@ -439,6 +450,10 @@ int rendgpu_batch_autotune(struct rendgpu_batch *b, uint32_t frames,
                            struct rendgpu_tune *best,
                            struct rendgpu_tune *log, uint32_t cap,
                            uint32_t *nlog);
+/* rendgpu_tune_save / rendgpu_tune_load for a batch (its signature covers
+ * every scene). */
+int rendgpu_batch_tune_save(struct rendgpu_batch *b, const char *path);
+int rendgpu_batch_tune_load(struct rendgpu_batch *b, const char *path);
 int rendgpu_batch_get_stream(struct rendgpu_batch *b, void **stream);
 /* rendgpu_set_resolve for every scene of the batch. */
 int rendgpu_batch_set_resolve(struct rendgpu_batch *b, uint32_t op,

@@ -172,6 +172,10 @@ class GpuLib:
                 ("rendgpu_sync", [vp]), ("rendgpu_get_stats", [vp, vp]),
                 ("rendgpu_get_lights", [vp, vp, u32, vp]),
                 ("rendgpu_capture", [vp, u32, u32]),
+                ("rendgpu_tune_save", [vp, C.c_char_p]),
+                ("rendgpu_tune_load", [vp, C.c_char_p]),
+                ("rendgpu_batch_tune_save", [vp, C.c_char_p]),
+                ("rendgpu_batch_tune_load", [vp, C.c_char_p]),
                 ("rendgpu_update_instances_device", [vp, vp, u32, u32]),
                 ("rendgpu_update_instances", [vp, vp, u32, u32]),
                 ("rendgpu_get_instances", [vp, vp, vp, u32, vp]),
@@ -310,6 +314,7 @@ class RenderData:
             raise RuntimeError(f"nbh_rdata_from_scene = {rc}")
         self.scene = scene
         self.buf = None
+        self.users = []  # renderers on this rdata, closed with it
         if width or height or spp:
             self.resize(width or self.rd.width, height or self.rd.height,
                         spp or self.rd.spp)
@@ -365,6 +370,11 @@ class RenderData:
 
     def close(self):
         if self.ptr:
+            # a GPU context keyed by this rdata must not outlive it (a new
+            # rdata at the same address would find it)
+            for u in self.users:
+                u.close()
+            self.users = []
             self.h.nbh_rend_release(self.ptr)
             self.h.nbh_rdata_delete(self.ptr)
             self.ptr = None
@@ -421,6 +431,7 @@ class GpuRenderer:
         if rc != 0:
             raise RendgpuError(rc, "rendgpu_init")
         self.live = True
+        rdata.users.append(self)
 
     def _ck(self, rc, what):
         if rc != 0:
@@ -488,6 +499,17 @@ class GpuRenderer:
         """Returns (best setting, every measured setting)."""
         return _autotune(self.g.rendgpu_autotune, self.ptr, frames, cap,
                          lambda rc: self._ck(rc, "autotune"))
+
+    def tune_save(self, path):
+        self._ck(self.g.rendgpu_tune_save(self.ptr, os.fsencode(path)),
+                 "tune_save")
+
+    def tune_load(self, path):
+        """1 when a stored setting was applied, 0 when none matched."""
+        rc = self.g.rendgpu_tune_load(self.ptr, os.fsencode(path))
+        if rc < 0:
+            self._ck(rc, "tune_load")
+        return rc
 
     # ---- neural radiance cache
     NRC_PARAMS = 5 * 4096 + 8 * 64
@@ -625,6 +647,8 @@ class BatchRenderer:
             raise RendgpuError(rc, "rendgpu_batch_init")
         self.h = h.value
         self.live = True
+        for r in self.rdatas:
+            r.users.append(self)
 
     def _ck(self, rc, what):
         if rc != 0:
@@ -680,6 +704,16 @@ class BatchRenderer:
     def autotune(self, frames=2, cap=64):
         return _autotune(self.g.rendgpu_batch_autotune, self.h, frames, cap,
                          lambda rc: self._ck(rc, "autotune"))
+
+    def tune_save(self, path):
+        self._ck(self.g.rendgpu_batch_tune_save(self.h, os.fsencode(path)),
+                 "tune_save")
+
+    def tune_load(self, path):
+        rc = self.g.rendgpu_batch_tune_load(self.h, os.fsencode(path))
+        if rc < 0:
+            self._ck(rc, "tune_load")
+        return rc
 
     def stream(self):
         s = C.c_void_p()

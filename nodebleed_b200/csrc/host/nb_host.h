@@ -97,8 +97,8 @@ double       nbh_scene_insttris(const struct nbh_scene *s); // instanced tris
 // fields get 640x360, 1, 5.  NBH_GLTF_NO_EXTRAS ignores the exact
 // transforms this library's writer stores in node extras (so the scene is
 // read as nodebleed would read it).  Returns 0, or -1 on any error (the
-// scene is then empty).  The writer emits one mesh per nbh_mesh (a single
-// material run each), one node per instance (TRS plus the exact matrix in
+// scene is then empty).  The writer emits one glTF mesh per host mesh, each
+// of a single material run, one node per instance (TRS plus the exact matrix in
 // extras) and a camera node; the .bin goes beside the .gltf with the same
 // basename, as nodebleed's importer expects (gltfimp.c:420-428).
 #define NBH_GLTF_NO_EXTRAS 1u

@@ -1838,12 +1838,135 @@ int autotune(Ctx *c, uint32_t frames, rendgpu_tune *best_out,
 	rc = set_tune(c, &best);
 	if (rc)
 		return rc;
+	c->tune.ms = best_ms;
 	NB_CK(c, cudaMemsetAsync(c->acc.p, 0, (size_t)c->npix * 12, c->stream));
 	NB_CK(c, cudaMemsetAsync(c->buf.p, 0, (size_t)c->npix * 4, c->stream));
 	NB_CK(c, cudaStreamSynchronize(c->stream));
 	if (best_out)
 		*best_out = best;
 	return 0;
+}
+
+// ------------------------------------------------------ tune store --
+//
+// Tuned launch parameters persist in a text file, one line per GPU model and
+// scene signature:  "<gpu>|<signature> block stack queue sched sort fuse ms".
+// The GPU key is the device name, SM count and compute capability; the
+// signature hashes (FNV-1a, 64 bit) what the tuned choice depends on: the
+// mode and every scene's triangle and instance counts, BVH depths, image size,
+// spp and path depth.
+
+std::string tune_gpu_key(const Ctx *c)
+{
+	cudaDeviceProp p;
+	if (cudaGetDeviceProperties(&p, c->device) != cudaSuccess)
+		return "unknown";
+	std::string name(p.name);
+	for (char &ch : name)
+		if (ch == ' ' || ch == '|')
+			ch = '_';
+	return name + ":" + std::to_string(p.multiProcessorCount) + ":" +
+	  std::to_string(p.major) + "." + std::to_string(p.minor);
+}
+
+std::string tune_signature(const Ctx *c)
+{
+	uint64_t h = 1469598103934665603ull;
+	auto mix = [&h](uint64_t v) {
+		for (int i = 0; i < 8; i++) {
+			h ^= (v >> (8 * i)) & 0xffu;
+			h *= 1099511628211ull;
+		}
+	};
+	mix(c->cfg.mode);
+	mix(c->sc.size());
+	for (const SceneHost &s : c->sc) {
+		mix(s.ntri);
+		mix(s.rd->instcnt);
+		mix(s.blas_depth);
+		mix(s.tlas_depth);
+		mix(s.W);
+		mix(s.H);
+		mix(s.spp);
+		mix(s.depth);
+	}
+	char buf[24];
+	std::snprintf(buf, sizeof(buf), "%016llx", (unsigned long long)h);
+	return buf;
+}
+
+int tune_save(Ctx *c, const char *path)
+{
+	int rc = ready(c, true);
+	if (rc)
+		return rc;
+	if (!path)
+		return fail(c, RENDGPU_EINVAL, "tune_save: null path");
+	std::string key = tune_gpu_key(c) + "|" + tune_signature(c);
+	std::vector<std::string> keep;
+	if (FILE *f = std::fopen(path, "r")) {
+		char line[512];
+		while (std::fgets(line, sizeof(line), f)) {
+			std::string l(line);
+			if (l.compare(0, key.size() + 1, key + " ") != 0)
+				keep.push_back(l);
+		}
+		std::fclose(f);
+	}
+	rendgpu_tune t = effective_tune(c);
+	char row[512];
+	std::snprintf(row, sizeof(row), "%s %u %u %u %u %u %u %.6g\n",
+	  key.c_str(), t.block, t.stack, t.queue, t.sched, t.sort, t.fuse,
+	  (double)c->tune.ms);
+	keep.push_back(row);
+	std::string tmp = std::string(path) + ".tmp";
+	FILE *f = std::fopen(tmp.c_str(), "w");
+	if (!f)
+		return fail(c, RENDGPU_EINVAL, "tune_save: cannot write " + tmp);
+	bool ok = true;
+	for (const std::string &l : keep)
+		ok = ok && std::fputs(l.c_str(), f) >= 0;
+	ok = (std::fclose(f) == 0) && ok;
+	if (!ok || std::rename(tmp.c_str(), path) != 0)
+		return fail(c, RENDGPU_EINVAL, "tune_save: cannot write " +
+		  std::string(path));
+	return 0;
+}
+
+// 1 when a stored setting for this GPU and scene signature was applied,
+// 0 when the file has none (or does not exist).
+int tune_load(Ctx *c, const char *path)
+{
+	int rc = ready(c, true);
+	if (rc)
+		return rc;
+	if (!path)
+		return fail(c, RENDGPU_EINVAL, "tune_load: null path");
+	std::string key = tune_gpu_key(c) + "|" + tune_signature(c);
+	FILE *f = std::fopen(path, "r");
+	if (!f)
+		return 0;
+	char line[512];
+	rendgpu_tune t{};
+	bool found = false;
+	while (!found && std::fgets(line, sizeof(line), f)) {
+		std::string l(line);
+		if (l.compare(0, key.size() + 1, key + " ") != 0)
+			continue;
+		double ms = 0.0;
+		found = std::sscanf(line + key.size() + 1, "%u %u %u %u %u %u %lf",
+		  &t.block, &t.stack, &t.queue, &t.sched, &t.sort, &t.fuse,
+		  &ms) == 7;
+		t.ms = (float)ms;
+	}
+	std::fclose(f);
+	if (!found)
+		return 0;
+	rc = set_tune(c, &t);
+	if (rc)
+		return rc;
+	c->tune.ms = t.ms;
+	return 1;
 }
 
 // ------------------------------------------------ allocation-free tracing --
@@ -2724,6 +2847,40 @@ int rendgpu_batch_get_tune(struct rendgpu_batch *b, struct rendgpu_tune *t)
 		return RENDGPU_EINVAL;
 	*t = effective_tune(c);
 	return 0;
+}
+
+int rendgpu_tune_save(struct rdata *rdp, const char *path)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	return tune_save(c, path);
+}
+
+int rendgpu_tune_load(struct rdata *rdp, const char *path)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	return tune_load(c, path);
+}
+
+int rendgpu_batch_tune_save(struct rendgpu_batch *b, const char *path)
+{
+	Ctx *c = find_batch(b);
+	if (!c)
+		return RENDGPU_EINVAL;
+	return tune_save(c, path);
+}
+
+int rendgpu_batch_tune_load(struct rendgpu_batch *b, const char *path)
+{
+	Ctx *c = find_batch(b);
+	if (!c)
+		return RENDGPU_EINVAL;
+	NB_CK(c, cudaSetDevice(c->device));
+	return tune_load(c, path);
 }
 
 int rendgpu_batch_autotune(struct rendgpu_batch *b, uint32_t frames,

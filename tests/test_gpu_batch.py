@@ -121,6 +121,41 @@ def test_autotune_returns_a_measured_setting(gpu):
     b.close()
 
 
+def test_tuned_setting_persists(gpu, tmp_path):
+    """rendgpu_(batch_)tune_save / _load: the tuned setting of a GPU model
+    and scene signature comes back in a later context of the same scenes,
+    and only there."""
+    keys = ("block", "stack", "queue", "sched", "sort", "fuse")
+    path = str(tmp_path / "tune.txt")
+    b = api.BatchRenderer(_rdatas(SCENES[:2]), max_depth=[3, 5],
+                          timing=True).upload()
+    best, _ = b.autotune(frames=1)
+    b.tune_save(path)
+    b.close()
+    b2 = api.BatchRenderer(_rdatas(SCENES[:2]), max_depth=[3, 5]).upload()
+    assert b2.tune_load(path) == 1
+    got = b2.get_tune()
+    assert all(got[k] == b2.get_tune()[k] for k in keys)
+    assert all(got[k] == best[k] for k in ("block", "stack", "queue",
+                                           "sched", "fuse"))
+    b2.close()
+    b3 = api.BatchRenderer(_rdatas(SCENES[:1]), max_depth=[3]).upload()
+    assert b3.tune_load(path) == 0  # another signature
+    b3.close()
+    rd = _rdatas([SCENES[1]])[0]
+    gr = api.GpuRenderer(rd, max_depth=SCENES[1][5]).upload()
+    gr.set_tune(block=128, stack=32, fuse=2)
+    want = gr.get_tune()
+    gr.tune_save(path)
+    gr.close()
+    gr2 = api.GpuRenderer(rd, max_depth=SCENES[1][5]).upload()
+    assert gr2.tune_load(path) == 1
+    got = gr2.get_tune()
+    assert all(got[k] == want[k] for k in keys)
+    gr2.close()
+    assert len(open(path).read().splitlines()) == 2
+
+
 def test_batch_rejects_radiance_cache_mode(gpu):
     rds = _rdatas(SCENES[:1])
     with pytest.raises(api.RendgpuError):

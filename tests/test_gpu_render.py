@@ -150,3 +150,21 @@ def test_tonemapped_resolve(gpu, op):
     with pytest.raises(api.RendgpuError):
         gr.set_resolve(3)
     gr.close()
+
+
+def test_gltf_scene_renders_like_the_in_memory_scene(gpu, tmp_path):
+    """Config 1 written as .gltf + .bin and loaded back by the host library
+    (nbh_scene_load_gltf) renders the same frame, bit for bit, as the scene
+    it was written from (640x360, 1 spp, depth 5)."""
+    src = api.Scene(api.SCENE_SMALL, 1)
+    path = str(tmp_path / "config1.gltf")
+    src.save_gltf(path)
+    got = api.Scene.load_gltf(path)
+    accs = []
+    for sc in (src, got):
+        rd = api.RenderData(sc, 640, 360, 1)
+        acc, rays, _, _ = _gpu_frame(rd, 5, api.MODE_PATH, 9)
+        assert rays > 640 * 360
+        accs.append(acc)
+        rd.close()
+    assert np.array_equal(accs[0].view(np.uint32), accs[1].view(np.uint32))
