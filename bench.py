@@ -66,9 +66,8 @@ def parse():
     p.add_argument("--nrc-width", type=int, default=1920)
     p.add_argument("--nrc-height", type=int, default=1080)
     p.add_argument("--nrc-frames", type=int, default=64)
-    p.add_argument("--nrc-ref-spp", type=int, default=1024,
-                   help="reference samples per pixel (the workload asks "
-                        "for 4096; 1024 keeps the default run short)")
+    p.add_argument("--nrc-ref-spp", type=int, default=4096,
+                   help="samples per pixel of the plain reference image")
     p.add_argument("--cpu-seconds", type=float, default=15.0,
                    help="target CPU time of the bounded CPU sample")
     p.add_argument("--no-batch", action="store_true",
@@ -79,7 +78,10 @@ def parse():
     p.add_argument("--stress-frames", type=int, default=2)
     p.add_argument("--stress-eval-width", type=int, default=960)
     p.add_argument("--stress-eval-height", type=int, default=540)
-    p.add_argument("--stress-ref-spp", type=int, default=256)
+    p.add_argument("--stress-ref-spp", type=int, default=4096)
+    p.add_argument("--update-reps", type=int, default=10,
+                   help="device-side scene updates timed on the stress "
+                        "scene")
     p.add_argument("--stress-nrc-frames", type=int, default=32)
     return p.parse_args()
 
@@ -369,6 +371,44 @@ def batch_eval(a, dev, flush):
             "unique_tris": sum(r["tris"] for r in rows)}
 
 
+def update_times(a, scene, rd, gr, stream):
+    """Per-frame cost of a transform change on a scene: the device path
+    (rendgpu_update_instances_device: inverse, world boxes, TLAS build or
+    refit, light table; CUDA events) against the host path the reference's
+    frame loop runs (upd_rinsts + rend_prepdynamic restated in the host
+    library, then rendgpu_upload_dynamic; wall clock)."""
+    import numpy as np
+    import torch
+    globs = torch.from_numpy(np.ascontiguousarray(scene.globs(),
+                                                  np.float32)).cuda()
+    torch.cuda.synchronize()
+    out = {}
+    for name, refit in (("device_build_ms", False), ("device_refit_ms", True)):
+        gr.update_instances(globs.data_ptr())  # first: builds
+        ev = []
+        for _ in range(a.update_reps):
+            with torch.cuda.stream(stream):
+                s, e = torch.cuda.Event(enable_timing=True), \
+                    torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+            gr.update_instances(globs.data_ptr(), refit=refit)
+            with torch.cuda.stream(stream):
+                e.record(stream)
+            ev.append((s, e))
+        torch.cuda.synchronize()
+        out[name] = _elapsed(ev) / a.update_reps
+    _, _, info = gr.instances()
+    out["device_tlas_nodes"], out["device_tlas_depth"] = info[0], info[1]
+    t0 = time.perf_counter()
+    for _ in range(max(1, a.update_reps // 5)):
+        rd.update_host()
+        gr.upload_dynamic()
+    out["host_ms"] = (time.perf_counter() - t0) * 1e3 / \
+        max(1, a.update_reps // 5)
+    out["instances"] = scene.insts
+    return out
+
+
 def stress_eval(a, dev, flush):
     """The stress workload: 128 BLAS of 1k-200k triangles, 4096 instances
     (the reference's cap), Lambertian / GGX (roughness U[0.05,0.5]) /
@@ -404,6 +444,7 @@ def stress_eval(a, dev, flush):
     ms = _elapsed(ev)
     st = gr.stats()
     lights, area = gr.lights()
+    upd = update_times(a, scene, rd, gr, stream)
     gr.close()
     out = {"workload": "stress: 128 BLAS (1k-200k tris log-uniform), 4096 "
                        "instances, Lambertian/GGX/mirror thirds, 8 quad "
@@ -414,7 +455,7 @@ def stress_eval(a, dev, flush):
            "samples_s": W * H * a.stress_frames / (ms / 1e3),
            "ms_per_frame": ms / a.stress_frames,
            "rays_per_frame": rays / a.stress_frames,
-           "max_stack": st["max_stack"]}
+           "max_stack": st["max_stack"], "scene_update": upd}
     if not a.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib as ol
@@ -518,13 +559,17 @@ def run_ours(a):
         rd.rd.buf = pinned.data_ptr()
         h2d = d2h = 0
         e2e_rays = 0
+        # the frame loop of a moving scene: new object->world matrices from
+        # host memory every frame; the device inverts them, rebuilds the
+        # TLAS and the light table (rendgpu_update_instances)
+        globs = np.ascontiguousarray(scene.globs(), np.float32)
         barrier()
         torch.cuda.synchronize()
         parts = [0.0, 0.0, 0.0]
         t0 = time.perf_counter()
         for _ in range(a.steps):
             t1 = time.perf_counter()
-            gr.upload_dynamic()
+            gr.update_instances(globs)
             h2d += gr.stats()["h2d_bytes"]
             t2 = time.perf_counter()
             e2e_rays += gr.frame()
@@ -537,12 +582,17 @@ def run_ours(a):
             parts[2] += t4 - t3
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
+        # the roofline frames below use the uploaded (host-built) TLAS, as
+        # the timed frames did
+        gr.upload_dynamic()
         e2e_rate, _, _ = job_rate(e2e_rays, dt, world)
         e2e = {"value": e2e_rate / 1e6, "unit": "Mrays/s",
                "h2d_bytes_per_step": h2d // a.steps,
                "d2h_bytes_per_step": d2h // a.steps,
-               "timing": "wall clock around upload_dynamic + render + "
-                         "readback of the ARGB8 image (pinned host)",
+               "timing": "wall clock around the scene update from host "
+                         "matrices (device inverse, TLAS build and light "
+                         "table) + render + readback of the ARGB8 image "
+                         "(pinned host)",
                "ms_upload_render_readback": [1e3 * x / a.steps
                                              for x in parts]}
 

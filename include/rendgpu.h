@@ -338,6 +338,11 @@ int rendgpu_get_lights(struct rdata *rd, float *out, uint32_t cap,
  * radiance cache keeps the encoding box of the upload.  Returns without
  * synchronising. */
 #define RENDGPU_UPDATE_REFIT 1u
+/* RENDGPU_UPDATE_TIGHT: bound each instance by every vertex of its mesh
+ * after the new matrix instead of the 8 transformed corners of its BLAS root
+ * box (a rotated instance's corner box can be much larger), and build or
+ * refit the TLAS over those boxes; rendgpu_get_instances then reports them. */
+#define RENDGPU_UPDATE_TIGHT 2u
 int rendgpu_update_instances_device(struct rdata *rd,
                                     const float *glob_device, uint32_t n,
                                     uint32_t flags);

@@ -416,7 +416,7 @@ class GpuRenderer:
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
                  timing=False, device=0, count=False, sched=0,
                  nrc_warmup=0, nrc_lr=0.0, graph=False, block=0,
-                 nrc_end=0, nrc_steps=0):
+                 nrc_end=0, nrc_steps=0, packet=False):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -427,6 +427,7 @@ class GpuRenderer:
         cfg.reserved[1] = nrc_warmup
         cfg.reserved[2] = nrc_end
         cfg.reserved[3] = nrc_steps
+        cfg.reserved[4] = 1 if packet else 0
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
         if rc != 0:
             raise RendgpuError(rc, "rendgpu_init")
@@ -557,11 +558,11 @@ class GpuRenderer:
         self._ck(self.g.rendgpu_set_resolve(self.ptr, op, exposure),
                  "set_resolve")
 
-    def update_instances(self, globs, refit=False):
+    def update_instances(self, globs, refit=False, tight=False):
         """Device-side scene update from (instances, 16) object->world
         matrices (host array: copied; else an integer device pointer)."""
         n = self.rdata.rd.instcnt
-        flags = 1 if refit else 0
+        flags = (1 if refit else 0) | (2 if tight else 0)
         if isinstance(globs, int):
             self._ck(self.g.rendgpu_update_instances_device(self.ptr, globs,
                                                             n, flags),

@@ -75,6 +75,8 @@ struct DevBuf {
 struct SceneHost {
 	nb_rdata *rd = nullptr;
 	std::unordered_map<uint32_t, uint32_t> root_of; // triofs -> BLAS root
+	// triofs -> (first, count) of the BLAS's triangles in the device array
+	std::unordered_map<uint32_t, std::pair<uint32_t, uint32_t>> tri_range;
 	// triofs -> mesh-local ids of its emissive triangles
 	std::unordered_map<uint32_t, std::vector<uint32_t>> emitters;
 	uint32_t nrm_base = 0, mtl_base = 0, inst_base = 0, ntri = 0, nmtl = 0;
@@ -139,7 +141,7 @@ struct Ctx {
 	// BLAS root boxes, new matrices, world boxes, TLAS build queues, slot
 	// ranges and instance order (refit), build info, emitter sources, area
 	DevBuf   dyn_root, dyn_glob, dyn_wbox, dyn_q, dyn_ranges, dyn_order,
-	         dyn_info, dyn_emit, dyn_area;
+	         dyn_info, dyn_emit, dyn_area, dyn_trange;
 	uint32_t dyn_nemit = 0;
 	bool     dyn_built = false;  // a device TLAS build ran (refit possible)
 	bool     dyn_active = false; // the device holds the current instances
@@ -343,6 +345,30 @@ int launch_trace(Ctx *c, const float4 *rays, const uint32_t *count,
 	default:
 		return too_deep(c);
 	}
+	NB_CK(c, cudaGetLastError());
+	return 0;
+}
+
+// Coherent camera-ray traversal (k_trace_packet): cfg.reserved[4] bit 0,
+// single-scene contexts whose deepest TLAS + BLAS chain fits the packet
+// stack (a visit pushes at most 7 entries more than it pops), not while
+// counting visits.
+constexpr int kPacketDepth = 128;
+
+bool packet_primary(const Ctx *c)
+{
+	return (c->cfg.reserved[4] & 1u) && c->sc.size() == 1 &&
+	  !(c->cfg.flags & RENDGPU_FLAG_COUNT) &&
+	  7u * (c->tlas_depth + c->blas_depth) + 2u <= (uint32_t)kPacketDepth;
+}
+
+int launch_trace_packet(Ctx *c, const float4 *rays, const uint32_t *count,
+                        uint32_t *work, float4 *hits, uint32_t *errs,
+                        unsigned long long *nrays)
+{
+	auto fn = k_trace_packet<kPacketDepth>;
+	fn<<<trace_grid(c, (const void *)fn, 0, 256), 256, 0, c->stream>>>(
+	  scene_of(c), rays, count, work, hits, errs, nrays);
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -933,6 +959,9 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 			if (fused && k > 0u)
 				rc = launch_fused(c, const_cast<FrameDev &>(F), F.q[cur],
 				  F.cnt + cur, k - 1u);
+			else if (k == 0u && packet_primary(c))
+				rc = launch_trace_packet(c, F.q[cur], F.cnt + cur,
+				  F.cnt + 4, F.hits, F.cnt + 3, F.rays);
 			else
 				rc = launch_trace(c, F.q[cur], F.cnt + cur, F.cnt + 4,
 				  F.hits, F.cnt + 3, F.rays);
@@ -1174,7 +1203,7 @@ void free_ctx(Ctx *c)
 	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat, &c->waitchk,
 	  &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob, &c->dyn_wbox,
 	  &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info, &c->dyn_emit,
-	  &c->dyn_area};
+	  &c->dyn_area, &c->dyn_trange};
 	for (DevBuf *b : bufs)
 		b->release();
 	for (int i = 0; i < kMaxEvents; i++)
@@ -1197,7 +1226,7 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec, &c->waitchk,
 	  &c->rfeat, &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob,
 	  &c->dyn_wbox, &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info,
-	  &c->dyn_emit, &c->dyn_area};
+	  &c->dyn_emit, &c->dyn_area, &c->dyn_trange};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
 		s += b->cap;
@@ -1281,6 +1310,7 @@ int upload_static_all(Ctx *c)
 			return fail(c, RENDGPU_ELIMIT, "instance count outside "
 			  "1..4096 (INST_ID_BITS = 12, rend.c:24)");
 		h.root_of.clear();
+		h.tri_range.clear();
 		h.blas_depth = 0;
 		uint32_t maxtri = 0, maxmtl = 0;
 		for (uint32_t i = 0; i < rd->instcnt; i++) {
@@ -1297,10 +1327,12 @@ int upload_static_all(Ctx *c)
 			uint32_t root = 0;
 			bvh_stats bs;
 			std::string err;
+			uint32_t first = (uint32_t)tris.size();
 			if (!convert_blas(rd, ri.triofs, nodes, tris, &root, &bs, &err))
 				return fail(c, RENDGPU_EINVAL, "BLAS of triofs " +
 				  std::to_string(ri.triofs) + ": " + err);
 			h.root_of[ri.triofs] = root;
+			h.tri_range[ri.triofs] = {first, (uint32_t)tris.size() - first};
 			h.blas_depth = std::max(h.blas_depth, bs.depth);
 		}
 		for (uint32_t t = 0; t < maxtri; t++)
@@ -1376,6 +1408,13 @@ int dyn_prepare(Ctx *c, uint64_t *bytes)
 		rb[2 * i] = make_float4(mi[0], mi[1], mi[2], 0.0f);
 		rb[2 * i + 1] = make_float4(ma[0], ma[1], ma[2], 0.0f);
 	}
+	// each instance's triangles in the device array (tight boxes)
+	std::vector<uint2> tr(std::max(n, 1u), make_uint2(0u, 0u));
+	for (uint32_t i = 0; i < n; i++) {
+		auto it = h.tri_range.find(rd->insts[i].triofs);
+		if (it != h.tri_range.end())
+			tr[i] = make_uint2(it->second.first, it->second.second);
+	}
 	std::vector<EmitSrc> es;
 	for (uint32_t i = 0; i < n; i++) {
 		const nb_rinst &ri = rd->insts[i];
@@ -1422,6 +1461,9 @@ int dyn_prepare(Ctx *c, uint64_t *bytes)
 	NB_CK(c, c->dyn_emit.ensure(std::max<size_t>(es.size(), 1) *
 	  sizeof(EmitSrc)));
 	NB_CK(c, c->dyn_area.ensure(16));
+	NB_CK(c, c->dyn_trange.ensure(tr.size() * sizeof(uint2)));
+	NB_CK(c, cudaMemcpyAsync(c->dyn_trange.p, tr.data(), tr.size() *
+	  sizeof(uint2), cudaMemcpyHostToDevice, c->stream));
 	NB_CK(c, cudaMemcpyAsync(c->dyn_root.p, rb.data(), rb.size() *
 	  sizeof(float4), cudaMemcpyHostToDevice, c->stream));
 	if (!es.empty())
@@ -1430,7 +1472,8 @@ int dyn_prepare(Ctx *c, uint64_t *bytes)
 	NB_CK(c, cudaMemsetAsync(c->dyn_info.p, 0, 4 * sizeof(uint32_t),
 	  c->stream));
 	// (pageable sources: the copies have read them when they return)
-	*bytes = rb.size() * sizeof(float4) + es.size() * sizeof(EmitSrc);
+	*bytes = rb.size() * sizeof(float4) + es.size() * sizeof(EmitSrc) +
+	  tr.size() * sizeof(uint2);
 	c->dyn_built = false;
 	c->dyn_active = false;
 	return 0;
@@ -1456,7 +1499,7 @@ int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
 		return fail(c, RENDGPU_ESTATE, "update: the uploaded light table "
 		  "skipped a degenerate emitter; upload non-degenerate transforms "
 		  "first");
-	if (flags & ~(uint32_t)RENDGPU_UPDATE_REFIT)
+	if (flags & ~(uint32_t)(RENDGPU_UPDATE_REFIT | RENDGPU_UPDATE_TIGHT))
 		return fail(c, RENDGPU_EINVAL, "update: unknown flags");
 	NB_CK(c, cudaSetDevice(c->device));
 	bool refit = (flags & RENDGPU_UPDATE_REFIT) && c->dyn_built;
@@ -1465,6 +1508,12 @@ int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
 	  c->dyn_root.as<float4>(), c->insts.as<float4>(),
 	  c->dyn_wbox.as<float4>(), c->berr.as<uint32_t>() + 1);
 	NB_CK(c, cudaGetLastError());
+	if ((flags & RENDGPU_UPDATE_TIGHT) && n) {
+		k_inst_tight<<<n, 256, 0, c->stream>>>(glob, n,
+		  c->dyn_trange.as<uint2>(), c->tris.as<float4>(),
+		  c->dyn_wbox.as<float4>());
+		NB_CK(c, cudaGetLastError());
+	}
 	if (!refit) {
 		TbArgs A;
 		A.wbox = c->dyn_wbox.as<float4>();

@@ -123,6 +123,61 @@ __global__ void __launch_bounds__(128) k_inst_update(
 	wbox[2u * i + 1u] = make_float4(hi[0], hi[1], hi[2], 0.0f);
 }
 
+// Tight world box of each instance: the bounds of every vertex of its BLAS
+// (trange: first triangle and count in the device triangle array) after
+// glob, one CTA per instance.  The reference bounds an instance by the 8
+// transformed corners of its root box, which a rotation inflates; a TLAS
+// over the tight boxes lets fewer rays enter instances they never touch.
+// The quantised TLAS boxes are padded by at least one quantum of 2^-22 of
+// the coordinates' magnitude, which covers the rounding of the transform.
+__device__ __forceinline__ void tb_warp_box(float lo[3], float hi[3]);
+
+__global__ void __launch_bounds__(256) k_inst_tight(
+  const float *__restrict__ glob, uint32_t n, const uint2 *__restrict__ trange,
+  const float4 *__restrict__ tris, float4 *wbox)
+{
+	__shared__ float part[8][6];
+	uint32_t i = blockIdx.x;
+	if (i >= n)
+		return;
+	const float *g = glob + 16u * i;
+	float m[12];
+	for (int k = 0; k < 12; k++)
+		m[k] = g[k];
+	uint2 r = trange[i];
+	float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+	float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+	for (uint32_t t = r.x + threadIdx.x; t < r.x + r.y; t += blockDim.x)
+		for (int v = 0; v < 3; v++) {
+			float4 p = __ldg(tris + 3u * t + v);
+			for (int a = 0; a < 3; a++) {
+				float w = __fadd_rn(__fadd_rn(__fadd_rn(
+				  __fmul_rn(m[4 * a], p.x), __fmul_rn(m[4 * a + 1], p.y)),
+				  __fmul_rn(m[4 * a + 2], p.z)), m[4 * a + 3]);
+				lo[a] = fminf(lo[a], w);
+				hi[a] = fmaxf(hi[a], w);
+			}
+		}
+	tb_warp_box(lo, hi);
+	uint32_t w = threadIdx.x >> 5;
+	if ((threadIdx.x & 31u) == 0)
+		for (int a = 0; a < 3; a++) {
+			part[w][a] = lo[a];
+			part[w][3 + a] = hi[a];
+		}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (uint32_t k = 1; k < (blockDim.x >> 5); k++)
+			for (int a = 0; a < 3; a++) {
+				part[0][a] = fminf(part[0][a], part[k][a]);
+				part[0][3 + a] = fmaxf(part[0][3 + a], part[k][3 + a]);
+			}
+		wbox[2u * i] = make_float4(part[0][0], part[0][1], part[0][2], 0.0f);
+		wbox[2u * i + 1u] = make_float4(part[0][3], part[0][4], part[0][5],
+		  0.0f);
+	}
+}
+
 // ----------------------------------------------------------- TLAS build --
 
 struct TbNode { // an open node: its instance range and box

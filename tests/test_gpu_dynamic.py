@@ -86,6 +86,20 @@ def test_device_update_matches_host_path(gpu):
     info = _compare(gd, gh, rd_d, rd_h, rays, "build")
     print(f"device TLAS: {info[0]} nodes, depth {info[1]}")
     assert np.array_equal(_bits(_frame(gd, rd_d)), _bits(_frame(gh, rd_h)))
+    # tight instance boxes (every transformed vertex): smaller boxes, another
+    # TLAS, the same hits
+    gd.update_instances(moved, tight=True)
+    _, wt, info_t = gd.instances()
+    wc = rd_h.aabbs()
+
+    def area(b):
+        d = np.maximum(b[:, 3:] - b[:, :3], 0.0).astype(np.float64)
+        return (d[:, 0] * d[:, 1] + d[:, 1] * d[:, 2] + d[:, 2] * d[:, 0])
+    assert area(wt).sum() < area(wc).sum()
+    assert info_t[2] == 0
+    assert np.array_equal(_bits(gd.trace(rays)), _bits(gh.trace(rays)))
+    assert np.array_equal(gd.occluded(rays), gh.occluded(rays))
+    assert np.array_equal(_bits(_frame(gd, rd_d)), _bits(_frame(gh, rd_h)))
     # a small further move, refitted on the device (device matrices)
     import torch
     moved2 = _move(moved, rng, 0.02, 0.05)
