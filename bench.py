@@ -569,7 +569,7 @@ def run_ours(a):
         t0 = time.perf_counter()
         for _ in range(a.steps):
             t1 = time.perf_counter()
-            gr.update_instances(globs)
+            gr.update_instances(globs, tight=True)
             h2d += gr.stats()["h2d_bytes"]
             t2 = time.perf_counter()
             e2e_rays += gr.frame()

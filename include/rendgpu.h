@@ -78,7 +78,10 @@ struct rendgpu_cfg {
 	                         frames of unbiased tracing (0 = 1); [2]: bounce
 	                         at which training paths end in the cache after
 	                         the warm-up (0 = 3); [3]: cache training steps
-	                         of 16384 samples per frame (0 = 6) */
+	                         of 16384 samples per frame (0 = 6); [4] bit 0:
+	                         keep the TLAS rendgpu_upload_dynamic converts
+	                         from rd->bnodes instead of the device rebuild
+	                         over tight instance boxes */
 };
 
 /* A ray for the batch calls: origin, tmax, direction (32 bytes). */
@@ -170,7 +173,13 @@ int rendgpu_release(struct rdata *rd);
 int rendgpu_upload_static(struct rdata *rd);
 
 /* After rend_prepdynamic (rend.c:3073): upload the TLAS, the instance
- * transforms and the light table. */
+ * transforms and the light table.  The TLAS in rd->bnodes is checked and
+ * converted (RENDGPU_EINVAL on a malformed tree; the context then needs a
+ * successful upload before it traces again).  A single-scene context then
+ * rebuilds it on the device over tight instance boxes (every vertex after
+ * the instance's matrix instead of its root box's 8 corners), no deeper
+ * than the converted tree: the same hits, fewer instances entered.
+ * cfg.reserved[4] bit 0 keeps the converted tree. */
 int rendgpu_upload_dynamic(struct rdata *rd);
 
 /* After rend_resaccum (rend.c:3092): size the device accumulator and the

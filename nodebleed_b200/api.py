@@ -416,7 +416,7 @@ class GpuRenderer:
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
                  timing=False, device=0, count=False, sched=0,
                  nrc_warmup=0, nrc_lr=0.0, graph=False, block=0,
-                 nrc_end=0, nrc_steps=0, packet=False):
+                 nrc_end=0, nrc_steps=0, ref_tlas=False):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -427,7 +427,7 @@ class GpuRenderer:
         cfg.reserved[1] = nrc_warmup
         cfg.reserved[2] = nrc_end
         cfg.reserved[3] = nrc_steps
-        cfg.reserved[4] = 1 if packet else 0
+        cfg.reserved[4] = 1 if ref_tlas else 0
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
         if rc != 0:
             raise RendgpuError(rc, "rendgpu_init")

@@ -306,36 +306,6 @@ __global__ void __launch_bounds__(256, 4) k_trace(DScene S, const float4 *rays,
 	  sstk + threadIdx.x, blockDim.x, sink);
 }
 
-// Coherent closest hits of camera rays (single-scene contexts): each warp
-// takes 32 consecutive queue entries (k_gen appends 8 pixels x 4 samples
-// of one tile row together) and traverses them as one packet
-// (trace_packet); DEPTH shared stack entries per warp.
-template <int DEPTH>
-__global__ void __launch_bounds__(256, 4) k_trace_packet(DScene S,
-                                                      const float4 *rays,
-                                                      const uint32_t *count,
-                                                      uint32_t *work,
-                                                      float4 *hits,
-                                                      uint32_t *errs,
-                                                      unsigned long long *nrays)
-{
-	__shared__ uint4 stk[8][DEPTH];
-	uint32_t n = *count;
-	if (blockIdx.x == 0 && threadIdx.x == 0 && nrays)
-		atomicAdd(nrays, (unsigned long long)n);
-	SinkRaw sink{hits, errs, nullptr};
-	const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-	for (;;) {
-		uint32_t base = 0;
-		if (lane == 0)
-			base = atomicAdd(work, 32u);
-		base = __shfl_sync(kFull, base, 0);
-		if (base >= n)
-			break;
-		trace_packet<DEPTH>(S, rays, n, base, stk[warp], sink);
-	}
-}
-
 // Any-hit trace of API rays: occl[i] = hit in (0, tmax).
 template <int SCHED, int STACK>
 __global__ void __launch_bounds__(256, 4) k_occluded(DScene S,

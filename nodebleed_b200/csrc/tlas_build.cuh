@@ -123,6 +123,44 @@ __global__ void __launch_bounds__(128) k_inst_update(
 	wbox[2u * i + 1u] = make_float4(hi[0], hi[1], hi[2], 0.0f);
 }
 
+// Object->world 4x4 (row-major) of each instance from its uploaded
+// world->object 3x4, inverted in FP64 (the affine inverse: 3x3 by
+// cofactors, translation -A^-1 b).  Feeds k_inst_tight when the TLAS is
+// rebuilt at upload time, where only the render data's inverse matrices
+// exist; the tight boxes it yields are padded by the TLAS quantisation, so
+// the inverse's rounding does not matter.  A singular matrix gives zeros.
+__global__ void __launch_bounds__(128) k_inst_glob(const float4 *insts,
+                                                   uint32_t n, float *glob)
+{
+	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const float4 *ip = insts + 4u * i;
+	float4 r0 = ip[0], r1 = ip[1], r2 = ip[2];
+	double A[9] = {r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r2.x, r2.y, r2.z};
+	double b[3] = {r0.w, r1.w, r2.w};
+	double c0 = A[4] * A[8] - A[5] * A[7], c1 = A[5] * A[6] - A[3] * A[8];
+	double c2 = A[3] * A[7] - A[4] * A[6];
+	double det = A[0] * c0 + A[1] * c1 + A[2] * c2;
+	float *g = glob + 16u * i;
+	for (int k = 0; k < 16; k++)
+		g[k] = 0.0f;
+	if (det == 0.0)
+		return;
+	double I[9] = {c0 / det, (A[2] * A[7] - A[1] * A[8]) / det,
+	  (A[1] * A[5] - A[2] * A[4]) / det, c1 / det,
+	  (A[0] * A[8] - A[2] * A[6]) / det, (A[2] * A[3] - A[0] * A[5]) / det,
+	  c2 / det, (A[1] * A[6] - A[0] * A[7]) / det,
+	  (A[0] * A[4] - A[1] * A[3]) / det};
+	for (int r = 0; r < 3; r++) {
+		for (int k = 0; k < 3; k++)
+			g[4 * r + k] = (float)I[3 * r + k];
+		g[4 * r + 3] = (float)-(I[3 * r] * b[0] + I[3 * r + 1] * b[1] +
+		  I[3 * r + 2] * b[2]);
+	}
+	g[15] = 1.0f;
+}
+
 // Tight world box of each instance: the bounds of every vertex of its BLAS
 // (trange: first triangle and count in the device triangle array) after
 // glob, one CTA per instance.  The reference bounds an instance by the 8

@@ -981,189 +981,6 @@ __device__ __forceinline__ void trace_two(const DScene &S,
 	  stk, stride, sink, rays2, n2, &sink2);
 }
 
-// ------------------------------------------------- coherent (packet) rays --
-//
-// Camera rays of neighbouring pixels enter mostly the same nodes.  A warp
-// then traverses once for its 32 rays: a stack entry is a child (TLAS or
-// BLAS node, or a triangle group) with the mask of the lanes whose rays
-// entered it and the smallest of their entry distances; a lane joins a
-// popped entry only if its bit is set and its closest hit so far is not
-// nearer than that bound.  Every node visit and triangle test then runs
-// with all joining lanes together.  One instance is current at a time:
-// entering another transforms every live lane's ray into its space.
-
-constexpr uint32_t kPkTlas = 0u, kPkBlas = 1u, kPkTris = 2u;
-
-// Stack entry: x = node index or first item, y = lane mask,
-// z = kind << 28 | count << 24 | instance, w = entry bound (float bits).
-__device__ __forceinline__ uint4 pk_entry(uint32_t idx, uint32_t mask,
-                                          uint32_t kind, uint32_t cnt,
-                                          uint32_t inst, float tmin)
-{
-	return make_uint4(idx, mask, kind << 28 | cnt << 24 | inst,
-	  __float_as_uint(tmin));
-}
-
-// Coherent closest hits of rays [base, base + 32) of a queue (whole warp;
-// lanes past n idle).  stk: this warp's DEPTH entries in shared memory.
-// Returns false on a stack overflow (the warp's rays are then abandoned).
-template <int DEPTH, class Sink>
-__device__ bool trace_packet(const DScene &S, const float4 *rays, uint32_t n,
-                             uint32_t base, uint4 *stk, Sink &sink)
-{
-	const uint32_t lane = threadIdx.x & 31u;
-	const uint32_t ri = base + lane;
-	const bool live = ri < n;
-	float4 ra = live ? rays[2u * ri] : make_float4(0, 0, 0, 0);
-	float4 rb = live ? rays[2u * ri + 1u] : make_float4(0, 0, 1, 0);
-	Trav T;
-	trav_start(T, ra, rb);
-	if (!live)
-		T.bt = 0.0f;
-	uint32_t cur = kNone; // instance whose space the rays are in
-	int sp = 0;
-	// single-scene contexts: the TLAS root is node 0
-	uint32_t lm = __ballot_sync(kFull, live);
-	if (lane == 0)
-		stk[0] = pk_entry(0u, lm, kPkTlas, 0u, 0u, 0.0f);
-	sp = 1;
-	__syncwarp();
-	bool ok = true;
-	while (sp > 0) {
-		uint4 e = stk[--sp];
-		__syncwarp();
-		float tmin = __uint_as_float(e.w);
-		bool p = ((e.y >> lane) & 1u) && live && T.bt * kWiden >= tmin;
-		uint32_t pm = __ballot_sync(kFull, p);
-		if (!pm)
-			continue;
-		uint32_t kind = e.z >> 28, inst = e.z & 0x00ffffffu;
-		// the rays' space: world for TLAS entries, the instance's otherwise
-		uint32_t want = kind == kPkTlas ? kNone : inst;
-		if (want != cur) {
-			if (want == kNone) {
-				tray_slab(T.r, ra.x, ra.y, ra.z, rb.x, rb.y, rb.z);
-			} else {
-				const float4 *ip = S.insts + 4u * want;
-				float o[3], d[3];
-				xform(__ldg(ip), __ldg(ip + 1), __ldg(ip + 2), ra.x, ra.y,
-				  ra.z, rb.x, rb.y, rb.z, o, d);
-				tray_slab(T.r, o[0], o[1], o[2], d[0], d[1], d[2]);
-				tray_watertight(T.r);
-			}
-			cur = want;
-		}
-		if (kind == kPkTris) {
-			uint32_t cnt = (e.z >> 24) & 0xfu;
-			for (uint32_t k = 0; k < cnt; k++) {
-				float t;
-				if (p && tri_hit(S.tris, e.x + k, T.r, T.bt, &t)) {
-					T.bt = t;
-					T.btri = e.x + k;
-					T.binst = inst;
-					T.found = true;
-				}
-			}
-			continue;
-		}
-		// node visit: per slot, the joining lanes that entered the child
-		// and their smallest entry distance
-		const nb_qnode *nodes = kind == kPkTlas ? S.tlas : S.blas;
-		const uint4 *q = reinterpret_cast<const uint4 *>(nodes + e.x);
-		uint4 w0 = __ldg(q), w1 = __ldg(q + 1), w2 = __ldg(q + 2);
-		uint4 w3 = __ldg(q + 3), w4 = __ldg(q + 4);
-		uint32_t imask = w0.w >> 24;
-		const TRay &r = T.r;
-		float scx = __uint_as_float((w0.w & 0xffu) << 23) * r.ix;
-		float scy = __uint_as_float(((w0.w >> 8) & 0xffu) << 23) * r.iy;
-		float scz = __uint_as_float(((w0.w >> 16) & 0xffu) << 23) * r.iz;
-		float bx = __fmaf_rn(-8388608.0f, scx,
-		  (__uint_as_float(w0.x) - r.ox) * r.ix);
-		float by = __fmaf_rn(-8388608.0f, scy,
-		  (__uint_as_float(w0.y) - r.oy) * r.iy);
-		float bz = __fmaf_rn(-8388608.0f, scz,
-		  (__uint_as_float(w0.z) - r.oz) * r.iz);
-		bool fx = signbit(r.ix), fy = signbit(r.iy), fz = signbit(r.iz);
-		uint32_t nx0 = fx ? w3.z : w2.x, nx1 = fx ? w3.w : w2.y;
-		uint32_t fx0 = fx ? w2.x : w3.z, fx1 = fx ? w2.y : w3.w;
-		uint32_t ny0 = fy ? w4.x : w2.z, ny1 = fy ? w4.y : w2.w;
-		uint32_t fy0 = fy ? w2.z : w4.x, fy1 = fy ? w2.w : w4.y;
-		uint32_t nz0 = fz ? w4.z : w3.x, nz1 = fz ? w4.w : w3.y;
-		uint32_t fz0 = fz ? w3.x : w4.z, fz1 = fz ? w3.y : w4.w;
-		uint32_t smask[8];
-		float stmin[8];
-#pragma unroll
-		for (int s = 0; s < 8; s++) {
-			int b = s & 3;
-			uint32_t wnx = s < 4 ? nx0 : nx1, wfx = s < 4 ? fx0 : fx1;
-			uint32_t wny = s < 4 ? ny0 : ny1, wfy = s < 4 ? fy0 : fy1;
-			uint32_t wnz = s < 4 ? nz0 : nz1, wfz = s < 4 ? fz0 : fz1;
-			float tnx = __fmaf_rn(qbf(wnx, b), scx, bx);
-			float tny = __fmaf_rn(qbf(wny, b), scy, by);
-			float tnz = __fmaf_rn(qbf(wnz, b), scz, bz);
-			float tfx = __fmaf_rn(qbf(wfx, b), scx, bx);
-			float tfy = __fmaf_rn(qbf(wfy, b), scy, by);
-			float tfz = __fmaf_rn(qbf(wfz, b), scz, bz);
-			float tn = fmax3(tnx, tny, fmaxf(tnz, 0.0f));
-			float tf = fmin3(tfx, tfy, fminf(tfz, T.bt));
-			bool hit = p && tn <= tf * kWiden;
-			smask[s] = __ballot_sync(kFull, hit);
-			stmin[s] = __uint_as_float(__reduce_min_sync(kFull,
-			  hit ? __float_as_uint(tn) : 0x7f800000u));
-		}
-		// push the entered children, farthest first (nearest on top)
-		uint32_t left = 0;
-#pragma unroll
-		for (int s = 0; s < 8; s++)
-			left |= smask[s] ? 1u << s : 0u;
-		if (sp + __popc(left) > DEPTH) {
-			ok = false;
-			break;
-		}
-		while (left) {
-			int far = -1;
-			float ft = -1.0f;
-#pragma unroll
-			for (int s = 0; s < 8; s++)
-				if (((left >> s) & 1u) && stmin[s] >= ft) {
-					ft = stmin[s];
-					far = s;
-				}
-			left &= ~(1u << far);
-			uint32_t m = 0, meta = 0;
-			float tm = 0.0f;
-#pragma unroll
-			for (int s = 0; s < 8; s++)
-				if (s == far) {
-					m = smask[s];
-					tm = stmin[s];
-				}
-			meta = ((far < 4 ? w1.z : w1.w) >> (8u * (far & 3))) & 0xffu;
-			uint4 ent;
-			if ((imask >> far) & 1u) {
-				uint32_t ci = w1.x + __popc(imask & ((1u << far) - 1u));
-				ent = pk_entry(ci, m, kind, 0u, inst, tm);
-			} else if (kind == kPkTlas) {
-				// an instance: enter its BLAS root
-				uint32_t it = __ldg(S.irefs + w1.y + (meta & 31u));
-				uint32_t root = __float_as_uint(__ldg(S.insts + 4u * it +
-				  3u).x);
-				ent = pk_entry(root, m, kPkBlas, 0u, it, tm);
-			} else {
-				ent = pk_entry(w1.y + (meta & 31u), m, kPkTris,
-				  ((meta >> 5) & 3u) + 1u, inst, tm);
-			}
-			if (lane == 0)
-				stk[sp] = ent;
-			sp++;
-		}
-		__syncwarp();
-	}
-	if (live)
-		sink(ri, T, ok ? 0u : 1u);
-	return ok;
-}
-
 // --------------------------------------------------------------- sinks --
 
 // Raw closest hit: (t, triangle index, instance, 0); t = FLT_MAX on a miss

@@ -218,7 +218,7 @@ def bruteforce(rd_ptr, rays):
     return ids, t
 
 
-def classify(rd_ptr, rays, ha, hb, eps_t, eps_b):
+def classify(rd_ptr, rays, ha, hb, eps_t, eps_b, eps_origin=0.0):
     """Compare two hit sets on the same rays.  Returns (n_same, ties,
     bad).  A disagreement is a tie when an FP64 re-intersection of both
     candidates shows either
@@ -227,6 +227,11 @@ def classify(rd_ptr, rays, ha, hb, eps_t, eps_b):
       error bounds of both), or
     * a candidate within eps_b (plus its Moeller-Trumbore error bound) of
       an edge, or outside by less.
+
+    * (eps_origin > 0) a candidate within eps_origin of the ray's origin:
+      the zone the renderer's own origin offset (EPS2, util.h:8) exists to
+      keep rays out of, where which implementation sees a surface is
+      decided by the rounding of its world->object transform.
 
     The Moeller-Trumbore bounds cover the reference's and the oracle's own
     evaluation of the test; eps_t/eps_b cover the reference's rcpps."""
@@ -252,7 +257,9 @@ def classify(rd_ptr, rays, ha, hb, eps_t, eps_b):
                        abs(ta[j] - tb[j]) <= eps_t * min(abs(ta[j]),
                                                          abs(tb[j])) +
                        ea[j][2] + eb[j][2])
-            if near_a or near_b or close_t:
+            at_origin = ((not miss_a[i] and abs(ta[j]) < eps_origin) or
+                         (not miss_b[i] and abs(tb[j]) < eps_origin))
+            if near_a or near_b or close_t or at_origin:
                 ties.append(i)
             else:
                 bad.append(i)

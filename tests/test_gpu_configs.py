@@ -35,6 +35,11 @@ pytestmark = pytest.mark.gpu
 # Moeller-Trumbore): at most 1 in 200 rays (measured: 0.03 % of the scale
 # scene's bounce rays, 0.21 % of the stress scene's rays).
 REF_TIE_FRAC = 1.0 / 200
+# Hits nearer the ray origin than the renderer's origin offset (util.h:8)
+# count as ties against the reference: bounce rays start EPS2 along their
+# direction, and a grazing one passes within rounding of the surface it
+# left, so which FP32 world->object transform sees that surface is noise.
+EPS2 = 1e-3
 # Occlusion disagreements with the reference that are not ties: none; ties
 # at most 1 in 500 shadow rays.
 OCCL_TIE_FRAC = 1.0 / 500
@@ -91,7 +96,8 @@ def _dump(what, **arrays):
 def _check_hits_vs_reference(rd, rays, hits, what):
     _need_ref()
     ref = ol.ref_trace(rd.ptr, rays)
-    same, ties, bad = ol.classify(rd.ptr, rays, hits, ref, RCP_T, RCP_B)
+    same, ties, bad = ol.classify(rd.ptr, rays, hits, ref, RCP_T, RCP_B,
+                                  eps_origin=EPS2)
     n = len(rays)
     # A disagreement beyond the tie bounds is the reference's error when the
     # GPU holds the FP64 closest hit (brute force over every entered

@@ -168,37 +168,3 @@ def test_gltf_scene_renders_like_the_in_memory_scene(gpu, tmp_path):
         accs.append(acc)
         rd.close()
     assert np.array_equal(accs[0].view(np.uint32), accs[1].view(np.uint32))
-
-
-@pytest.mark.parametrize("fam,w,h,spp,depth", [
-    (api.SCENE_SMALL, 640, 360, 1, 5), (api.SCENE_SCALE, 480, 270, 4, 8),
-    (api.SCENE_STRESS, 320, 180, 1, 16)])
-def test_packet_camera_rays(gpu, fam, w, h, spp, depth):
-    """Coherent (packet) traversal of the camera rays (cfg.reserved[4]):
-    the frame's bounce-0 hits equal the single-ray kernel's on the same
-    rays (traced again through rendgpu_trace_rays), apart from hits tied in
-    t, and the image matches the single-ray frame."""
-    scene = api.Scene(fam, 1)
-    rd = api.RenderData(scene, w, h, spp)
-    gp = api.GpuRenderer(rd, max_depth=depth, seed=4, packet=True).upload()
-    gp.capture([0], w * h * spp)
-    samples = rd.rd.samples
-    rays_p = gp.frame()
-    rd.rd.samples = samples
-    gp.readback(1)
-    acc_p = rd.acc().copy()
-    r0, h0, _, counts = gp.captured(0)
-    assert counts[0] == counts[1] == w * h * spp
-    single = gp.trace(r0)
-    diff = np.nonzero(single.view(np.uint32).reshape(-1, 4)[:, 3] !=
-                      h0.view(np.uint32).reshape(-1, 4)[:, 3])[0]
-    assert len(diff) <= max(2, len(r0) // 10000), len(diff)
-    if len(diff):
-        t0, _ = ol.reintersect(rd.ptr, r0[diff], single["id"][diff])
-        t1, _ = ol.reintersect(rd.ptr, r0[diff], h0["id"][diff])
-        assert np.allclose(t0, t1, rtol=1e-5)
-    gp.close()
-    acc_s, rays_s, _, _ = _gpu_frame(rd, depth, api.MODE_PATH, 4)
-    same = np.all(acc_p == acc_s, axis=2).mean()
-    assert same > 0.999, same
-    assert abs(int(rays_p) - int(rays_s)) <= 0.001 * rays_s

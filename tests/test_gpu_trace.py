@@ -38,7 +38,9 @@ def _check_against_oracle(rd, rays, hits):
     if ties:
         pick = np.array(ties[:32])
         ok = ol.agrees_with_truth(rd.ptr, rays[pick], hits[pick])
-        assert ok.mean() >= 0.9, (ok.mean(), pick[~ok][:5])
+        # at least 9 in 10 (one miss allowed in a small sample)
+        assert ok.sum() >= len(ok) - max(1, len(ok) // 10), \
+            (ok.mean(), pick[~ok][:5])
     # where the triangle agrees, the refined hit is bit-identical
     m = (hits["id"] == ref["id"]) & (hits["t"] < ol.FLT_MAX)
     assert np.array_equal(hits["t"][m].view(np.uint32),
