@@ -482,12 +482,13 @@ def stress_eval(a, dev, flush):
                              a.stress_eval_height, depth, a.stress_ref_spp)
     ev_ = nrc_eval.equal_time(scene, a.stress_eval_width,
                               a.stress_eval_height, depth,
-                              a.stress_nrc_frames, ref)
+                              a.stress_nrc_frames, ref, batch=True)
     out["equal_time"] = {"width": a.stress_eval_width,
                          "height": a.stress_eval_height,
                          "reference_spp": a.stress_ref_spp,
                          "nrc": {k: ev_["nrc"][k] for k in
-                                 ("frames", "ms", "relmse", "rays")},
+                                 ("frames", "ms", "relmse", "rays",
+                                  "batched")},
                          "plain": ev_["plain"],
                          "ratio_plain_over_nrc":
                              ev_["ratio_plain_over_nrc"],

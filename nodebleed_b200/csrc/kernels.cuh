@@ -402,6 +402,21 @@ __global__ void __launch_bounds__(256) k_refine(DScene S, const float4 *rays,
 	}
 }
 
+// Radiance-cache position of a vertex: in its scene's box, clamped to
+// [0,1], with the scene's feature code added to x (nrc_encode decodes it;
+// its box is then the identity), and the path index.
+__device__ __forceinline__ float4 nrc_entry_pos(const ScenePar *P,
+                                                const float pos[3],
+                                                uint32_t path)
+{
+	float v[3];
+	for (int a = 0; a < 3; a++)
+		v[a] = fminf(fmaxf(__fmul_rn(__fsub_rn(pos[a], __ldg(&P->nrc_lo[a])),
+		  __ldg(&P->nrc_inv[a])), 0.0f), 1.0f);
+	return make_float4(__fadd_rn(v[0], __ldg(&P->nrc_off)), v[1], v[2],
+	  __uint_as_float(path));
+}
+
 // Shade the hits of queue `cur` at bounce k; append next rays to queue
 // 1-cur and shadow rays to the shadow queue.
 __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
@@ -533,8 +548,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 							uint32_t qi = atomicAdd(&F.cnt[40], 1u);
 							if (qi < F.nq_cap) {
 								float4 *q = F.nq + 4u * qi;
-								q[0] = make_float4(pos[0], pos[1], pos[2],
-								  __uint_as_float(path));
+								q[0] = nrc_entry_pos(P, pos, path);
 								q[1] = make_float4(-d[0], -d[1], -d[2], T.x);
 								q[2] = make_float4(n[0], n[1], n[2], T.y);
 								q[3] = make_float4(col[0], col[1], col[2],
@@ -546,8 +560,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 							uint32_t ri = atomicAdd(&F.cnt[41], 1u);
 							if (ri < F.nrec_cap) {
 								float4 *q = F.nrec + 6u * ri;
-								q[0] = make_float4(pos[0], pos[1], pos[2],
-								  __uint_as_float(path));
+								q[0] = nrc_entry_pos(P, pos, path);
 								q[1] = make_float4(-d[0], -d[1], -d[2], 0.0f);
 								q[2] = make_float4(n[0], n[1], n[2], 0.0f);
 								q[3] = make_float4(col[0], col[1], col[2],

@@ -59,21 +59,35 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // normal, albedo) -> 64 BF16 features:
 //   0..35  position in the scene box, per axis sin/cos(2^k pi x), k = 0..5
 //   36..43 direction (theta/pi, phi/2pi), sin/cos(2^k pi u), k = 0..1
-//   44..46 (normal + 1) / 2,  47..49 albedo,  50..63 zero
+//   44..46 (normal + 1) / 2,  47..49 albedo,  50..63 zero (in a batch of
+//   scenes: one of them 1, telling scenes 2..15 apart, see nrc_encode)
 struct NrcBox {
 	float lo[3], inv[3]; // position -> [0,1]^3
 };
 
+// The frame's entries hold positions already mapped into their scene's box
+// (k_shade), with the scene's feature code 2 k (k = 1..14, 0 for the first
+// scene of a batch and for single-scene contexts) added to x; `scene_code`
+// decodes it into feature 49 + k and the box is then the identity.
 __device__ __forceinline__ void nrc_encode(const float *in, const NrcBox &B,
-                                           uint4 *out)
+                                           uint4 *out, bool scene_code = false)
 {
 	float f[64];
 #pragma unroll
 	for (int i = 0; i < 64; i++)
 		f[i] = 0.0f;
+	float px = in[0];
+	if (scene_code) {
+		int k = (int)floorf(px * 0.5f);
+		if (k >= 1 && k <= 14) {
+			px = px - (float)(2 * k);
+			f[49 + k] = 1.0f;
+		}
+	}
 #pragma unroll
 	for (int a = 0; a < 3; a++) {
-		float x = fminf(fmaxf((in[a] - B.lo[a]) * B.inv[a], 0.0f), 1.0f);
+		float x = fminf(fmaxf(((a == 0 ? px : in[a]) - B.lo[a]) * B.inv[a],
+		  0.0f), 1.0f);
 #pragma unroll
 		for (int k = 0; k < 6; k++) {
 			float s, c;
@@ -315,7 +329,8 @@ template <bool Q>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
              float4 *out, const uint32_t *ncount, uint32_t *err,
-             const float4 *qe, NrcBox box, float4 *pL, uint32_t npath)
+             const float4 *qe, NrcBox box, float4 *pL, uint32_t npath,
+             bool scode)
 {
 	if (ncount)
 		n = min(*ncount, n);
@@ -352,7 +367,7 @@ k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
 				  d = __ldg(e + 3);
 				float raw[12] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z,
 				  d.x, d.y, d.z};
-				nrc_encode(raw, box, pk);
+				nrc_encode(raw, box, pk, scode);
 				meta_next = make_float4(a.w, b.w, c.w, d.w);
 			} else {
 #pragma unroll
@@ -961,7 +976,8 @@ __global__ void k_nrc_encode(const float *raw, uint32_t n, NrcBox B,
 // direction, normal and albedo in .xyz.
 __global__ void k_nrc_encode_entries(const float4 *e, uint32_t stride,
                                      const uint32_t *count, uint32_t cap,
-                                     NrcBox B, __nv_bfloat16 *feats)
+                                     NrcBox B, __nv_bfloat16 *feats,
+                                     bool scode)
 {
 	uint32_t n = min(*count, cap);
 	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -970,7 +986,8 @@ __global__ void k_nrc_encode_entries(const float4 *e, uint32_t stride,
 		float4 a = q[0], b = q[1], c = q[2], d = q[3];
 		float raw[12] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z,
 		  d.x, d.y, d.z};
-		nrc_encode(raw, B, reinterpret_cast<uint4 *>(feats + 64ull * i));
+		nrc_encode(raw, B, reinterpret_cast<uint4 *>(feats + 64ull * i),
+		  scode);
 	}
 }
 

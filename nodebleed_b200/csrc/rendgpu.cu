@@ -91,6 +91,7 @@ struct SceneHost {
 	// 8-bit resolve (rendgpu_set_resolve): 0 = the reference's pack
 	uint32_t resolve = 0;
 	float    exposure = 1.0f;
+	NrcBox   nbox{}; // radiance-cache encoding box (rendgpu_upload_dynamic)
 };
 
 struct Ctx {
@@ -693,16 +694,21 @@ int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out)
 	k_mlp_fwd_tc<false><<<grid, kTcThreads, smem, c->stream>>>(
 	  c->mlp_wbf.as<__nv_bfloat16>(), static_cast<const __nv_bfloat16 *>(feats),
 	  n, out, nullptr, c->berr.as<uint32_t>() + 1, nullptr, c->box, nullptr,
-	  0u);
+	  0u, false);
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
 
-// The frame's cache queries (min(*count, cap) entries of 4 float4, made on
-// the device): encode, infer and add each output to its path's radiance in
-// one kernel.
+// Identity encoding box: the frame's entries carry positions k_shade has
+// mapped into their scene's box already (with the scene's feature code).
+constexpr NrcBox kUnitBox = {{0.0f, 0.0f, 0.0f}, {1.0f, 1.0f, 1.0f}};
+
+// Cache queries (min(*count, cap) entries of 4 float4, made on the device):
+// encode, infer and add each output to its path's radiance in one kernel.
+// frame: entries written by k_shade (positions in their scene's box, scene
+// features); else world positions in the context's box.
 int nrc_query(Ctx *c, const float4 *q, const uint32_t *count, uint32_t cap,
-              float4 *pL, uint32_t npath, uint32_t *errs)
+              float4 *pL, uint32_t npath, uint32_t *errs, bool frame)
 {
 	if (cap == 0)
 		return 0;
@@ -713,7 +719,7 @@ int nrc_query(Ctx *c, const float4 *q, const uint32_t *count, uint32_t cap,
 		return rc;
 	k_mlp_fwd_tc<true><<<grid, kTcThreads, smem, c->stream>>>(
 	  c->mlp_wbf.as<__nv_bfloat16>(), nullptr, cap, nullptr, count, errs, q,
-	  c->box, pL, npath);
+	  frame ? kUnitBox : c->box, pL, npath, frame);
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -828,6 +834,14 @@ int frame_params(Ctx *c, bool nrc, FrameArgs *A)
 		P.inv = 1.0f / (float)(rd->samples + rd->spp);
 		P.resolve = h.resolve;
 		P.exposure = h.exposure;
+		// one cache serves a batch: each scene in its own box, scenes
+		// 2..15 with a feature of their own (scene 16 shares scene 2's)
+		for (int a = 0; a < 3; a++) {
+			P.nrc_lo[a] = h.nbox.lo[a];
+			P.nrc_inv[a] = h.nbox.inv[a];
+		}
+		P.nrc_off = i == 0 ? 0.0f : (float)(2u * ((uint32_t)(i - 1) % 14u +
+		  1u));
 		P.bg[0] = rd->bgcol.x;
 		P.bg[1] = rd->bgcol.y;
 		P.bg[2] = rd->bgcol.z;
@@ -998,7 +1012,7 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		E->nrc = c->nev;
 		ev_record(c);
 		rc = nrc_query(c, F.nq, F.cnt + 40, c->nq_cap, F.pL, c->npaths,
-		  F.cnt + 3);
+		  F.cnt + 3, true);
 		if (rc)
 			return rc;
 		c->st.launches += 1;
@@ -1015,8 +1029,8 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		k_nrc_targets<<<grid_for(c, c->nrec_cap, 256), 256, 0, c->stream>>>(
 		  F.nrec, F.cnt + 41, c->nrec_cap, F.pL, c->rtgt.as<float4>());
 		k_nrc_encode_entries<<<grid_for(c, c->nrec_cap, 128), 128, 0,
-		  c->stream>>>(F.nrec, 6u, F.cnt + 41, c->nrec_cap, c->box,
-		  c->rfeat.as<__nv_bfloat16>());
+		  c->stream>>>(F.nrec, 6u, F.cnt + 41, c->nrec_cap, kUnitBox,
+		  c->rfeat.as<__nv_bfloat16>(), true);
 		NB_CK(c, cudaGetLastError());
 		for (uint32_t s = 0; s < nrc_steps(c); s++) {
 			rc = nrc_train(c, c->rfeat.p, c->rtgt.as<float4>(), kNrcBatch, 1,
@@ -1452,6 +1466,8 @@ int dyn_prepare(Ctx *c, uint64_t *bytes)
 	return 0;
 }
 
+uint32_t device_tlas_limit(const Ctx *c);
+
 // New object->world matrices (device, 16 floats each, rd->insts order) ->
 // instance records, world boxes, TLAS (built, or refitted when asked and a
 // device build exists) and light table, all on the context's stream.
@@ -1500,9 +1516,10 @@ int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
 		A.ranges = c->dyn_ranges.as<uint2>();
 		A.order = c->dyn_order.as<uint32_t>();
 		A.info = c->dyn_info.as<uint32_t>();
-		// the host-converted TLAS sized the traversal stack; the device
-		// tree stays within its depth (at least a balanced tree's)
-		A.depth_limit = h.tlas_depth;
+		// the uploaded trees sized the traversal stack; the device tree
+		// stays within what it holds
+		A.depth_limit = device_tlas_limit(c);
+		h.tlas_depth = c->tlas_depth = A.depth_limit;
 		k_tlas_build<<<1, kTbWarps * 32, 0, c->stream>>>(A);
 	} else {
 		k_tlas_refit<<<grid_for(c, nn * 32u, 256), 256, 0, c->stream>>>(
@@ -1536,6 +1553,20 @@ bool rebuilds_tlas(const Ctx *c)
 	return !c->batch && c->sc.size() == 1 && !(c->cfg.reserved[4] & 1u);
 }
 
+// Depth a device-built TLAS may reach: the levels the traversal stack chosen
+// for the uploaded trees leaves beside the deepest BLAS (at least the
+// converted TLAS's depth).  SAH splits then rarely meet the cap, and the
+// context's TLAS depth becomes that bound, so the stack stays the same.
+uint32_t device_tlas_limit(const Ctx *c)
+{
+	uint32_t need = need_stack(c), st = 0;
+	for (int s : kStacks)
+		if (!st && need <= (uint32_t)s)
+			st = (uint32_t)s;
+	uint32_t room = st ? st - c->blas_depth - 2u : 0u;
+	return std::max(room, c->tlas_depth);
+}
+
 int rebuild_tlas_tight(Ctx *c)
 {
 	SceneHost &h = c->sc[0];
@@ -1559,11 +1590,12 @@ int rebuild_tlas_tight(Ctx *c)
 	A.ranges = c->dyn_ranges.as<uint2>();
 	A.order = c->dyn_order.as<uint32_t>();
 	A.info = c->dyn_info.as<uint32_t>();
-	A.depth_limit = h.tlas_depth;
+	A.depth_limit = device_tlas_limit(c);
 	k_tlas_build<<<1, kTbWarps * 32, 0, c->stream>>>(A);
 	NB_CK(c, cudaGetLastError());
 	NB_CK(c, cudaStreamSynchronize(c->stream));
 	h.tlas_root = 0u;
+	h.tlas_depth = c->tlas_depth = A.depth_limit;
 	c->dyn_built = true;
 	return 0;
 }
@@ -1618,9 +1650,9 @@ int upload_dynamic_all(Ctx *c)
 		h.light_off = (uint32_t)lights.size();
 		lights.insert(lights.end(), h.lights.begin(), h.lights.end());
 	}
-	{
-		// radiance-cache encoding box: the first scene's instance bounds
-		const nb_rdata *rd = c->sc[0].rd;
+	for (SceneHost &h : c->sc) {
+		// radiance-cache encoding box of each scene: its instance bounds
+		const nb_rdata *rd = h.rd;
 		float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
 		float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
 		for (uint32_t i = 0; i < rd->instcnt; i++) {
@@ -1633,10 +1665,11 @@ int upload_dynamic_all(Ctx *c)
 			}
 		}
 		for (int a = 0; a < 3; a++) {
-			c->box.lo[a] = lo[a];
-			c->box.inv[a] = hi[a] > lo[a] ? 1.0f / (hi[a] - lo[a]) : 1.0f;
+			h.nbox.lo[a] = lo[a];
+			h.nbox.inv[a] = hi[a] > lo[a] ? 1.0f / (hi[a] - lo[a]) : 1.0f;
 		}
 	}
+	c->box = c->sc[0].nbox; // the box of the query / encode calls
 	c->ninst = (uint32_t)gi.size();
 	// device-side updates (single-scene contexts) rebuild the TLAS in place:
 	// room for max(instances, 1) nodes
@@ -2492,7 +2525,7 @@ int rendgpu_nrc_query_device(struct rdata *rdp, const float *entries,
 	NB_CK(c, cudaSetDevice(c->device));
 	return nrc_query(c, reinterpret_cast<const float4 *>(entries), nullptr, n,
 	  reinterpret_cast<float4 *>(radiance), npath,
-	  c->berr.as<uint32_t>() + 1);
+	  c->berr.as<uint32_t>() + 1, false);
 }
 
 int rendgpu_nrc_train_device(struct rdata *rdp, const void *feats,
@@ -2798,7 +2831,7 @@ int rendgpu_batch_init(struct rdata *const *rds, uint32_t n,
                        const struct rendgpu_cfg *cfg,
                        struct rendgpu_batch **out)
 {
-	if (!out || !cfg || cfg->mode == RENDGPU_MODE_NRC)
+	if (!out || !cfg)
 		return RENDGPU_EINVAL;
 	Ctx *c = nullptr;
 	int rc = new_ctx(reinterpret_cast<nb_rdata *const *>(rds), n, max_depth,

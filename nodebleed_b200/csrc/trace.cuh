@@ -45,6 +45,10 @@ struct ScenePar {
 	float    fwd[3], aspect;
 	float    fdist, focrad, pad2[2];
 	uint64_t seed, pad3;
+	// radiance cache: position -> [0,1]^3 in this scene's box, plus nrc_off
+	// (0 for scene 0, else 2 k: the scene's one-hot feature k, 1..14)
+	float    nrc_lo[3], nrc_off;
+	float    nrc_inv[3], pad4;
 };
 
 struct DScene {

@@ -20,6 +20,15 @@ def reference(scene, w, h, depth, spp, seed=99, spp_per_frame=16):
     return img.astype(np.float32)
 
 
+def relmse_host(acc, samples, ref):
+    """The relMSE of rendgpu_relmse_device computed on the host in FP64:
+    mean of (x - r)^2 / (r^2 + 0.01) with x = acc * (1 / samples as FP32)."""
+    inv = np.float32(1.0) / np.float32(samples)
+    x = np.asarray(acc, np.float32).astype(np.float64) * np.float64(inv)
+    r = np.asarray(ref, np.float32).astype(np.float64)
+    return float(np.mean((x - r) ** 2 / (r * r + 0.01)))
+
+
 def _load_cache_kernels(depth):
     """Two radiance-cache frames of a tiny scene on a throwaway context, so
     the first launch of each cache kernel (module loading) is not counted
@@ -39,24 +48,42 @@ def equal_time(scene, w, h, depth, frames, ref, seed=1, **nrc_kw):
     same device time; relMSE of both accumulated images against `ref`.
     nrc_kw go to the cache renderer (nrc_warmup, nrc_end, nrc_lr)."""
     import torch
+    batch = nrc_kw.pop("batch", False)
     _load_cache_kernels(depth)
     ref_dev = torch.from_numpy(np.ascontiguousarray(ref, np.float32)).cuda()
     out = {}
     rd = api.RenderData(scene, w, h, 1)
-    gn = api.GpuRenderer(rd, max_depth=depth, mode=api.MODE_NRC, seed=seed,
-                         timing=True, **nrc_kw).upload()
+    if batch:
+        # the cache frames through the batch API (one launch sequence over
+        # shared queues, as a batch of scenes runs them)
+        gn = api.BatchRenderer([rd], max_depth=depth, mode=api.MODE_NRC,
+                               seed=seed, timing=True).upload()
+
+        def stats():
+            return gn.stats()[0]
+
+        def err():
+            gn.readback(1)
+            return relmse_host(rd.acc(), rd.rd.samples, ref)
+    else:
+        gn = api.GpuRenderer(rd, max_depth=depth, mode=api.MODE_NRC,
+                             seed=seed, timing=True, **nrc_kw).upload()
+        stats = gn.stats
+
+        def err():
+            return gn.relmse(ref_dev.data_ptr())
     t_nrc, rays_nrc, curve = 0.0, 0, []
     for f in range(frames):
         rays_nrc += gn.frame()
-        st = gn.stats()
+        st = stats()
         t_nrc += st["ms_frame"]
         if f in (0, frames // 4, frames // 2, frames - 1):
-            curve.append((f + 1, t_nrc, gn.relmse(ref_dev.data_ptr())))
-    out["nrc"] = {"frames": frames, "ms": t_nrc,
-                  "relmse": gn.relmse(ref_dev.data_ptr()),
+            curve.append((f + 1, t_nrc, err()))
+    out["nrc"] = {"frames": frames, "ms": t_nrc, "relmse": err(),
                   "rays": rays_nrc, "queries_last": st["nrc_queries"],
                   "records_last": st["nrc_records"],
-                  "ms_cache_last": st["ms_nrc"], "curve": curve}
+                  "ms_cache_last": st["ms_nrc"], "curve": curve,
+                  "batched": bool(batch)}
     gn.close()
     rd.close()
     rd = api.RenderData(scene, w, h, 1)

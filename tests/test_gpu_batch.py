@@ -156,10 +156,53 @@ def test_tuned_setting_persists(gpu, tmp_path):
     assert len(open(path).read().splitlines()) == 2
 
 
-def test_batch_rejects_radiance_cache_mode(gpu):
-    rds = _rdatas(SCENES[:1])
-    with pytest.raises(api.RendgpuError):
-        api.BatchRenderer(rds, mode=api.MODE_NRC)
+def test_batched_radiance_cache(gpu):
+    """RENDGPU_MODE_NRC in a batch: one cache serves every scene (each in
+    its own encoding box, the scenes told apart by input features).  The
+    warm-up frame, which traces every path unbiased while the cache trains,
+    is bit-identical to each scene's own warm-up frame; later frames end
+    paths in the cache of every scene, and its images stay as close to a
+    converged reference as each scene's own cache gets."""
+    from nodebleed_b200 import nrc_eval
+    scenes = SCENES[1:3]
+    depths = [s[5] for s in scenes]
+    rds = _rdatas(scenes)
+    b = api.BatchRenderer(rds, max_depth=depths, mode=api.MODE_NRC,
+                          seed=7).upload()
+    b.frame()
+    b.readback(1)
+    warm = [rd.acc().copy() for rd in rds]
+    tot, _ = b.stats()
+    assert tot["nrc_records"] > 0 and tot["nrc_queries"] == 0
+    frames = 6
+    for _ in range(frames - 1):
+        b.frame()
+        tot, per = b.stats()
+        assert tot["nrc_queries"] > 0 and tot["device_errors"] == 0
+    b.readback(1)
+    got = [rd.acc() / rd.rd.samples for rd in rds]
+    b.close()
+
+    def relmse(x, r):
+        return float(np.mean((x - r) ** 2 / (r ** 2 + 1e-2)))
+    for i, (fam, seed, w, h, spp, depth) in enumerate(scenes):
+        rd = _rdatas([scenes[i]])[0]
+        g = api.GpuRenderer(rd, max_depth=depth, mode=api.MODE_NRC,
+                            seed=7).upload()
+        g.frame()
+        g.readback(1)
+        assert np.array_equal(rd.acc(), warm[i]), i
+        for _ in range(frames - 1):
+            g.frame()
+        g.readback(1)
+        alone = rd.acc() / rd.rd.samples
+        g.close()
+        ref = nrc_eval.reference(api.Scene(fam, seed), w, h, depth, 256)
+        e_b, e_a = relmse(got[i], ref), relmse(alone, ref)
+        print(f"scene {i}: relMSE batched cache {e_b:.4f}, own cache "
+              f"{e_a:.4f}")
+        assert np.isfinite(got[i]).all()
+        assert e_b <= 3.0 * e_a + 0.01, (i, e_b, e_a)
 
 
 @pytest.mark.parametrize("tune", [{"sort": 1}, {"sort": 1, "queue": 9000}])

@@ -103,8 +103,12 @@ def test_forward_matches_oracle(gpu, n):
     emean = np.mean(np.abs(got - ref)) / scale
     print(f"forward n={n}: max error {emax:.3e}, mean error {emean:.3e} "
           "of the output scale")
-    assert emax < 1e-2
-    assert emean < 1e-3
+    # The oracle rounds the same tensors to BF16, so only the order of the
+    # FP32 accumulation differs: measured at most 3.6e-3 (a hidden
+    # activation whose BF16 rounding flips, carried to the output) and a
+    # mean of 7.3e-7 of the output scale.
+    assert emax < 8e-3
+    assert emean < 1e-5
     gr.close()
 
 
@@ -204,15 +208,18 @@ def test_gradients_match_oracle(gpu, n):
     got = g.cpu().numpy().astype(np.float64)
     w = gr.nrc_weights()
     ref_loss, ref = no.loss_grad(w, f64, t, bf=True)
+    # with the oracle rounding the same tensors to BF16 only the FP32
+    # accumulation order differs: measured loss error <= 3.4e-7 and
+    # per-layer relative L2 errors <= 1.1e-5
     lerr = abs(loss.value - ref_loss) / ref_loss
-    assert lerr < 1e-3
+    assert lerr < 1e-5
     errs = []
     for l in range(6):
         sl = slice(l * no.SQ, (l + 1) * no.SQ) if l < 5 else \
             slice(5 * no.SQ, 5 * no.SQ + 3 * 64)
         err = np.linalg.norm(got[sl] - ref[sl]) / np.linalg.norm(ref[sl])
         errs.append(err)
-        assert err < 3e-2, (l, err)
+        assert err < 1e-4, (l, err)
     print(f"gradients n={n}: loss error {lerr:.3e}, per-layer relative L2 "
           "errors " + " ".join(f"{e:.3e}" for e in errs))
     assert (got[5 * no.SQ + 3 * 64:] == 0).all()
