@@ -437,7 +437,12 @@ int rendgpu_tune_load(struct rdata *rd, const char *path);
  * rend_prepdynamic, rend_resaccum); max_depth[i] bounds scene i's paths
  * (NULL: cfg->max_depth for all).  Every scene's image is bit-identical to
  * the same scene rendered alone with the same cfg.  At most 4096 instances
- * over all scenes (hit ids keep 12 instance bits); PATH and PRIMARY modes.
+ * over all scenes (hit ids keep 12 instance bits).  In RENDGPU_MODE_NRC one
+ * radiance cache serves the batch: each scene's positions are encoded in
+ * its own box, and scenes 2..15 get an input feature of their own (scene
+ * 16 shares scene 2's); the warm-up frame is bit-identical to each scene's
+ * alone, later frames depend on what all scenes trained.  Cache frames are
+ * launched directly, not from a graph. */
  * batch_render renders one frame of every scene (rd->samples of each keys
  * its random streams; the caller bumps samples afterwards, as main.c does)
  * and adds each scene's rays to its rd->rays. */

@@ -202,7 +202,9 @@ def test_batched_radiance_cache(gpu):
         print(f"scene {i}: relMSE batched cache {e_b:.4f}, own cache "
               f"{e_a:.4f}")
         assert np.isfinite(got[i]).all()
-        assert e_b <= 3.0 * e_a + 0.01, (i, e_b, e_a)
+        # measured 0.0006 / 0.0006 and 0.0028 / 0.0027; the order of the
+        # device-side record appends varies from run to run
+        assert e_b <= 1.5 * e_a + 5e-4, (i, e_b, e_a)
 
 
 @pytest.mark.parametrize("tune", [{"sort": 1}, {"sort": 1, "queue": 9000}])

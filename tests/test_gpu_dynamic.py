@@ -213,7 +213,9 @@ def test_upload_rebuild_matches_reference_tlas(gpu, fam, param):
     rd_r = api.RenderData(scene, 240, 135, 1)
     gt = api.GpuRenderer(rd_t, max_depth=6, seed=3).upload()
     gr = api.GpuRenderer(rd_r, max_depth=6, seed=3, ref_tlas=True).upload()
-    assert gt.stats()["max_stack"] == gr.stats()["max_stack"]
+    # the same traversal stack (the rebuilt tree may use the levels that
+    # stack has to spare beside the deepest BLAS)
+    assert gt.get_tune()["stack"] == gr.get_tune()["stack"]
     rays = np.concatenate([ol.random_rays(rd_t, 60000, seed=6, spread=20.0),
                            ol.camera_rays(rd_t)[::2]])
     assert np.array_equal(_bits(gt.trace(rays)), _bits(gr.trace(rays)))
