@@ -442,7 +442,7 @@ int rendgpu_tune_load(struct rdata *rd, const char *path);
  * its own box, and scenes 2..15 get an input feature of their own (scene
  * 16 shares scene 2's); the warm-up frame is bit-identical to each scene's
  * alone, later frames depend on what all scenes trained.  Cache frames are
- * launched directly, not from a graph. */
+ * launched directly, not from a graph.
  * batch_render renders one frame of every scene (rd->samples of each keys
  * its random streams; the caller bumps samples afterwards, as main.c does)
  * and adds each scene's rays to its rd->rays. */

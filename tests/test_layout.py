@@ -43,6 +43,22 @@ def _header_symbols(path):
     return sorted(set(re.findall(r"\b(rendgpu_[a-z_]+)\s*\(", text)))
 
 
+@pytest.mark.parametrize("lang,std", [("c", "-std=c11"),
+                                      ("c++", "-std=c++17")])
+def test_header_compiles_alone(tmp_path, lang, std):
+    """include/rendgpu.h is self-contained C and C++ (what a binding's
+    build compiles)."""
+    import subprocess
+    src = tmp_path / ("t.c" if lang == "c" else "t.cpp")
+    src.write_text('#include "rendgpu.h"\nint main(void) { return '
+                   'RENDGPU_OK; }\n')
+    cc = "gcc" if lang == "c" else "g++"
+    r = subprocess.run([cc, std, "-Wall", "-Wextra", "-Werror",
+                        "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
+                        str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_gpu_library_exports_every_header_symbol():
     syms = _header_symbols(os.path.join(ROOT, "include", "rendgpu.h"))
     assert len(syms) >= 17
