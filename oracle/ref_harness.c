@@ -387,3 +387,164 @@ int refh_gltf_import(const char *path, unsigned int *counts, float *vrts,
 	scene_release(&s);
 	return 0;
 }
+
+// rend.c:171, declared by main.c:114.
+void mulpos(float *ox, float *oy, float *oz, float m[16], float x, float y,
+            float z);
+
+// A render data built entirely by nodebleed's own host code from a glTF
+// file, in the order its frame loop runs (main.c:226-249, 252-270):
+// imp_gltf_f, rend_init, rend_resaccum, the mesh/material/instance copy,
+// rend_prepstatic, scene_updtransforms and scene_updcams, the instance
+// update, rend_prepdynamic and the camera constants.  The copy (cpy_rdata
+// main.c:53-112), the instance update (upd_rinsts main.c:117-157) and the
+// camera constants (upd_rcam main.c:159-195) sit in main.c, which needs
+// SDL2, so their steps are written out below; they call the reference's own
+// mat4_inv, mulpos and bcmin8/bcmax8.  NULL on failure; free with
+// refh_rdata_free.  rend_staticinit must have run.
+struct rdata *refh_gltf_rdata(const char *path, unsigned int w,
+                              unsigned int h, unsigned int spp)
+{
+	struct scene s;
+	memset(&s, 0, sizeof(s));
+	char name[4096];
+	size_t len = strlen(path);
+	if (len >= sizeof(name))
+		return NULL;
+	memcpy(name, path, len + 1);
+	imp_gltf_f(&s, name);
+	s.bgcol = (struct vec3){0.4f, 0.4f, 0.4f}; // main.c:230
+	unsigned int maxtris = 0, maxinsts = 0;
+	for (unsigned int k = 0; k < s.meshcnt; k++)
+		maxtris += s.meshes[k].icnt / 3;
+	for (unsigned int i = 0; i < s.nodecnt; i++)
+		if (s.objs[i].flags & MESH)
+			maxinsts++;
+	struct rdata *rd = aligned_alloc(64, (sizeof(*rd) + 63) & ~(size_t)63);
+	if (!rd) {
+		scene_release(&s);
+		return NULL;
+	}
+	memset(rd, 0, sizeof(*rd));
+	rend_init(rd, s.mtlmax, maxtris, maxinsts, spp);
+	rend_resaccum(rd, w, h);
+
+	// meshes: triangles and per-triangle normals with the material of
+	// their run; each mesh's first triangle and count
+	unsigned int *triofs = calloc(s.meshcnt ? s.meshcnt : 1, sizeof(int));
+	unsigned int *tricnt = calloc(s.meshcnt ? s.meshcnt : 1, sizeof(int));
+	unsigned int t = 0;
+	for (unsigned int k = 0; k < s.meshcnt; k++) {
+		const struct mesh *m = &s.meshes[k];
+		const unsigned int *ix = m->inds;
+		triofs[k] = t;
+		for (unsigned int r = 0; r < m->mcnt; r++)
+			for (unsigned int q = 0; q < m->mtls[r].tricnt; q++) {
+				rd->tris[t].v0 = m->vrts[ix[0]];
+				rd->tris[t].v1 = m->vrts[ix[1]];
+				rd->tris[t].v2 = m->vrts[ix[2]];
+				rd->nrms[t].n0 = m->nrms[ix[0]];
+				rd->nrms[t].n1 = m->nrms[ix[1]];
+				rd->nrms[t].n2 = m->nrms[ix[2]];
+				rd->nrms[t].mtlid = m->mtls[r].mtlid;
+				ix += 3;
+				t++;
+			}
+		tricnt[k] = m->icnt / 3;
+	}
+	for (unsigned int i = 0; i < s.mtlcnt; i++)
+		memcpy(&rd->mtls[i], &s.mtls[i], sizeof(*rd->mtls));
+	unsigned int n = 0;
+	for (unsigned int i = 0; i < s.nodecnt; i++) {
+		struct obj *o = &s.objs[i];
+		if (!(o->flags & MESH))
+			continue;
+		memset(&rd->insts[n], 0, sizeof(rd->insts[n]));
+		rd->insts[n].flags = o->flags;
+		rd->insts[n].triofs = triofs[o->objid];
+		rd->insts[n].tricnt = tricnt[o->objid];
+		o->instid = (int)n++;
+	}
+	rd->instcnt = n;
+	rd->bgcol = s.bgcol;
+	free(triofs);
+	free(tricnt);
+
+	rend_prepstatic(rd);
+	scene_updtransforms(&s);
+	scene_updcams(&s);
+
+	// instances: world->object 3x4 from the inverse of the node's matrix,
+	// world box from the 8 corners of the BLAS root's box after the matrix
+	for (unsigned int i = 0; i < s.nodecnt; i++) {
+		struct obj *o = &s.objs[i];
+		if (!(o->flags & MESH))
+			continue;
+		struct rinst *ri = &rd->insts[o->instid];
+		float *g = s.tfmats[i].glob;
+		float inv[16];
+		mat4_inv(inv, g);
+		memcpy(ri->globinv, inv, sizeof(ri->globinv));
+		struct bnode8 *root = &rd->bnodes[ri->triofs << 1];
+		float lo[3] = {bcmin8(root->minx8)[0], bcmin8(root->miny8)[0],
+		  bcmin8(root->minz8)[0]};
+		float hi[3] = {bcmax8(root->maxx8)[0], bcmax8(root->maxy8)[0],
+		  bcmax8(root->maxz8)[0]};
+		struct vec3 mi = {FLT_MAX, FLT_MAX, FLT_MAX};
+		struct vec3 ma = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+		for (int c = 0; c < 8; c++) {
+			struct vec3 v;
+			mulpos(&v.x, &v.y, &v.z, g, c & 1 ? lo[0] : hi[0],
+			  c & 2 ? lo[1] : hi[1], c & 4 ? lo[2] : hi[2]);
+			mi = vec3_min(mi, v);
+			ma = vec3_max(ma, v);
+		}
+		rd->aabbs[o->instid] = (struct aabb){.min = mi, .max = ma};
+	}
+	rend_prepdynamic(rd);
+
+	// camera constants of the current camera
+	const struct cam *c = &s.cams[s.currcam];
+	float aspect = (float)w / (float)h;
+	float tv = tanf(0.5f * c->vfov * PI / 180.0f);
+	float tf = tanf(0.5f * c->focangle * PI / 180.0f);
+	struct rcam *rc = &rd->cam;
+	memset(rc, 0, sizeof(*rc));
+	rc->eye = c->eye;
+	rc->tanvfov = tv;
+	rc->ri = c->ri;
+	rc->focdist = c->focdist;
+	rc->up = c->up;
+	rc->tanfangle = tf;
+	rc->fwd = c->fwd;
+	rc->aspect = aspect;
+	rc->eyex8 = _mm256_set1_ps(c->eye.x);
+	rc->eyey8 = _mm256_set1_ps(c->eye.y);
+	rc->eyez8 = _mm256_set1_ps(c->eye.z);
+	rc->rix8 = _mm256_set1_ps(c->ri.x);
+	rc->riy8 = _mm256_set1_ps(c->ri.y);
+	rc->riz8 = _mm256_set1_ps(c->ri.z);
+	rc->upx8 = _mm256_set1_ps(c->up.x);
+	rc->upy8 = _mm256_set1_ps(c->up.y);
+	rc->upz8 = _mm256_set1_ps(c->up.z);
+	rc->fwdx8 = _mm256_set1_ps(c->fwd.x);
+	rc->fwdy8 = _mm256_set1_ps(c->fwd.y);
+	rc->fwdz8 = _mm256_set1_ps(c->fwd.z);
+	rc->rw8 = _mm256_set1_ps(1.0f / (float)w);
+	rc->rh8 = _mm256_set1_ps(1.0f / (float)h);
+	rc->aspect8 = _mm256_set1_ps(aspect);
+	rc->fdist8 = _mm256_set1_ps(c->focdist);
+	rc->fovfdist8 = _mm256_set1_ps(2.0f * tv * c->focdist);
+	rc->focangle8 = _mm256_set1_ps(tf);
+	rc->focrad8 = _mm256_set1_ps(tf * c->focdist);
+	scene_release(&s);
+	return rd;
+}
+
+void refh_rdata_free(struct rdata *rd)
+{
+	if (!rd)
+		return;
+	rend_release(rd);
+	free(rd);
+}

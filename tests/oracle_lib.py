@@ -87,6 +87,47 @@ def ref():
     return _REF
 
 
+class RefRenderData:
+    """A struct rdata built entirely by the reference's own host code from a
+    glTF file (refh_gltf_rdata): its importer, BVH builds, matrix inverse
+    and camera constants.  Offers what GpuRenderer and the oracle read from
+    an api.RenderData (ptr, rd, acc, users, close)."""
+
+    def __init__(self, path, w, h, spp):
+        from nodebleed_b200 import api
+        R = ref()
+        if R is None:
+            raise RuntimeError("reference build not present")
+        R.refh_gltf_rdata.restype = C.c_void_p
+        R.refh_gltf_rdata.argtypes = [C.c_char_p, C.c_uint32, C.c_uint32,
+                                      C.c_uint32]
+        R.refh_rdata_free.argtypes = [C.c_void_p]
+        self._R, self._api = R, api
+        self.ptr = R.refh_gltf_rdata(os.fsencode(path), w, h, spp)
+        if not self.ptr:
+            raise RuntimeError("refh_gltf_rdata failed")
+        self.users = []
+        self.buf = np.zeros(w * h, np.uint32)
+        self.rd.buf = self.buf.ctypes.data
+
+    @property
+    def rd(self):
+        return self._api.RData.from_address(self.ptr)
+
+    def acc(self):
+        r = self.rd
+        a = (C.c_float * (r.width * r.height * 3)).from_address(r.acc)
+        return np.ctypeslib.as_array(a).reshape(r.height, r.width, 3)
+
+    def close(self):
+        if self.ptr:
+            for u in self.users:
+                u.close()
+            self.users = []
+            self._R.refh_rdata_free(self.ptr)
+            self.ptr = None
+
+
 def ggx_sample(n, wo, alpha, f0, r0, r1):
     """(ok, wi, weight) of the oracle's GGX sampling step."""
     f = lambda v: np.ascontiguousarray(v, np.float32)

@@ -141,6 +141,68 @@ def test_loader_matches_reference_importer(tmp_path):
     assert np.allclose(ours_cam, cam, rtol=1e-5, atol=1e-5)
 
 
+def test_reference_built_render_data(tmp_path):
+    """The same file through nodebleed's own host code end to end
+    (refh_gltf_rdata: imp_gltf_f, rend_init, the main.c copy, rend_prepstatic,
+    upd_rinsts with its mat4_inv, rend_prepdynamic, upd_rcam) against this
+    library's loader and bridge: triangles, normals, materials and every BLAS
+    byte-identical; instance matrices, boxes and camera within the FP32
+    rounding of the two matrix paths; the oracle's image of both alike."""
+    if ol.ref() is None:
+        pytest.skip("reference build not present")
+    from test_oracle import _lights_numpy
+    src = api.Scene(api.SCENE_SMALL, 1)
+    path = str(tmp_path / "config1.gltf")
+    src.save_gltf(path)
+    w, h = 160, 90
+    ref_rd = ol.RefRenderData(path, w, h, 1)
+    ours = api.Scene.load_gltf(path, extras=False)
+    rd = api.RenderData(ours, w, h, 1)
+    r, q = ref_rd.rd, rd.rd
+    assert (r.instcnt, r.width, r.height, r.spp) == \
+        (q.instcnt, q.width, q.height, q.spp)
+    nt = ours.tris
+    # every word but the pads, which main.c leaves as rend_init's malloc
+    # left them
+    used = {"tris": [0, 1, 2, 4, 5, 6, 8, 9, 10],
+            "nrms": [0, 1, 2, 3, 4, 5, 6, 8, 9, 10]}
+    for f, cols in used.items():
+        a = _arr(getattr(r, f), 12 * nt, np.uint32).reshape(nt, 12)
+        b = _arr(getattr(q, f), 12 * nt, np.uint32).reshape(nt, 12)
+        assert np.array_equal(a[:, cols], b[:, cols]), f
+    nm = ours.s.mtlcnt
+    # the pad word differs: main.c copies sizeof(struct rmtl) = 32 bytes
+    # from each 28-byte struct mtl, so its pad holds the next material's
+    # first word; nothing reads it
+    assert np.array_equal(_arr(r.mtls, 8 * nm, np.uint32).reshape(nm, 8)[:, :7],
+                          _arr(q.mtls, 8 * nm, np.uint32).reshape(nm, 8)[:, :7])
+    ri = _arr(r.insts, 16 * r.instcnt, np.uint32).reshape(-1, 16)
+    qi = _arr(q.insts, 16 * q.instcnt, np.uint32).reshape(-1, 16)
+    assert np.array_equal(ri[:, 12:15], qi[:, 12:15])  # flags, triofs, cnt
+    for ofs, cnt in {(int(a[13]), int(a[14])) for a in qi}:
+        nb = 2 * cnt * 256
+        assert np.array_equal(_arr(r.bnodes + 512 * ofs, nb, np.uint8),
+                              _arr(q.bnodes + 512 * ofs, nb, np.uint8)), ofs
+    assert np.allclose(ri[:, :12].view(np.float32),
+                       qi[:, :12].view(np.float32), rtol=1e-4, atol=1e-5)
+    assert np.allclose(_arr(r.aabbs, 8 * r.instcnt, np.float32),
+                       _arr(q.aabbs, 8 * q.instcnt, np.float32),
+                       rtol=1e-4, atol=1e-4)
+    assert np.allclose(np.frombuffer(bytes(r.cam), np.float32)[:16],
+                       np.frombuffer(bytes(q.cam), np.float32)[:16],
+                       rtol=1e-5, atol=1e-5)
+    assert np.array_equal(np.frombuffer(bytes(r.bgcol), np.uint32),
+                          np.frombuffer(bytes(q.bgcol), np.uint32))
+    lights, area = _lights_numpy(rd)
+    img_r, _ = ol.orc_render(ref_rd, lights, area, 5, seed=4)
+    img_q, _ = ol.orc_render(rd, lights, area, 5, seed=4)
+    err = np.mean((img_r - img_q) ** 2 / (img_q ** 2 + 1e-2))
+    assert err < 1e-4, err
+    assert np.all(img_r == img_q, axis=2).mean() > 0.5
+    ref_rd.close()
+    rd.close()
+
+
 def test_loader_rejects_malformed(tmp_path):
     bad = tmp_path / "bad.gltf"
     bad.write_text('{"asset": {"version": "2.0"}, "meshes": [')

@@ -305,3 +305,32 @@ def test_stack_overflow_is_reported_not_faulted(gpu, scale_rd):
     assert np.array_equal(again.view(np.uint32), good.view(np.uint32))
     assert g.rendgpu_sync(gr.ptr) == 0
     gr.close()
+
+
+def test_reference_built_render_data(gpu, tmp_path):
+    """The drop-in claim end to end: config 1 (640x360, depth 5) written as
+    glTF and turned into a render data by nodebleed's own host code alone
+    (refh_gltf_rdata: imp_gltf_f, the main.c copy, rend_prepstatic,
+    upd_rinsts with its mat4_inv, rend_prepdynamic, upd_rcam).  The GPU frame
+    of that render data against the oracle's, and the frame's rays of
+    bounces 0-2 against the reference's intersect_tlas on it."""
+    _need_ref()
+    src = api.Scene(api.SCENE_SMALL, 1)
+    path = str(tmp_path / "config1.gltf")
+    src.save_gltf(path)
+    rd = ol.RefRenderData(path, 640, 360, 1)
+    acc, rays, lights, area = _gpu_frame(rd, 5, 1)
+    rad, orays = ol.orc_render(rd, lights, area, 5, seed=1)
+    same = float(np.all(acc == rad, axis=2).mean())
+    print(f"reference-built config 1: {same:.5f} of pixels bit-identical, "
+          f"relMSE {relmse(acc, rad):.2e}, rays {rays} vs {orays}")
+    assert same > 0.98, same
+    assert relmse(acc, rad) < 2e-3
+    assert abs(int(rays) - int(orays)) <= 0.01 * orays
+    got = _frame_capture(rd, 5, [0, 1, 2], 60000, seed=1)
+    fr = np.concatenate([got[k][0] for k in got])
+    fh = np.concatenate([got[k][1] for k in got])
+    _check_hits_vs_reference(rd, fr, fh, "reference-built config 1 "
+                             "bounces 0-2")
+    _check_against_oracle(rd, fr, fh)
+    rd.close()
