@@ -81,7 +81,8 @@ struct rendgpu_cfg {
 	                         of 16384 samples per frame (0 = 6); [4] bit 0:
 	                         keep the TLAS rendgpu_upload_dynamic converts
 	                         from rd->bnodes instead of the device rebuild
-	                         over tight instance boxes */
+	                         over tight instance boxes; [5] bit 0: no hash
+	                         grid in the cache's position encoding */
 };
 
 /* A ray for the batch calls: origin, tmax, direction (32 bytes). */
@@ -249,16 +250,29 @@ int rendgpu_trace_rays_device_noalloc(struct rdata *rd,
  * with 5 hidden layers of 64 ReLU units and 3 linear outputs, BF16 on the
  * tensor cores with FP32 master weights and Adam (beta 0.9/0.99, eps 1e-15).
  * Parameters: RENDGPU_NRC_PARAMS floats, layer l (0..4: 64x64, 5: 8x64 of
- * which 3 rows are used) stored [out][in] at offset l * 4096. */
+ * which 3 rows are used) stored [out][in] at offset l * 4096.
+ * The position also goes through a trainable multiresolution hash grid
+ * (Mueller et al. 2022): 8 levels of 2^15 entries of 2 FP32 features,
+ * RENDGPU_NRC_GRID_PARAMS floats, level l at offset l * 65536, entry e at
+ * 2 e; lattices of 16, 28, 52, 95, 172, 312, 565 and 1024 cells per axis
+ * over the scene box, levels 0 and 1 indexed densely (x + (r+1)(y + (r+1)
+ * z)), the others by (x ^ 2654435761 y ^ 805459861 z) mod 2^15.
+ * cfg.reserved[5] bit 0 turns the grid off (its features are then 0). */
 #define RENDGPU_NRC_PARAMS (5 * 4096 + 8 * 64)
+#define RENDGPU_NRC_GRID_PARAMS (8 * 32768 * 2)
 
 /* (Re)initialise the weights (Xavier uniform from `seed`), zero Adam. */
 int rendgpu_nrc_reset(struct rdata *rd, uint64_t seed);
 /* Copy the FP32 master weights out (write = 0) or in (write = 1). */
 int rendgpu_nrc_weights(struct rdata *rd, float *host, int write);
+/* Copy the hash grid out (write = 0) or in (write = 1). */
+int rendgpu_nrc_grid(struct rdata *rd, float *host, int write);
 /* 12 floats per query (world position, outgoing direction, normal,
- * albedo) -> 64 BF16 features (frequency-encoded position in the scene
- * box, encoded direction, normal, albedo, zero padding). */
+ * albedo) -> 64 BF16 features: 0..15 the hash grid's features of the
+ * position in the scene box (level l at 2l, 2l+1), 16..33 the position's
+ * sin/cos(2^k pi x), k = 0..2, per axis, 34..41 the encoded direction,
+ * 42..44 the normal mapped to [0,1], 45..47 the albedo, the rest zero.
+ * Initialises the cache from cfg->seed if rendgpu_nrc_reset has not. */
 int rendgpu_nrc_encode_device(struct rdata *rd, const float *raw_device,
                               uint32_t n, void *feats_device);
 /* MLP outputs (r, g, b, 0) per query (tcgen05 tensor cores, TMEM
@@ -295,6 +309,15 @@ int rendgpu_nrc_query_device(struct rdata *rd, const float *entries_device,
 int rendgpu_nrc_train_device(struct rdata *rd, const void *feats_device,
                              const float *targets_device, uint32_t n,
                              int update, float *grad_device, float *loss_host);
+/* The same from raw inputs (12 floats per query, as for
+ * rendgpu_nrc_encode_device): encoded with the current grid, and the grid
+ * trained too: grid_grad_device (RENDGPU_NRC_GRID_PARAMS floats, may be
+ * NULL) receives its gradient, update = 1 also takes the grid's Adam
+ * step.  Needs rendgpu_upload_dynamic (the scene box). */
+int rendgpu_nrc_train_raw_device(struct rdata *rd, const float *raw_device,
+                                 const float *targets_device, uint32_t n,
+                                 int update, float *grad_device,
+                                 float *grid_grad_device, float *loss_host);
 
 /* relMSE of this context's accumulated image (acc / rd->samples) against a
  * reference image (W*H*3 floats, device memory): mean over pixels and

@@ -169,6 +169,9 @@ class GpuLib:
                 ("rendgpu_check_bounded_wait", [vp, u32, vp]),
                 ("rendgpu_nrc_train_device", [vp, vp, vp, u32, C.c_int, vp,
                                               vp]),
+                ("rendgpu_nrc_train_raw_device", [vp, vp, vp, u32, C.c_int,
+                                                  vp, vp, vp]),
+                ("rendgpu_nrc_grid", [vp, vp, C.c_int]),
                 ("rendgpu_sync", [vp]), ("rendgpu_get_stats", [vp, vp]),
                 ("rendgpu_get_lights", [vp, vp, u32, vp]),
                 ("rendgpu_capture", [vp, u32, u32]),
@@ -416,7 +419,7 @@ class GpuRenderer:
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
                  timing=False, device=0, count=False, sched=0,
                  nrc_warmup=0, nrc_lr=0.0, graph=False, block=0,
-                 nrc_end=0, nrc_steps=0, ref_tlas=False):
+                 nrc_end=0, nrc_steps=0, ref_tlas=False, nrc_grid=True):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -427,6 +430,7 @@ class GpuRenderer:
         cfg.reserved[1] = nrc_warmup
         cfg.reserved[2] = nrc_end
         cfg.reserved[3] = nrc_steps
+        cfg.reserved[5] = 0 if nrc_grid else 1
         cfg.reserved[4] = 1 if ref_tlas else 0
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
         if rc != 0:
@@ -528,6 +532,19 @@ class GpuRenderer:
         w = np.ascontiguousarray(w, np.float32)
         self._ck(self.g.rendgpu_nrc_weights(self.ptr, w.ctypes.data, 1),
                  "nrc_weights")
+
+    NRC_GRID_PARAMS = 8 * 32768 * 2
+
+    def nrc_grid(self, t=None):
+        """Get (t is None) or set the hash grid's FP32 table."""
+        if t is None:
+            out = np.zeros(self.NRC_GRID_PARAMS, np.float32)
+            self._ck(self.g.rendgpu_nrc_grid(self.ptr, out.ctypes.data, 0),
+                     "nrc_grid")
+            return out
+        t = np.ascontiguousarray(t, np.float32)
+        self._ck(self.g.rendgpu_nrc_grid(self.ptr, t.ctypes.data, 1),
+                 "nrc_grid")
 
     def relmse(self, ref_device_ptr):
         """relMSE of the accumulated image against a device reference
@@ -631,7 +648,7 @@ class BatchRenderer:
     or one per scene."""
 
     def __init__(self, rdatas, max_depth=5, mode=MODE_PATH, seed=1,
-                 timing=False, device=0, sched=0, block=0):
+                 timing=False, device=0, sched=0, block=0, nrc_grid=True):
         self.g = gpu_lib().L
         self.rdatas = list(rdatas)
         n = len(self.rdatas)
@@ -641,6 +658,7 @@ class BatchRenderer:
         ptrs = (C.c_void_p * n)(*[r.ptr for r in self.rdatas])
         cfg = make_cfg(max(depths), mode, seed, timing, device, False, sched,
                        True, block)
+        cfg.reserved[5] = 0 if nrc_grid else 1
         h = C.c_void_p()
         rc = self.g.rendgpu_batch_init(ptrs, n, self.depths, C.byref(cfg),
                                        C.byref(h))

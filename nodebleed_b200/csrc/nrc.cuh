@@ -55,48 +55,151 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 
 // ------------------------------------------------------------- encoding --
 
+// Multiresolution hash grid of the position (Mueller, Evans, Schied and
+// Keller, "Instant Neural Graphics Primitives with a Multiresolution Hash
+// Encoding", SIGGRAPH 2022): kGridLevels levels of kGridT entries of two
+// trainable FP32 features.  Level l lays a lattice of grid_res(l) cells per
+// axis over the unit box (16 to 1024, growing by 2^(6/7)); its corners are
+// indexed densely where all (res + 1)^3 of them fit the level's table and
+// by a spatial hash otherwise (the primes of Teschner et al. 2003), and a
+// position's two features are the trilinear blend of its cell's 8 corners.
+// The coarse levels carry smooth variation, the fine ones the detail a
+// sin/cos encoding of the whole scene box cannot resolve.
+constexpr int kGridLevels = 8;
+constexpr uint32_t kGridT = 1u << 15;
+constexpr int kGridParams = kGridLevels * (int)kGridT * 2;
+
+__host__ __device__ constexpr uint32_t grid_res(int l)
+{
+	return l == 0 ? 16u : l == 1 ? 28u : l == 2 ? 52u : l == 3 ? 95u :
+	  l == 4 ? 172u : l == 5 ? 312u : l == 6 ? 565u : 1024u;
+}
+
+// Entry (float2 index) of lattice corner (x, y, z) of level l; scenes of a
+// batch after the first hash with their own code, so they do not share
+// entries by design (they may collide, as hashed corners do).
+__host__ __device__ __forceinline__ uint32_t grid_index(int l, uint32_t x,
+                                                        uint32_t y, uint32_t z,
+                                                        uint32_t scene)
+{
+	uint32_t r1 = grid_res(l) + 1u;
+	uint32_t i;
+	if (scene == 0u && r1 * r1 * r1 <= kGridT)
+		i = x + r1 * (y + r1 * z);
+	else
+		i = x ^ (y * 2654435761u) ^ (z * 805459861u) ^ (scene * 0x9e3779b9u);
+	return (i & (kGridT - 1u)) + (uint32_t)l * kGridT;
+}
+
+// Cell and in-cell position of x (in [0,1]) on level l.
+__device__ __forceinline__ void grid_cell(int l, float x, uint32_t *c,
+                                          float *w)
+{
+	uint32_t res = grid_res(l);
+	float p = __fmul_rn(x, (float)res);
+	uint32_t ci = min((uint32_t)p, res - 1u);
+	*c = ci;
+	*w = __fsub_rn(p, (float)ci);
+}
+
+// Trilinear weight of corner b (bit a: upper corner on axis a).
+__device__ __forceinline__ float grid_weight(int b, const float w[3])
+{
+	float wx = (b & 1) ? w[0] : __fsub_rn(1.0f, w[0]);
+	float wy = (b & 2) ? w[1] : __fsub_rn(1.0f, w[1]);
+	float wz = (b & 4) ? w[2] : __fsub_rn(1.0f, w[2]);
+	return __fmul_rn(__fmul_rn(wx, wy), wz);
+}
+
+// The 2 kGridLevels grid features of position x (unit box).
+__device__ __forceinline__ void grid_features(const float2 *__restrict__ g,
+                                              const float x[3],
+                                              uint32_t scene, float *f)
+{
+#pragma unroll
+	for (int l = 0; l < kGridLevels; l++) {
+		uint32_t c[3];
+		float w[3];
+#pragma unroll
+		for (int a = 0; a < 3; a++)
+			grid_cell(l, x[a], &c[a], &w[a]);
+		float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+		for (int b = 0; b < 8; b++) {
+			float2 v = __ldg(g + grid_index(l, c[0] + (b & 1),
+			  c[1] + ((b >> 1) & 1), c[2] + ((b >> 2) & 1), scene));
+			float wt = grid_weight(b, w);
+			f0 = __fmaf_rn(wt, v.x, f0);
+			f1 = __fmaf_rn(wt, v.y, f1);
+		}
+		f[2 * l] = f0;
+		f[2 * l + 1] = f1;
+	}
+}
+
 // Raw cache inputs (12 floats: world position, outgoing direction, shading
 // normal, albedo) -> 64 BF16 features:
-//   0..35  position in the scene box, per axis sin/cos(2^k pi x), k = 0..5
-//   36..43 direction (theta/pi, phi/2pi), sin/cos(2^k pi u), k = 0..1
-//   44..46 (normal + 1) / 2,  47..49 albedo,  50..63 zero (in a batch of
-//   scenes: one of them 1, telling scenes 2..15 apart, see nrc_encode)
+//   0..15  hash grid of the position in the scene box (level l: 2l, 2l+1;
+//          zero without a grid)
+//   16..33 the same position, per axis sin/cos(2^k pi x), k = 0..2
+//   34..41 direction (theta/pi, phi/2pi), sin/cos(2^k pi u), k = 0..1
+//   42..44 (normal + 1) / 2,  45..47 albedo,  48..63 zero (in a batch of
+//   scenes: one of 50..63 is 1, telling scenes 2..15 apart, see nrc_encode)
 struct NrcBox {
 	float lo[3], inv[3]; // position -> [0,1]^3
 };
 
-// The frame's entries hold positions already mapped into their scene's box
-// (k_shade), with the scene's feature code 2 k (k = 1..14, 0 for the first
-// scene of a batch and for single-scene contexts) added to x; `scene_code`
-// decodes it into feature 49 + k and the box is then the identity.
+// Position in the unit box and scene index of a raw input: the frame's
+// entries hold positions already mapped into their scene's box (k_shade),
+// with the scene's feature code 2 k (k = 1..14, 0 for the first scene of a
+// batch and for single-scene contexts) added to x; `scene_code` decodes it
+// (the box is then the identity).
+__device__ __forceinline__ uint32_t nrc_position(const float *in,
+                                                 const NrcBox &B,
+                                                 bool scene_code, float x[3])
+{
+	float px = in[0];
+	uint32_t scene = 0u;
+	if (scene_code) {
+		int k = (int)floorf(px * 0.5f);
+		if (k >= 1 && k <= 14) {
+			px = px - (float)(2 * k);
+			scene = (uint32_t)k;
+		}
+	}
+#pragma unroll
+	for (int a = 0; a < 3; a++)
+		x[a] = fminf(fmaxf(((a == 0 ? px : in[a]) - B.lo[a]) * B.inv[a],
+		  0.0f), 1.0f);
+	return scene;
+}
+
+// grid: the hash grid's FP32 table (kGridParams floats), or null.
 __device__ __forceinline__ void nrc_encode(const float *in, const NrcBox &B,
-                                           uint4 *out, bool scene_code = false)
+                                           uint4 *out, bool scene_code = false,
+                                           const float2 *grid = nullptr)
 {
 	float f[64];
 #pragma unroll
 	for (int i = 0; i < 64; i++)
 		f[i] = 0.0f;
-	float px = in[0];
-	if (scene_code) {
-		int k = (int)floorf(px * 0.5f);
-		if (k >= 1 && k <= 14) {
-			px = px - (float)(2 * k);
-			f[49 + k] = 1.0f;
-		}
-	}
+	float x[3];
+	uint32_t scene = nrc_position(in, B, scene_code, x);
+	if (scene)
+		f[49 + scene] = 1.0f;
+	if (grid)
+		grid_features(grid, x, scene, f);
 #pragma unroll
 	for (int a = 0; a < 3; a++) {
-		float x = fminf(fmaxf(((a == 0 ? px : in[a]) - B.lo[a]) * B.inv[a],
-		  0.0f), 1.0f);
 #pragma unroll
-		for (int k = 0; k < 6; k++) {
+		for (int k = 0; k < 3; k++) {
 			float s, c;
 			// sin/cos(2^k pi x) = sin/cos(2 pi * frac(x 2^(k-1)))
-			float u = x * ldexpf(1.0f, k - 1);
+			float u = x[a] * ldexpf(1.0f, k - 1);
 			u = u - floorf(u);
 			sincospif(2.0f * u, &s, &c);
-			f[a * 12 + 2 * k] = s;
-			f[a * 12 + 2 * k + 1] = c;
+			f[16 + a * 6 + 2 * k] = s;
+			f[16 + a * 6 + 2 * k + 1] = c;
 		}
 	}
 	float dz = fminf(fmaxf(in[5], -1.0f), 1.0f);
@@ -109,13 +212,13 @@ __device__ __forceinline__ void nrc_encode(const float *in, const NrcBox &B,
 		for (int k = 0; k < 2; k++) {
 			float s, c;
 			sincospif(ldexpf(1.0f, k) * ang[j], &s, &c);
-			f[36 + j * 4 + 2 * k] = s;
-			f[36 + j * 4 + 2 * k + 1] = c;
+			f[34 + j * 4 + 2 * k] = s;
+			f[34 + j * 4 + 2 * k + 1] = c;
 		}
 #pragma unroll
 	for (int a = 0; a < 3; a++) {
-		f[44 + a] = 0.5f * (in[6 + a] + 1.0f);
-		f[47 + a] = in[9 + a];
+		f[42 + a] = 0.5f * (in[6 + a] + 1.0f);
+		f[45 + a] = in[9 + a];
 	}
 #pragma unroll
 	for (int i = 0; i < 64; i += 8) {
@@ -330,7 +433,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
              float4 *out, const uint32_t *ncount, uint32_t *err,
              const float4 *qe, NrcBox box, float4 *pL, uint32_t npath,
-             bool scode)
+             bool scode, const float2 *grid)
 {
 	if (ncount)
 		n = min(*ncount, n);
@@ -367,7 +470,7 @@ k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
 				  d = __ldg(e + 3);
 				float raw[12] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z,
 				  d.x, d.y, d.z};
-				nrc_encode(raw, box, pk, scode);
+				nrc_encode(raw, box, pk, scode, grid);
 				meta_next = make_float4(a.w, b.w, c.w, d.w);
 			} else {
 #pragma unroll
@@ -963,31 +1066,153 @@ __global__ void k_mlp_adam(float *wf, float *m, float *v, const float *part,
 // --------------------------------------------- encoding and frame kernels --
 
 __global__ void k_nrc_encode(const float *raw, uint32_t n, NrcBox B,
-                             __nv_bfloat16 *feats)
+                             __nv_bfloat16 *feats, const float2 *grid)
 {
 	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
 	     i += gridDim.x * blockDim.x)
 		nrc_encode(raw + 12ull * i, B,
-		  reinterpret_cast<uint4 *>(feats + 64ull * i));
+		  reinterpret_cast<uint4 *>(feats + 64ull * i), false, grid);
+}
+
+// The training batch's rows: samples [off, off + n) of the
+// min(*ncount, cap) made on the device, off = offset mod that count (as
+// k_mlp_fb_tc takes them); without ncount, rows [0, n).
+__device__ __forceinline__ uint32_t batch_rows(const uint32_t *ncount,
+                                               uint32_t offset, uint32_t cap,
+                                               uint32_t n, uint32_t *off)
+{
+	*off = 0u;
+	if (!ncount)
+		return n;
+	uint32_t total = min(*ncount, cap);
+	*off = total ? offset % total : 0u;
+	return min(n, total - *off);
 }
 
 // Features of cache queries / training records produced by k_shade: the
 // first four float4 of each entry (stride float4s) hold position, outgoing
-// direction, normal and albedo in .xyz.
+// direction, normal and albedo in .xyz.  Entries [off, off + n) of the
+// batch_rows selection, written to feats[off ...].
 __global__ void k_nrc_encode_entries(const float4 *e, uint32_t stride,
-                                     const uint32_t *count, uint32_t cap,
-                                     NrcBox B, __nv_bfloat16 *feats,
-                                     bool scode)
+                                     const uint32_t *count, uint32_t offset,
+                                     uint32_t cap, uint32_t n, NrcBox B,
+                                     __nv_bfloat16 *feats, bool scode,
+                                     const float2 *grid)
 {
-	uint32_t n = min(*count, cap);
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-	     i += gridDim.x * blockDim.x) {
+	uint32_t off;
+	n = batch_rows(count, offset, cap, n, &off);
+	for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n;
+	     r += gridDim.x * blockDim.x) {
+		uint32_t i = off + r;
 		const float4 *q = e + (size_t)stride * i;
 		float4 a = q[0], b = q[1], c = q[2], d = q[3];
 		float raw[12] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z,
 		  d.x, d.y, d.z};
 		nrc_encode(raw, B, reinterpret_cast<uint4 *>(feats + 64ull * i),
-		  scode);
+		  scode, grid);
+	}
+}
+
+// Gradient of the hash grid from a training batch's layer-0 output
+// gradient (dz0: [rows][64] BF16, as k_mlp_fb_tc writes it): per row
+// dL/dfeature_j = sum_o dz0[o] W0[o][j] for the 16 grid features (W0 the
+// BF16 copy the forward pass used), spread over each level's 8 cell
+// corners with their trilinear weights into gg (FP32, atomics).  Rows are
+// the entries of batch_rows (stride float4s each, raw inputs as for
+// k_nrc_encode_entries, position box B); without ncount, e holds 12
+// floats per row (the public raw layout).
+__global__ void __launch_bounds__(128) k_grid_grad(
+  const float4 *e, const float *raw, uint32_t stride, const uint32_t *ncount,
+  uint32_t offset, uint32_t cap, uint32_t n, NrcBox B, bool scode,
+  const __nv_bfloat16 *dz0, const __nv_bfloat16 *wbf, float *gg)
+{
+	__shared__ float w0[64][2 * kGridLevels + 1];
+	for (uint32_t i = threadIdx.x; i < 64u * 2u * kGridLevels; i += blockDim.x) {
+		uint32_t o = i / (2u * kGridLevels), j = i % (2u * kGridLevels);
+		w0[o][j] = __bfloat162float(wbf[o * 64u + j]);
+	}
+	__syncthreads();
+	uint32_t off;
+	n = batch_rows(ncount, offset, cap, n, &off);
+	for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n;
+	     r += gridDim.x * blockDim.x) {
+		float df[2 * kGridLevels];
+#pragma unroll
+		for (int j = 0; j < 2 * kGridLevels; j++)
+			df[j] = 0.0f;
+		const uint4 *dzr = reinterpret_cast<const uint4 *>(dz0 + 64ull * r);
+		bool any = false;
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			uint4 v = dzr[q];
+			uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+			for (int h = 0; h < 8; h++) {
+				float d = __uint_as_float((h & 1) ? (wv[h >> 1] & 0xffff0000u) :
+				  (wv[h >> 1] << 16));
+				if (d == 0.0f)
+					continue;
+				any = true;
+#pragma unroll
+				for (int j = 0; j < 2 * kGridLevels; j++)
+					df[j] = __fmaf_rn(d, w0[8 * q + h][j], df[j]);
+			}
+		}
+		if (!any)
+			continue;
+		float in[12];
+		if (ncount) {
+			const float4 *q = e + (size_t)stride * (off + r);
+			float4 a = q[0];
+			in[0] = a.x;
+			in[1] = a.y;
+			in[2] = a.z;
+		} else {
+			for (int k = 0; k < 3; k++)
+				in[k] = raw[12ull * r + k];
+		}
+		float x[3];
+		uint32_t scene = nrc_position(in, B, scode, x);
+#pragma unroll
+		for (int l = 0; l < kGridLevels; l++) {
+			if (df[2 * l] == 0.0f && df[2 * l + 1] == 0.0f)
+				continue;
+			uint32_t c[3];
+			float w[3];
+#pragma unroll
+			for (int a = 0; a < 3; a++)
+				grid_cell(l, x[a], &c[a], &w[a]);
+#pragma unroll
+			for (int b = 0; b < 8; b++) {
+				uint32_t k = grid_index(l, c[0] + (b & 1),
+				  c[1] + ((b >> 1) & 1), c[2] + ((b >> 2) & 1), scene);
+				float wt = grid_weight(b, w);
+				atomicAdd(gg + 2u * k, __fmul_rn(wt, df[2 * l]));
+				atomicAdd(gg + 2u * k + 1u, __fmul_rn(wt, df[2 * l + 1]));
+			}
+		}
+	}
+}
+
+// One Adam step of the hash grid from the gradient gg (then cleared);
+// g_out receives the gradient when not null.
+__global__ void k_grid_adam(float *t, float *m, float *v, float *gg,
+                            float *g_out, int update, float lr, float beta1,
+                            float beta2, float eps, float bc1, float bc2)
+{
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGridParams;
+	     i += gridDim.x * blockDim.x) {
+		float g = gg[i];
+		gg[i] = 0.0f;
+		if (g_out)
+			g_out[i] = g;
+		if (!update)
+			continue;
+		float mi = beta1 * m[i] + (1.0f - beta1) * g;
+		float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
+		m[i] = mi;
+		v[i] = vi;
+		t[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
 	}
 }
 

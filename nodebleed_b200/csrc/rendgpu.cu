@@ -126,6 +126,8 @@ struct Ctx {
 	// forward / transposed copies, per-CTA gradient partials and losses
 	DevBuf mlp_wf, mlp_m, mlp_v, mlp_wbf, mlp_wbt, mlp_part, mlp_loss;
 	DevBuf mlp_act, mlp_dz; // training: layer inputs and output gradients
+	// the position hash grid: FP32 table, Adam moments, gradient
+	DevBuf grid_t, grid_m, grid_v, grid_g;
 	uint32_t mlp_step = 0;
 	bool     mlp_ready = false;
 	NrcBox   box{};
@@ -557,8 +559,21 @@ float nrc_lr(const Ctx *c)
 	return lr > 0.0f ? lr : 1e-2f;
 }
 
+// The position hash grid is on unless cfg.reserved[5] bit 0 turns it off
+// (the grid features are then zero).
+bool nrc_grid(const Ctx *c)
+{
+	return !(c->cfg.reserved[5] & 1u);
+}
+
+const float2 *grid_of(Ctx *c)
+{
+	return nrc_grid(c) ? c->grid_t.as<float2>() : nullptr;
+}
+
 // Xavier-uniform FP32 master weights from a seeded PCG32 stream, zero Adam
-// moments, BF16 copies refreshed on the device.
+// moments, BF16 copies refreshed on the device; the hash grid's entries
+// uniform in +-1e-4 from the same stream (as instant-NGP initialises them).
 int nrc_reset(Ctx *c, uint64_t seed)
 {
 	NB_CK(c, c->mlp_wf.ensure(kMlpParams * sizeof(float)));
@@ -592,6 +607,19 @@ int nrc_reset(Ctx *c, uint64_t seed)
 	}
 	NB_CK(c, cudaMemcpyAsync(c->mlp_wf.p, w.data(), w.size() * 4,
 	  cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, c->grid_t.ensure(kGridParams * sizeof(float)));
+	NB_CK(c, c->grid_m.ensure(kGridParams * sizeof(float)));
+	NB_CK(c, c->grid_v.ensure(kGridParams * sizeof(float)));
+	NB_CK(c, c->grid_g.ensure(kGridParams * sizeof(float)));
+	std::vector<float> gt(kGridParams);
+	for (float &x : gt)
+		x = ((float)(next() >> 8) * 0x1p-24f * 2.0f - 1.0f) * 1e-4f;
+	NB_CK(c, cudaMemcpyAsync(c->grid_t.p, gt.data(), gt.size() * 4,
+	  cudaMemcpyHostToDevice, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->grid_m.p, 0, kGridParams * 4, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->grid_v.p, 0, kGridParams * 4, c->stream));
+	NB_CK(c, cudaMemsetAsync(c->grid_g.p, 0, kGridParams * 4, c->stream));
+	// (pageable sources: the copies have read them when they return)
 	NB_CK(c, cudaMemsetAsync(c->mlp_m.p, 0, kMlpParams * 4, c->stream));
 	NB_CK(c, cudaMemsetAsync(c->mlp_v.p, 0, kMlpParams * 4, c->stream));
 	NB_CK(c, cudaMemsetAsync(c->mlp_wbt.p, 0, kMlpParamsT * 2, c->stream));
@@ -694,7 +722,7 @@ int nrc_infer(Ctx *c, const void *feats, uint32_t n, float4 *out)
 	k_mlp_fwd_tc<false><<<grid, kTcThreads, smem, c->stream>>>(
 	  c->mlp_wbf.as<__nv_bfloat16>(), static_cast<const __nv_bfloat16 *>(feats),
 	  n, out, nullptr, c->berr.as<uint32_t>() + 1, nullptr, c->box, nullptr,
-	  0u, false);
+	  0u, false, nullptr);
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -719,18 +747,33 @@ int nrc_query(Ctx *c, const float4 *q, const uint32_t *count, uint32_t cap,
 		return rc;
 	k_mlp_fwd_tc<true><<<grid, kTcThreads, smem, c->stream>>>(
 	  c->mlp_wbf.as<__nv_bfloat16>(), nullptr, cap, nullptr, count, errs, q,
-	  frame ? kUnitBox : c->box, pL, npath, frame);
+	  frame ? kUnitBox : c->box, pL, npath, frame, grid_of(c));
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
 
+// Where a training batch's positions come from, for the hash grid's
+// gradient: entries of `stride` float4s (selected as the batch's rows are,
+// with the device count) or raw inputs of 12 floats per row; their box and
+// scene-code flag as the encoding used them.  g_out (kGridParams floats)
+// receives the grid's gradient when not null.
+struct GridSrc {
+	const float4 *e = nullptr;
+	const float  *raw = nullptr;
+	uint32_t      stride = 0;
+	NrcBox        box{};
+	bool          scode = false;
+	float        *g_out = nullptr;
+};
+
 // Gradient of a batch (and optionally one Adam step).  g_out (device,
 // kMlpParams floats) receives the summed gradient when not null; *loss the
-// batch loss when not null (synchronises).
+// batch loss when not null (synchronises).  With gs (and the grid on) the
+// hash grid gets its gradient and Adam step too.
 int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
               int update, float *g_out, float *loss,
               const uint32_t *ncount = nullptr, uint32_t offset = 0,
-              uint32_t cap = 0)
+              uint32_t cap = 0, const GridSrc *gs = nullptr)
 {
 	if (n == 0)
 		return 0;
@@ -765,6 +808,16 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 	  c->mlp_act.as<__nv_bfloat16>(), c->mlp_dz.as<__nv_bfloat16>(), npad,
 	  rows_per, c->mlp_part.as<float>(), c->berr.as<uint32_t>() + 1);
 	NB_CK(c, cudaGetLastError());
+	// the grid's gradient reads the BF16 layer-0 weights of this forward
+	// pass: before the MLP's Adam step replaces them
+	bool with_grid = gs && nrc_grid(c) && (gs->e || gs->raw);
+	if (with_grid) {
+		k_grid_grad<<<grid_for(c, n, 128), 128, 0, c->stream>>>(gs->e,
+		  gs->raw, gs->stride, ncount, offset, cap, n, gs->box, gs->scode,
+		  c->mlp_dz.as<__nv_bfloat16>(), c->mlp_wbf.as<__nv_bfloat16>(),
+		  c->grid_g.as<float>());
+		NB_CK(c, cudaGetLastError());
+	}
 	if (update)
 		c->mlp_step++;
 	float bc1 = 1.0f - std::pow(kAdamBeta1, (float)std::max(c->mlp_step, 1u));
@@ -775,6 +828,13 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 	  kAdamBeta1, kAdamBeta2, kAdamEps, bc1, bc2,
 	  c->mlp_wbf.as<__nv_bfloat16>(), c->mlp_wbt.as<__nv_bfloat16>());
 	NB_CK(c, cudaGetLastError());
+	if (with_grid) {
+		k_grid_adam<<<grid_for(c, kGridParams, 256), 256, 0, c->stream>>>(
+		  c->grid_t.as<float>(), c->grid_m.as<float>(), c->grid_v.as<float>(),
+		  c->grid_g.as<float>(), gs->g_out, update, nrc_lr(c), kAdamBeta1,
+		  kAdamBeta2, kAdamEps, bc1, bc2);
+		NB_CK(c, cudaGetLastError());
+	}
 	if (loss) {
 		std::vector<float> l(grid);
 		NB_CK(c, cudaMemcpyAsync(l.data(), c->mlp_loss.p, grid * 4,
@@ -1028,17 +1088,26 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		ev_record(c);
 		k_nrc_targets<<<grid_for(c, c->nrec_cap, 256), 256, 0, c->stream>>>(
 		  F.nrec, F.cnt + 41, c->nrec_cap, F.pL, c->rtgt.as<float4>());
-		k_nrc_encode_entries<<<grid_for(c, c->nrec_cap, 128), 128, 0,
-		  c->stream>>>(F.nrec, 6u, F.cnt + 41, c->nrec_cap, kUnitBox,
-		  c->rfeat.as<__nv_bfloat16>(), true);
 		NB_CK(c, cudaGetLastError());
+		// each step encodes its batch with the grid as the last step left
+		// it, trains, and moves the grid with its own gradient
+		GridSrc gs;
+		gs.e = F.nrec;
+		gs.stride = 6u;
+		gs.box = kUnitBox;
+		gs.scode = true;
 		for (uint32_t s = 0; s < nrc_steps(c); s++) {
+			k_nrc_encode_entries<<<grid_for(c, kNrcBatch, 128), 128, 0,
+			  c->stream>>>(F.nrec, 6u, F.cnt + 41, s * kNrcBatch,
+			  c->nrec_cap, kNrcBatch, kUnitBox, c->rfeat.as<__nv_bfloat16>(),
+			  true, grid_of(c));
+			NB_CK(c, cudaGetLastError());
 			rc = nrc_train(c, c->rfeat.p, c->rtgt.as<float4>(), kNrcBatch, 1,
-			  nullptr, nullptr, F.cnt + 41, s * kNrcBatch, c->nrec_cap);
+			  nullptr, nullptr, F.cnt + 41, s * kNrcBatch, c->nrec_cap, &gs);
 			if (rc)
 				return rc;
 		}
-		c->st.launches += 2 + 3 * nrc_steps(c);
+		c->st.launches += 1 + (nrc_grid(c) ? 6 : 4) * nrc_steps(c);
 		ev_record(c);
 	}
 	ev_record(c); // last
@@ -1185,7 +1254,8 @@ void free_ctx(Ctx *c)
 	  &c->nrms, &c->mtls, &c->lights, &c->sp, &c->scn, &c->sortbuf, &c->q0, &c->q1, &c->hits, &c->shadow,
 	  &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
 	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_act,
-	  &c->mlp_dz, &c->mlp_wf,
+	  &c->mlp_dz, &c->mlp_wf, &c->grid_t, &c->grid_m, &c->grid_v,
+	  &c->grid_g,
 	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
 	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat, &c->waitchk,
 	  &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob, &c->dyn_wbox,
@@ -1208,7 +1278,8 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->sortbuf, &c->q0, &c->q1, &c->hits,
 	  &c->shadow, &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf,
 	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
-	  &c->mlp_act, &c->mlp_dz,
+	  &c->mlp_act, &c->mlp_dz, &c->grid_t, &c->grid_m, &c->grid_v,
+	  &c->grid_g,
 	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
 	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec, &c->waitchk,
 	  &c->rfeat, &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob,
@@ -1468,6 +1539,18 @@ int dyn_prepare(Ctx *c, uint64_t *bytes)
 
 uint32_t device_tlas_limit(const Ctx *c);
 
+// k_tlas_build with its instance boxes in dynamic shared memory (up to
+// 128 KB beside 42 KB of static shared memory).
+cudaError_t launch_tlas_build(Ctx *c, const TbArgs &A)
+{
+	cudaError_t e = cudaFuncSetAttribute(k_tlas_build,
+	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem(kTbMaxInst));
+	if (e != cudaSuccess)
+		return e;
+	k_tlas_build<<<1, kTbWarps * 32, tb_smem(A.n), c->stream>>>(A);
+	return cudaGetLastError();
+}
+
 // New object->world matrices (device, 16 floats each, rd->insts order) ->
 // instance records, world boxes, TLAS (built, or refitted when asked and a
 // device build exists) and light table, all on the context's stream.
@@ -1520,7 +1603,7 @@ int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
 		// stays within what it holds
 		A.depth_limit = device_tlas_limit(c);
 		h.tlas_depth = c->tlas_depth = A.depth_limit;
-		k_tlas_build<<<1, kTbWarps * 32, 0, c->stream>>>(A);
+		NB_CK(c, launch_tlas_build(c, A));
 	} else {
 		k_tlas_refit<<<grid_for(c, nn * 32u, 256), 256, 0, c->stream>>>(
 		  c->dyn_wbox.as<float4>(), c->dyn_order.as<uint32_t>(),
@@ -1591,8 +1674,7 @@ int rebuild_tlas_tight(Ctx *c)
 	A.order = c->dyn_order.as<uint32_t>();
 	A.info = c->dyn_info.as<uint32_t>();
 	A.depth_limit = device_tlas_limit(c);
-	k_tlas_build<<<1, kTbWarps * 32, 0, c->stream>>>(A);
-	NB_CK(c, cudaGetLastError());
+	NB_CK(c, launch_tlas_build(c, A));
 	NB_CK(c, cudaStreamSynchronize(c->stream));
 	h.tlas_root = 0u;
 	h.tlas_depth = c->tlas_depth = A.depth_limit;
@@ -2469,8 +2551,13 @@ int rendgpu_nrc_encode_device(struct rdata *rdp, const float *raw, uint32_t n,
 	if (n == 0)
 		return 0;
 	NB_CK(c, cudaSetDevice(c->device));
+	if (!c->mlp_ready) {
+		int rc = nrc_reset(c, c->cfg.seed);
+		if (rc)
+			return rc;
+	}
 	k_nrc_encode<<<grid_for(c, n, 128), 128, 0, c->stream>>>(raw, n, c->box,
-	  static_cast<__nv_bfloat16 *>(feats));
+	  static_cast<__nv_bfloat16 *>(feats), grid_of(c));
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -2543,6 +2630,56 @@ int rendgpu_nrc_train_device(struct rdata *rdp, const void *feats,
 	NB_CK(c, cudaSetDevice(c->device));
 	return nrc_train(c, feats, reinterpret_cast<const float4 *>(targets), n,
 	  update, grad, loss);
+}
+
+int rendgpu_nrc_train_raw_device(struct rdata *rdp, const float *raw,
+                                 const float *targets, uint32_t n, int update,
+                                 float *grad, float *grid_grad, float *loss)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c)
+		return RENDGPU_EINVAL;
+	if (!c->mlp_ready)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_nrc_reset must come first");
+	if (!c->have_dynamic)
+		return fail(c, RENDGPU_ESTATE, "upload_dynamic must come first");
+	if (n && (!raw || misaligned16(targets)))
+		return fail(c, RENDGPU_EINVAL, "raw must be a non-null device "
+		  "pointer, targets non-null and 16-byte aligned");
+	if (n == 0)
+		return 0;
+	NB_CK(c, cudaSetDevice(c->device));
+	NB_CK(c, c->rfeat.ensure((size_t)n * 128));
+	k_nrc_encode<<<grid_for(c, n, 128), 128, 0, c->stream>>>(raw, n, c->box,
+	  c->rfeat.as<__nv_bfloat16>(), grid_of(c));
+	NB_CK(c, cudaGetLastError());
+	GridSrc gs;
+	gs.raw = raw;
+	gs.box = c->box;
+	gs.g_out = grid_grad;
+	int rc = nrc_train(c, c->rfeat.p, reinterpret_cast<const float4 *>(
+	  targets), n, update, grad, loss, nullptr, 0, 0, &gs);
+	if (rc == 0 && grid_grad && !nrc_grid(c))
+		NB_CK(c, cudaMemsetAsync(grid_grad, 0, kGridParams * 4, c->stream));
+	return rc;
+}
+
+int rendgpu_nrc_grid(struct rdata *rdp, float *host, int write)
+{
+	Ctx *c = find_ctx(rdp);
+	if (!c || !host)
+		return RENDGPU_EINVAL;
+	if (!c->mlp_ready)
+		return fail(c, RENDGPU_ESTATE, "rendgpu_nrc_reset must come first");
+	NB_CK(c, cudaSetDevice(c->device));
+	if (write)
+		NB_CK(c, cudaMemcpyAsync(c->grid_t.p, host, kGridParams * 4,
+		  cudaMemcpyHostToDevice, c->stream));
+	else
+		NB_CK(c, cudaMemcpyAsync(host, c->grid_t.p, kGridParams * 4,
+		  cudaMemcpyDeviceToHost, c->stream));
+	NB_CK(c, cudaStreamSynchronize(c->stream));
+	return 0;
 }
 
 int rendgpu_relmse_device(struct rdata *rdp, const float *ref, double *out)

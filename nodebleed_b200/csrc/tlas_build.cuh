@@ -274,10 +274,11 @@ __device__ __forceinline__ int tb_bin(float c, float cmn, float scale)
 	return b < 0 ? 0 : (b > kTbBins - 1 ? kTbBins - 1 : b);
 }
 
+// Box of instance i (wbox in global or, in the build, shared memory).
 __device__ __forceinline__ void tb_load(const float4 *wbox, uint32_t i,
                                         float lo[3], float hi[3])
 {
-	float4 a = __ldg(wbox + 2u * i), b = __ldg(wbox + 2u * i + 1u);
+	float4 a = wbox[2u * i], b = wbox[2u * i + 1u];
 	lo[0] = a.x; lo[1] = a.y; lo[2] = a.z;
 	hi[0] = b.x; hi[1] = b.y; hi[2] = b.z;
 }
@@ -613,14 +614,26 @@ __device__ void tb_node(const TbArgs &A, uint16_t *idx, uint16_t *tmp,
 	atomicMax(&A.info[1], nd.depth);
 }
 
-// The whole TLAS in one CTA of kTbWarps warps.
+// Dynamic shared memory of k_tlas_build for n instances: their boxes.
+__host__ __device__ constexpr size_t tb_smem(uint32_t n)
+{
+	return (size_t)2u * n * sizeof(float4);
+}
+
+// The whole TLAS in one CTA of kTbWarps warps.  The instance boxes are
+// staged in dynamic shared memory (tb_smem(n) bytes), so the passes over a
+// node's instances (bounds, bins, partition) read shared memory, not L2.
 __global__ void __launch_bounds__(kTbWarps * 32) k_tlas_build(TbArgs A)
 {
+	extern __shared__ float4 sbox[];
 	__shared__ uint16_t sidx[kTbMaxInst], stmp[kTbMaxInst];
 	__shared__ TbBin bins[kTbWarps][3 * kTbBins];
 	__shared__ TbChild chs[kTbWarps][8];
 	__shared__ uint32_t s_node, s_item, s_cnt[2];
 	const uint32_t tid = threadIdx.x, warp = tid >> 5;
+	for (uint32_t i = tid; i < 2u * A.n; i += blockDim.x)
+		sbox[i] = A.wbox[i];
+	A.wbox = sbox;
 	for (uint32_t i = tid; i < A.n; i += blockDim.x)
 		sidx[i] = (uint16_t)i;
 	if (tid == 0) {

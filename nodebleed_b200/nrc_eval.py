@@ -57,7 +57,8 @@ def equal_time(scene, w, h, depth, frames, ref, seed=1, **nrc_kw):
         # the cache frames through the batch API (one launch sequence over
         # shared queues, as a batch of scenes runs them)
         gn = api.BatchRenderer([rd], max_depth=depth, mode=api.MODE_NRC,
-                               seed=seed, timing=True).upload()
+                               seed=seed, timing=True,
+                               nrc_grid=nrc_kw.get("nrc_grid", True)).upload()
 
         def stats():
             return gn.stats()[0]

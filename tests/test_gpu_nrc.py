@@ -64,8 +64,14 @@ def _random_raw(rd, n, seed=0):
 
 
 def test_encode_matches_oracle(gpu):
+    """All 64 features, the hash grid's with a table of entries in
+    [-1, 1] (level 0 and 1 dense, the rest hashed)."""
     import torch
     rd, gr = _setup()
+    table = np.random.default_rng(8).uniform(
+        -1, 1, no.GRID_PARAMS).astype(np.float32)
+    gr.nrc_grid(table)
+    assert np.array_equal(gr.nrc_grid(), table)
     raw = _random_raw(rd, 4099)
     out = torch.zeros((len(raw), 64), dtype=torch.bfloat16, device="cuda")
     d_raw = _dev(raw)
@@ -75,9 +81,105 @@ def test_encode_matches_oracle(gpu):
     gr.g.rendgpu_sync(gr.ptr)
     got = out.float().cpu().numpy()
     lo, hi = _box(rd)
-    ref = no.encode(raw, lo.astype(np.float32), hi.astype(np.float32))
-    assert np.abs(got - ref).max() < 8e-3
-    assert (got[:, 50:] == 0).all()
+    ref = no.encode(raw, lo.astype(np.float32), hi.astype(np.float32), table)
+    err = np.abs(got - ref)
+    print(f"encode: max error {err.max():.2e} (grid features "
+          f"{err[:, :16].max():.2e})")
+    assert err.max() < 8e-3
+    assert np.abs(ref[:, :16]).max() > 0.3
+    assert (got[:, 48:] == 0).all()
+    gr.close()
+
+
+def _grid_batch(gr, rd, n, seed):
+    """A training batch of raw inputs (device) and its targets, with random
+    MLP weights and a random table."""
+    rng = np.random.default_rng(seed)
+    table = rng.uniform(-0.5, 0.5, no.GRID_PARAMS).astype(np.float32)
+    gr.nrc_grid(table)
+    raw = _random_raw(rd, n, seed)
+    t = rng.uniform(0, 2, (n, 4)).astype(np.float32)
+    return table, raw, t
+
+
+@pytest.mark.parametrize("n", [1000, 16384])
+def test_grid_gradient_matches_oracle(gpu, n):
+    """rendgpu_nrc_train_raw_device: the table's gradient (d loss /
+    d feature = dz_0 W_0 spread over the trilinear corners) and the MLP's
+    against the oracle on the same BF16-rounded features."""
+    import torch
+    rd, gr = _setup(13)
+    table, raw, t = _grid_batch(gr, rd, n, 5)
+    d_raw, d_t = _dev(raw), _dev(t)
+    g = torch.zeros(no.NPARAMS, dtype=torch.float32, device="cuda")
+    gg = torch.zeros(no.GRID_PARAMS, dtype=torch.float32, device="cuda")
+    loss = C.c_float()
+    torch.cuda.synchronize()
+    gr._ck(gr.g.rendgpu_nrc_train_raw_device(
+        gr.ptr, d_raw.data_ptr(), d_t.data_ptr(), n, 0, g.data_ptr(),
+        gg.data_ptr(), C.byref(loss)), "train_raw")
+    assert gr.g.rendgpu_sync(gr.ptr) == 0
+    w = gr.nrc_weights()
+    lo, hi = _box(rd)
+    lo32, hi32 = lo.astype(np.float32), hi.astype(np.float32)
+    feats = no.bf16(no.encode(raw, lo32, hi32, table))
+    ref_loss, ref = no.loss_grad(w, feats, t, bf=True)
+    dfeat = no.feature_grad(w, feats, t, bf=True)[:, :16]
+    x = no.unit_position(raw, lo32, hi32)
+    ref_gg = no.grid_grad(x, dfeat)
+    got_gg = gg.cpu().numpy().astype(np.float64)
+    gerr = np.linalg.norm(got_gg - ref_gg) / np.linalg.norm(ref_gg)
+    lerr = abs(loss.value - ref_loss) / ref_loss
+    got = g.cpu().numpy().astype(np.float64)
+    merr = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    print(f"grid gradient n={n}: relative L2 error {gerr:.3e}, MLP "
+          f"{merr:.3e}, loss {lerr:.3e}, entries touched "
+          f"{np.count_nonzero(got_gg)}")
+    assert gerr < 1e-3
+    assert merr < 1e-3
+    assert lerr < 1e-4
+    # update = 0 leaves the table as it was
+    assert np.array_equal(gr.nrc_grid(), table)
+    gr.close()
+
+
+def test_grid_adam_step_matches_oracle(gpu):
+    import torch
+    rd, gr = _setup(17)
+    table, raw, t = _grid_batch(gr, rd, 2048, 6)
+    d_raw, d_t = _dev(raw), _dev(t)
+    gg = torch.zeros(no.GRID_PARAMS, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    gr._ck(gr.g.rendgpu_nrc_train_raw_device(
+        gr.ptr, d_raw.data_ptr(), d_t.data_ptr(), len(raw), 1, None,
+        gg.data_ptr(), None), "train_raw")
+    assert gr.g.rendgpu_sync(gr.ptr) == 0
+    g64 = gg.cpu().numpy().astype(np.float64)
+    m = 0.1 * g64
+    v = 0.01 * g64 * g64
+    ref = table - 1e-2 * (m / 0.1) / (np.sqrt(v / 0.01) + 1e-15)
+    got = gr.nrc_grid().astype(np.float64)
+    assert np.abs(got - ref).max() < 1e-6
+    assert np.count_nonzero(got != table) > 1000
+    gr.close()
+
+
+def test_grid_off_leaves_features_zero(gpu):
+    import torch
+    scene = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(scene)
+    gr = api.GpuRenderer(rd, nrc_grid=False).upload()
+    gr.nrc_reset(3)
+    raw = _random_raw(rd, 300)
+    out = torch.ones((len(raw), 64), dtype=torch.bfloat16, device="cuda")
+    d_raw = _dev(raw)
+    torch.cuda.synchronize()
+    gr._ck(gr.g.rendgpu_nrc_encode_device(gr.ptr, d_raw.data_ptr(), len(raw),
+                                          out.data_ptr()), "encode")
+    gr.g.rendgpu_sync(gr.ptr)
+    got = out.float().cpu().numpy()
+    assert (got[:, :16] == 0).all() and (got[:, 16:34] != 0).any()
+    gr.close()
     gr.close()
 
 

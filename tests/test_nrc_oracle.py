@@ -70,3 +70,27 @@ def test_adam_moves_against_gradient():
     w2, m, v = no.adam(w, np.zeros_like(w), np.zeros_like(w), g, 1)
     d = (w2 - w)[g != 0]
     assert np.allclose(d, -1e-2 * np.sign(g[g != 0]), rtol=1e-6)
+
+
+def test_grid_features_and_gradient_are_adjoint():
+    """The hash grid's features are linear in the table and grid_grad is
+    their adjoint: <grid_grad(x, d), T> = sum d * features(T, x); the
+    trilinear weights of a cell sum to 1, and a constant table gives that
+    constant as every feature."""
+    rng = np.random.default_rng(3)
+    x = rng.uniform(0, 1, (500, 3)).astype(np.float32)
+    x[:5] = [[0, 0, 0], [1, 1, 1], [1, 0, 0.5], [0.5, 1, 0], [1e-7, 1, 1]]
+    T = rng.normal(size=no.GRID_PARAMS)
+    d = rng.normal(size=(len(x), 16))
+    lhs = np.dot(no.grid_grad(x, d), T)
+    rhs = np.sum(d * no.grid_features(T, x))
+    assert abs(lhs - rhs) <= 1e-9 * abs(rhs)
+    for l in range(no.GRID_LEVELS):
+        idx, wt = no.grid_corners(x, l)
+        assert np.allclose(wt.sum(1), 1.0)
+        assert idx.min() >= l * no.GRID_T and idx.max() < (l + 1) * no.GRID_T
+    f = no.grid_features(np.full(no.GRID_PARAMS, 0.25), x)
+    assert np.allclose(f, 0.25)
+    # dense levels: distinct corners get distinct entries
+    idx, _ = no.grid_corners(np.array([[0.3, 0.6, 0.9]], np.float32), 0)
+    assert len(set(idx[0])) == 8
