@@ -82,7 +82,8 @@ struct rendgpu_cfg {
 	                         keep the TLAS rendgpu_upload_dynamic converts
 	                         from rd->bnodes instead of the device rebuild
 	                         over tight instance boxes; [5] bit 0: no hash
-	                         grid in the cache's position encoding */
+	                         grid in the cache's position encoding; [6]:
+	                         cache training paths per frame (0 = 65536) */
 };
 
 /* A ray for the batch calls: origin, tmax, direction (32 bytes). */
@@ -252,14 +253,15 @@ int rendgpu_trace_rays_device_noalloc(struct rdata *rd,
  * Parameters: RENDGPU_NRC_PARAMS floats, layer l (0..4: 64x64, 5: 8x64 of
  * which 3 rows are used) stored [out][in] at offset l * 4096.
  * The position also goes through a trainable multiresolution hash grid
- * (Mueller et al. 2022): 8 levels of 2^15 entries of 2 FP32 features,
- * RENDGPU_NRC_GRID_PARAMS floats, level l at offset l * 65536, entry e at
+ * (Mueller et al. 2022): 8 levels of 2^17 entries of 2 FP32 features,
+ * RENDGPU_NRC_GRID_PARAMS floats, level l at offset l * 262144, entry e at
  * 2 e; lattices of 16, 28, 52, 95, 172, 312, 565 and 1024 cells per axis
  * over the scene box, levels 0 and 1 indexed densely (x + (r+1)(y + (r+1)
- * z)), the others by (x ^ 2654435761 y ^ 805459861 z) mod 2^15.
+ * z)), the others by (x ^ 2654435761 y ^ 805459861 z) mod 2^17.  Its Adam
+ * steps are lazy: entries a batch does not touch keep their state.
  * cfg.reserved[5] bit 0 turns the grid off (its features are then 0). */
 #define RENDGPU_NRC_PARAMS (5 * 4096 + 8 * 64)
-#define RENDGPU_NRC_GRID_PARAMS (8 * 32768 * 2)
+#define RENDGPU_NRC_GRID_PARAMS (8 * 131072 * 2)
 
 /* (Re)initialise the weights (Xavier uniform from `seed`), zero Adam. */
 int rendgpu_nrc_reset(struct rdata *rd, uint64_t seed);

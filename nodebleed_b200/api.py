@@ -419,7 +419,8 @@ class GpuRenderer:
     def __init__(self, rdata, max_depth=5, mode=MODE_PATH, seed=1,
                  timing=False, device=0, count=False, sched=0,
                  nrc_warmup=0, nrc_lr=0.0, graph=False, block=0,
-                 nrc_end=0, nrc_steps=0, ref_tlas=False, nrc_grid=True):
+                 nrc_end=0, nrc_steps=0, ref_tlas=False, nrc_grid=True,
+                 nrc_train_paths=0):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -430,8 +431,9 @@ class GpuRenderer:
         cfg.reserved[1] = nrc_warmup
         cfg.reserved[2] = nrc_end
         cfg.reserved[3] = nrc_steps
-        cfg.reserved[5] = 0 if nrc_grid else 1
         cfg.reserved[4] = 1 if ref_tlas else 0
+        cfg.reserved[5] = 0 if nrc_grid else 1
+        cfg.reserved[6] = nrc_train_paths
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
         if rc != 0:
             raise RendgpuError(rc, "rendgpu_init")
@@ -533,7 +535,7 @@ class GpuRenderer:
         self._ck(self.g.rendgpu_nrc_weights(self.ptr, w.ctypes.data, 1),
                  "nrc_weights")
 
-    NRC_GRID_PARAMS = 8 * 32768 * 2
+    NRC_GRID_PARAMS = 8 * 131072 * 2
 
     def nrc_grid(self, t=None):
         """Get (t is None) or set the hash grid's FP32 table."""

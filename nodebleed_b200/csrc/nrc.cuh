@@ -66,7 +66,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // The coarse levels carry smooth variation, the fine ones the detail a
 // sin/cos encoding of the whole scene box cannot resolve.
 constexpr int kGridLevels = 8;
-constexpr uint32_t kGridT = 1u << 15;
+constexpr uint32_t kGridT = 1u << 17;
 constexpr int kGridParams = kGridLevels * (int)kGridT * 2;
 
 __host__ __device__ constexpr uint32_t grid_res(int l)
@@ -111,6 +111,28 @@ __device__ __forceinline__ float grid_weight(int b, const float w[3])
 	return __fmul_rn(__fmul_rn(wx, wy), wz);
 }
 
+// The two features of level l at position x (unit box).
+__device__ __forceinline__ float2 grid_level(const float2 *__restrict__ g,
+                                             const float x[3], uint32_t scene,
+                                             int l)
+{
+	uint32_t c[3];
+	float w[3];
+#pragma unroll
+	for (int a = 0; a < 3; a++)
+		grid_cell(l, x[a], &c[a], &w[a]);
+	float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+	for (int b = 0; b < 8; b++) {
+		float2 v = __ldg(g + grid_index(l, c[0] + (b & 1),
+		  c[1] + ((b >> 1) & 1), c[2] + ((b >> 2) & 1), scene));
+		float wt = grid_weight(b, w);
+		f0 = __fmaf_rn(wt, v.x, f0);
+		f1 = __fmaf_rn(wt, v.y, f1);
+	}
+	return make_float2(f0, f1);
+}
+
 // The 2 kGridLevels grid features of position x (unit box).
 __device__ __forceinline__ void grid_features(const float2 *__restrict__ g,
                                               const float x[3],
@@ -118,22 +140,9 @@ __device__ __forceinline__ void grid_features(const float2 *__restrict__ g,
 {
 #pragma unroll
 	for (int l = 0; l < kGridLevels; l++) {
-		uint32_t c[3];
-		float w[3];
-#pragma unroll
-		for (int a = 0; a < 3; a++)
-			grid_cell(l, x[a], &c[a], &w[a]);
-		float f0 = 0.0f, f1 = 0.0f;
-#pragma unroll
-		for (int b = 0; b < 8; b++) {
-			float2 v = __ldg(g + grid_index(l, c[0] + (b & 1),
-			  c[1] + ((b >> 1) & 1), c[2] + ((b >> 2) & 1), scene));
-			float wt = grid_weight(b, w);
-			f0 = __fmaf_rn(wt, v.x, f0);
-			f1 = __fmaf_rn(wt, v.y, f1);
-		}
-		f[2 * l] = f0;
-		f[2 * l + 1] = f1;
+		float2 v = grid_level(g, x, scene, l);
+		f[2 * l] = v.x;
+		f[2 * l + 1] = v.y;
 	}
 }
 
@@ -185,8 +194,10 @@ __device__ __forceinline__ void nrc_encode(const float *in, const NrcBox &B,
 		f[i] = 0.0f;
 	float x[3];
 	uint32_t scene = nrc_position(in, B, scene_code, x);
-	if (scene)
-		f[49 + scene] = 1.0f;
+	// constant indices only, so f stays in registers
+#pragma unroll
+	for (uint32_t k = 1; k <= 14; k++)
+		f[49 + k] = scene == k ? 1.0f : 0.0f;
 	if (grid)
 		grid_features(grid, x, scene, f);
 #pragma unroll
@@ -433,7 +444,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
              float4 *out, const uint32_t *ncount, uint32_t *err,
              const float4 *qe, NrcBox box, float4 *pL, uint32_t npath,
-             bool scode, const float2 *grid)
+             bool scode, const uint4 *gq)
 {
 	if (ncount)
 		n = min(*ncount, n);
@@ -470,7 +481,13 @@ k_mlp_fwd_tc(const __nv_bfloat16 *wbf, const __nv_bfloat16 *feats, uint32_t n,
 				  d = __ldg(e + 3);
 				float raw[12] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z,
 				  d.x, d.y, d.z};
-				nrc_encode(raw, box, pk, scode, grid);
+				nrc_encode(raw, box, pk, scode);
+				// the hash grid's features 0..15, gathered beforehand by
+				// k_grid_query_feats at full occupancy
+				if (gq) {
+					pk[0] = __ldg(gq + 2ull * rr);
+					pk[1] = __ldg(gq + 2ull * rr + 1u);
+				}
 				meta_next = make_float4(a.w, b.w, c.w, d.w);
 			} else {
 #pragma unroll
@@ -1074,6 +1091,29 @@ __global__ void k_nrc_encode(const float *raw, uint32_t n, NrcBox B,
 		  reinterpret_cast<uint4 *>(feats + 64ull * i), false, grid);
 }
 
+// Hash-grid features of cache queries (entries of 4 float4, position in
+// the first), one thread per (query, level): out[8 q + l] = the level's two
+// features as BF16 (what nrc_encode packs into features 2l, 2l + 1).
+// n = min(*count, cap) queries (count null: cap).
+__global__ void k_grid_query_feats(const float4 *qe, const uint32_t *count,
+                                   uint32_t cap, NrcBox B, bool scode,
+                                   const float2 *grid, uint32_t *out)
+{
+	uint32_t n = count ? min(*count, cap) : cap;
+	const uint32_t work = n * (uint32_t)kGridLevels;
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < work;
+	     t += gridDim.x * blockDim.x) {
+		uint32_t r = t / (uint32_t)kGridLevels;
+		int l = (int)(t % (uint32_t)kGridLevels);
+		float4 a = __ldg(qe + 4ull * r);
+		float in[3] = {a.x, a.y, a.z};
+		float x[3];
+		uint32_t scene = nrc_position(in, B, scode, x);
+		float2 v = grid_level(grid, x, scene, l);
+		out[t] = pack_bf16(v.x, v.y);
+	}
+}
+
 // The training batch's rows: samples [off, off + n) of the
 // min(*ncount, cap) made on the device, off = offset mod that count (as
 // k_mlp_fb_tc takes them); without ncount, rows [0, n).
@@ -1117,31 +1157,34 @@ __global__ void k_nrc_encode_entries(const float4 *e, uint32_t stride,
 // gradient (dz0: [rows][64] BF16, as k_mlp_fb_tc writes it): per row
 // dL/dfeature_j = sum_o dz0[o] W0[o][j] for the 16 grid features (W0 the
 // BF16 copy the forward pass used), spread over each level's 8 cell
-// corners with their trilinear weights into gg (FP32, atomics).  Rows are
-// the entries of batch_rows (stride float4s each, raw inputs as for
-// k_nrc_encode_entries, position box B); without ncount, e holds 12
+// corners with their trilinear weights into gg (FP32 pairs, vector
+// atomics).  One thread per (row, level), so a 16k-row batch fills the GPU.
+// Rows are the entries of batch_rows (stride float4s each, raw inputs as
+// for k_nrc_encode_entries, position box B); without ncount, raw holds 12
 // floats per row (the public raw layout).
-__global__ void __launch_bounds__(128) k_grid_grad(
+__global__ void __launch_bounds__(256) k_grid_grad(
   const float4 *e, const float *raw, uint32_t stride, const uint32_t *ncount,
   uint32_t offset, uint32_t cap, uint32_t n, NrcBox B, bool scode,
-  const __nv_bfloat16 *dz0, const __nv_bfloat16 *wbf, float *gg)
+  const __nv_bfloat16 *dz0, const __nv_bfloat16 *wbf, float2 *gg)
 {
-	__shared__ float w0[64][2 * kGridLevels + 1];
-	for (uint32_t i = threadIdx.x; i < 64u * 2u * kGridLevels; i += blockDim.x) {
-		uint32_t o = i / (2u * kGridLevels), j = i % (2u * kGridLevels);
-		w0[o][j] = __bfloat162float(wbf[o * 64u + j]);
+	// W0's grid columns, transposed; the odd row pitch spreads the levels
+	// of one o over different banks
+	__shared__ float w0[2 * kGridLevels][65];
+	for (uint32_t i = threadIdx.x; i < 64u * 2u * kGridLevels;
+	     i += blockDim.x) {
+		uint32_t j = i / 64u, o = i % 64u;
+		w0[j][o] = __bfloat162float(wbf[o * 64u + j]);
 	}
 	__syncthreads();
 	uint32_t off;
 	n = batch_rows(ncount, offset, cap, n, &off);
-	for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n;
-	     r += gridDim.x * blockDim.x) {
-		float df[2 * kGridLevels];
-#pragma unroll
-		for (int j = 0; j < 2 * kGridLevels; j++)
-			df[j] = 0.0f;
+	const uint32_t work = n * (uint32_t)kGridLevels;
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < work;
+	     t += gridDim.x * blockDim.x) {
+		uint32_t r = t / (uint32_t)kGridLevels;
+		int l = (int)(t % (uint32_t)kGridLevels);
 		const uint4 *dzr = reinterpret_cast<const uint4 *>(dz0 + 64ull * r);
-		bool any = false;
+		float d0 = 0.0f, d1 = 0.0f;
 #pragma unroll
 		for (int q = 0; q < 8; q++) {
 			uint4 v = dzr[q];
@@ -1150,20 +1193,15 @@ __global__ void __launch_bounds__(128) k_grid_grad(
 			for (int h = 0; h < 8; h++) {
 				float d = __uint_as_float((h & 1) ? (wv[h >> 1] & 0xffff0000u) :
 				  (wv[h >> 1] << 16));
-				if (d == 0.0f)
-					continue;
-				any = true;
-#pragma unroll
-				for (int j = 0; j < 2 * kGridLevels; j++)
-					df[j] = __fmaf_rn(d, w0[8 * q + h][j], df[j]);
+				d0 = __fmaf_rn(d, w0[2 * l][8 * q + h], d0);
+				d1 = __fmaf_rn(d, w0[2 * l + 1][8 * q + h], d1);
 			}
 		}
-		if (!any)
+		if (d0 == 0.0f && d1 == 0.0f)
 			continue;
-		float in[12];
+		float in[3];
 		if (ncount) {
-			const float4 *q = e + (size_t)stride * (off + r);
-			float4 a = q[0];
+			float4 a = e[(size_t)stride * (off + r)];
 			in[0] = a.x;
 			in[1] = a.y;
 			in[2] = a.z;
@@ -1173,46 +1211,61 @@ __global__ void __launch_bounds__(128) k_grid_grad(
 		}
 		float x[3];
 		uint32_t scene = nrc_position(in, B, scode, x);
+		uint32_t c[3];
+		float w[3];
 #pragma unroll
-		for (int l = 0; l < kGridLevels; l++) {
-			if (df[2 * l] == 0.0f && df[2 * l + 1] == 0.0f)
-				continue;
-			uint32_t c[3];
-			float w[3];
+		for (int a = 0; a < 3; a++)
+			grid_cell(l, x[a], &c[a], &w[a]);
 #pragma unroll
-			for (int a = 0; a < 3; a++)
-				grid_cell(l, x[a], &c[a], &w[a]);
-#pragma unroll
-			for (int b = 0; b < 8; b++) {
-				uint32_t k = grid_index(l, c[0] + (b & 1),
-				  c[1] + ((b >> 1) & 1), c[2] + ((b >> 2) & 1), scene);
-				float wt = grid_weight(b, w);
-				atomicAdd(gg + 2u * k, __fmul_rn(wt, df[2 * l]));
-				atomicAdd(gg + 2u * k + 1u, __fmul_rn(wt, df[2 * l + 1]));
-			}
+		for (int b = 0; b < 8; b++) {
+			uint32_t k = grid_index(l, c[0] + (b & 1), c[1] + ((b >> 1) & 1),
+			  c[2] + ((b >> 2) & 1), scene);
+			float wt = grid_weight(b, w);
+			atomicAdd(gg + k, make_float2(__fmul_rn(wt, d0),
+			  __fmul_rn(wt, d1)));
 		}
 	}
 }
 
-// One Adam step of the hash grid from the gradient gg (then cleared);
-// g_out receives the gradient when not null.
-__global__ void k_grid_adam(float *t, float *m, float *v, float *gg,
-                            float *g_out, int update, float lr, float beta1,
-                            float beta2, float eps, float bc1, float bc2)
+// One Adam step of the hash grid from the gradient gg (then cleared), four
+// parameters per thread; g_out receives the gradient when not null.  Lazy
+// (sparse) Adam: only parameters the batch touched (nonzero gradient) move
+// and decay their moments; the others, most of a large table, are not read
+// at all.  A parameter's first update is the dense one.
+__global__ void k_grid_adam(float4 *__restrict__ t, float4 *__restrict__ m,
+                            float4 *__restrict__ v, float4 *__restrict__ gg,
+                            float4 *__restrict__ g_out, int update, float lr,
+                            float beta1, float beta2, float eps, float bc1,
+                            float bc2)
 {
-	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGridParams;
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGridParams / 4;
 	     i += gridDim.x * blockDim.x) {
-		float g = gg[i];
-		gg[i] = 0.0f;
+		float4 g4 = gg[i];
+		bool any = g4.x != 0.0f || g4.y != 0.0f || g4.z != 0.0f ||
+		  g4.w != 0.0f;
 		if (g_out)
-			g_out[i] = g;
+			g_out[i] = g4;
+		if (!any)
+			continue;
+		gg[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 		if (!update)
 			continue;
-		float mi = beta1 * m[i] + (1.0f - beta1) * g;
-		float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
-		m[i] = mi;
-		v[i] = vi;
-		t[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+		float4 m4 = m[i], v4 = v[i], t4 = t[i];
+		float *gp = &g4.x, *mp = &m4.x, *vp = &v4.x, *tp = &t4.x;
+#pragma unroll
+		for (int k = 0; k < 4; k++) {
+			float g = gp[k];
+			if (g == 0.0f)
+				continue;
+			float mi = beta1 * mp[k] + (1.0f - beta1) * g;
+			float vi = beta2 * vp[k] + (1.0f - beta2) * g * g;
+			mp[k] = mi;
+			vp[k] = vi;
+			tp[k] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+		}
+		m[i] = m4;
+		v[i] = v4;
+		t[i] = t4;
 	}
 }
 

@@ -128,6 +128,10 @@ struct Ctx {
 	DevBuf mlp_act, mlp_dz; // training: layer inputs and output gradients
 	// the position hash grid: FP32 table, Adam moments, gradient
 	DevBuf grid_t, grid_m, grid_v, grid_g;
+	DevBuf qgrid; // the queries' grid features (16 BF16 each)
+	// side stream of the grid's training kernels and its fork/join events
+	cudaStream_t aux = nullptr;
+	cudaEvent_t  ev_fork = nullptr, ev_grad = nullptr, ev_join = nullptr;
 	uint32_t mlp_step = 0;
 	bool     mlp_ready = false;
 	NrcBox   box{};
@@ -576,6 +580,11 @@ const float2 *grid_of(Ctx *c)
 // uniform in +-1e-4 from the same stream (as instant-NGP initialises them).
 int nrc_reset(Ctx *c, uint64_t seed)
 {
+	if (!c->aux) {
+		NB_CK(c, cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
+		for (cudaEvent_t *e : {&c->ev_fork, &c->ev_grad, &c->ev_join})
+			NB_CK(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+	}
 	NB_CK(c, c->mlp_wf.ensure(kMlpParams * sizeof(float)));
 	NB_CK(c, c->mlp_m.ensure(kMlpParams * sizeof(float)));
 	NB_CK(c, c->mlp_v.ensure(kMlpParams * sizeof(float)));
@@ -659,7 +668,11 @@ uint32_t nrc_steps(const Ctx *c)
 {
 	return c->cfg.reserved[3] ? std::min(c->cfg.reserved[3], 64u) : 6u;
 }
-constexpr uint32_t kNrcTrainPaths = 65536; // training paths per frame (2^16)
+// Training paths per frame (cfg.reserved[6]; 0 = 2^16).
+uint32_t nrc_train_paths(const Ctx *c)
+{
+	return c->cfg.reserved[6] ? c->cfg.reserved[6] : 65536u;
+}
 
 // Radiance-cache buffers of a frame: queries and their features/outputs
 // for every path, records for the training paths' vertices.
@@ -671,8 +684,10 @@ int nrc_frame_buffers(Ctx *c)
 			return rc;
 	}
 	uint32_t np = c->npaths;
-	// about 2^16 training paths, and never more than 1 path in 16
-	c->nrc_stride = std::max(16u, np / kNrcTrainPaths);
+	// about nrc_train_paths training paths, and by default never more than
+	// 1 path in 16 (1 in 4 when the count is set)
+	c->nrc_stride = std::max(c->cfg.reserved[6] ? 4u : 16u,
+	  np / std::max(nrc_train_paths(c), 1u));
 	uint32_t verts = c->cfg.max_depth > 1 ? c->cfg.max_depth - 1 : 1;
 	// warm-up frames record from every path; later frames overwrite the
 	// capacity-limited prefix only, so cap at 4 batches per frame worth of
@@ -745,9 +760,20 @@ int nrc_query(Ctx *c, const float4 *q, const uint32_t *count, uint32_t cap,
 	int rc = fwd_tc_setup<true>(c, cap, &grid, &smem);
 	if (rc)
 		return rc;
+	NrcBox box = frame ? kUnitBox : c->box;
+	const uint4 *gq = nullptr;
+	if (nrc_grid(c)) {
+		// the queries' grid features first, gathered at full occupancy
+		NB_CK(c, c->qgrid.ensure((size_t)cap * 32));
+		k_grid_query_feats<<<grid_for(c, cap * (uint32_t)kGridLevels, 256),
+		  256, 0, c->stream>>>(q, count, cap, box, frame, grid_of(c),
+		  c->qgrid.as<uint32_t>());
+		NB_CK(c, cudaGetLastError());
+		gq = c->qgrid.as<uint4>();
+	}
 	k_mlp_fwd_tc<true><<<grid, kTcThreads, smem, c->stream>>>(
 	  c->mlp_wbf.as<__nv_bfloat16>(), nullptr, cap, nullptr, count, errs, q,
-	  frame ? kUnitBox : c->box, pL, npath, frame, grid_of(c));
+	  box, pL, npath, frame, gq);
 	NB_CK(c, cudaGetLastError());
 	return 0;
 }
@@ -795,6 +821,32 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 	  c->mlp_loss.as<float>(), ncount, offset, cap,
 	  c->berr.as<uint32_t>() + 1);
 	NB_CK(c, cudaGetLastError());
+	if (update)
+		c->mlp_step++;
+	float bc1 = 1.0f - std::pow(kAdamBeta1, (float)std::max(c->mlp_step, 1u));
+	float bc2 = 1.0f - std::pow(kAdamBeta2, (float)std::max(c->mlp_step, 1u));
+	// the grid's gradient and Adam step on the side stream, beside pass 2
+	// and the MLP's step (they read pass 1's outputs and write only the
+	// grid); the MLP's step waits for the gradient, which reads this
+	// forward pass's BF16 W0, and the caller's next work for the grid
+	bool with_grid = gs && nrc_grid(c) && (gs->e || gs->raw) && c->aux;
+	if (with_grid) {
+		NB_CK(c, cudaEventRecord(c->ev_fork, c->stream));
+		NB_CK(c, cudaStreamWaitEvent(c->aux, c->ev_fork, 0));
+		k_grid_grad<<<grid_for(c, n * (uint32_t)kGridLevels, 256), 256, 0,
+		  c->aux>>>(gs->e, gs->raw, gs->stride, ncount, offset, cap, n,
+		  gs->box, gs->scode, c->mlp_dz.as<__nv_bfloat16>(),
+		  c->mlp_wbf.as<__nv_bfloat16>(), c->grid_g.as<float2>());
+		NB_CK(c, cudaGetLastError());
+		NB_CK(c, cudaEventRecord(c->ev_grad, c->aux));
+		k_grid_adam<<<grid_for(c, kGridParams / 4, 256), 256, 0,
+		  c->aux>>>(c->grid_t.as<float4>(), c->grid_m.as<float4>(),
+		  c->grid_v.as<float4>(), c->grid_g.as<float4>(),
+		  reinterpret_cast<float4 *>(gs->g_out), update, nrc_lr(c),
+		  kAdamBeta1, kAdamBeta2, kAdamEps, bc1, bc2);
+		NB_CK(c, cudaGetLastError());
+		NB_CK(c, cudaEventRecord(c->ev_join, c->aux));
+	}
 	// pass 2: split-K weight-gradient UMMAs, (splits x 6 layers) CTAs
 	uint32_t chunks = (npad + (uint32_t)kDwChunk - 1u) / (uint32_t)kDwChunk;
 	uint32_t splits = std::min<uint32_t>(32u, chunks);
@@ -808,33 +860,16 @@ int nrc_train(Ctx *c, const void *feats, const float4 *targets, uint32_t n,
 	  c->mlp_act.as<__nv_bfloat16>(), c->mlp_dz.as<__nv_bfloat16>(), npad,
 	  rows_per, c->mlp_part.as<float>(), c->berr.as<uint32_t>() + 1);
 	NB_CK(c, cudaGetLastError());
-	// the grid's gradient reads the BF16 layer-0 weights of this forward
-	// pass: before the MLP's Adam step replaces them
-	bool with_grid = gs && nrc_grid(c) && (gs->e || gs->raw);
-	if (with_grid) {
-		k_grid_grad<<<grid_for(c, n, 128), 128, 0, c->stream>>>(gs->e,
-		  gs->raw, gs->stride, ncount, offset, cap, n, gs->box, gs->scode,
-		  c->mlp_dz.as<__nv_bfloat16>(), c->mlp_wbf.as<__nv_bfloat16>(),
-		  c->grid_g.as<float>());
-		NB_CK(c, cudaGetLastError());
-	}
-	if (update)
-		c->mlp_step++;
-	float bc1 = 1.0f - std::pow(kAdamBeta1, (float)std::max(c->mlp_step, 1u));
-	float bc2 = 1.0f - std::pow(kAdamBeta2, (float)std::max(c->mlp_step, 1u));
+	if (with_grid)
+		NB_CK(c, cudaStreamWaitEvent(c->stream, c->ev_grad, 0));
 	k_mlp_adam<<<grid_for(c, kMlpParams, 256), 256, 0, c->stream>>>(
 	  c->mlp_wf.as<float>(), c->mlp_m.as<float>(), c->mlp_v.as<float>(),
 	  c->mlp_part.as<float>(), (int)splits, g_out, update, nrc_lr(c),
 	  kAdamBeta1, kAdamBeta2, kAdamEps, bc1, bc2,
 	  c->mlp_wbf.as<__nv_bfloat16>(), c->mlp_wbt.as<__nv_bfloat16>());
 	NB_CK(c, cudaGetLastError());
-	if (with_grid) {
-		k_grid_adam<<<grid_for(c, kGridParams, 256), 256, 0, c->stream>>>(
-		  c->grid_t.as<float>(), c->grid_m.as<float>(), c->grid_v.as<float>(),
-		  c->grid_g.as<float>(), gs->g_out, update, nrc_lr(c), kAdamBeta1,
-		  kAdamBeta2, kAdamEps, bc1, bc2);
-		NB_CK(c, cudaGetLastError());
-	}
+	if (with_grid)
+		NB_CK(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
 	if (loss) {
 		std::vector<float> l(grid);
 		NB_CK(c, cudaMemcpyAsync(l.data(), c->mlp_loss.p, grid * 4,
@@ -1075,7 +1110,7 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		  F.cnt + 3, true);
 		if (rc)
 			return rc;
-		c->st.launches += 1;
+		c->st.launches += nrc_grid(c) ? 2 : 1;
 		ev_record(c);
 	}
 	k_accum<<<grid_for(c, c->npix, 256), 256, 0, c->stream>>>(S, F);
@@ -1255,7 +1290,7 @@ void free_ctx(Ctx *c)
 	  &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf, &c->cnt,
 	  &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr, &c->mlp_act,
 	  &c->mlp_dz, &c->mlp_wf, &c->grid_t, &c->grid_m, &c->grid_v,
-	  &c->grid_g,
+	  &c->grid_g, &c->qgrid,
 	  &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt, &c->mlp_part,
 	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat, &c->waitchk,
 	  &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob, &c->dyn_wbox,
@@ -1266,6 +1301,11 @@ void free_ctx(Ctx *c)
 	for (int i = 0; i < kMaxEvents; i++)
 		if (c->ev[i])
 			cudaEventDestroy(c->ev[i]);
+	for (cudaEvent_t e : {c->ev_fork, c->ev_grad, c->ev_join})
+		if (e)
+			cudaEventDestroy(e);
+	if (c->aux)
+		cudaStreamDestroy(c->aux);
 	if (c->stream)
 		cudaStreamDestroy(c->stream);
 	delete c;
@@ -1279,7 +1319,7 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->shadow, &c->scol, &c->pT, &c->pL, &c->rng, &c->acc, &c->buf,
 	  &c->cnt, &c->rays, &c->brays, &c->braw, &c->bhits, &c->berr,
 	  &c->mlp_act, &c->mlp_dz, &c->grid_t, &c->grid_m, &c->grid_v,
-	  &c->grid_g,
+	  &c->grid_g, &c->qgrid,
 	  &c->mlp_wf, &c->mlp_m, &c->mlp_v, &c->mlp_wbf, &c->mlp_wbt,
 	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec, &c->waitchk,
 	  &c->rfeat, &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob,
@@ -2643,9 +2683,10 @@ int rendgpu_nrc_train_raw_device(struct rdata *rdp, const float *raw,
 		return fail(c, RENDGPU_ESTATE, "rendgpu_nrc_reset must come first");
 	if (!c->have_dynamic)
 		return fail(c, RENDGPU_ESTATE, "upload_dynamic must come first");
-	if (n && (!raw || misaligned16(targets)))
+	if (n && (!raw || misaligned16(targets) ||
+	  (grid_grad && misaligned16(grid_grad))))
 		return fail(c, RENDGPU_EINVAL, "raw must be a non-null device "
-		  "pointer, targets non-null and 16-byte aligned");
+		  "pointer, targets (and grid_grad) 16-byte aligned");
 	if (n == 0)
 		return 0;
 	NB_CK(c, cudaSetDevice(c->device));

@@ -85,7 +85,7 @@ def adam(w, m, v, g, step, lr=1e-2, b1=0.9, b2=0.99, eps=1e-15):
 # axis over the unit box; corners indexed densely where (res + 1)^3 fits a
 # level's table, else by the spatial hash of Teschner et al. 2003.
 GRID_LEVELS = 8
-GRID_T = 1 << 15
+GRID_T = 1 << 17
 GRID_RES = (16, 28, 52, 95, 172, 312, 565, 1024)
 GRID_PARAMS = GRID_LEVELS * GRID_T * 2
 
