@@ -147,6 +147,7 @@ struct Ctx {
 	// device-side scene update (rendgpu_update_instances*): per-instance
 	// BLAS root boxes, new matrices, world boxes, TLAS build queues, slot
 	// ranges and instance order (refit), build info, emitter sources, area
+	DevBuf   dyn_idx, dyn_ctr; // device TLAS build: order, counters
 	DevBuf   dyn_root, dyn_glob, dyn_wbox, dyn_q, dyn_ranges, dyn_order,
 	         dyn_info, dyn_emit, dyn_area, dyn_trange;
 	uint32_t dyn_nemit = 0;
@@ -1295,7 +1296,7 @@ void free_ctx(Ctx *c)
 	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat, &c->waitchk,
 	  &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob, &c->dyn_wbox,
 	  &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info, &c->dyn_emit,
-	  &c->dyn_area, &c->dyn_trange};
+	  &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr};
 	for (DevBuf *b : bufs)
 		b->release();
 	for (int i = 0; i < kMaxEvents; i++)
@@ -1324,7 +1325,7 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec, &c->waitchk,
 	  &c->rfeat, &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob,
 	  &c->dyn_wbox, &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info,
-	  &c->dyn_emit, &c->dyn_area, &c->dyn_trange};
+	  &c->dyn_emit, &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
 		s += b->cap;
@@ -1579,16 +1580,51 @@ int dyn_prepare(Ctx *c, uint64_t *bytes)
 
 uint32_t device_tlas_limit(const Ctx *c);
 
-// k_tlas_build with its instance boxes in dynamic shared memory (up to
-// 128 KB beside 42 KB of static shared memory).
-cudaError_t launch_tlas_build(Ctx *c, const TbArgs &A)
+// Device TLAS build over the world boxes in dyn_wbox (n instances of the
+// single scene), one launch per level up to the depth limit (levels past
+// the tree's depth find no open node and return at once); returns the
+// depth limit used.
+int tlas_build(Ctx *c, uint32_t n, uint32_t *limit)
 {
-	cudaError_t e = cudaFuncSetAttribute(k_tlas_build,
-	  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tb_smem(kTbMaxInst));
-	if (e != cudaSuccess)
-		return e;
-	k_tlas_build<<<1, kTbWarps * 32, tb_smem(A.n), c->stream>>>(A);
-	return cudaGetLastError();
+	uint32_t nn = std::max(n, 1u);
+	NB_CK(c, c->dyn_idx.ensure((size_t)2 * nn * sizeof(uint16_t)));
+	NB_CK(c, c->dyn_ctr.ensure(4 * sizeof(uint32_t)));
+	TbArgs A;
+	A.wbox = c->dyn_wbox.as<float4>();
+	A.n = n;
+	A.inst_base = 0u;
+	A.nodes = c->tlas.as<nb_qnode>();
+	A.node_cap = nn;
+	A.irefs = c->irefs.as<uint32_t>();
+	A.qa = c->dyn_q.as<TbNode>();
+	A.qb = c->dyn_q.as<TbNode>() + nn;
+	A.ranges = c->dyn_ranges.as<uint2>();
+	A.order = c->dyn_order.as<uint32_t>();
+	A.info = c->dyn_info.as<uint32_t>();
+	A.idx = c->dyn_idx.as<uint16_t>();
+	A.tmp = c->dyn_idx.as<uint16_t>() + nn;
+	A.ctr = c->dyn_ctr.as<uint32_t>();
+	// the uploaded trees sized the traversal stack; the device tree stays
+	// within what it holds
+	A.depth_limit = device_tlas_limit(c);
+	k_tlas_init<<<1, 512, 0, c->stream>>>(A);
+	NB_CK(c, cudaGetLastError());
+	uint64_t open = 1; // at most this many open nodes on a level
+	for (uint32_t level = 0; level < A.depth_limit; level++) {
+		// the level writes its children into the other queue
+		NB_CK(c, cudaMemsetAsync(A.ctr + 2u + ((level & 1u) ^ 1u), 0,
+		  sizeof(uint32_t), c->stream));
+		uint64_t nodes = std::min<uint64_t>(open, nn);
+		uint32_t grid = (uint32_t)std::min<uint64_t>((nodes +
+		  kTbLevelWarps - 1) / kTbLevelWarps, (uint64_t)c->nsm * 8u);
+		k_tlas_level<<<grid, kTbLevelWarps * 32, 0, c->stream>>>(A, level);
+		NB_CK(c, cudaGetLastError());
+		open *= 8u;
+	}
+	k_tlas_finish<<<grid_for(c, nn, 256), 256, 0, c->stream>>>(A);
+	NB_CK(c, cudaGetLastError());
+	*limit = A.depth_limit;
+	return 0;
 }
 
 // New object->world matrices (device, 16 floats each, rd->insts order) ->
@@ -1627,23 +1663,11 @@ int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
 		NB_CK(c, cudaGetLastError());
 	}
 	if (!refit) {
-		TbArgs A;
-		A.wbox = c->dyn_wbox.as<float4>();
-		A.n = n;
-		A.inst_base = 0u;
-		A.nodes = c->tlas.as<nb_qnode>();
-		A.node_cap = nn;
-		A.irefs = c->irefs.as<uint32_t>();
-		A.qa = c->dyn_q.as<TbNode>();
-		A.qb = c->dyn_q.as<TbNode>() + nn;
-		A.ranges = c->dyn_ranges.as<uint2>();
-		A.order = c->dyn_order.as<uint32_t>();
-		A.info = c->dyn_info.as<uint32_t>();
-		// the uploaded trees sized the traversal stack; the device tree
-		// stays within what it holds
-		A.depth_limit = device_tlas_limit(c);
-		h.tlas_depth = c->tlas_depth = A.depth_limit;
-		NB_CK(c, launch_tlas_build(c, A));
+		uint32_t limit = 0;
+		rc = tlas_build(c, n, &limit);
+		if (rc)
+			return rc;
+		h.tlas_depth = c->tlas_depth = limit;
 	} else {
 		k_tlas_refit<<<grid_for(c, nn * 32u, 256), 256, 0, c->stream>>>(
 		  c->dyn_wbox.as<float4>(), c->dyn_order.as<uint32_t>(),
@@ -1701,23 +1725,13 @@ int rebuild_tlas_tight(Ctx *c)
 	  c->dyn_trange.as<uint2>(), c->tris.as<float4>(),
 	  c->dyn_wbox.as<float4>());
 	NB_CK(c, cudaGetLastError());
-	TbArgs A;
-	A.wbox = c->dyn_wbox.as<float4>();
-	A.n = n;
-	A.inst_base = 0u;
-	A.nodes = c->tlas.as<nb_qnode>();
-	A.node_cap = nn;
-	A.irefs = c->irefs.as<uint32_t>();
-	A.qa = c->dyn_q.as<TbNode>();
-	A.qb = c->dyn_q.as<TbNode>() + nn;
-	A.ranges = c->dyn_ranges.as<uint2>();
-	A.order = c->dyn_order.as<uint32_t>();
-	A.info = c->dyn_info.as<uint32_t>();
-	A.depth_limit = device_tlas_limit(c);
-	NB_CK(c, launch_tlas_build(c, A));
+	uint32_t limit = 0;
+	int rc = tlas_build(c, n, &limit);
+	if (rc)
+		return rc;
 	NB_CK(c, cudaStreamSynchronize(c->stream));
 	h.tlas_root = 0u;
-	h.tlas_depth = c->tlas_depth = A.depth_limit;
+	h.tlas_depth = c->tlas_depth = limit;
 	c->dyn_built = true;
 	return 0;
 }

@@ -10,9 +10,10 @@
 //
 //   k_inst_update   inverse (the FP64 cofactor sequence of the host bridge,
 //                   so world->object bits match it) and world box per instance
-//   k_tlas_build    one CTA: top-down binned SAH straight into the 8-wide
-//                   quantised node layout (gpulayout.h), one warp per open
-//                   node, level by level
+//   k_tlas_init, k_tlas_level, k_tlas_finish
+//                   top-down binned SAH straight into the 8-wide quantised
+//                   node layout (gpulayout.h), one launch per tree level,
+//                   one warp per open node over all SMs
 //   k_tlas_refit    same topology, child boxes recomputed from the instance
 //                   ranges the last build recorded, all nodes in parallel
 //   k_light_update  world-space emitting triangles and their area CDF (the
@@ -34,7 +35,6 @@
 namespace nb {
 
 constexpr uint32_t kTbMaxInst = 4096; // hit ids keep 12 instance bits
-constexpr int kTbWarps = 16;
 constexpr int kTbBins = 16;
 
 // ------------------------------------------------------ instance update --
@@ -235,6 +235,8 @@ struct TbArgs {
 	uint32_t     *order;    // instance order of the ranges (n)
 	uint32_t     *info;     // [0] nodes, [1] depth, [2] overflow
 	uint32_t      depth_limit;
+	uint16_t     *idx, *tmp; // instance order being partitioned (n each)
+	uint32_t     *ctr;       // [0] nodes, [1] items, [2]/[3] queue a/b
 };
 
 struct TbBin {
@@ -614,88 +616,107 @@ __device__ void tb_node(const TbArgs &A, uint16_t *idx, uint16_t *tmp,
 	atomicMax(&A.info[1], nd.depth);
 }
 
-// Dynamic shared memory of k_tlas_build for n instances: their boxes.
-__host__ __device__ constexpr size_t tb_smem(uint32_t n)
-{
-	return (size_t)2u * n * sizeof(float4);
-}
+// The build, level by level: k_tlas_init opens the root, then one
+// k_tlas_level launch per tree level builds that level's open nodes, one
+// warp per node over all SMs (the nodes of a level are independent), and
+// k_tlas_finish records the node count and the instance order.  State
+// between launches lives in global memory: the instance order (A.idx,
+// A.tmp), the two level queues and the counters A.ctr: [0] nodes, [1] leaf
+// items, [2] / [3] entries of queue a / b.
 
-// The whole TLAS in one CTA of kTbWarps warps.  The instance boxes are
-// staged in dynamic shared memory (tb_smem(n) bytes), so the passes over a
-// node's instances (bounds, bins, partition) read shared memory, not L2.
-__global__ void __launch_bounds__(kTbWarps * 32) k_tlas_build(TbArgs A)
+// Root node over all instances (one CTA), counters reset.
+__global__ void __launch_bounds__(512) k_tlas_init(TbArgs A)
 {
-	extern __shared__ float4 sbox[];
-	__shared__ uint16_t sidx[kTbMaxInst], stmp[kTbMaxInst];
-	__shared__ TbBin bins[kTbWarps][3 * kTbBins];
-	__shared__ TbChild chs[kTbWarps][8];
-	__shared__ uint32_t s_node, s_item, s_cnt[2];
-	const uint32_t tid = threadIdx.x, warp = tid >> 5;
-	for (uint32_t i = tid; i < 2u * A.n; i += blockDim.x)
-		sbox[i] = A.wbox[i];
-	A.wbox = sbox;
-	for (uint32_t i = tid; i < A.n; i += blockDim.x)
-		sidx[i] = (uint16_t)i;
-	if (tid == 0) {
-		s_node = 1u;
-		s_item = 0u;
-		s_cnt[0] = A.n ? 1u : 0u;
-		s_cnt[1] = 0u;
-		A.info[1] = 1u;
-		A.info[2] = 0u;
-	}
-	__syncthreads();
-	if (warp == 0) {
-		float lo[3], hi[3];
-		tb_range_box(A.wbox, sidx, 0u, A.n, lo, hi);
-		if (tid == 0) {
-			TbNode r;
-			r.start = 0u;
-			r.cnt = A.n;
-			r.node = 0u;
-			r.depth = 1u;
-			for (int a = 0; a < 3; a++) {
-				r.lo[a] = lo[a];
-				r.hi[a] = hi[a];
-			}
-			A.qa[0] = r;
-			if (A.n == 0u) {
-				// no instances: a root without children
-				float cmin[8][3], cmax[8][3];
-				for (int s = 0; s < 8; s++)
-					for (int a = 0; a < 3; a++) {
-						cmin[s][a] = 1.0f;
-						cmax[s][a] = -1.0f;
-					}
-				nb_qnode q;
-				memset(&q, 0, sizeof(q));
-				quantise_node_hd(cmin, cmax, &q);
-				A.nodes[0] = q;
-				for (int s = 0; s < 8; s++)
-					A.ranges[s] = make_uint2(0u, 0u);
-			}
+	__shared__ float part[16][6];
+	const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+	float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+	float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+	for (uint32_t i = tid; i < A.n; i += blockDim.x) {
+		A.idx[i] = (uint16_t)i;
+		float l[3], h[3];
+		tb_load(A.wbox, i, l, h);
+		for (int a = 0; a < 3; a++) {
+			lo[a] = fminf(lo[a], l[a]);
+			hi[a] = fmaxf(hi[a], h[a]);
 		}
 	}
+	tb_warp_box(lo, hi);
+	if (lane == 0)
+		for (int a = 0; a < 3; a++) {
+			part[warp][a] = lo[a];
+			part[warp][3 + a] = hi[a];
+		}
 	__syncthreads();
-	int cur = 0;
-	for (int level = 0; level < 64; level++) {
-		uint32_t cnt = s_cnt[cur];
-		if (cnt == 0u)
-			break;
-		TbNode *q = cur ? A.qb : A.qa, *nq = cur ? A.qa : A.qb;
-		for (uint32_t k = warp; k < cnt; k += kTbWarps)
-			tb_node(A, sidx, stmp, bins[warp], chs[warp], q[k], nq,
-			  &s_cnt[cur ^ 1], &s_node, &s_item);
-		__syncthreads();
-		if (tid == 0)
-			s_cnt[cur] = 0u;
-		cur ^= 1;
-		__syncthreads();
+	if (tid != 0)
+		return;
+	for (uint32_t w = 1; w < (blockDim.x >> 5); w++)
+		for (int a = 0; a < 3; a++) {
+			part[0][a] = fminf(part[0][a], part[w][a]);
+			part[0][3 + a] = fmaxf(part[0][3 + a], part[w][3 + a]);
+		}
+	TbNode r;
+	r.start = 0u;
+	r.cnt = A.n;
+	r.node = 0u;
+	r.depth = 1u;
+	for (int a = 0; a < 3; a++) {
+		r.lo[a] = part[0][a];
+		r.hi[a] = part[0][3 + a];
 	}
-	for (uint32_t i = tid; i < A.n; i += blockDim.x)
-		A.order[i] = sidx[i];
-	if (tid == 0)
-		A.info[0] = s_node;
+	A.qa[0] = r;
+	A.ctr[0] = 1u;
+	A.ctr[1] = 0u;
+	A.ctr[2] = A.n ? 1u : 0u;
+	A.ctr[3] = 0u;
+	A.info[1] = 1u;
+	A.info[2] = 0u;
+	if (A.n == 0u) {
+		// no instances: a root without children
+		float cmin[8][3], cmax[8][3];
+		for (int s = 0; s < 8; s++)
+			for (int a = 0; a < 3; a++) {
+				cmin[s][a] = 1.0f;
+				cmax[s][a] = -1.0f;
+			}
+		nb_qnode q;
+		memset(&q, 0, sizeof(q));
+		quantise_node_hd(cmin, cmax, &q);
+		A.nodes[0] = q;
+		for (int s = 0; s < 8; s++)
+			A.ranges[s] = make_uint2(0u, 0u);
+	}
+}
+
+constexpr int kTbLevelWarps = 4; // warps (open nodes in flight) per CTA
+
+// The open nodes of one level (queue a for even levels, b for odd ones),
+// one warp each; their inner children go to the other queue, whose count
+// the host zeroed before the launch.
+__global__ void __launch_bounds__(kTbLevelWarps * 32) k_tlas_level(
+  TbArgs A, uint32_t level)
+{
+	__shared__ TbBin bins[kTbLevelWarps][3 * kTbBins];
+	__shared__ TbChild chs[kTbLevelWarps][8];
+	const uint32_t warp = threadIdx.x >> 5;
+	const uint32_t cur = level & 1u;
+	const TbNode *q = cur ? A.qb : A.qa;
+	TbNode *nq = cur ? A.qa : A.qb;
+	const uint32_t cnt = A.ctr[2u + cur];
+	const uint32_t nw = gridDim.x * (uint32_t)kTbLevelWarps;
+	for (uint32_t k = blockIdx.x * (uint32_t)kTbLevelWarps + warp; k < cnt;
+	     k += nw)
+		tb_node(A, A.idx, A.tmp, bins[warp], chs[warp], q[k], nq,
+		  &A.ctr[2u + (cur ^ 1u)], &A.ctr[0], &A.ctr[1]);
+}
+
+// Node count and the instance order of the node ranges (for the refit).
+__global__ void k_tlas_finish(TbArgs A)
+{
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n;
+	     i += gridDim.x * blockDim.x)
+		A.order[i] = A.idx[i];
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		A.info[0] = A.ctr[0];
 }
 
 // Refit: the topology of the last build, child boxes recomputed from the
