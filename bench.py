@@ -47,6 +47,9 @@ def parse():
     p.add_argument("--depth", type=int, default=WORKLOAD["depth"])
     p.add_argument("--blas", type=int, default=0,
                    help="BLAS count (0 = the workload's 64)")
+    p.add_argument("--ref-blas", action="store_true",
+                   help="trace the reference's BVH8 BLASes converted node "
+                   "for node instead of the library's own build")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--sort", type=int, default=0,
@@ -508,7 +511,8 @@ def run_ours(a):
     scene = api.Scene(WORKLOAD["family"], WORKLOAD["seed"], a.blas)
     rd = api.RenderData(scene, a.width, a.height, a.spp)
     gr = api.GpuRenderer(rd, max_depth=a.depth, seed=1 + rank, timing=True,
-                         device=dev, sched=a.sched).upload()
+                         device=dev, sched=a.sched,
+                         ref_blas=a.ref_blas).upload()
     if a.sort or a.block or a.fuse:
         gr.set_tune(sort=a.sort, block=a.block, fuse=a.fuse)
     stream = torch.cuda.ExternalStream(gr.stream(), device=dev)
@@ -621,7 +625,8 @@ def run_ours(a):
         # one context per rdata: the counting context replaces the timed one
         gr.close()
         gc = api.GpuRenderer(rd, max_depth=a.depth, seed=1 + rank,
-                             count=True, device=dev, sched=a.sched).upload()
+                             count=True, device=dev, sched=a.sched,
+                             ref_blas=a.ref_blas).upload()
         gc.frame()
         sc = gc.stats()
         visits = {"nodes_per_ray": sc["node_visits"] / sc["closest_rays"],

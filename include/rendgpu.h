@@ -81,7 +81,11 @@ struct rendgpu_cfg {
 	                         of 16384 samples per frame (0 = 6); [4] bit 0:
 	                         keep the TLAS rendgpu_upload_dynamic converts
 	                         from rd->bnodes instead of the device rebuild
-	                         over tight instance boxes; [5] bit 0: no hash
+	                         over tight instance boxes; [4] bit 1: keep the
+	                         BLASes rendgpu_upload_static converts from
+	                         rd->bnodes instead of building its own (SAH
+	                         binary build collapsed to 8-wide nodes by
+	                         cost); [5] bit 0: no hash
 	                         grid in the cache's position encoding; [6]:
 	                         cache training paths per frame (0 = 65536) */
 };

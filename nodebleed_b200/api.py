@@ -420,7 +420,7 @@ class GpuRenderer:
                  timing=False, device=0, count=False, sched=0,
                  nrc_warmup=0, nrc_lr=0.0, graph=False, block=0,
                  nrc_end=0, nrc_steps=0, ref_tlas=False, nrc_grid=True,
-                 nrc_train_paths=0):
+                 nrc_train_paths=0, ref_blas=False):
         self.g = gpu_lib().L
         self.rdata = rdata
         self.ptr = rdata.ptr
@@ -431,7 +431,7 @@ class GpuRenderer:
         cfg.reserved[1] = nrc_warmup
         cfg.reserved[2] = nrc_end
         cfg.reserved[3] = nrc_steps
-        cfg.reserved[4] = 1 if ref_tlas else 0
+        cfg.reserved[4] = (1 if ref_tlas else 0) | (2 if ref_blas else 0)
         cfg.reserved[5] = 0 if nrc_grid else 1
         cfg.reserved[6] = nrc_train_paths
         rc = self.g.rendgpu_init(self.ptr, C.byref(cfg))
@@ -650,7 +650,8 @@ class BatchRenderer:
     or one per scene."""
 
     def __init__(self, rdatas, max_depth=5, mode=MODE_PATH, seed=1,
-                 timing=False, device=0, sched=0, block=0, nrc_grid=True):
+                 timing=False, device=0, sched=0, block=0, nrc_grid=True,
+                 ref_blas=False):
         self.g = gpu_lib().L
         self.rdatas = list(rdatas)
         n = len(self.rdatas)
@@ -660,6 +661,7 @@ class BatchRenderer:
         ptrs = (C.c_void_p * n)(*[r.ptr for r in self.rdatas])
         cfg = make_cfg(max(depths), mode, seed, timing, device, False, sched,
                        True, block)
+        cfg.reserved[4] = 2 if ref_blas else 0
         cfg.reserved[5] = 0 if nrc_grid else 1
         h = C.c_void_p()
         rc = self.g.rendgpu_batch_init(ptrs, n, self.depths, C.byref(cfg),

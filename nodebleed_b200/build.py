@@ -62,7 +62,8 @@ def build_gpu(force=False):
     out = os.path.join(HERE, "libnbgpu.so")
     cu = os.path.join(CSRC, "rendgpu.cu")
     cpp = os.path.join(CSRC, "layout.cpp")
-    deps = [cu, cpp] + [os.path.join(CSRC, f) for f in
+    cpp2 = os.path.join(CSRC, "blas_build.cpp")
+    deps = [cu, cpp, cpp2] + [os.path.join(CSRC, f) for f in
                         ("trace.cuh", "kernels.cuh", "nrc.cuh", "gpulayout.h",
                          "layout.hpp", "qnode.h", "tlas_build.cuh",
                          os.path.join("host", "nb_rdata.h"))]
@@ -73,12 +74,15 @@ def build_gpu(force=False):
     os.makedirs(tmp, exist_ok=True)
     o1 = os.path.join(tmp, "layout.o")
     o2 = os.path.join(tmp, "rendgpu.o")
+    o3 = os.path.join(tmp, "blas_build.o")
     _run(["g++", "-std=c++17", "-O2", "-fPIC", "-Wall", "-I", CSRC,
           "-c", cpp, "-o", o1])
+    _run(["g++", "-std=c++17", "-O2", "-fPIC", "-Wall", "-I", CSRC,
+          "-c", cpp2, "-o", o3])
     _run([NVCC, "-std=c++17", "-O3", "-lineinfo", "-fmad=false",
           "-Xptxas", "-v", "-Xcompiler", "-fPIC", "-I", CSRC] + ARCH +
          ["-c", cu, "-o", o2])
-    _run([NVCC, "-shared", "-o", out, o1, o2] + ARCH)
+    _run([NVCC, "-shared", "-o", out, o1, o3, o2] + ARCH)
     return out
 
 

@@ -47,6 +47,38 @@ float build_lights(const nb_rdata *rd, std::vector<nb_glight> &lights,
                    const std::unordered_map<uint32_t,
                    std::vector<uint32_t>> *emitters = nullptr);
 
+// Settings of the BLAS build (blas_build.cpp): SAH cost of visiting an
+// 8-wide node and of testing one triangle, per unit of box area.
+struct blas_params {
+	float c_node = 1.0f;
+	float c_tri = 0.3f;
+};
+
+// One BLAS in the GPU layout with node and item indices from 0 (append_blas
+// moves them to their place in the shared arrays).
+struct blas_out {
+	std::vector<nb_qnode> nodes;
+	std::vector<nb_gtri> tris;
+	uint32_t depth = 0;
+};
+
+// SAH binary build + optimal 8-wide collapse of the mesh's triangles
+// rd->tris[triofs .. triofs + tricnt).  Returns false with `err` set on a
+// mesh it cannot build (no triangles, non-finite vertices).
+bool build_blas(const nb_rdata *rd, uint32_t triofs, uint32_t tricnt,
+                const blas_params &prm, blas_out *out, std::string *err);
+
+// build_blas of several meshes on the host's cores.
+bool build_blas_many(const nb_rdata *rd, const std::vector<uint32_t> &triofs,
+                     const std::vector<uint32_t> &tricnt,
+                     const blas_params &prm, std::vector<blas_out> &out,
+                     std::string *err);
+
+// Append a built BLAS to the shared node and triangle arrays; *root gets
+// its root node index.
+void append_blas(const blas_out &b, std::vector<nb_qnode> &nodes,
+                 std::vector<nb_gtri> &tris, uint32_t *root);
+
 // Quantise one node: child boxes (min/max per slot; empty slots have
 // min > max) into n (origin, exponents, qlo/qhi).  Exposed for tests.
 void quantise_node(const float cmin[8][3], const float cmax[8][3],

@@ -1390,6 +1390,14 @@ int new_ctx(nb_rdata *const *rds, uint32_t n, const uint32_t *max_depth,
 
 // ------------------------------------------------------------- uploads --
 
+// BLASes built for the traversal (blas_build.cpp: SAH binary build, optimal
+// 8-wide collapse) unless cfg.reserved[4] bit 1 keeps the reference's BVH8
+// from rd->bnodes, converted node for node.  Hits do not depend on the tree.
+bool own_blas(const Ctx *c)
+{
+	return !(c->cfg.reserved[4] & 2u);
+}
+
 // BLAS of every scene (rend_prepstatic output) into the shared node and
 // triangle arrays; normals and materials of all scenes back to back, with
 // each scene's material ids offset by its material base.
@@ -1412,6 +1420,7 @@ int upload_static_all(Ctx *c)
 		h.tri_range.clear();
 		h.blas_depth = 0;
 		uint32_t maxtri = 0, maxmtl = 0;
+		std::vector<uint32_t> uofs, ucnt; // distinct meshes in order
 		for (uint32_t i = 0; i < rd->instcnt; i++) {
 			const nb_rinst &ri = rd->insts[i];
 			if (ri.tricnt == 0)
@@ -1423,16 +1432,33 @@ int upload_static_all(Ctx *c)
 			maxtri = std::max(maxtri, ri.triofs + ri.tricnt);
 			if (h.root_of.count(ri.triofs))
 				continue;
-			uint32_t root = 0;
-			bvh_stats bs;
-			std::string err;
+			h.root_of[ri.triofs] = 0;
+			uofs.push_back(ri.triofs);
+			ucnt.push_back(ri.tricnt);
+		}
+		std::vector<blas_out> built;
+		std::string err;
+		if (own_blas(c) && !build_blas_many(rd, uofs, ucnt, blas_params(),
+		  built, &err))
+			return fail(c, RENDGPU_EINVAL, err);
+		for (size_t k = 0; k < uofs.size(); k++) {
+			uint32_t root = 0, depth = 0;
 			uint32_t first = (uint32_t)tris.size();
-			if (!convert_blas(rd, ri.triofs, nodes, tris, &root, &bs, &err))
-				return fail(c, RENDGPU_EINVAL, "BLAS of triofs " +
-				  std::to_string(ri.triofs) + ": " + err);
-			h.root_of[ri.triofs] = root;
-			h.tri_range[ri.triofs] = {first, (uint32_t)tris.size() - first};
-			h.blas_depth = std::max(h.blas_depth, bs.depth);
+			if (own_blas(c)) {
+				append_blas(built[k], nodes, tris, &root);
+				depth = built[k].depth;
+				built[k] = blas_out();
+			} else {
+				bvh_stats bs;
+				if (!convert_blas(rd, uofs[k], nodes, tris, &root, &bs,
+				  &err))
+					return fail(c, RENDGPU_EINVAL, "BLAS of triofs " +
+					  std::to_string(uofs[k]) + ": " + err);
+				depth = bs.depth;
+			}
+			h.root_of[uofs[k]] = root;
+			h.tri_range[uofs[k]] = {first, (uint32_t)tris.size() - first};
+			h.blas_depth = std::max(h.blas_depth, depth);
 		}
 		for (uint32_t t = 0; t < maxtri; t++)
 			maxmtl = std::max(maxmtl, rd->nrms[t].mtlid + 1u);
@@ -2119,6 +2145,7 @@ std::string tune_signature(const Ctx *c)
 		}
 	};
 	mix(c->cfg.mode);
+	mix(own_blas(c) ? 1u : 0u);
 	mix(c->sc.size());
 	for (const SceneHost &s : c->sc) {
 		mix(s.ntri);

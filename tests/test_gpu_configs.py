@@ -179,6 +179,28 @@ def test_scale_frame_rays_match_reference(gpu, scale_rd):
     gr.close()
 
 
+def test_own_blas_matches_converted_blas(gpu, scale_rd):
+    """The library's own BLAS build (SAH binary build collapsed to 8-wide
+    nodes) and the reference's BVH8 converted node for node give the same
+    closest hits on config 2's bounce rays: t bit-identical everywhere, the
+    triangle only differing where two triangles are hit at the same t."""
+    rd = scale_rd
+    got = _frame_capture(rd, 8, [1, 2], 100000, seed=3)
+    rays = np.concatenate([got[k][0] for k in got])
+    ga = api.GpuRenderer(rd).upload()
+    gb = api.GpuRenderer(rd, ref_blas=True).upload()
+    ha, hb = ga.trace(rays), gb.trace(rays)
+    oa, ob = ga.occluded(rays), gb.occluded(rays)
+    ga.close()
+    gb.close()
+    assert np.array_equal(ha["t"].view(np.uint32), hb["t"].view(np.uint32))
+    diff = ha["id"] != hb["id"]
+    print(f"own vs converted BLAS: {len(rays)} rays, {int(diff.sum())} "
+          "different triangles at the same t")
+    assert diff.sum() <= max(2, len(rays) // 2000)
+    assert np.array_equal(oa, ob)
+
+
 def test_stress_rays_match_reference(gpu, stress_rd):
     """Config 5's scene (4096 instances, the deepest stacks): bounce and
     shadow rays of a 960x540 depth-16 frame, plus random and camera rays."""
