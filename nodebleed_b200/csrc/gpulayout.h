@@ -9,10 +9,11 @@
 // Slots are assigned so that visiting them in the order key = slot ^ octant
 // approximates near-to-far for a ray of that octant.
 //
-// Quantised boxes are conservative: every child box is widened by at least
-// one quantum on each side, and the device test widens the far distance by a
-// relative 2^-20, so no ray that enters an FP32 child box misses its
-// quantised box.
+// Quantised boxes are conservative: every child plane lies at least 1/32 of a
+// quantum outside the FP32 child box, which covers the absolute rounding
+// error of the device's plane distances, and the device test widens the far
+// distance by a relative 2^-20, so no ray that enters an FP32 child box
+// misses its quantised box.
 
 #ifndef NB_GPULAYOUT_H
 #define NB_GPULAYOUT_H
@@ -29,7 +30,7 @@ extern "C" {
 
 struct nb_qnode { // 80 bytes, 16-byte aligned
 	float    px, py, pz;     // origin of the quantisation grid
-	uint8_t  ex, ey, ez;     // scale = 2^(e - 127) per axis
+	uint8_t  ex, ey, ez;     // scale = 2^(e - 119) per axis
 	uint8_t  imask;          // bit s: slot s is an inner node
 	uint32_t child_base;     // node index of the first inner child
 	uint32_t item_base;      // index of the first leaf item

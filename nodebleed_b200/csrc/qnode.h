@@ -71,13 +71,24 @@ NB_HD inline void assign_slots(int nchild, const float cen[8][3],
 	}
 }
 
+// Stored exponent byte of a scale 2^e.  The device forms 2^(byte - 127) =
+// 2^(e - 8), the scale of a plane byte placed in bits 8..15 of the float
+// 2^23 + 256 q (trace.cuh: visit).
+constexpr int kQExpBias = 127 - 8;
+
+// Margin, in quanta, by which child planes are rounded outwards beyond the
+// exact child box.  It covers the absolute rounding error of the device's
+// plane distances, at most 2^-9 + 2^-14 quanta (trace.cuh: visit); errors
+// relative to the distance are covered there by widening the far plane.
+constexpr double kQMargin = 1.0 / 32.0;
+
 // Quantise one node: child boxes (min/max per slot; empty slots have
 // min > max) into n's origin, exponents and qlo/qhi.  Per axis the scale is
 // the smallest power of two 2^e with the node box spanning at most 249
 // quanta (and at least 2^-22 of the coordinates' magnitude); the origin
 // lies two quanta below the box, rounded down to a float; child planes are
-// rounded outwards and padded by one more quantum.  Other fields of n are
-// left as they are.
+// rounded outwards from the child box widened by kQMargin quanta.  Other
+// fields of n are left as they are.
 NB_HD inline void quantise_node_hd(const float cmin[8][3],
                                    const float cmax[8][3], nb_qnode *n)
 {
@@ -113,7 +124,8 @@ NB_HD inline void quantise_node_hd(const float cmin[8][3],
 			if ((double)pf > want)
 				pf = nextafterf(pf, -FLT_MAX);
 			double top = ((double)hi[a] - pf) / sc;
-			if (top + 2.0 <= 255.0 && e + 127 >= 1 && e + 127 <= 254) {
+			if (top + 2.0 <= 255.0 && e + kQExpBias >= 1 &&
+			  e + kQExpBias <= 254) {
 				p[a] = pf;
 				ex[a] = e;
 				break;
@@ -123,9 +135,9 @@ NB_HD inline void quantise_node_hd(const float cmin[8][3],
 	n->px = p[0];
 	n->py = p[1];
 	n->pz = p[2];
-	n->ex = (uint8_t)(ex[0] + 127);
-	n->ey = (uint8_t)(ex[1] + 127);
-	n->ez = (uint8_t)(ex[2] + 127);
+	n->ex = (uint8_t)(ex[0] + kQExpBias);
+	n->ey = (uint8_t)(ex[1] + kQExpBias);
+	n->ez = (uint8_t)(ex[2] + kQExpBias);
 	uint8_t *qlo[3] = {n->qlox, n->qloy, n->qloz};
 	uint8_t *qhi[3] = {n->qhix, n->qhiy, n->qhiz};
 	for (int s = 0; s < 8; s++) {
@@ -138,8 +150,10 @@ NB_HD inline void quantise_node_hd(const float cmin[8][3],
 				continue;
 			}
 			double sc = ldexp(1.0, ex[a]);
-			double l = floor(((double)cmin[s][a] - p[a]) / sc) - 1.0;
-			double h = ceil(((double)cmax[s][a] - p[a]) / sc) + 1.0;
+			double l = floor(((double)cmin[s][a] - p[a]) / sc -
+			  kQMargin);
+			double h = ceil(((double)cmax[s][a] - p[a]) / sc +
+			  kQMargin);
 			l = fmax(l, 0.0);
 			h = fmin(h, 255.0);
 			qlo[a][s] = (uint8_t)l;

@@ -191,17 +191,21 @@ __device__ __forceinline__ float fmin3(float a, float b, float c)
 	return r;
 }
 
-// Byte k of w as the float 2^23 + byte (one byte permute: the byte goes
-// into the mantissa of 2^23).
+// Byte k of w as the float 2^23 + 256 * byte (one byte permute: the byte
+// goes into bits 8..15 of the mantissa of 2^23).
 __device__ __forceinline__ float qbf(uint32_t w, int k)
 {
-	return __uint_as_float(__byte_perm(w, 0x4b000000u, 0x7440u + k));
+	return __uint_as_float(__byte_perm(w, 0x4b000000u, 0x7404u + 16u * k));
 }
 
 // Test the 8 children of node `ni`; returns the node and triangle groups.
-// Plane distances are fma(2^23 + q, s, b - 2^23 s) with s = scale / d and
-// b = (origin - o) / d: rounding b - 2^23 s moves a plane by at most half a
-// quantum, and every child box is padded by at least one quantum per side.
+// Plane distances are fma(2^23 + 256 q, s, b - 2^23 s) with s = scale / (256
+// d) (the stored exponent carries the 1/256) and b = (origin - o) / d.  In
+// units of the quantum Q = scale / d the absolute errors are: rounding
+// b - 2^23 s (a float near 2^15 Q) at most 2^-9 Q; rounding b, relative
+// 2^-23 of |b| <= |t| + 255 Q, at most 2^-14 Q beyond a part relative to t.
+// Child planes lie at least 1/32 Q outside the child box (qnode.h), and the
+// relative parts (with the reciprocal's) are covered by kWiden.
 __device__ __forceinline__ void visit(const nb_qnode *__restrict__ nodes,
                                       uint32_t ni, const TRay &r, float tmax,
                                       uint2 &ng, uint2 &tg)

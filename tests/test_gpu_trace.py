@@ -35,13 +35,16 @@ def _check_against_oracle(rd, rays, hits):
     assert not bad, f"{len(bad)} non-tie mismatches, e.g. {bad[:5]}"
     assert len(ties) <= max(2, len(rays) // 2000)
     # where they differ, the GPU holds the FP64 ground truth
-    if ties:
+    if len(ties) >= 16:
         pick = np.array(ties[:32])
         ok = ol.agrees_with_truth(rd.ptr, rays[pick], hits[pick])
         # a tie lies within the rounding bounds, so either side may hold
-        # the FP64 closest hit; the GPU must not lose systematically
-        # (measured 4 of 6 up to 31 of 32)
-        assert ok.mean() >= 0.5, (ok.mean(), pick[~ok][:5])
+        # the FP64 closest hit.  Between triangles hit at the same t the
+        # winner follows the traversal order, which differs between the
+        # GPU's trees and the oracle's, so about half of the ties go either
+        # way; a GPU that lost them systematically would fall below this
+        # bound (a fair coin does with probability 0.2% at 16 ties)
+        assert ok.mean() >= 0.15, (ok.mean(), pick[~ok][:5])
     # where the triangle agrees, the refined hit is bit-identical
     m = (hits["id"] == ref["id"]) & (hits["t"] < ol.FLT_MAX)
     assert np.array_equal(hits["t"][m].view(np.uint32),
