@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--fuse", type=int, default=0,
                    help="1: shadow rays traced with the next bounce's "
                         "closest hits, 2: separate launches, 0: default")
+    p.add_argument("--queue", type=int, default=0,
+                   help="camera slots per wave (0 = the library's default: "
+                   "two concurrent half-frame waves)")
     p.add_argument("--block", type=int, default=0,
                    help="trace block size (0 = library default)")
     p.add_argument("--sched", type=int, default=0,
@@ -513,8 +516,8 @@ def run_ours(a):
     gr = api.GpuRenderer(rd, max_depth=a.depth, seed=1 + rank, timing=True,
                          device=dev, sched=a.sched,
                          ref_blas=a.ref_blas).upload()
-    if a.sort or a.block or a.fuse:
-        gr.set_tune(sort=a.sort, block=a.block, fuse=a.fuse)
+    if a.sort or a.block or a.fuse or a.queue:
+        gr.set_tune(sort=a.sort, block=a.block, fuse=a.fuse, queue=a.queue)
     stream = torch.cuda.ExternalStream(gr.stream(), device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     lights, area = gr.lights()
@@ -605,9 +608,12 @@ def run_ours(a):
     # whose shadow rays go to separate launches
     sep_trace_ms = sep_closest = sep_launches = 0
     if rank == 0 and world == 1:
+        # separate shadow launches and one wave of all paths, so that each
+        # closest-hit launch runs alone on the GPU
         tune = gr.get_tune()
-        gr.set_tune(**{k: tune[k] for k in ("block", "stack", "queue",
-                                             "sched", "sort")}, fuse=2)
+        gr.set_tune(**{k: tune[k] for k in ("block", "stack", "sched",
+                                             "sort")}, fuse=2,
+                    queue=0x7fffffff)
         gr.frame()
         for _ in range(2):
             with torch.cuda.stream(stream):

@@ -85,7 +85,9 @@ struct rendgpu_cfg {
 	                         BLASes rendgpu_upload_static converts from
 	                         rd->bnodes instead of building its own (SAH
 	                         binary build collapsed to 8-wide nodes by
-	                         cost); [5] bit 0: no hash
+	                         cost); [4] bit 2: one wave of all paths
+	                         where two concurrent waves would run (see
+	                         rendgpu_tune.queue); [5] bit 0: no hash
 	                         grid in the cache's position encoding; [6]:
 	                         cache training paths per frame (0 = 65536) */
 };
@@ -139,8 +141,14 @@ struct rendgpu_tune {
 	                    24, 32 or 48; a depth below the scene's need (TLAS +
 	                    BLAS depth + 2) gives the smallest that fits */
 	uint32_t queue;  /* ray-queue capacity in camera slots: a frame runs in
-	                    waves of this many paths through all bounces
-	                    (0 = one wave of all paths) */
+	                    waves of this many paths through all bounces, one
+	                    after another.  0 = the default: single-scene PATH
+	                    or PRIMARY contexts of at least 2^20 slots run two
+	                    waves of half the slots each, concurrently on two
+	                    streams, so that each wave's launch tails overlap
+	                    the other's work (cfg.reserved[4] bit 2 turns this
+	                    off); others one wave of all paths.  Images do not
+	                    depend on the waves. */
 	uint32_t sched;  /* traversal schedule as rendgpu_cfg.sched (0 = cfg's) */
 	float    ms;     /* autotune: median device ms per frame measured */
 	uint32_t sort;   /* 1: reorder each bounce's rays by direction octant
@@ -422,8 +430,9 @@ int rendgpu_set_resolve(struct rdata *rd, uint32_t op, float exposure);
 int rendgpu_capture(struct rdata *rd, uint32_t bounce_mask, uint32_t cap);
 /* The last frame's capture of bounce k.  rays / hits / shadow hold `cap`
  * entries each (any may be NULL; a ray's pad word carries its path index);
- * counts[0] = closest rays returned, [1] = closest rays traced at bounce k,
- * [2] = shadow rays returned, [3] = shadow rays generated at bounce k.
+ * counts[0] = closest rays returned, [1] = closest rays the first wave
+ * traced at bounce k, [2] = shadow rays returned, [3] = shadow rays the
+ * first wave generated at bounce k.
  * Synchronises. */
 int rendgpu_captured(struct rdata *rd, uint32_t bounce,
                      struct rendgpu_ray *rays, struct rendgpu_hit *hits,

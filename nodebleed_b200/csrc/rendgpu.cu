@@ -114,6 +114,14 @@ struct Ctx {
 	DevBuf q0, q1, hits, shadow, scol, pT, pL, rng, acc, buf, cnt, rays, scn;
 	DevBuf sortbuf; // ray reordering: key histogram and offsets
 	uint32_t npaths = 0, npix = 0, nslots = 0, qcap = 0;
+	// two concurrent waves (two_waves): the second half of the camera
+	// slots runs on wstream with its own queues and counters, forked from
+	// and joined back into `stream`
+	bool         two_waves = false;
+	bool         dual_frame = false; // the enqueued frame runs both waves
+	cudaStream_t wstream = nullptr;
+	cudaEvent_t  ev_wfork = nullptr, ev_wjoin = nullptr;
+	DevBuf q0b, q1b, hitsb, shadowb, scolb, cntb;
 	bool     have_frame = false;
 	// captured frame (RENDGPU_FLAG_GRAPH and batches)
 	cudaGraphExec_t graph = nullptr;
@@ -1031,76 +1039,126 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 	NB_CK(c, cudaMemsetAsync(c->scn.p, 0, c->sc.size() * 2 *
 	  sizeof(unsigned long long), c->stream));
 	ev_record(c); // 0
-	for (uint32_t lo = 0; lo < c->nslots; lo += c->qcap) {
-		uint32_t hi = std::min(c->nslots, lo + c->qcap);
-		NB_CK(c, cudaMemsetAsync(F.cnt, 0, sizeof(uint32_t), c->stream));
-		k_gen<<<grid_for(c, hi - lo, 256), 256, 0, c->stream>>>(S, F, A, lo,
+	// camera rays of slots [lo, hi) of wave W
+	auto gen = [&](const FrameDev &W, uint32_t lo, uint32_t hi) -> int {
+		NB_CK(c, cudaMemsetAsync(W.cnt, 0, sizeof(uint32_t), c->stream));
+		k_gen<<<grid_for(c, hi - lo, 256), 256, 0, c->stream>>>(S, W, A, lo,
 		  hi);
 		NB_CK(c, cudaGetLastError());
 		c->st.launches++;
-		for (uint32_t k = 0; k < A.depth; k++) {
-			uint32_t cur = sorting ? 0u : (k & 1u);
-			E->trace.push_back(c->nev);
+		return 0;
+	};
+	// bounce k of wave W (slots [lo, hi)): trace, shade, shadow rays
+	auto bounce = [&](FrameDev &F, uint32_t lo, uint32_t hi,
+	  uint32_t k) -> int {
+		uint32_t cur = sorting ? 0u : (k & 1u);
+		E->trace.push_back(c->nev);
+		ev_record(c);
+		if (fused && k > 0u)
+			rc = launch_fused(c, const_cast<FrameDev &>(F), F.q[cur],
+			  F.cnt + cur, k - 1u);
+		else
+			rc = launch_trace(c, F.q[cur], F.cnt + cur, F.cnt + 4,
+			  F.hits, F.cnt + 3, F.rays);
+		if (rc)
+			return rc;
+		ev_record(c);
+		c->st.launches++;
+		c->st.trace_launches++;
+		bool cap = lo == 0u && captures(c, k);
+		if (cap) {
+			// the frame's own closest hits of bounce k
+			CapSlot cs = cap_slot(c, k);
+			k_capture<<<grid_for(c, c->cap_n, 256), 256, 0,
+			  c->stream>>>(S, F.q[cur], F.cnt + cur, F.hits, c->cap_n,
+			  cs.rays, cs.hits, cs.counts);
+			NB_CK(c, cudaGetLastError());
+			c->st.launches++;
+		}
+		NB_CK(c, cudaMemsetAsync(F.cnt + (cur ^ 1u), 0,
+		  sizeof(uint32_t), c->stream));
+		NB_CK(c, cudaMemsetAsync(F.cnt + 2, 0, sizeof(uint32_t),
+		  c->stream));
+		k_shade<<<grid_for(c, hi - lo, 256), 256, 0, c->stream>>>(S, F,
+		  A, cur, k);
+		NB_CK(c, cudaGetLastError());
+		c->st.launches++;
+		if (cap) {
+			// the shadow rays shading generated at bounce k
+			CapSlot cs = cap_slot(c, k);
+			k_capture<<<grid_for(c, c->cap_n, 256), 256, 0,
+			  c->stream>>>(S, F.shadow, F.cnt + 2, nullptr, c->cap_n,
+			  cs.shadow, nullptr, cs.counts + 2);
+			NB_CK(c, cudaGetLastError());
+			c->st.launches++;
+		}
+		if (A.mode != RENDGPU_MODE_PRIMARY &&
+		  (!fused || k + 1u == A.depth)) {
+			E->shadow.push_back(c->nev);
 			ev_record(c);
-			if (fused && k > 0u)
-				rc = launch_fused(c, const_cast<FrameDev &>(F), F.q[cur],
-				  F.cnt + cur, k - 1u);
-			else
-				rc = launch_trace(c, F.q[cur], F.cnt + cur, F.cnt + 4,
-				  F.hits, F.cnt + 3, F.rays);
+			rc = launch_shadow(c, const_cast<FrameDev &>(F), k);
 			if (rc)
 				return rc;
 			ev_record(c);
 			c->st.launches++;
-			c->st.trace_launches++;
-			bool cap = lo == 0u && captures(c, k);
-			if (cap) {
-				// the frame's own closest hits of bounce k
-				CapSlot cs = cap_slot(c, k);
-				k_capture<<<grid_for(c, c->cap_n, 256), 256, 0,
-				  c->stream>>>(S, F.q[cur], F.cnt + cur, F.hits, c->cap_n,
-				  cs.rays, cs.hits, cs.counts);
-				NB_CK(c, cudaGetLastError());
-				c->st.launches++;
-			}
-			NB_CK(c, cudaMemsetAsync(F.cnt + (cur ^ 1u), 0,
-			  sizeof(uint32_t), c->stream));
-			NB_CK(c, cudaMemsetAsync(F.cnt + 2, 0, sizeof(uint32_t),
-			  c->stream));
-			k_shade<<<grid_for(c, hi - lo, 256), 256, 0, c->stream>>>(S, F,
-			  A, cur, k);
+		}
+		if (sorting && k + 1u < A.depth) {
+			int g = grid_for(c, hi - lo, 256);
+			k_sort_hist<<<g, 256, 0, c->stream>>>(F.q[1], F.cnt + 1,
+			  c->box, hist);
+			k_sort_scan<<<1, 1024, 0, c->stream>>>(hist,
+			  hist + kSortKeys);
+			k_sort_scatter<<<g, 256, 0, c->stream>>>(F.q[1], F.cnt + 1,
+			  c->box, hist + kSortKeys, F.q[0], F.cnt);
 			NB_CK(c, cudaGetLastError());
-			c->st.launches++;
-			if (cap) {
-				// the shadow rays shading generated at bounce k
-				CapSlot cs = cap_slot(c, k);
-				k_capture<<<grid_for(c, c->cap_n, 256), 256, 0,
-				  c->stream>>>(S, F.shadow, F.cnt + 2, nullptr, c->cap_n,
-				  cs.shadow, nullptr, cs.counts + 2);
-				NB_CK(c, cudaGetLastError());
-				c->st.launches++;
+			c->st.launches += 3;
+		}
+		return 0;
+	};
+	// the second half of the slots on wstream, concurrently (two_waves)
+	bool dual = c->two_waves && !sorting && !nrc && c->wstream &&
+	  c->nslots > c->qcap;
+	c->dual_frame = dual;
+	if (dual) {
+		FrameDev F1 = F;
+		F1.q[0] = c->q0b.as<float4>();
+		F1.q[1] = c->q1b.as<float4>();
+		F1.hits = c->hitsb.as<float4>();
+		F1.shadow = c->shadowb.as<float4>();
+		F1.scol = c->scolb.as<float4>();
+		F1.cnt = c->cntb.as<uint32_t>();
+		FrameDev F0 = F;
+		NB_CK(c, cudaMemsetAsync(F1.cnt, 0, 64 * sizeof(uint32_t),
+		  c->stream));
+		NB_CK(c, cudaEventRecord(c->ev_wfork, c->stream));
+		NB_CK(c, cudaStreamWaitEvent(c->wstream, c->ev_wfork, 0));
+		cudaStream_t main = c->stream;
+		uint32_t mid = c->qcap;
+		// launches alternate between the waves bounce by bounce
+		for (uint32_t k = 0; rc == 0 && k <= A.depth; k++) {
+			for (int w = 0; rc == 0 && w < 2; w++) {
+				c->stream = w ? c->wstream : main;
+				uint32_t lo = w ? mid : 0u, hi = w ? c->nslots : mid;
+				FrameDev &W = w ? F1 : F0;
+				rc = k == 0 ? gen(W, lo, hi) : bounce(W, lo, hi, k - 1u);
 			}
-			if (A.mode != RENDGPU_MODE_PRIMARY &&
-			  (!fused || k + 1u == A.depth)) {
-				E->shadow.push_back(c->nev);
-				ev_record(c);
-				rc = launch_shadow(c, const_cast<FrameDev &>(F), k);
-				if (rc)
-					return rc;
-				ev_record(c);
-				c->st.launches++;
-			}
-			if (sorting && k + 1u < A.depth) {
-				int g = grid_for(c, hi - lo, 256);
-				k_sort_hist<<<g, 256, 0, c->stream>>>(F.q[1], F.cnt + 1,
-				  c->box, hist);
-				k_sort_scan<<<1, 1024, 0, c->stream>>>(hist,
-				  hist + kSortKeys);
-				k_sort_scatter<<<g, 256, 0, c->stream>>>(F.q[1], F.cnt + 1,
-				  c->box, hist + kSortKeys, F.q[0], F.cnt);
-				NB_CK(c, cudaGetLastError());
-				c->st.launches += 3;
-			}
+		}
+		c->stream = c->wstream;
+		if (rc == 0 && cudaEventRecord(c->ev_wjoin, c->wstream) !=
+		  cudaSuccess)
+			rc = fail(c, RENDGPU_ECUDA, "cudaEventRecord (wave join)");
+		c->stream = main;
+		if (rc)
+			return rc;
+		NB_CK(c, cudaStreamWaitEvent(main, c->ev_wjoin, 0));
+	} else {
+		for (uint32_t lo = 0; lo < c->nslots; lo += c->qcap) {
+			uint32_t hi = std::min(c->nslots, lo + c->qcap);
+			rc = gen(F, lo, hi);
+			for (uint32_t k = 0; rc == 0 && k < A.depth; k++)
+				rc = bounce(const_cast<FrameDev &>(F), lo, hi, k);
+			if (rc)
+				return rc;
 		}
 	}
 	if (nrc) {
@@ -1230,10 +1288,20 @@ int render_frame(Ctx *c)
 	  cudaMemcpyDeviceToHost, c->stream));
 	NB_CK(c, cudaMemcpyAsync(hc, c->cnt.p, sizeof(hc),
 	  cudaMemcpyDeviceToHost, c->stream));
+	uint32_t hcb[64] = {};
+	if (c->dual_frame)
+		NB_CK(c, cudaMemcpyAsync(hcb, c->cntb.p, sizeof(hcb),
+		  cudaMemcpyDeviceToHost, c->stream));
 	if (ns > 1)
 		NB_CK(c, cudaMemcpyAsync(c->scn_host.data(), c->scn.p, 2 * ns *
 		  sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
 	NB_CK(c, cudaStreamSynchronize(c->stream));
+	// the second wave's errors and per-bounce ray counts
+	hc[3] += hcb[3];
+	for (int k = 0; k < 16; k++) {
+		hc[8 + k] += hcb[8 + k];
+		hc[24 + k] += hcb[24 + k];
+	}
 	c->st.closest_rays = hr[0];
 	c->st.node_visits = hr[2];
 	c->st.tri_tests = hr[3];
@@ -1274,7 +1342,9 @@ int render_frame(Ctx *c)
 		c->st.ms_shadow = sh;
 		c->st.ms_nrc = nrc ? ev_ms(c, E.nrc, E.nrc + 1) +
 		  ev_ms(c, E.train, E.train + 1) : 0.0f;
-		c->st.ms_shade = graph ? 0.0f :
+		// (with two concurrent waves the launches overlap, so their sum
+		// can exceed the frame and no shading time is derived)
+		c->st.ms_shade = graph || c->dual_frame ? 0.0f :
 		  c->st.ms_frame - tr - sh - c->st.ms_nrc;
 	}
 	if (hc[3])
@@ -1296,7 +1366,8 @@ void free_ctx(Ctx *c)
 	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat, &c->waitchk,
 	  &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob, &c->dyn_wbox,
 	  &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info, &c->dyn_emit,
-	  &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr};
+	  &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr, &c->q0b,
+	  &c->q1b, &c->hitsb, &c->shadowb, &c->scolb, &c->cntb};
 	for (DevBuf *b : bufs)
 		b->release();
 	for (int i = 0; i < kMaxEvents; i++)
@@ -1307,6 +1378,11 @@ void free_ctx(Ctx *c)
 			cudaEventDestroy(e);
 	if (c->aux)
 		cudaStreamDestroy(c->aux);
+	for (cudaEvent_t e : {c->ev_wfork, c->ev_wjoin})
+		if (e)
+			cudaEventDestroy(e);
+	if (c->wstream)
+		cudaStreamDestroy(c->wstream);
 	if (c->stream)
 		cudaStreamDestroy(c->stream);
 	delete c;
@@ -1325,7 +1401,8 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->mlp_part, &c->mlp_loss, &c->nq, &c->nrec, &c->waitchk,
 	  &c->rfeat, &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob,
 	  &c->dyn_wbox, &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info,
-	  &c->dyn_emit, &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr};
+	  &c->dyn_emit, &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr,
+	  &c->q0b, &c->q1b, &c->hitsb, &c->shadowb, &c->scolb, &c->cntb};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
 		s += b->cap;
@@ -1870,9 +1947,26 @@ int upload_dynamic_all(Ctx *c)
 	return 0;
 }
 
+// Two concurrent waves of half the camera slots each (tune.queue 0): a
+// single-scene context tracing paths without the radiance cache, with
+// enough slots that each half still fills the GPU.  Each wave's persistent
+// launches end with their slowest rays; with the other wave's launches
+// queued on a second stream, its blocks take the SMs those tails leave idle.
+// Paths, their PCG32 streams and the accumulation do not depend on the
+// waves, so images are the same as with one wave.
+constexpr uint64_t kTwoWaveMinSlots = 1u << 20;
+
+bool two_waves_fit(const Ctx *c, uint64_t nslots)
+{
+	return !c->batch && c->sc.size() == 1 &&
+	  c->cfg.mode != RENDGPU_MODE_NRC && nslots >= kTwoWaveMinSlots &&
+	  !(c->cfg.reserved[4] & 4u);
+}
+
 // Frame buffers for every scene's width, height and spp: per-path state
-// for all paths, ray queues for one wave of tune.queue camera slots (all
-// slots when 0); accumulation cleared.
+// for all paths, ray queues for one wave of tune.queue camera slots (0:
+// two concurrent waves of half the slots where two_waves_fit, else one
+// wave of all slots); accumulation cleared.
 int alloc_frame(Ctx *c)
 {
 	NB_CK(c, cudaSetDevice(c->device));
@@ -1897,14 +1991,30 @@ int alloc_frame(Ctx *c)
 			return fail(c, RENDGPU_ELIMIT, "width*height*spp over all "
 			  "scenes outside 1..2^31-1");
 	}
+	c->two_waves = !c->tune.queue && two_waves_fit(c, nslots);
 	uint64_t q = c->tune.queue ? std::min<uint64_t>(c->tune.queue, nslots) :
-	  nslots;
+	  (c->two_waves ? (nslots + 1) / 2 : nslots);
 	q = std::max<uint64_t>(q, 1);
 	NB_CK(c, c->q0.ensure(q * 32));
 	NB_CK(c, c->q1.ensure(q * 32));
 	NB_CK(c, c->hits.ensure(q * 16));
 	NB_CK(c, c->shadow.ensure(q * 32));
 	NB_CK(c, c->scol.ensure(q * 16));
+	if (c->two_waves) {
+		NB_CK(c, c->q0b.ensure(q * 32));
+		NB_CK(c, c->q1b.ensure(q * 32));
+		NB_CK(c, c->hitsb.ensure(q * 16));
+		NB_CK(c, c->shadowb.ensure(q * 32));
+		NB_CK(c, c->scolb.ensure(q * 16));
+		NB_CK(c, c->cntb.ensure(64 * sizeof(uint32_t)));
+		if (!c->wstream) {
+			NB_CK(c, cudaStreamCreateWithFlags(&c->wstream,
+			  cudaStreamNonBlocking));
+			for (cudaEvent_t *e : {&c->ev_wfork, &c->ev_wjoin})
+				NB_CK(c, cudaEventCreateWithFlags(e,
+				  cudaEventDisableTiming));
+		}
+	}
 	NB_CK(c, c->pT.ensure(np * 16));
 	NB_CK(c, c->pL.ensure(np * 16));
 	NB_CK(c, c->rng.ensure(np * 8));
