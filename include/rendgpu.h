@@ -48,7 +48,9 @@ enum rendgpu_mode {
 	                             hit; 2^16 training paths per frame, unbiased
 	                             up to bounce reserved[2] (default 3) where
 	                             the cache ends them too (self-training),
-	                             train it */
+	                             train it: a frame's records train the
+	                             cache during the next frame, beside its
+	                             traversal and before its queries */
 };
 
 enum rendgpu_flags {
@@ -129,7 +131,9 @@ struct rendgpu_stats {
 	uint32_t nrc_queries;    /* radiance-cache queries of the frame */
 	uint32_t nrc_records;    /* training vertices recorded in the frame */
 	float    ms_nrc;         /* cache inference + training (TIMING flag) */
-	float    nrc_loss;       /* loss of the frame's last training step */
+	float    nrc_loss;       /* loss of the last training step in the frame
+	                            (radiance-cache frames train on the previous
+	                            frame's records; 0 in the first frame) */
 };
 
 /* Launch parameters of a context (rendgpu_set_tune / rendgpu_autotune).
@@ -142,8 +146,8 @@ struct rendgpu_tune {
 	                    BLAS depth + 2) gives the smallest that fits */
 	uint32_t queue;  /* ray-queue capacity in camera slots: a frame runs in
 	                    waves of this many paths through all bounces, one
-	                    after another.  0 = the default: single-scene PATH
-	                    or PRIMARY contexts of at least 2^20 slots run two
+	                    after another.  0 = the default: single-scene
+	                    contexts of at least 2^20 slots run two
 	                    waves of half the slots each, concurrently on two
 	                    streams, so that each wave's launch tails overlap
 	                    the other's work (cfg.reserved[4] bit 2 turns this

@@ -46,6 +46,8 @@ struct FrameDev {
 	float4   *nq;
 	float4   *nrec;
 	uint32_t  nq_cap, nrec_cap;
+	uint32_t *ncnt; // [0] queries, [1] records (cnt + 40 of the frame's
+	                // first wave; every wave appends to the same arrays)
 };
 
 // Path flags kept in the bits of pT.w.
@@ -545,7 +547,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 						bool end = k >= A.nrc_end || !train;
 						if (end) {
 							// radiance cache query: the path ends here
-							uint32_t qi = atomicAdd(&F.cnt[40], 1u);
+							uint32_t qi = atomicAdd(&F.ncnt[0], 1u);
 							if (qi < F.nq_cap) {
 								float4 *q = F.nq + 4u * qi;
 								q[0] = nrc_entry_pos(P, pos, path);
@@ -557,7 +559,7 @@ __global__ void __launch_bounds__(256) k_shade(DScene S, FrameDev F,
 							queried = true;
 						}
 						if (train && !end) {
-							uint32_t ri = atomicAdd(&F.cnt[41], 1u);
+							uint32_t ri = atomicAdd(&F.ncnt[1], 1u);
 							if (ri < F.nrec_cap) {
 								float4 *q = F.nrec + 6u * ri;
 								q[0] = nrc_entry_pos(P, pos, path);

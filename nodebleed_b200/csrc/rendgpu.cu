@@ -144,6 +144,14 @@ struct Ctx {
 	bool     mlp_ready = false;
 	NrcBox   box{};
 	DevBuf   nq, nrec, rfeat, rtgt; // radiance-cache frame data
+	// deferred training: frame f's records (nrec / nrecb by rec_parity)
+	// train the cache on tstream during frame f + 1; nsnap keeps each
+	// buffer's record count
+	DevBuf       nrecb, nsnap;
+	cudaStream_t tstream = nullptr;
+	cudaEvent_t  ev_tfork = nullptr, ev_tdone = nullptr;
+	bool         train_pending = false;
+	uint32_t     rec_parity = 0;
 	DevBuf   waitchk;                // rendgpu_check_bounded_wait
 	uint32_t nq_cap = 0, nrec_cap = 0, nrc_stride = 1;
 	uint32_t nrc_frames = 0; // radiance-cache frames rendered so far
@@ -517,9 +525,10 @@ FrameDev frame_of(Ctx *c)
 	F.npaths = c->npaths;
 	F.npix = c->npix;
 	F.nq = c->nq.as<float4>();
-	F.nrec = c->nrec.as<float4>();
+	F.nrec = (c->rec_parity ? c->nrecb : c->nrec).as<float4>();
 	F.nq_cap = c->nq_cap;
 	F.nrec_cap = c->nrec_cap;
+	F.ncnt = F.cnt + 40;
 	return F;
 }
 
@@ -589,6 +598,7 @@ const float2 *grid_of(Ctx *c)
 // uniform in +-1e-4 from the same stream (as instant-NGP initialises them).
 int nrc_reset(Ctx *c, uint64_t seed)
 {
+	c->train_pending = false; // records of earlier frames no longer train
 	if (!c->aux) {
 		NB_CK(c, cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
 		for (cudaEvent_t *e : {&c->ev_fork, &c->ev_grad, &c->ev_join})
@@ -703,9 +713,20 @@ int nrc_frame_buffers(Ctx *c)
 	// vertices beyond the steady-state need
 	uint32_t ntrain = np / c->nrc_stride + 1;
 	c->nq_cap = np;
-	c->nrec_cap = std::max(ntrain * verts + 64, nrc_steps(c) * kNrcBatch);
+	uint32_t cap = std::max(ntrain * verts + 64, nrc_steps(c) * kNrcBatch);
+	if (cap != c->nrec_cap)
+		c->train_pending = false; // the record buffers may move
+	c->nrec_cap = cap;
 	NB_CK(c, c->nq.ensure((size_t)np * 64));
 	NB_CK(c, c->nrec.ensure((size_t)c->nrec_cap * 96));
+	NB_CK(c, c->nrecb.ensure((size_t)c->nrec_cap * 96));
+	NB_CK(c, c->nsnap.ensure(2 * sizeof(uint32_t)));
+	if (!c->tstream) {
+		NB_CK(c, cudaStreamCreateWithFlags(&c->tstream,
+		  cudaStreamNonBlocking));
+		for (cudaEvent_t *e : {&c->ev_tfork, &c->ev_tdone})
+			NB_CK(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+	}
 	NB_CK(c, c->rfeat.ensure((size_t)c->nrec_cap * 128));
 	NB_CK(c, c->rtgt.ensure((size_t)c->nrec_cap * 16));
 	return 0;
@@ -1015,6 +1036,36 @@ struct FrameEvents {
 	int nrc = -1, train = -1;
 };
 
+// nrc_steps Adam steps of kNrcBatch training records each from `recs`
+// (*count records, targets in rtgt) on c->stream: each step encodes its
+// batch with the grid as the last step left it, trains, and moves the grid
+// with its own gradient.
+int train_records(Ctx *c, const float4 *recs, const uint32_t *count,
+                  FrameEvents *E)
+{
+	E->train = c->nev;
+	ev_record(c);
+	GridSrc gs;
+	gs.e = recs;
+	gs.stride = 6u;
+	gs.box = kUnitBox;
+	gs.scode = true;
+	for (uint32_t s = 0; s < nrc_steps(c); s++) {
+		k_nrc_encode_entries<<<grid_for(c, kNrcBatch, 128), 128, 0,
+		  c->stream>>>(recs, 6u, count, s * kNrcBatch, c->nrec_cap,
+		  kNrcBatch, kUnitBox, c->rfeat.as<__nv_bfloat16>(), true,
+		  grid_of(c));
+		NB_CK(c, cudaGetLastError());
+		int rc = nrc_train(c, c->rfeat.p, c->rtgt.as<float4>(), kNrcBatch,
+		  1, nullptr, nullptr, count, s * kNrcBatch, c->nrec_cap, &gs);
+		if (rc)
+			return rc;
+	}
+	c->st.launches += (nrc_grid(c) ? 6 : 4) * nrc_steps(c);
+	ev_record(c);
+	return 0;
+}
+
 // The launch sequence of one frame: every wave of camera slots through all
 // bounces (trace, shade, shadow), cache inference, accumulation, cache
 // training.  Sizes and counts are read on the device, so the sequence is
@@ -1039,6 +1090,29 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 	NB_CK(c, cudaMemsetAsync(c->scn.p, 0, c->sc.size() * 2 *
 	  sizeof(unsigned long long), c->stream));
 	ev_record(c); // 0
+	// The previous frame's records train the cache on tstream, forked after
+	// this frame's bounce-1 launches so that the training kernels take the
+	// SMs the traversal's tails leave idle; the queries wait for it.  Every
+	// frame's queries thus see the cache trained on all earlier frames, as
+	// when each frame trained at its end.
+	bool train_enq = false;
+	auto deferred_train = [&]() -> int {
+		if (!nrc || !c->train_pending || train_enq)
+			return 0;
+		train_enq = true;
+		const float4 *prev = (c->rec_parity ? c->nrec : c->nrecb).as<float4>();
+		const uint32_t *pcnt = c->nsnap.as<uint32_t>() + (c->rec_parity ^ 1u);
+		NB_CK(c, cudaEventRecord(c->ev_tfork, c->stream));
+		NB_CK(c, cudaStreamWaitEvent(c->tstream, c->ev_tfork, 0));
+		cudaStream_t main = c->stream;
+		c->stream = c->tstream;
+		int r = train_records(c, prev, pcnt, E);
+		if (r == 0 && cudaEventRecord(c->ev_tdone, c->tstream) !=
+		  cudaSuccess)
+			r = fail(c, RENDGPU_ECUDA, "cudaEventRecord (training done)");
+		c->stream = main;
+		return r;
+	};
 	// camera rays of slots [lo, hi) of wave W
 	auto gen = [&](const FrameDev &W, uint32_t lo, uint32_t hi) -> int {
 		NB_CK(c, cudaMemsetAsync(W.cnt, 0, sizeof(uint32_t), c->stream));
@@ -1113,10 +1187,12 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 			NB_CK(c, cudaGetLastError());
 			c->st.launches += 3;
 		}
+		if (nrc && k == 1u && lo == 0u)
+			return deferred_train();
 		return 0;
 	};
 	// the second half of the slots on wstream, concurrently (two_waves)
-	bool dual = c->two_waves && !sorting && !nrc && c->wstream &&
+	bool dual = c->two_waves && !sorting && c->wstream &&
 	  c->nslots > c->qcap;
 	c->dual_frame = dual;
 	if (dual) {
@@ -1134,7 +1210,10 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		NB_CK(c, cudaStreamWaitEvent(c->wstream, c->ev_wfork, 0));
 		cudaStream_t main = c->stream;
 		uint32_t mid = c->qcap;
-		// launches alternate between the waves bounce by bounce
+		// launches alternate between the waves bounce by bounce (starting
+		// the second wave a bounce later, so that the first wave's short
+		// training-path bounces of a radiance-cache frame ran beside the
+		// second's bounce 1, measured 3% slower cache frames)
 		for (uint32_t k = 0; rc == 0 && k <= A.depth; k++) {
 			for (int w = 0; rc == 0 && w < 2; w++) {
 				c->stream = w ? c->wstream : main;
@@ -1162,6 +1241,11 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 		}
 	}
 	if (nrc) {
+		rc = deferred_train(); // frames of fewer than two bounces
+		if (rc)
+			return rc;
+		if (train_enq)
+			NB_CK(c, cudaStreamWaitEvent(c->stream, c->ev_tdone, 0));
 		// cache inference for the queries of this frame
 		E->nrc = c->nev;
 		ev_record(c);
@@ -1176,33 +1260,16 @@ int enqueue_frame(Ctx *c, const FrameDev &F, const FrameArgs &A,
 	NB_CK(c, cudaGetLastError());
 	c->st.launches++;
 	if (nrc) {
-		// train on this frame's records: targets from the finished paths,
-		// then nrc_steps Adam steps of kNrcBatch samples each
-		E->train = c->nev;
-		ev_record(c);
+		// targets of this frame's records from the finished paths (before
+		// the next frame's camera rays reset the path radiance) and the
+		// record count; the next frame trains on them
 		k_nrc_targets<<<grid_for(c, c->nrec_cap, 256), 256, 0, c->stream>>>(
 		  F.nrec, F.cnt + 41, c->nrec_cap, F.pL, c->rtgt.as<float4>());
 		NB_CK(c, cudaGetLastError());
-		// each step encodes its batch with the grid as the last step left
-		// it, trains, and moves the grid with its own gradient
-		GridSrc gs;
-		gs.e = F.nrec;
-		gs.stride = 6u;
-		gs.box = kUnitBox;
-		gs.scode = true;
-		for (uint32_t s = 0; s < nrc_steps(c); s++) {
-			k_nrc_encode_entries<<<grid_for(c, kNrcBatch, 128), 128, 0,
-			  c->stream>>>(F.nrec, 6u, F.cnt + 41, s * kNrcBatch,
-			  c->nrec_cap, kNrcBatch, kUnitBox, c->rfeat.as<__nv_bfloat16>(),
-			  true, grid_of(c));
-			NB_CK(c, cudaGetLastError());
-			rc = nrc_train(c, c->rfeat.p, c->rtgt.as<float4>(), kNrcBatch, 1,
-			  nullptr, nullptr, F.cnt + 41, s * kNrcBatch, c->nrec_cap, &gs);
-			if (rc)
-				return rc;
-		}
-		c->st.launches += 1 + (nrc_grid(c) ? 6 : 4) * nrc_steps(c);
-		ev_record(c);
+		NB_CK(c, cudaMemcpyAsync(c->nsnap.as<uint32_t>() + c->rec_parity,
+		  F.cnt + 41, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+		  c->stream));
+		c->st.launches++;
 	}
 	ev_record(c); // last
 	return 0;
@@ -1277,8 +1344,17 @@ int render_frame(Ctx *c)
 		c->st.trace_launches = c->graph_trace_launches;
 	} else {
 		rc = enqueue_frame(c, F, A, nrc, &E);
-		if (rc)
+		if (rc) {
+			c->train_pending = false;
 			return rc;
+		}
+	}
+	// radiance cache: this frame's records train during the next frame
+	bool trained = nrc && E.train >= 0;
+	uint32_t tpar = c->rec_parity ^ 1u; // the buffer trained this frame
+	if (nrc) {
+		c->train_pending = true;
+		c->rec_parity ^= 1u;
 	}
 	unsigned long long hr[4];
 	uint32_t hc[64];
@@ -1312,16 +1388,22 @@ int render_frame(Ctx *c)
 		c->scn_host[0] = hr[0];
 		c->scn_host[1] = hr[1];
 	}
-	if (nrc) {
-		// loss of the last Adam step (partials of its CTAs)
+	c->st.nrc_loss = 0.0f;
+	if (trained) {
+		// loss of the last Adam step (partials of its CTAs) over the
+		// previous frame's records, which trained in this frame (the
+		// queries waited for it, and the stream has been synchronised)
 		float lp[1024];
 		uint32_t ng = std::min<uint32_t>(c->train_grid, 1024);
+		uint32_t tcnt = 0;
 		NB_CK(c, cudaMemcpy(lp, c->mlp_loss.p, ng * 4,
 		  cudaMemcpyDeviceToHost));
+		NB_CK(c, cudaMemcpy(&tcnt, c->nsnap.as<uint32_t>() + tpar,
+		  sizeof(tcnt), cudaMemcpyDeviceToHost));
 		double sl = 0.0;
 		for (uint32_t i = 0; i < ng; i++)
 			sl += lp[i];
-		uint32_t used = std::min(std::min(hc[41], c->nrec_cap), kNrcBatch);
+		uint32_t used = std::min(std::min(tcnt, c->nrec_cap), kNrcBatch);
 		c->st.nrc_loss = used ? (float)(sl / (3.0 * used)) : 0.0f;
 	}
 	c->st.nrc_queries = nrc ? std::min(hc[40], c->nq_cap) : 0;
@@ -1341,11 +1423,11 @@ int render_frame(Ctx *c)
 		c->st.ms_trace = tr;
 		c->st.ms_shadow = sh;
 		c->st.ms_nrc = nrc ? ev_ms(c, E.nrc, E.nrc + 1) +
-		  ev_ms(c, E.train, E.train + 1) : 0.0f;
+		  (trained ? ev_ms(c, E.train, E.train + 1) : 0.0f) : 0.0f;
 		// (with two concurrent waves the launches overlap, so their sum
 		// can exceed the frame and no shading time is derived)
 		c->st.ms_shade = graph || c->dual_frame ? 0.0f :
-		  c->st.ms_frame - tr - sh - c->st.ms_nrc;
+		  std::max(0.0f, c->st.ms_frame - tr - sh - c->st.ms_nrc);
 	}
 	if (hc[3])
 		return fail(c, RENDGPU_EDEVICE, "device error: rays abandoned "
@@ -1367,7 +1449,8 @@ void free_ctx(Ctx *c)
 	  &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob, &c->dyn_wbox,
 	  &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info, &c->dyn_emit,
 	  &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr, &c->q0b,
-	  &c->q1b, &c->hitsb, &c->shadowb, &c->scolb, &c->cntb};
+	  &c->q1b, &c->hitsb, &c->shadowb, &c->scolb, &c->cntb, &c->nrecb,
+	  &c->nsnap};
 	for (DevBuf *b : bufs)
 		b->release();
 	for (int i = 0; i < kMaxEvents; i++)
@@ -1378,11 +1461,14 @@ void free_ctx(Ctx *c)
 			cudaEventDestroy(e);
 	if (c->aux)
 		cudaStreamDestroy(c->aux);
-	for (cudaEvent_t e : {c->ev_wfork, c->ev_wjoin})
+	for (cudaEvent_t e : {c->ev_wfork, c->ev_wjoin, c->ev_tfork,
+	  c->ev_tdone})
 		if (e)
 			cudaEventDestroy(e);
 	if (c->wstream)
 		cudaStreamDestroy(c->wstream);
+	if (c->tstream)
+		cudaStreamDestroy(c->tstream);
 	if (c->stream)
 		cudaStreamDestroy(c->stream);
 	delete c;
@@ -1402,7 +1488,8 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->rfeat, &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob,
 	  &c->dyn_wbox, &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info,
 	  &c->dyn_emit, &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr,
-	  &c->q0b, &c->q1b, &c->hitsb, &c->shadowb, &c->scolb, &c->cntb};
+	  &c->q0b, &c->q1b, &c->hitsb, &c->shadowb, &c->scolb, &c->cntb,
+	  &c->nrecb, &c->nsnap};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
 		s += b->cap;
@@ -1948,8 +2035,9 @@ int upload_dynamic_all(Ctx *c)
 }
 
 // Two concurrent waves of half the camera slots each (tune.queue 0): a
-// single-scene context tracing paths without the radiance cache, with
-// enough slots that each half still fills the GPU.  Each wave's persistent
+// single-scene context with enough slots that each half still fills the
+// GPU.  Radiance-cache queries and training records of both waves go to the
+// same arrays through the first wave's counters.  Each wave's persistent
 // launches end with their slowest rays; with the other wave's launches
 // queued on a second stream, its blocks take the SMs those tails leave idle.
 // Paths, their PCG32 streams and the accumulation do not depend on the
@@ -1958,8 +2046,7 @@ constexpr uint64_t kTwoWaveMinSlots = 1u << 20;
 
 bool two_waves_fit(const Ctx *c, uint64_t nslots)
 {
-	return !c->batch && c->sc.size() == 1 &&
-	  c->cfg.mode != RENDGPU_MODE_NRC && nslots >= kTwoWaveMinSlots &&
+	return !c->batch && c->sc.size() == 1 && nslots >= kTwoWaveMinSlots &&
 	  !(c->cfg.reserved[4] & 4u);
 }
 
