@@ -89,7 +89,10 @@ struct rendgpu_cfg {
 	                         binary build collapsed to 8-wide nodes by
 	                         cost); [4] bit 2: one wave of all paths
 	                         where two concurrent waves would run (see
-	                         rendgpu_tune.queue); [5] bit 0: no hash
+	                         rendgpu_tune.queue); [4] bit 3: device TLAS
+	                         builds split level by level, greedily into 8
+	                         children, instead of one CTA's binary SAH tree
+	                         collapsed by cost; [5] bit 0: no hash
 	                         grid in the cache's position encoding; [6]:
 	                         cache training paths per frame (0 = 65536) */
 };

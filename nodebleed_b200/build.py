@@ -65,7 +65,7 @@ def build_gpu(force=False):
     cpp2 = os.path.join(CSRC, "blas_build.cpp")
     deps = [cu, cpp, cpp2] + [os.path.join(CSRC, f) for f in
                         ("trace.cuh", "kernels.cuh", "nrc.cuh", "gpulayout.h",
-                         "layout.hpp", "qnode.h", "tlas_build.cuh",
+                         "layout.hpp", "qnode.h", "tlas_build.cuh", "tlas_cta.cuh",
                          os.path.join("host", "nb_rdata.h"))]
     deps.append(os.path.join(ROOT, "include", "rendgpu.h"))
     if not force and _newer(out, deps):

@@ -26,6 +26,7 @@
 #include "layout.hpp"
 #include "nrc.cuh"
 #include "tlas_build.cuh"
+#include "tlas_cta.cuh"
 
 namespace nb {
 namespace {
@@ -164,6 +165,7 @@ struct Ctx {
 	// BLAS root boxes, new matrices, world boxes, TLAS build queues, slot
 	// ranges and instance order (refit), build info, emitter sources, area
 	DevBuf   dyn_idx, dyn_ctr; // device TLAS build: order, counters
+	DevBuf   dyn_bvh;          // single-CTA build: binary tree, tables
 	DevBuf   dyn_root, dyn_glob, dyn_wbox, dyn_q, dyn_ranges, dyn_order,
 	         dyn_info, dyn_emit, dyn_area, dyn_trange;
 	uint32_t dyn_nemit = 0;
@@ -1448,7 +1450,8 @@ void free_ctx(Ctx *c)
 	  &c->mlp_loss, &c->nq, &c->nrec, &c->rfeat, &c->waitchk,
 	  &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob, &c->dyn_wbox,
 	  &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info, &c->dyn_emit,
-	  &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr, &c->q0b,
+	  &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr, &c->dyn_bvh,
+	  &c->q0b,
 	  &c->q1b, &c->hitsb, &c->shadowb, &c->scolb, &c->cntb, &c->nrecb,
 	  &c->nsnap};
 	for (DevBuf *b : bufs)
@@ -1488,7 +1491,7 @@ uint64_t held_bytes(const Ctx *c)
 	  &c->rfeat, &c->rtgt, &c->capbuf, &c->dyn_root, &c->dyn_glob,
 	  &c->dyn_wbox, &c->dyn_q, &c->dyn_ranges, &c->dyn_order, &c->dyn_info,
 	  &c->dyn_emit, &c->dyn_area, &c->dyn_trange, &c->dyn_idx, &c->dyn_ctr,
-	  &c->q0b, &c->q1b, &c->hitsb, &c->shadowb, &c->scolb, &c->cntb,
+	  &c->dyn_bvh, &c->q0b, &c->q1b, &c->hitsb, &c->shadowb, &c->scolb, &c->cntb,
 	  &c->nrecb, &c->nsnap};
 	uint64_t s = 0;
 	for (const DevBuf *b : bufs)
@@ -1797,6 +1800,26 @@ int tlas_build(Ctx *c, uint32_t n, uint32_t *limit)
 	// the uploaded trees sized the traversal stack; the device tree stays
 	// within what it holds
 	A.depth_limit = device_tlas_limit(c);
+	if (!(c->cfg.reserved[4] & 8u)) {
+		// one CTA: binary SAH tree, collapse by cost, 8-wide encoding
+		size_t m = 2 * (size_t)nn, o_cost = m * sizeof(TcNode);
+		size_t o_kd = o_cost + m * 8 * sizeof(float), o_prev = o_kd + m * 8;
+		size_t o_q = (o_prev + m + 15) & ~(size_t)15;
+		NB_CK(c, c->dyn_bvh.ensure(o_q + 6 * (size_t)nn * sizeof(uint32_t)));
+		unsigned char *base = c->dyn_bvh.as<unsigned char>();
+		TcArgs T;
+		T.A = A;
+		T.bn = reinterpret_cast<TcNode *>(base);
+		T.cost = reinterpret_cast<float *>(base + o_cost);
+		T.kd = base + o_kd;
+		T.prev = base + o_prev;
+		T.qa = reinterpret_cast<uint32_t *>(base + o_q);
+		T.qb = T.qa + 3 * (size_t)nn;
+		k_tlas_cta<<<1, kCbThreads, 0, c->stream>>>(T);
+		NB_CK(c, cudaGetLastError());
+		*limit = A.depth_limit;
+		return 0;
+	}
 	k_tlas_init<<<1, 512, 0, c->stream>>>(A);
 	NB_CK(c, cudaGetLastError());
 	uint64_t open = 1; // at most this many open nodes on a level
