@@ -389,7 +389,11 @@ def update_times(a, scene, rd, gr, stream):
                                                   np.float32)).cuda()
     torch.cuda.synchronize()
     out = {}
-    for name, refit in (("device_build_ms", False), ("device_refit_ms", True)):
+    # the default level-by-level build, the one-CTA build collapsed by
+    # cost (RENDGPU_UPDATE_COLLAPSE), and a refit of the default build
+    for name, kw in (("device_build_collapse_ms", {"collapse": True}),
+                     ("device_build_ms", {}),
+                     ("device_refit_ms", {"refit": True})):
         gr.update_instances(globs.data_ptr())  # first: builds
         ev = []
         for _ in range(a.update_reps):
@@ -397,7 +401,7 @@ def update_times(a, scene, rd, gr, stream):
                 s, e = torch.cuda.Event(enable_timing=True), \
                     torch.cuda.Event(enable_timing=True)
                 s.record(stream)
-            gr.update_instances(globs.data_ptr(), refit=refit)
+            gr.update_instances(globs.data_ptr(), **kw)
             with torch.cuda.stream(stream):
                 e.record(stream)
             ev.append((s, e))

@@ -577,11 +577,13 @@ class GpuRenderer:
         self._ck(self.g.rendgpu_set_resolve(self.ptr, op, exposure),
                  "set_resolve")
 
-    def update_instances(self, globs, refit=False, tight=False):
+    def update_instances(self, globs, refit=False, tight=False,
+                         collapse=False):
         """Device-side scene update from (instances, 16) object->world
         matrices (host array: copied; else an integer device pointer)."""
         n = self.rdata.rd.instcnt
-        flags = (1 if refit else 0) | (2 if tight else 0)
+        flags = (1 if refit else 0) | (2 if tight else 0) | \
+            (4 if collapse else 0)
         if isinstance(globs, int):
             self._ck(self.g.rendgpu_update_instances_device(self.ptr, globs,
                                                             n, flags),

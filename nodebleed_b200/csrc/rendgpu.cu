@@ -1777,7 +1777,7 @@ uint32_t device_tlas_limit(const Ctx *c);
 // single scene), one launch per level up to the depth limit (levels past
 // the tree's depth find no open node and return at once); returns the
 // depth limit used.
-int tlas_build(Ctx *c, uint32_t n, uint32_t *limit)
+int tlas_build(Ctx *c, uint32_t n, uint32_t *limit, bool collapse)
 {
 	uint32_t nn = std::max(n, 1u);
 	NB_CK(c, c->dyn_idx.ensure((size_t)2 * nn * sizeof(uint16_t)));
@@ -1800,7 +1800,7 @@ int tlas_build(Ctx *c, uint32_t n, uint32_t *limit)
 	// the uploaded trees sized the traversal stack; the device tree stays
 	// within what it holds
 	A.depth_limit = device_tlas_limit(c);
-	if (!(c->cfg.reserved[4] & 8u)) {
+	if (collapse) {
 		// one CTA: binary SAH tree, collapse by cost, 8-wide encoding
 		size_t m = 2 * (size_t)nn, o_cost = m * sizeof(TcNode);
 		size_t o_kd = o_cost + m * 8 * sizeof(float), o_prev = o_kd + m * 8;
@@ -1815,7 +1815,10 @@ int tlas_build(Ctx *c, uint32_t n, uint32_t *limit)
 		T.prev = base + o_prev;
 		T.qa = reinterpret_cast<uint32_t *>(base + o_q);
 		T.qb = T.qa + 3 * (size_t)nn;
-		k_tlas_cta<<<1, kCbThreads, 0, c->stream>>>(T);
+		size_t dyn = tc_dyn_smem(nn);
+		NB_CK(c, cudaFuncSetAttribute(k_tlas_cta,
+		  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+		k_tlas_cta<<<1, kCbThreads, dyn, c->stream>>>(T);
 		NB_CK(c, cudaGetLastError());
 		*limit = A.depth_limit;
 		return 0;
@@ -1860,7 +1863,8 @@ int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
 		return fail(c, RENDGPU_ESTATE, "update: the uploaded light table "
 		  "skipped a degenerate emitter; upload non-degenerate transforms "
 		  "first");
-	if (flags & ~(uint32_t)(RENDGPU_UPDATE_REFIT | RENDGPU_UPDATE_TIGHT))
+	if (flags & ~(uint32_t)(RENDGPU_UPDATE_REFIT | RENDGPU_UPDATE_TIGHT |
+	  RENDGPU_UPDATE_COLLAPSE))
 		return fail(c, RENDGPU_EINVAL, "update: unknown flags");
 	NB_CK(c, cudaSetDevice(c->device));
 	bool refit = (flags & RENDGPU_UPDATE_REFIT) && c->dyn_built;
@@ -1877,7 +1881,8 @@ int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
 	}
 	if (!refit) {
 		uint32_t limit = 0;
-		rc = tlas_build(c, n, &limit);
+		rc = tlas_build(c, n, &limit,
+		  (flags & RENDGPU_UPDATE_COLLAPSE) != 0u);
 		if (rc)
 			return rc;
 		h.tlas_depth = c->tlas_depth = limit;
@@ -1939,7 +1944,7 @@ int rebuild_tlas_tight(Ctx *c)
 	  c->dyn_wbox.as<float4>());
 	NB_CK(c, cudaGetLastError());
 	uint32_t limit = 0;
-	int rc = tlas_build(c, n, &limit);
+	int rc = tlas_build(c, n, &limit, !(c->cfg.reserved[4] & 8u));
 	if (rc)
 		return rc;
 	NB_CK(c, cudaStreamSynchronize(c->stream));

@@ -822,10 +822,30 @@ __device__ void tc_emit(const TcArgs &T, TcShared &S)
 	}
 }
 
-// The whole build (one CTA of kCbThreads threads).
-__global__ void __launch_bounds__(kCbThreads, 1) k_tlas_cta(TcArgs T)
+// Dynamic shared memory of the build over n instances: their boxes (two
+// float4 each, as in wbox) and the two instance orders.
+__host__ __device__ inline size_t tc_dyn_smem(uint32_t n)
+{
+	return (size_t)n * 32u + (((size_t)n * 4u + 15u) & ~(size_t)15u);
+}
+
+// The whole build (one CTA of kCbThreads threads).  The instance boxes and
+// orders live in shared memory for the build; the world boxes in global
+// memory stay as they are for the refit.
+__global__ void __launch_bounds__(kCbThreads, 1) k_tlas_cta(TcArgs Tg)
 {
 	__shared__ TcShared S;
+	extern __shared__ float4 tc_dyn[];
+	TcArgs T = Tg;
+	{
+		float4 *sbox = tc_dyn;
+		uint16_t *sidx = reinterpret_cast<uint16_t *>(tc_dyn + 2u * Tg.A.n);
+		for (uint32_t i = threadIdx.x; i < 2u * Tg.A.n; i += kCbThreads)
+			sbox[i] = Tg.A.wbox[i];
+		T.A.wbox = sbox;
+		T.A.idx = sidx;
+		T.A.tmp = sidx + Tg.A.n;
+	}
 	const TbArgs &A = T.A;
 	const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
 	const uint32_t n = A.n;
@@ -853,6 +873,7 @@ __global__ void __launch_bounds__(kCbThreads, 1) k_tlas_cta(TcArgs T)
 	const uint32_t cap = 3u * A.depth_limit; // deepest binary leaf allowed
 	for (uint32_t i = tid; i < n; i += kCbThreads)
 		A.idx[i] = (uint16_t)i;
+	__syncthreads(); // the boxes copied above
 	if (tid == 0) {
 		S.over = 0u;
 		S.nnodes = 1u;

@@ -113,6 +113,15 @@ def test_device_update_matches_host_path(gpu):
     assert np.array_equal(_bits(gd.trace(rays)), _bits(gh.trace(rays)))
     assert np.array_equal(gd.occluded(rays), gh.occluded(rays))
     assert np.array_equal(_bits(_frame(gd, rd_d)), _bits(_frame(gh, rd_h)))
+    # the one-CTA build collapsed by cost: another TLAS, the same hits; the
+    # refit below then keeps its topology
+    gd.update_instances(moved, tight=True, collapse=True)
+    _, _, info_c = gd.instances()
+    print(f"collapsed device TLAS: {info_c[0]} nodes, depth {info_c[1]}")
+    assert info_c[2] == 0
+    assert np.array_equal(_bits(gd.trace(rays)), _bits(gh.trace(rays)))
+    assert np.array_equal(gd.occluded(rays), gh.occluded(rays))
+    assert np.array_equal(_bits(_frame(gd, rd_d)), _bits(_frame(gh, rd_h)))
     # a small further move, refitted on the device (device matrices)
     import torch
     for s in range(10):
