@@ -44,10 +44,28 @@ namespace {
 
 // Shared conversion of one tree.  leaf(ofs, items) appends the leaf's items
 // and returns their count (0 = malformed).
+// Widen [lo, hi] by 2^-20 of its magnitude, rounded outwards (world boxes
+// of a TLAS: they come from transformed corners rounded to FP32, and the
+// quantised planes keep only 1/32 of a quantum outside a child box).
+void widen_box(float *lo, float *hi)
+{
+	double m = std::fmax(std::fabs((double)*lo), std::fabs((double)*hi)) *
+	  std::ldexp(1.0, -20);
+	double l = (double)*lo - m, h = (double)*hi + m;
+	float lf = (float)l, hf = (float)h;
+	if ((double)lf > l)
+		lf = std::nextafter(lf, -FLT_MAX);
+	if ((double)hf < h)
+		hf = std::nextafter(hf, FLT_MAX);
+	*lo = lf;
+	*hi = hf;
+}
+
 template <class LeafFn>
 bool convert_tree(const uint8_t *base, uint64_t limit,
                   std::vector<nb_qnode> &nodes, uint32_t root_index,
-                  LeafFn leaf, bvh_stats *st, std::string *err)
+                  LeafFn leaf, bvh_stats *st, std::string *err,
+                  bool widen = false)
 {
 	std::deque<qitem> q;
 	q.push_back({0u, root_index, 1u});
@@ -108,6 +126,9 @@ bool convert_tree(const uint8_t *base, uint64_t limit,
 			cmax[s][0] = bn->maxx8[j];
 			cmax[s][1] = bn->maxy8[j];
 			cmax[s][2] = bn->maxz8[j];
+			if (widen)
+				for (int a = 0; a < 3; a++)
+					widen_box(&cmin[s][a], &cmax[s][a]);
 		}
 		quantise_node(cmin, cmax, &qn);
 		// inner children contiguous in slot order
@@ -211,7 +232,7 @@ bool convert_tlas(const nb_rdata *rd, std::vector<nb_qnode> &nodes,
 		irefs.push_back(inst_base + inst);
 		return 1;
 	};
-	bool ok = convert_tree(base, limit, nodes, *root, leaf, st, err);
+	bool ok = convert_tree(base, limit, nodes, *root, leaf, st, err, true);
 	st->items = (uint32_t)irefs.size() - items0;
 	return ok;
 }

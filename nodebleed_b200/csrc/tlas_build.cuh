@@ -276,13 +276,23 @@ __device__ __forceinline__ int tb_bin(float c, float cmn, float scale)
 	return b < 0 ? 0 : (b > kTbBins - 1 ? kTbBins - 1 : b);
 }
 
-// Box of instance i (wbox in global or, in the build, shared memory).
+// Box of instance i (wbox in global or, in the build, shared memory),
+// widened per axis by 2^-20 of its coordinates' magnitude: the world boxes
+// come from transformed vertices or corners rounded to FP32, and the
+// widening covers that rounding whatever the quantisation of the TLAS
+// (whose planes only keep 1/32 of a quantum outside a child box, and a
+// node of coplanar instances has a tiny quantum along that axis).
 __device__ __forceinline__ void tb_load(const float4 *wbox, uint32_t i,
                                         float lo[3], float hi[3])
 {
 	float4 a = wbox[2u * i], b = wbox[2u * i + 1u];
 	lo[0] = a.x; lo[1] = a.y; lo[2] = a.z;
 	hi[0] = b.x; hi[1] = b.y; hi[2] = b.z;
+	for (int k = 0; k < 3; k++) {
+		float pad = __fmul_ru(fmaxf(fabsf(lo[k]), fabsf(hi[k])), 0x1p-20f);
+		lo[k] = __fsub_rd(lo[k], pad);
+		hi[k] = __fadd_ru(hi[k], pad);
+	}
 }
 
 // Warp-wide min / max of 3-vectors.
