@@ -57,6 +57,11 @@ def parse():
     p.add_argument("--fuse", type=int, default=0,
                    help="1: shadow rays traced with the next bounce's "
                         "closest hits, 2: separate launches, 0: default")
+    p.add_argument("--update-levels", action="store_true",
+                   help="e2e frames rebuild the TLAS level by level "
+                   "(RENDGPU_UPDATE_LEVELS) instead of the library's "
+                   "choice (the collapsed one-CTA build up to 2048 "
+                   "instances)")
     p.add_argument("--queue", type=int, default=0,
                    help="camera slots per wave (0 = the library's default: "
                    "two concurrent half-frame waves)")
@@ -392,9 +397,10 @@ def update_times(a, scene, rd, gr, stream):
     # the default level-by-level build, the one-CTA build collapsed by
     # cost (RENDGPU_UPDATE_COLLAPSE), and a refit of the default build
     for name, kw in (("device_build_collapse_ms", {"collapse": True}),
-                     ("device_build_ms", {}),
-                     ("device_refit_ms", {"refit": True})):
-        gr.update_instances(globs.data_ptr())  # first: builds
+                     ("device_build_ms", {"collapse": False}),
+                     ("device_refit_ms", {"refit": True,
+                                          "collapse": False})):
+        gr.update_instances(globs.data_ptr(), collapse=False)  # builds
         ev = []
         for _ in range(a.update_reps):
             with torch.cuda.stream(stream):
@@ -581,7 +587,8 @@ def run_ours(a):
         t0 = time.perf_counter()
         for _ in range(a.steps):
             t1 = time.perf_counter()
-            gr.update_instances(globs, tight=True)
+            gr.update_instances(globs, tight=True,
+                                collapse=False if a.update_levels else None)
             h2d += gr.stats()["h2d_bytes"]
             t2 = time.perf_counter()
             e2e_rays += gr.frame()

@@ -397,12 +397,16 @@ int rendgpu_get_lights(struct rdata *rd, float *out, uint32_t cap,
  * box (a rotated instance's corner box can be much larger), and build or
  * refit the TLAS over those boxes; rendgpu_get_instances then reports them. */
 #define RENDGPU_UPDATE_TIGHT 2u
-/* RENDGPU_UPDATE_COLLAPSE: build the TLAS as one CTA's binary SAH tree
- * collapsed into 8-wide nodes by cost, as the upload-time rebuild does
- * (faster traversal: +2.5% on the 1024-instance scale frame; slower build:
- * about 1.2 ms for 1024 instances and 3 ms for 4096, against 0.4 and 0.8
- * ms for the default level-by-level build). */
+/* How an update builds the TLAS.  By default scenes of up to 2048
+ * instances get one CTA's binary SAH tree collapsed into 8-wide nodes by
+ * cost, as the upload-time rebuild does, and larger ones a greedy 8-way
+ * split level by level over all SMs.  Measured: 0.57 against 0.43 ms for
+ * 1026 instances, the collapsed tree then 2.5% faster to traverse (scale
+ * frame); 1.7 against 0.8 ms for 4096 instances, no faster to traverse
+ * (stress frame).  RENDGPU_UPDATE_COLLAPSE / RENDGPU_UPDATE_LEVELS choose
+ * one of them whatever the size (not both). */
 #define RENDGPU_UPDATE_COLLAPSE 4u
+#define RENDGPU_UPDATE_LEVELS 8u
 int rendgpu_update_instances_device(struct rdata *rd,
                                     const float *glob_device, uint32_t n,
                                     uint32_t flags);

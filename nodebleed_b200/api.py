@@ -578,12 +578,14 @@ class GpuRenderer:
                  "set_resolve")
 
     def update_instances(self, globs, refit=False, tight=False,
-                         collapse=False):
+                         collapse=None):
         """Device-side scene update from (instances, 16) object->world
-        matrices (host array: copied; else an integer device pointer)."""
+        matrices (host array: copied; else an integer device pointer).
+        collapse: None = the library's choice by instance count, True =
+        the collapsed one-CTA TLAS build, False = level by level."""
         n = self.rdata.rd.instcnt
         flags = (1 if refit else 0) | (2 if tight else 0) | \
-            (4 if collapse else 0)
+            (0 if collapse is None else (4 if collapse else 8))
         if isinstance(globs, int):
             self._ck(self.g.rendgpu_update_instances_device(self.ptr, globs,
                                                             n, flags),

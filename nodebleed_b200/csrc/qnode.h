@@ -117,13 +117,14 @@ NB_HD inline void quantise_node_hd(const float cmin[8][3],
 		double need = fmax(fmax(ext / 249.0, floor_scale), ldexp(1.0, -100));
 		int e = ceil_log2(need);
 		for (;; e++) {
-			double sc = ldexp(1.0, e);
+			// a power of two: multiplying by 2^-e divides exactly
+			double sc = ldexp(1.0, e), isc = ldexp(1.0, -e);
 			// origin two quanta below lo, rounded down to a float
 			double want = (double)lo[a] - 2.0 * sc;
 			float pf = (float)want;
 			if ((double)pf > want)
 				pf = nextafterf(pf, -FLT_MAX);
-			double top = ((double)hi[a] - pf) / sc;
+			double top = ((double)hi[a] - pf) * isc;
 			if (top + 2.0 <= 255.0 && e + kQExpBias >= 1 &&
 			  e + kQExpBias <= 254) {
 				p[a] = pf;
@@ -149,10 +150,10 @@ NB_HD inline void quantise_node_hd(const float cmin[8][3],
 				qhi[a][s] = 0;
 				continue;
 			}
-			double sc = ldexp(1.0, ex[a]);
-			double l = floor(((double)cmin[s][a] - p[a]) / sc -
+			double isc = ldexp(1.0, -ex[a]);
+			double l = floor(((double)cmin[s][a] - p[a]) * isc -
 			  kQMargin);
-			double h = ceil(((double)cmax[s][a] - p[a]) / sc +
+			double h = ceil(((double)cmax[s][a] - p[a]) * isc +
 			  kQMargin);
 			l = fmax(l, 0.0);
 			h = fmin(h, 255.0);

@@ -1864,8 +1864,11 @@ int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
 		  "skipped a degenerate emitter; upload non-degenerate transforms "
 		  "first");
 	if (flags & ~(uint32_t)(RENDGPU_UPDATE_REFIT | RENDGPU_UPDATE_TIGHT |
-	  RENDGPU_UPDATE_COLLAPSE))
+	  RENDGPU_UPDATE_COLLAPSE | RENDGPU_UPDATE_LEVELS))
 		return fail(c, RENDGPU_EINVAL, "update: unknown flags");
+	if ((flags & RENDGPU_UPDATE_COLLAPSE) && (flags & RENDGPU_UPDATE_LEVELS))
+		return fail(c, RENDGPU_EINVAL, "update: COLLAPSE and LEVELS "
+		  "exclude each other");
 	NB_CK(c, cudaSetDevice(c->device));
 	bool refit = (flags & RENDGPU_UPDATE_REFIT) && c->dyn_built;
 	uint32_t nn = std::max(n, 1u);
@@ -1881,8 +1884,9 @@ int update_instances(Ctx *c, const float *glob, uint32_t n, uint32_t flags)
 	}
 	if (!refit) {
 		uint32_t limit = 0;
-		rc = tlas_build(c, n, &limit,
-		  (flags & RENDGPU_UPDATE_COLLAPSE) != 0u);
+		bool collapse = (flags & RENDGPU_UPDATE_COLLAPSE) ||
+		  (!(flags & RENDGPU_UPDATE_LEVELS) && n <= kCollapseMaxInst);
+		rc = tlas_build(c, n, &limit, collapse);
 		if (rc)
 			return rc;
 		h.tlas_depth = c->tlas_depth = limit;
@@ -2071,6 +2075,11 @@ int upload_dynamic_all(Ctx *c)
 // Paths, their PCG32 streams and the accumulation do not depend on the
 // waves, so images are the same as with one wave.
 constexpr uint64_t kTwoWaveMinSlots = 1u << 20;
+
+// Largest instance count whose per-frame TLAS update uses the collapsed
+// one-CTA build by default (above it the level-by-level build is cheaper
+// per frame than what its tree saves in traversal).
+constexpr uint32_t kCollapseMaxInst = 2048;
 
 bool two_waves_fit(const Ctx *c, uint64_t nslots)
 {
