@@ -34,6 +34,11 @@ namespace {
 // Traversal stack depths with compiled kernel variants (entries of 8
 // bytes per thread in shared memory), and the default trace block size.
 constexpr int kStacks[3] = {24, 32, 48};
+
+// Largest instance count whose per-frame TLAS update uses the collapsed
+// one-CTA build by default (above it the level-by-level build is cheaper
+// per frame than what its tree saves in traversal).
+constexpr uint32_t kCollapseMaxInst = 2048;
 constexpr int kStackMax = 48;
 // A deliberately small stack, compiled for the ray-batch calls only and used
 // only when rendgpu_tune.force asks for it: rays whose traversal needs more
@@ -2075,11 +2080,6 @@ int upload_dynamic_all(Ctx *c)
 // Paths, their PCG32 streams and the accumulation do not depend on the
 // waves, so images are the same as with one wave.
 constexpr uint64_t kTwoWaveMinSlots = 1u << 20;
-
-// Largest instance count whose per-frame TLAS update uses the collapsed
-// one-CTA build by default (above it the level-by-level build is cheaper
-// per frame than what its tree saves in traversal).
-constexpr uint32_t kCollapseMaxInst = 2048;
 
 bool two_waves_fit(const Ctx *c, uint64_t nslots)
 {
