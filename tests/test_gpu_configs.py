@@ -212,8 +212,10 @@ def test_two_waves_render_the_same_frame(gpu):
     scene = api.Scene(api.SCENE_SCALE, 1)
     rd = api.RenderData(scene, 1920, 1080, 1)
     out = []
-    for queue in (0, 0x7fffffff):
-        gr = api.GpuRenderer(rd, max_depth=8, seed=4).upload()
+    # two waves, one wave, and two waves captured into a CUDA graph (the
+    # second stream's launches joined into the capture)
+    for queue, graph in ((0, False), (0x7fffffff, False), (0, True)):
+        gr = api.GpuRenderer(rd, max_depth=8, seed=4, graph=graph).upload()
         gr.set_tune(queue=queue)
         samples = rd.rd.samples
         gr.frame()
@@ -226,9 +228,10 @@ def test_two_waves_render_the_same_frame(gpu):
         gr.close()
     rd.close()
     scene.close()
-    (a0, c0, s0, b0), (a1, c1, s1, b1) = out
-    assert (c0, s0) == (c1, s1) and list(b0) == list(b1)
-    assert np.array_equal(a0.view(np.uint32), a1.view(np.uint32))
+    (a0, c0, s0, b0) = out[0]
+    for (a1, c1, s1, b1) in out[1:]:
+        assert (c0, s0) == (c1, s1) and list(b0) == list(b1)
+        assert np.array_equal(a0.view(np.uint32), a1.view(np.uint32))
 
 
 def test_stress_rays_match_reference(gpu, stress_rd):
