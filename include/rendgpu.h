@@ -418,6 +418,17 @@ int rendgpu_update_instances(struct rdata *rd, const float *glob, uint32_t n,
  * build overflow flag) of the last device-side update, which must exist
  * when wbox or info is asked for.  Any pointer may be NULL.  Returns the
  * number of instances copied (<= cap).  Synchronises. */
+/* The BLAS rendgpu_upload_static builds for the mesh rd->tris[triofs ..
+ * triofs + tricnt), built in host memory only (no device, no context; for
+ * checks of the tree): nodes in the GPU layout (struct nb_qnode of
+ * gpulayout.h, 80 bytes, root first, node_cap of them) and triangles
+ * (struct nb_gtri, 48 bytes, tri_cap of them); info = (nodes, triangles,
+ * depth).  Buffers that are too small (or NULL) are left untouched, so a
+ * first call with NULLs returns the sizes.  No counterpart in the reference,
+ * whose build is rend.c:458-709. */
+int rendgpu_blas_host(struct rdata *rd, uint32_t triofs, uint32_t tricnt,
+                      void *nodes, uint32_t node_cap, void *tris,
+                      uint32_t tri_cap, uint32_t info[3]);
 int rendgpu_get_instances(struct rdata *rd, float *xf, float *wbox,
                           uint32_t cap, uint32_t info[3]);
 

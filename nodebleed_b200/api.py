@@ -182,6 +182,7 @@ class GpuLib:
                 ("rendgpu_update_instances_device", [vp, vp, u32, u32]),
                 ("rendgpu_update_instances", [vp, vp, u32, u32]),
                 ("rendgpu_get_instances", [vp, vp, vp, u32, vp]),
+                ("rendgpu_blas_host", [vp, u32, u32, vp, u32, vp, u32, vp]),
                 ("rendgpu_set_resolve", [vp, u32, C.c_float]),
                 ("rendgpu_batch_set_resolve", [vp, u32, C.c_float]),
                 ("rendgpu_captured", [vp, u32, vp, vp, vp, vp]),

@@ -3122,6 +3122,29 @@ int rendgpu_update_instances(struct rdata *rdp, const float *glob,
 	return rc;
 }
 
+int rendgpu_blas_host(struct rdata *rdp, uint32_t triofs, uint32_t tricnt,
+                      void *nodes, uint32_t node_cap, void *tris,
+                      uint32_t tri_cap, uint32_t info[3])
+{
+	if (!rdp || !info || tricnt == 0)
+		return RENDGPU_EINVAL;
+	const nb_rdata *rd = reinterpret_cast<const nb_rdata *>(rdp);
+	if (!rd->tris)
+		return RENDGPU_EINVAL;
+	blas_out b;
+	std::string err;
+	if (!build_blas(rd, triofs, tricnt, blas_params(), &b, &err))
+		return RENDGPU_EINVAL;
+	info[0] = (uint32_t)b.nodes.size();
+	info[1] = (uint32_t)b.tris.size();
+	info[2] = b.depth;
+	if (nodes && node_cap >= b.nodes.size())
+		std::memcpy(nodes, b.nodes.data(), b.nodes.size() * sizeof(nb_qnode));
+	if (tris && tri_cap >= b.tris.size())
+		std::memcpy(tris, b.tris.data(), b.tris.size() * sizeof(nb_gtri));
+	return 0;
+}
+
 int rendgpu_get_instances(struct rdata *rdp, float *xf, float *wbox,
                           uint32_t cap, uint32_t info[3])
 {

@@ -1,0 +1,122 @@
+"""The library's own BLAS build on the CPU (rendgpu_blas_host: the tree
+rendgpu_upload_static builds, in host memory, without a GPU): every triangle
+of the mesh in exactly one leaf with its vertices unchanged, child and item
+indices in range, every quantised child box at least 1/32 of a quantum
+outside the triangles below it, and the depth the build reports."""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from nodebleed_b200 import api
+
+# struct nb_qnode / nb_gtri (gpulayout.h), struct rinst / rtri (rend.h)
+QNODE = np.dtype([("p", "<f4", (3,)), ("e", "u1", (3,)), ("imask", "u1"),
+                  ("child_base", "<u4"), ("item_base", "<u4"),
+                  ("meta", "u1", (8,)), ("qlo", "u1", (3, 8)),
+                  ("qhi", "u1", (3, 8))])
+GTRI = np.dtype([("v0", "<f4", (3,)), ("prim", "<u4"), ("v1", "<f4", (3,)),
+                 ("pad1", "<u4"), ("v2", "<f4", (3,)), ("pad2", "<u4")])
+RINST = np.dtype([("globinv", "<f4", (12,)), ("flags", "<u4"),
+                  ("triofs", "<u4"), ("tricnt", "<u4"), ("pad", "<u4")])
+RTRI = np.dtype([("v0", "<f4", (3,)), ("p0", "<f4"), ("v1", "<f4", (3,)),
+                 ("p1", "<f4"), ("v2", "<f4", (3,)), ("p2", "<f4")])
+EXP_BIAS = 119  # stored exponent byte = e + 127 - 8 (qnode.h kQExpBias)
+
+
+def _array(ptr, dtype, n):
+    raw = (C.c_ubyte * (dtype.itemsize * n)).from_address(ptr)
+    return np.frombuffer(raw, dtype).copy()
+
+
+def _build(rd, triofs, tricnt):
+    g = api.gpu_lib().L
+    info = (C.c_uint32 * 3)()
+    assert g.rendgpu_blas_host(rd.ptr, triofs, tricnt, None, 0, None, 0,
+                               info) == 0
+    nodes = np.zeros(info[0], QNODE)
+    tris = np.zeros(info[1], GTRI)
+    assert g.rendgpu_blas_host(rd.ptr, triofs, tricnt, nodes.ctypes.data,
+                               len(nodes), tris.ctypes.data, len(tris),
+                               info) == 0
+    return nodes, tris, int(info[2])
+
+
+def _check(nodes, tris, depth, mesh):
+    verts = np.stack([tris["v0"], tris["v1"], tris["v2"]], 1).astype(
+        np.float64)                                   # (items, 3, 3)
+    seen = np.zeros(len(mesh), np.int64)
+    maxd = [0]
+
+    def walk(ni, d):
+        """Checks node ni; returns the bounds of its triangles."""
+        assert 0 <= ni < len(nodes)
+        maxd[0] = max(maxd[0], d)
+        n = nodes[ni]
+        scale = np.ldexp(1.0, n["e"].astype(np.int64) - EXP_BIAS)
+        p = n["p"].astype(np.float64)
+        lo_all = np.full(3, np.inf)
+        hi_all = np.full(3, -np.inf)
+        for s in range(8):
+            inner = (int(n["imask"]) >> s) & 1
+            meta = int(n["meta"][s])
+            if inner:
+                below = bin(int(n["imask"]) & ((1 << s) - 1)).count("1")
+                clo, chi = walk(int(n["child_base"]) + below, d + 1)
+            elif meta & 0x80:
+                cnt = ((meta >> 5) & 3) + 1
+                first = int(n["item_base"]) + (meta & 31)
+                assert first + cnt <= len(tris)
+                for k in range(first, first + cnt):
+                    prim = int(tris["prim"][k])
+                    seen[prim] += 1
+                    t = mesh[prim]
+                    for a, b in (("v0", "v0"), ("v1", "v1"), ("v2", "v2")):
+                        assert np.array_equal(tris[a][k].view(np.uint32),
+                                              t[b].view(np.uint32))
+                v = verts[first:first + cnt].reshape(-1, 3)
+                clo, chi = v.min(0), v.max(0)
+            else:
+                continue
+            qlo = p + n["qlo"][:, s] * scale
+            qhi = p + n["qhi"][:, s] * scale
+            assert np.all(qlo <= clo - scale / 32), (ni, s, qlo - clo)
+            assert np.all(qhi >= chi + scale / 32), (ni, s, qhi - chi)
+            lo_all = np.minimum(lo_all, clo)
+            hi_all = np.maximum(hi_all, chi)
+        assert np.isfinite(lo_all).all(), f"node {ni} without children"
+        return lo_all, hi_all
+
+    walk(0, 1)
+    assert np.all(seen == 1), np.nonzero(seen != 1)[0][:5]
+    assert maxd[0] == depth
+
+
+@pytest.mark.parametrize("fam,param", [(api.SCENE_TINY, 0),
+                                       (api.SCENE_SCALE, 3)])
+def test_blas_build_host(fam, param):
+    scene = api.Scene(fam, 1, param)
+    rd = api.RenderData(scene, 64, 36, 1)
+    insts = _array(rd.rd.insts, RINST, rd.rd.instcnt)
+    meshes = sorted({(int(i["triofs"]), int(i["tricnt"])) for i in insts})
+    total = sum(c for _, c in meshes)
+    alltris = _array(rd.rd.tris, RTRI, max(o + c for o, c in meshes))
+    for triofs, tricnt in meshes:
+        nodes, tris, depth = _build(rd, triofs, tricnt)
+        assert len(tris) == tricnt and depth >= 1
+        _check(nodes, tris, depth, alltris[triofs:triofs + tricnt])
+    assert total > 0
+    rd.close()
+    scene.close()
+
+
+def test_blas_build_host_rejects_bad_arguments():
+    g = api.gpu_lib().L
+    info = (C.c_uint32 * 3)()
+    assert g.rendgpu_blas_host(None, 0, 1, None, 0, None, 0, info) == -1
+    scene = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(scene, 16, 9, 1)
+    assert g.rendgpu_blas_host(rd.ptr, 0, 0, None, 0, None, 0, info) == -1
+    rd.close()
+    scene.close()
