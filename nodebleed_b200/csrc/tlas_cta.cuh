@@ -13,9 +13,10 @@
 //      binary node and budget 1..8 the cheapest forest of 8-wide nodes, cost
 //      = surface area of each 8-wide node (every leaf holds one instance, so
 //      the leaves add the same to every tree and drop out);
-//   3. the 8-wide nodes top-down, one thread per node, encoded as the greedy
-//      build encodes them (qnode.h), with per-slot instance ranges for the
-//      refit.
+//   3. the 8-wide nodes top-down, one warp per node on levels of up to
+//      kCbWarpEmitMax nodes (the slot assignment across the warp), one
+//      thread per node on wider ones, encoded as the greedy build encodes
+//      them (qnode.h), with per-slot instance ranges for the refit.
 // Depth: the traversal stack was sized for depth_limit TLAS levels.  SAH
 // splits are kept only while a median-split finish of the subtree stays
 // within binary depth 3 * depth_limit, and if the collapse by cost comes
@@ -36,6 +37,7 @@ constexpr int kCbBins = 32;      // bins per axis of a CTA split
 constexpr int kCbWarpBins = 16;  // bins per axis of a warp split
 constexpr uint32_t kCbBig = 512; // nodes split by the whole CTA
 constexpr int kCbMaxLevels = 160; // binary levels (3 * depth_limit bound)
+constexpr uint32_t kCbWarpEmitMax = 128; // levels emitted a warp per node
 
 struct TcNode { // binary node
 	float    lo[3], hi[3];
@@ -664,11 +666,62 @@ __device__ void tc_widest_node(const TcArgs &T, uint32_t q)
 		T.kd[8u * q + j - 1u] = (uint8_t)(ll ? 1u : (rl ? j - 1u : j / 2u));
 }
 
+// assign_slots (qnode.h) with the whole warp: each lane scores two of the
+// 64 (child, slot) pairs, and each greedy round takes the best remaining
+// pair by a warp argmax (the lowest pair index c * 8 + s on equal scores,
+// the order in which the sequential loop keeps the first maximum), so every
+// lane gets the sequential assignment.
+__device__ void tc_assign_slots_warp(int nchild, const float cen[8][3],
+                                     const float nc[3], int slot_of[8])
+{
+	const int lane = (int)(threadIdx.x & 31u);
+	float sc[2];
+	bool ok[2];
+	for (int h = 0; h < 2; h++) {
+		int p = lane + 32 * h, c = p >> 3, sl = p & 7;
+		ok[h] = c < nchild;
+		float v = 0.0f;
+		if (ok[h])
+			for (int a = 0; a < 3; a++)
+				v += (cen[c][a] - nc[a]) * ((sl >> a) & 1 ? 1.0f : -1.0f);
+		sc[h] = v;
+	}
+	for (int i = 0; i < 8; i++)
+		slot_of[i] = -1;
+	for (int round = 0; round < nchild; round++) {
+		float bv = -FLT_MAX;
+		int bi = -1;
+		for (int h = 0; h < 2; h++)
+			if (ok[h] && (bi < 0 || sc[h] > bv)) {
+				bv = sc[h];
+				bi = lane + 32 * h;
+			}
+		for (int o = 16; o > 0; o >>= 1) {
+			float ov = __shfl_xor_sync(kFull, bv, o);
+			int oi = __shfl_xor_sync(kFull, bi, o);
+			if (oi >= 0 && (bi < 0 || ov > bv || (ov == bv && oi < bi))) {
+				bv = ov;
+				bi = oi;
+			}
+		}
+		int bc = bi >> 3, bs = bi & 7;
+		slot_of[bc] = bs;
+		for (int h = 0; h < 2; h++) {
+			int p = lane + 32 * h;
+			if ((p >> 3) == bc || (p & 7) == bs)
+				ok[h] = false;
+		}
+	}
+}
+
 // Encode the 8-wide node `out` for binary node q at depth `depth`: its
 // children from the collapse tables, slots, quantised boxes, leaf items,
-// refit ranges; inner children go to the next queue (one thread).
+// refit ranges; inner children go to the next queue.  One thread, or with
+// `warp` the whole warp: every lane finds the children, the warp assigns
+// the slots, lane 0 encodes and writes.
 __device__ void tc_emit_node(const TcArgs &T, TcShared &S, uint32_t q,
-                             uint32_t out, uint32_t depth, uint32_t *nextq)
+                             uint32_t out, uint32_t depth, uint32_t *nextq,
+                             bool warp)
 {
 	const TbArgs &A = T.A;
 	const TcNode nd = T.bn[q];
@@ -716,7 +769,13 @@ __device__ void tc_emit_node(const TcArgs &T, TcShared &S, uint32_t q,
 	for (int a = 0; a < 3; a++)
 		ncen[a] = 0.5f * (nd.lo[a] + nd.hi[a]);
 	int slot_of[8], child_at[8];
-	assign_slots(nk, cen, ncen, slot_of);
+	if (warp) {
+		tc_assign_slots_warp(nk, cen, ncen, slot_of);
+		if ((threadIdx.x & 31u) != 0u)
+			return;
+	} else {
+		assign_slots(nk, cen, ncen, slot_of);
+	}
 	for (int s = 0; s < 8; s++)
 		child_at[s] = -1;
 	for (int c = 0; c < nk; c++)
@@ -797,9 +856,18 @@ __device__ void tc_emit(const TcArgs &T, TcShared &S)
 		uint32_t nq = S.qn;
 		if (nq == 0u)
 			break;
-		for (uint32_t e = tid; e < nq; e += kCbThreads)
-			tc_emit_node(T, S, cur[3u * e], cur[3u * e + 1u],
-			  cur[3u * e + 2u], nxt);
+		// A warp per node while that takes a few rounds of the 32 warps;
+		// on wider levels lane 0's serial encoding would queue up, and a
+		// thread per node is faster.
+		if (nq <= kCbWarpEmitMax) {
+			for (uint32_t e = tid >> 5; e < nq; e += (uint32_t)kCbWarps)
+				tc_emit_node(T, S, cur[3u * e], cur[3u * e + 1u],
+				  cur[3u * e + 2u], nxt, true);
+		} else {
+			for (uint32_t e = tid; e < nq; e += (uint32_t)kCbThreads)
+				tc_emit_node(T, S, cur[3u * e], cur[3u * e + 1u],
+				  cur[3u * e + 2u], nxt, false);
+		}
 		__syncthreads();
 		if (tid == 0) {
 			S.qn = S.qn2;
