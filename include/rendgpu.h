@@ -418,8 +418,11 @@ int rendgpu_update_instances(struct rdata *rd, const float *glob, uint32_t n,
  * build overflow flag) of the last device-side update, which must exist
  * when wbox or info is asked for.  Any pointer may be NULL.  Returns the
  * number of instances copied (<= cap).  Synchronises. */
+int rendgpu_get_instances(struct rdata *rd, float *xf, float *wbox,
+                          uint32_t cap, uint32_t info[3]);
 /* The BLAS rendgpu_upload_static builds for the mesh rd->tris[triofs ..
- * triofs + tricnt), built in host memory only (no device, no context; for
+ * triofs + tricnt), which must be the triangle range of one of rd's
+ * instances, built in host memory only (no device, no context; for
  * checks of the tree): nodes in the GPU layout (struct nb_qnode of
  * gpulayout.h, 80 bytes, root first, node_cap of them) and triangles
  * (struct nb_gtri, 48 bytes, tri_cap of them); info = (nodes, triangles,
@@ -429,8 +432,6 @@ int rendgpu_update_instances(struct rdata *rd, const float *glob, uint32_t n,
 int rendgpu_blas_host(struct rdata *rd, uint32_t triofs, uint32_t tricnt,
                       void *nodes, uint32_t node_cap, void *tris,
                       uint32_t tri_cap, uint32_t info[3]);
-int rendgpu_get_instances(struct rdata *rd, float *xf, float *wbox,
-                          uint32_t cap, uint32_t info[3]);
 
 /* 8-bit resolve of the frame image (rd->buf through rendgpu_readback),
  * done in the accumulation pass of every later frame.  The reference packs

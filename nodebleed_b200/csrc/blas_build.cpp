@@ -242,12 +242,15 @@ struct Builder {
 	}
 
 	// Collapse tables (Ylitie et al. 2017, section 3.1).
-	std::vector<float> cost;     // 8 per binary node: budget 1..8
+	std::vector<double> cost;    // 8 per binary node: budget 1..8
 	std::vector<uint8_t> kd;     // 8 per node: left budget of budget j
 	std::vector<uint8_t> prev;   // bit j: cost[j] taken from budget j-1
 	std::vector<uint8_t> asleaf; // budget 1 is a leaf
 
-	void collapse_costs(float c_node, float c_tri)
+	// In double: surface areas of boxes with coordinates near the float
+	// range (1e20 and up) overflow a float, and infinite costs would make a
+	// node of more than kLeafMax triangles look no worse as a leaf.
+	void collapse_costs(double c_node, double c_tri)
 	{
 		size_t m = bn.size();
 		cost.assign(8 * m, 0.0f);
@@ -256,10 +259,10 @@ struct Builder {
 		asleaf.assign(m, 0);
 		for (size_t q = m; q-- > 0;) {
 			const BNode &b = bn[q];
-			float A = (float)b.box.area();
-			float cl = b.count <= (uint32_t)kLeafMax ?
-			  A * c_tri * (float)b.count : FLT_MAX;
-			float *C = &cost[8 * q];
+			double A = b.box.area();
+			bool fits = b.count <= (uint32_t)kLeafMax;
+			double cl = fits ? A * c_tri * (double)b.count : HUGE_VAL;
+			double *C = &cost[8 * q];
 			if (b.left == kNone) {
 				for (int i = 0; i < 8; i++)
 					C[i] = cl;
@@ -267,15 +270,15 @@ struct Builder {
 				prev[q] = 0xfe;
 				continue;
 			}
-			const float *L = &cost[8 * (size_t)b.left];
-			const float *R = &cost[8 * (size_t)b.right];
-			float dist[9];
+			const double *L = &cost[8 * (size_t)b.left];
+			const double *R = &cost[8 * (size_t)b.right];
+			double dist[9];
 			uint8_t karg[9] = {};
 			for (int j = 2; j <= 8; j++) {
-				float best = FLT_MAX;
+				double best = HUGE_VAL;
 				int bk = 1;
 				for (int k = 1; k < j; k++) {
-					float v = L[k - 1] + R[j - k - 1];
+					double v = L[k - 1] + R[j - k - 1];
 					if (v < best) {
 						best = v;
 						bk = k;
@@ -285,8 +288,8 @@ struct Builder {
 				karg[j] = (uint8_t)bk;
 				kd[8 * q + (j - 1)] = (uint8_t)bk;
 			}
-			float cn = A * c_node + dist[8];
-			if (cl <= cn) {
+			double cn = A * c_node + dist[8];
+			if (fits && cl <= cn) {
 				C[0] = cl;
 				asleaf[q] = 1;
 			} else {
@@ -351,14 +354,17 @@ bool build_blas(const nb_rdata *rd, uint32_t triofs, uint32_t tricnt,
 		b.hi[0] = std::max(std::max(t.v0.x, t.v1.x), t.v2.x);
 		b.hi[1] = std::max(std::max(t.v0.y, t.v1.y), t.v2.y);
 		b.hi[2] = std::max(std::max(t.v0.z, t.v1.z), t.v2.z);
-		for (int a = 0; a < 3; a++) {
-			if (!std::isfinite(b.lo[a]) || !std::isfinite(b.hi[a])) {
+		// the vertices themselves: std::min and std::max drop a NaN
+		const float vs[9] = {t.v0.x, t.v0.y, t.v0.z, t.v1.x, t.v1.y,
+		  t.v1.z, t.v2.x, t.v2.y, t.v2.z};
+		for (float v : vs)
+			if (!std::isfinite(v)) {
 				*err = "non-finite vertex in triangle " +
 				  std::to_string(i);
 				return false;
 			}
+		for (int a = 0; a < 3; a++)
 			B.cen[3 * (size_t)i + a] = 0.5f * b.lo[a] + 0.5f * b.hi[a];
-		}
 		B.pbox[i] = b;
 		B.idx[i] = i;
 	}

@@ -3129,7 +3129,14 @@ int rendgpu_blas_host(struct rdata *rdp, uint32_t triofs, uint32_t tricnt,
 	if (!rdp || !info || tricnt == 0)
 		return RENDGPU_EINVAL;
 	const nb_rdata *rd = reinterpret_cast<const nb_rdata *>(rdp);
-	if (!rd->tris)
+	if (!rd->tris || !rd->insts)
+		return RENDGPU_EINVAL;
+	// rdata holds no triangle count: the range must be an instance's mesh
+	bool known = false;
+	for (uint32_t i = 0; i < rd->instcnt && !known; i++)
+		known = rd->insts[i].triofs == triofs &&
+		  rd->insts[i].tricnt == tricnt;
+	if (!known)
 		return RENDGPU_EINVAL;
 	blas_out b;
 	std::string err;

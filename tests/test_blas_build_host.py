@@ -120,3 +120,81 @@ def test_blas_build_host_rejects_bad_arguments():
     assert g.rendgpu_blas_host(rd.ptr, 0, 0, None, 0, None, 0, info) == -1
     rd.close()
     scene.close()
+
+
+def _writable(ptr, dtype, n):
+    raw = (C.c_ubyte * (dtype.itemsize * n)).from_address(ptr)
+    return np.frombuffer(raw, dtype)
+
+
+def _planted(kind, n, rng):
+    """n triangles (n, 3 vertices, xyz) of one degenerate or extreme kind."""
+    if kind == "identical":      # every centroid and box the same
+        return np.broadcast_to(rng.normal(size=(1, 3, 3)), (n, 3, 3))
+    if kind == "points":         # zero-size boxes on a line, duplicates
+        p = np.zeros((n, 1, 3))
+        p[:, 0, 0] = rng.integers(0, 7, n)
+        return np.broadcast_to(p, (n, 3, 3))
+    if kind == "flat":           # zero extent along z
+        v = rng.normal(size=(n, 3, 3))
+        v[:, :, 2] = 0.5
+        return v
+    if kind == "huge":
+        return rng.normal(size=(n, 3, 3)) * 1e30
+    if kind == "tiny":
+        return rng.normal(size=(n, 3, 3)) * 1e-30
+    if kind == "mixed":          # small triangles inside huge node boxes
+        v = rng.normal(size=(n, 3, 3))
+        v[: n // 2] *= 1e20
+        v[n // 2:] = v[n // 2:] * 1e-3 + 1.0
+        return v
+    return rng.normal(size=(n, 3, 3)) * rng.uniform(0.01, 10.0, (n, 1, 1))
+
+
+@pytest.mark.parametrize("kind", ["identical", "points", "flat", "huge",
+                                  "tiny", "mixed", "random"])
+@pytest.mark.parametrize("count", [1, 2, 5, 9, 128, 129, 320])
+def test_blas_build_host_degenerate_and_extreme(kind, count):
+    """Planted meshes: one instance's range cut to `count` triangles (the
+    sweep / binned split boundary at 128 included) and its triangles
+    replaced by coincident, point-like, flat, huge, tiny or mixed-scale
+    ones; the tree must still hold every triangle once inside conservative
+    boxes."""
+    scene = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(scene, 16, 9, 1)
+    insts = _writable(rd.rd.insts, RINST, rd.rd.instcnt)
+    big = int(np.argmax(insts["tricnt"]))
+    triofs = int(insts["triofs"][big])
+    assert count <= int(insts["tricnt"][big])
+    insts["tricnt"][big] = count
+    rng = np.random.default_rng(count * 31 + len(kind))
+    v = _planted(kind, count, rng).astype(np.float32)
+    tris = _writable(rd.rd.tris, RTRI, triofs + count)[triofs:]
+    for k, name in enumerate(("v0", "v1", "v2")):
+        tris[name] = v[:, k]
+    mesh = tris.copy()
+    nodes, out, depth = _build(rd, triofs, count)
+    assert len(out) == count and depth >= 1
+    _check(nodes, out, depth, mesh)
+    rd.close()
+    scene.close()
+
+
+def test_blas_build_host_rejects_unknown_ranges_and_nan():
+    scene = api.Scene(api.SCENE_TINY, 1)
+    rd = api.RenderData(scene, 16, 9, 1)
+    g = api.gpu_lib().L
+    info = (C.c_uint32 * 3)()
+    insts = _writable(rd.rd.insts, RINST, rd.rd.instcnt)
+    triofs, tricnt = int(insts["triofs"][0]), int(insts["tricnt"][0])
+    # a range no instance uses (it could run past the triangle array)
+    assert g.rendgpu_blas_host(rd.ptr, triofs, tricnt + 1, None, 0, None, 0,
+                               info) == -1
+    assert g.rendgpu_blas_host(rd.ptr, triofs + 1, tricnt, None, 0, None, 0,
+                               info) == -1
+    tris = _writable(rd.rd.tris, RTRI, triofs + tricnt)
+    tris["v1"][triofs + tricnt - 1] = np.float32("nan")
+    assert g.rendgpu_blas_host(rd.ptr, triofs, tricnt, None, 0, None, 0,
+                               info) == -1
+    rd.close()
+    scene.close()
