@@ -36,7 +36,10 @@ NB_HD inline int ceil_log2(double x)
 // Greedy assignment of children to slots: slot s prefers children lying
 // towards (+/-x, +/-y, +/-z) by its bits, so that ascending slot ^ octant is
 // roughly near-to-far for rays of that octant (after Ylitie, Karras and
-// Laine 2017).  cen: child box centres, nc: node box centre.
+// Laine 2017).  cen: child box centres, nc: node box centre.  A round in
+// which no score beats -FLT_MAX (NaN or -inf scores, from centres that
+// overflowed) takes the first free (child, slot) pair, so every child gets
+// a slot.
 NB_HD inline void assign_slots(int nchild, const float cen[8][3],
                                const float nc[3], int slot_of[8])
 {
@@ -48,13 +51,17 @@ NB_HD inline void assign_slots(int nchild, const float cen[8][3],
 		slot_of[i] = -1;
 	for (int round = 0; round < nchild; round++) {
 		float best = -FLT_MAX;
-		int bc = -1, bs = -1;
+		int bc = -1, bs = -1, fc = -1, fs = -1;
 		for (int c = 0; c < nchild; c++) {
 			if (used_c[c])
 				continue;
 			for (int s = 0; s < 8; s++) {
 				if (used_s[s])
 					continue;
+				if (fc < 0) {
+					fc = c;
+					fs = s;
+				}
 				float sc = 0.0f;
 				for (int a = 0; a < 3; a++)
 					sc += (cen[c][a] - nc[a]) *
@@ -65,6 +72,10 @@ NB_HD inline void assign_slots(int nchild, const float cen[8][3],
 					bs = s;
 				}
 			}
+		}
+		if (bc < 0) {
+			bc = fc;
+			bs = fs;
 		}
 		used_c[bc] = used_s[bs] = true;
 		slot_of[bc] = bs;
@@ -81,6 +92,13 @@ constexpr int kQExpBias = 127 - 8;
 // plane distances, at most 2^-9 + 2^-14 quanta (trace.cuh: visit); errors
 // relative to the distance are covered there by widening the far plane.
 constexpr double kQMargin = 1.0 / 32.0;
+
+// Bound on the node frame's coordinates: infinite child bounds (a transform
+// that overflows float, vertices next to FLT_MAX) are clamped to +-2^125 for
+// the origin and exponent, so the exponent search always ends with a finite
+// origin.  Child planes beyond the frame saturate at 0 and 255: geometry
+// farther out than 2^125 (4.25e37) need not lie inside its box.
+constexpr float kQFrameMax = 4.2535296e37f; // 2^125
 
 // Quantise one node: child boxes (min/max per slot; empty slots have
 // min > max) into n's origin, exponents and qlo/qhi.  Per axis the scale is
@@ -108,6 +126,10 @@ NB_HD inline void quantise_node_hd(const float cmin[8][3],
 	if (!any)
 		for (int a = 0; a < 3; a++)
 			lo[a] = hi[a] = 0.0f;
+	for (int a = 0; a < 3; a++) {
+		lo[a] = fminf(fmaxf(lo[a], -kQFrameMax), kQFrameMax);
+		hi[a] = fminf(fmaxf(hi[a], -kQFrameMax), kQFrameMax);
+	}
 	float p[3];
 	int ex[3];
 	for (int a = 0; a < 3; a++) {
@@ -116,6 +138,8 @@ NB_HD inline void quantise_node_hd(const float cmin[8][3],
 		  fabs((double)hi[a])) * ldexp(1.0, -22);
 		double need = fmax(fmax(ext / 249.0, floor_scale), ldexp(1.0, -100));
 		int e = ceil_log2(need);
+		// ends by e = 254 - kQExpBias at the latest, whatever the input;
+		// the frame bound keeps it far below that
 		for (;; e++) {
 			// a power of two: multiplying by 2^-e divides exactly
 			double sc = ldexp(1.0, e), isc = ldexp(1.0, -e);
@@ -125,8 +149,8 @@ NB_HD inline void quantise_node_hd(const float cmin[8][3],
 			if ((double)pf > want)
 				pf = nextafterf(pf, -FLT_MAX);
 			double top = ((double)hi[a] - pf) * isc;
-			if (top + 2.0 <= 255.0 && e + kQExpBias >= 1 &&
-			  e + kQExpBias <= 254) {
+			if ((top + 2.0 <= 255.0 && e + kQExpBias >= 1) ||
+			  e + kQExpBias >= 254) {
 				p[a] = pf;
 				ex[a] = e;
 				break;
@@ -155,8 +179,10 @@ NB_HD inline void quantise_node_hd(const float cmin[8][3],
 			  kQMargin);
 			double h = ceil(((double)cmax[s][a] - p[a]) * isc +
 			  kQMargin);
-			l = fmax(l, 0.0);
-			h = fmin(h, 255.0);
+			// both ends saturate: a child beyond the clamped frame
+			// can lie wholly above 255 or below 0
+			l = fmin(fmax(l, 0.0), 255.0);
+			h = fmin(fmax(h, 0.0), 255.0);
 			qlo[a][s] = (uint8_t)l;
 			qhi[a][s] = (uint8_t)h;
 		}

@@ -670,7 +670,9 @@ __device__ void tc_widest_node(const TcArgs &T, uint32_t q)
 // 64 (child, slot) pairs, and each greedy round takes the best remaining
 // pair by a warp argmax (the lowest pair index c * 8 + s on equal scores,
 // the order in which the sequential loop keeps the first maximum), so every
-// lane gets the sequential assignment.
+// lane gets the sequential assignment.  Scores are clamped to -FLT_MAX
+// (NaN included): a total order on which all lanes agree, and the lowest
+// free pair when nothing beats -FLT_MAX, as in the sequential loop.
 __device__ void tc_assign_slots_warp(int nchild, const float cen[8][3],
                                      const float nc[3], int slot_of[8])
 {
@@ -684,7 +686,7 @@ __device__ void tc_assign_slots_warp(int nchild, const float cen[8][3],
 		if (ok[h])
 			for (int a = 0; a < 3; a++)
 				v += (cen[c][a] - nc[a]) * ((sl >> a) & 1 ? 1.0f : -1.0f);
-		sc[h] = v;
+		sc[h] = fmaxf(v, -FLT_MAX);
 	}
 	for (int i = 0; i < 8; i++)
 		slot_of[i] = -1;

@@ -23,6 +23,7 @@ RINST = np.dtype([("globinv", "<f4", (12,)), ("flags", "<u4"),
 RTRI = np.dtype([("v0", "<f4", (3,)), ("p0", "<f4"), ("v1", "<f4", (3,)),
                  ("p1", "<f4"), ("v2", "<f4", (3,)), ("p2", "<f4")])
 EXP_BIAS = 119  # stored exponent byte = e + 127 - 8 (qnode.h kQExpBias)
+FRAME_MAX = 2.0 ** 125  # node frames are clamped here (qnode.h kQFrameMax)
 
 
 def _array(ptr, dtype, n):
@@ -81,8 +82,13 @@ def _check(nodes, tris, depth, mesh):
                 continue
             qlo = p + n["qlo"][:, s] * scale
             qhi = p + n["qhi"][:, s] * scale
-            assert np.all(qlo <= clo - scale / 32), (ni, s, qlo - clo)
-            assert np.all(qhi >= chi + scale / 32), (ni, s, qhi - chi)
+            # contained unless the child reaches beyond the clamped frame
+            inside = (clo >= -FRAME_MAX) & (chi <= FRAME_MAX)
+            assert np.all((qlo <= clo - scale / 32) | ~inside), \
+                (ni, s, qlo - clo)
+            assert np.all((qhi >= chi + scale / 32) | ~inside), \
+                (ni, s, qhi - chi)
+            assert np.all(np.isfinite(qlo) & np.isfinite(qhi))
             lo_all = np.minimum(lo_all, clo)
             hi_all = np.maximum(hi_all, chi)
         assert np.isfinite(lo_all).all(), f"node {ni} without children"
@@ -143,6 +149,12 @@ def _planted(kind, n, rng):
         return rng.normal(size=(n, 3, 3)) * 1e30
     if kind == "tiny":
         return rng.normal(size=(n, 3, 3)) * 1e-30
+    if kind == "fltmax":         # next to the float range's ends
+        return rng.uniform(-1.0, 1.0, (n, 3, 3)) * 3.4e38
+    if kind == "beyond":         # half wholly outside the 2^125 frame
+        v = rng.uniform(0.0, 1.0, (n, 3, 3))
+        v[: (n + 1) // 2] = 1e38 + v[: (n + 1) // 2] * 2.4e38
+        return v
     if kind == "mixed":          # small triangles inside huge node boxes
         v = rng.normal(size=(n, 3, 3))
         v[: n // 2] *= 1e20
@@ -151,15 +163,18 @@ def _planted(kind, n, rng):
     return rng.normal(size=(n, 3, 3)) * rng.uniform(0.01, 10.0, (n, 1, 1))
 
 
+@pytest.mark.timeout(120)
 @pytest.mark.parametrize("kind", ["identical", "points", "flat", "huge",
-                                  "tiny", "mixed", "random"])
+                                  "tiny", "mixed", "fltmax", "beyond",
+                                  "random"])
 @pytest.mark.parametrize("count", [1, 2, 5, 9, 128, 129, 320])
 def test_blas_build_host_degenerate_and_extreme(kind, count):
     """Planted meshes: one instance's range cut to `count` triangles (the
     sweep / binned split boundary at 128 included) and its triangles
-    replaced by coincident, point-like, flat, huge, tiny or mixed-scale
-    ones; the tree must still hold every triangle once inside conservative
-    boxes."""
+    replaced by coincident, point-like, flat, huge, tiny, mixed-scale or
+    near-FLT_MAX ones; the tree must still hold every triangle once inside
+    conservative boxes (the build must end: an unbounded exponent search
+    once spun on infinite frames)."""
     scene = api.Scene(api.SCENE_TINY, 1)
     rd = api.RenderData(scene, 16, 9, 1)
     insts = _writable(rd.rd.insts, RINST, rd.rd.instcnt)
