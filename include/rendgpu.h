@@ -190,8 +190,11 @@ int rendgpu_init(struct rdata *rd, const struct rendgpu_cfg *cfg);
 int rendgpu_release(struct rdata *rd);
 
 /* After rend_prepstatic (rend.c:3033): upload every BLAS reachable from
- * rd->insts (converted to the GPU node layout), triangles, normals and
- * materials. */
+ * rd->insts, triangles, normals and materials.  The BLASes are built by the
+ * library on the host's cores (binary SAH tree collapsed to the GPU node
+ * layout; rendgpu_blas_host shows one), or converted node for node from the
+ * reference's with cfg.reserved[4] bit 1.  A mesh with a NaN or infinite
+ * vertex fails the built form with RENDGPU_EINVAL. */
 int rendgpu_upload_static(struct rdata *rd);
 
 /* After rend_prepdynamic (rend.c:3073): upload the TLAS, the instance
