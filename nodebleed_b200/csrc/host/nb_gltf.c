@@ -302,6 +302,7 @@ struct gl_load {
 	int              cam_done;
 	unsigned int     instcap;
 	int              err;
+	uint8_t         *seen;   // per node: reached from a scene root
 };
 
 static int comp_size(uint32_t c)
@@ -572,6 +573,12 @@ static int load_nodes(struct gl_load *L, int node_id, const float pg[16],
 	int node = j_at(d, nodes, node_id);
 	if (node < 0 || depth > 64)
 		return -1;
+	// glTF nodes form trees (at most one parent each): a node reached twice
+	// is a cycle or a shared child, and shared children repeated on every
+	// level would take up to 2^64 visits within the depth bound
+	if (L->seen[node_id])
+		return -1;
+	L->seen[node_id] = 1;
 	float loc[16], g[16];
 	if (node_local(d, node, loc))
 		return -1;
@@ -697,6 +704,9 @@ int nbh_scene_load_gltf(struct nbh_scene *s, const char *path,
 	int sc = j_at(d, j_get(d, 0, "scenes"),
 	  (int)j_num(d, j_get(d, 0, "scene"), 0));
 	int roots = j_get(d, sc, "nodes");
+	L.seen = calloc((size_t)j_len(d, j_get(d, 0, "nodes")) + 1, 1);
+	if (!L.seen)
+		goto out;
 	static const float ident[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0,
 	  0, 0, 0, 1};
 	for (int i = 0; i < j_len(d, roots); i++)
@@ -733,6 +743,7 @@ out:
 		nbh_scene_free(s);
 	free(L.views);
 	free(L.accs);
+	free(L.seen);
 	free(L.d.t);
 	free(txt);
 	free(bin);

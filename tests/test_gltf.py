@@ -212,3 +212,113 @@ def test_loader_rejects_malformed(tmp_path):
     missing.write_text('{"buffers": [{"uri": "absent.bin"}], "meshes": []}')
     with pytest.raises(RuntimeError):
         api.Scene.load_gltf(str(missing))
+
+
+def _corruptions(doc, binlen):
+    """(name, edit of the parsed .gltf, expected: 'error' or 'loads')."""
+    import copy
+    nacc = len(doc["accessors"])
+    idx_acc = doc["meshes"][0]["primitives"][0]["indices"]
+    nnodes = len(doc["nodes"])
+
+    def edit(f):
+        def run(d):
+            d = copy.deepcopy(d)
+            f(d)
+            return d
+        return run
+
+    def chain(d, shared):
+        # nodes nnodes.. nnodes+39: each lists the next as its children
+        # (twice when shared), reached from the scene root
+        base = len(d["nodes"])
+        for i in range(40):
+            nxt = [base + i + 1] * (2 if shared else 1) if i < 39 else []
+            d["nodes"].append({"children": nxt} if nxt else {})
+        d["scenes"][d.get("scene", 0)]["nodes"].append(base)
+
+    def cycle(d):
+        d["nodes"][0].setdefault("children", []).append(0)
+
+    def root_twice(d):
+        roots = d["scenes"][d.get("scene", 0)]["nodes"]
+        roots.append(roots[0])
+
+    return [
+        ("huge accessor count", edit(lambda d: d["accessors"][0].update(
+            count=10 ** 9)), "error"),
+        ("view past the buffer", edit(lambda d: d["bufferViews"][0].update(
+            byteOffset=binlen)), "error"),
+        ("view longer than the buffer", edit(
+            lambda d: d["bufferViews"][-1].update(byteLength=binlen * 4)),
+         "loads"),
+        ("accessor offset past its view", edit(
+            lambda d: d["accessors"][idx_acc].update(byteOffset=1 << 30)),
+         "error"),
+        ("index count not a multiple of 3", edit(
+            lambda d: d["accessors"][idx_acc].update(
+                count=d["accessors"][idx_acc]["count"] - 1)), "error"),
+        ("float indices", edit(lambda d: d["accessors"][idx_acc].update(
+            componentType=5126)), "error"),
+        ("positions as VEC2", edit(lambda d: d["accessors"][
+            d["meshes"][0]["primitives"][0]["attributes"]["POSITION"]
+        ].update(type="VEC2")), "error"),
+        ("accessor out of range", edit(
+            lambda d: d["meshes"][0]["primitives"][0].update(
+                indices=nacc + 5)), "error"),
+        ("mesh out of range", edit(lambda d: [
+            n.update(mesh=len(d["meshes"]) + 3) for n in d["nodes"]
+            if "mesh" in n][:1]), "error"),
+        ("material out of range (the first material instead)", edit(
+            lambda d: d["meshes"][0]["primitives"][0].update(material=999)),
+         "loads"),
+        ("child out of range", edit(lambda d: d["nodes"][0].setdefault(
+            "children", []).append(nnodes + 100)), "error"),
+        ("node cycle", edit(cycle), "error"),
+        ("root listed twice", edit(root_twice), "error"),
+        ("deep chain of 40 nodes", edit(lambda d: chain(d, False)),
+         "loads"),
+        ("shared children on 40 levels", edit(lambda d: chain(d, True)),
+         "error"),
+        ("matrix of 15 numbers", edit(lambda d: d["nodes"][0].update(
+            matrix=[1.0] * 15)), "error"),
+    ]
+
+
+@pytest.mark.timeout(300)
+def test_loader_malformed_files_fail_cleanly(tmp_path):
+    """One corruption at a time of a valid saved scene: the loader returns
+    an error (or loads, where the format allows it) and never crashes or
+    runs away; each load runs in its own process, so a crash shows as a
+    signal."""
+    import json
+    import subprocess
+    import sys
+    src = api.Scene(api.SCENE_SMALL, 1)
+    good = tmp_path / "good.gltf"
+    src.save_gltf(str(good))
+    doc = json.loads(good.read_text())
+    binlen = os.path.getsize(str(tmp_path / "good.bin"))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    probe = ("import sys; from nodebleed_b200 import api\n"
+             "try:\n    api.Scene.load_gltf(sys.argv[1])\n"
+             "except RuntimeError:\n    sys.exit(3)\n")
+    for k, (name, fn, want) in enumerate(_corruptions(doc, binlen)):
+        d = fn(doc)
+        d["buffers"][0]["uri"] = "good.bin"
+        path = tmp_path / ("bad%d.gltf" % k)
+        path.write_text(json.dumps(d))
+        r = subprocess.run([sys.executable, "-c", probe, str(path)],
+                           cwd=root, capture_output=True, text=True,
+                           timeout=60)
+        assert r.returncode in (0, 3), (name, r.returncode, r.stderr[-500:])
+        assert r.returncode == (3 if want == "error" else 0), \
+            (name, want, r.returncode)
+    # a truncated .bin
+    (tmp_path / "short.bin").write_bytes(
+        (tmp_path / "good.bin").read_bytes()[:binlen // 2])
+    d = json.loads(good.read_text())
+    d["buffers"][0]["uri"] = "short.bin"
+    (tmp_path / "short.gltf").write_text(json.dumps(d))
+    with pytest.raises(RuntimeError):
+        api.Scene.load_gltf(str(tmp_path / "short.gltf"))
