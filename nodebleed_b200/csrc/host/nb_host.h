@@ -68,6 +68,9 @@ struct nbh_scene {
 	unsigned int    pad;
 };
 
+#define NBH_MAX_SPHERE_FREQ 1024u // 21 M triangles
+#define NBH_MAX_BLAS 4096u        // the reference's instance cap
+
 // Workload ids (one per synthetic scene family).
 enum {
 	NBH_SCENE_SMALL = 1,   // 1 icosphere BLAS x4 + ground + quad light
@@ -80,7 +83,10 @@ enum {
 
 // Generate a seeded scene.  `param` tunes the family: for BATCH it is the
 // scene index 0..15; for SMALL/TINY it scales the triangle budget (0 =
-// default); for SCALE/STRESS/GLOSSY it is the BLAS count (0 = default).
+// default, at most NBH_MAX_SPHERE_FREQ: the sphere's subdivision, 20 f^2
+// triangles); for SCALE/STRESS/GLOSSY it is the BLAS count (0 = default, at
+// most NBH_MAX_BLAS).  Returns -1 for an unknown family or a param above
+// its bound.
 int  nbh_scene_gen(struct nbh_scene *s, int family, uint64_t seed,
                    unsigned int param);
 void nbh_scene_free(struct nbh_scene *s);

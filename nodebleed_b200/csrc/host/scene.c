@@ -620,6 +620,13 @@ int nbh_scene_gen(struct nbh_scene *s, int family, uint64_t seed,
 	struct pcg r;
 	pcg_seed(&r, seed, (uint64_t)family * 0x9e3779b97f4a7c15ull + param);
 	int rc = -1;
+	int field = family == NBH_SCENE_SCALE || family == NBH_SCENE_STRESS ||
+	  family == NBH_SCENE_GLOSSY;
+	if ((family == NBH_SCENE_SMALL || family == NBH_SCENE_TINY) &&
+	  param > NBH_MAX_SPHERE_FREQ)
+		return -1;
+	if (field && param > NBH_MAX_BLAS)
+		return -1;
 	switch (family) {
 	case NBH_SCENE_SMALL:
 		rc = scene_small(&b, &r, param ? (int)param : 32, 640, 360, 1, 5);

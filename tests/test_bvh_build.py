@@ -80,3 +80,19 @@ def test_build_invariants_small():
             else:
                 stack.append(int(ch[j]))
     assert (seen == 1).all()
+
+
+def test_scene_generator_rejects_unknown_family_and_oversized_params():
+    """nbh_scene_gen returns -1 (RuntimeError here) for an unknown family
+    and for params above NBH_MAX_SPHERE_FREQ (SMALL/TINY) or NBH_MAX_BLAS
+    (SCALE/STRESS/GLOSSY), instead of generating an unbounded scene."""
+    for fam, param in ((7, 0), (api.SCENE_TINY, 1025),
+                       (api.SCENE_SMALL, 1 << 31),
+                       (api.SCENE_SCALE, 4097),
+                       (api.SCENE_STRESS, 0xffffffff)):
+        with pytest.raises(RuntimeError):
+            api.Scene(fam, 1, param)
+    # params within the bounds still generate
+    s = api.Scene(api.SCENE_TINY, 1, 8)
+    assert s.tris > 0
+    s.close()
