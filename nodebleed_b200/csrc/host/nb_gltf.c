@@ -305,6 +305,31 @@ struct gl_load {
 	uint8_t         *seen;   // per node: reached from a scene root
 };
 
+// Integer fields: the default when absent; a number that is not an integer
+// within [lo, hi] sets L->err, which fails the load, and gives the default
+// (instead of an out-of-range conversion to int, undefined in C).
+static double j_intval(struct gl_load *L, int k, double dflt, double lo,
+                       double hi)
+{
+	double v = j_num(&L->d, k, dflt);
+	if (k >= 0 && L->d.t[k].type == J_NUM &&
+	  !(v >= lo && v <= hi && v == floor(v))) {
+		L->err = 1;
+		return dflt;
+	}
+	return v;
+}
+
+static int j_index(struct gl_load *L, int k, int dflt)
+{
+	return (int)j_intval(L, k, dflt, 0.0, 2147483647.0);
+}
+
+static uint32_t j_u32(struct gl_load *L, int k, uint32_t dflt)
+{
+	return (uint32_t)j_intval(L, k, dflt, 0.0, 4294967295.0);
+}
+
 static int comp_size(uint32_t c)
 {
 	return c == 5121 ? 1 : c == 5123 ? 2 : c == 5125 || c == 5126 ? 4 : 0;
@@ -400,8 +425,8 @@ static int load_mesh(struct gl_load *L, int mesh, struct nbh_mesh *o)
 	for (int p = 0; p < np; p++) {
 		int pr = j_at(d, prims, p);
 		int attr = j_get(d, pr, "attributes");
-		int pa = (int)j_num(d, j_get(d, attr, "POSITION"), -1);
-		int ia = (int)j_num(d, j_get(d, pr, "indices"), -1);
+		int pa = j_index(L, j_get(d, attr, "POSITION"), -1);
+		int ia = j_index(L, j_get(d, pr, "indices"), -1);
 		if (pa < 0 || pa >= L->naccs || ia < 0 || ia >= L->naccs)
 			return -1;
 		vcnt += L->accs[pa].cnt;
@@ -419,10 +444,10 @@ static int load_mesh(struct gl_load *L, int mesh, struct nbh_mesh *o)
 	for (int p = 0; p < np; p++) {
 		int pr = j_at(d, prims, p);
 		int attr = j_get(d, pr, "attributes");
-		int pa = (int)j_num(d, j_get(d, attr, "POSITION"), -1);
-		int na = (int)j_num(d, j_get(d, attr, "NORMAL"), -1);
-		int ia = (int)j_num(d, j_get(d, pr, "indices"), -1);
-		int mi = (int)j_num(d, j_get(d, pr, "material"), 0);
+		int pa = j_index(L, j_get(d, attr, "POSITION"), -1);
+		int na = j_index(L, j_get(d, attr, "NORMAL"), -1);
+		int ia = j_index(L, j_get(d, pr, "indices"), -1);
+		int mi = j_index(L, j_get(d, pr, "material"), 0);
 		if (mi < 0 || (unsigned int)mi >= L->s->mtlcnt)
 			mi = 0;
 		// POSITION and NORMAL: float VEC3; indices: u8/u16/u32 SCALAR
@@ -589,8 +614,8 @@ static int load_nodes(struct gl_load *L, int node_id, const float pg[16],
 		if (gk >= 0 && j_floats(d, gk, g, 16))
 			return -1;
 	}
-	int mesh = (int)j_num(d, j_get(d, node, "mesh"), -1);
-	int cam = (int)j_num(d, j_get(d, node, "camera"), -1);
+	int mesh = j_index(L, j_get(d, node, "mesh"), -1);
+	int cam = j_index(L, j_get(d, node, "camera"), -1);
 	if (cam >= 0) {
 		if (L->cam_done)
 			goto children; // the first camera node only
@@ -623,7 +648,7 @@ static int load_nodes(struct gl_load *L, int node_id, const float pg[16],
 children:;
 	int ch = j_get(d, node, "children");
 	for (int i = 0; i < j_len(d, ch); i++) {
-		int c = (int)j_num(d, j_at(d, ch, i), -1);
+		int c = j_index(L, j_at(d, ch, i), -1);
 		if (c < 0 || load_nodes(L, c, g, depth + 1))
 			return -1;
 	}
@@ -665,9 +690,9 @@ int nbh_scene_load_gltf(struct nbh_scene *s, const char *path,
 	L.views = calloc((size_t)L.nviews + 1, sizeof(*L.views));
 	for (int i = 0; L.views && i < L.nviews; i++) {
 		int v = j_at(d, va, i);
-		L.views[i].off = (uint32_t)j_num(d, j_get(d, v, "byteOffset"), 0);
-		L.views[i].len = (uint32_t)j_num(d, j_get(d, v, "byteLength"), 0);
-		L.views[i].stride = (uint32_t)j_num(d, j_get(d, v, "byteStride"),
+		L.views[i].off = j_u32(&L, j_get(d, v, "byteOffset"), 0);
+		L.views[i].len = j_u32(&L, j_get(d, v, "byteLength"), 0);
+		L.views[i].stride = j_u32(&L, j_get(d, v, "byteStride"),
 		  0);
 	}
 	int aa = j_get(d, 0, "accessors");
@@ -678,14 +703,16 @@ int nbh_scene_load_gltf(struct nbh_scene *s, const char *path,
 	for (int i = 0; i < L.naccs; i++) {
 		int a = j_at(d, aa, i);
 		struct gl_acc *A = &L.accs[i];
-		A->view = (int)j_num(d, j_get(d, a, "bufferView"), -1);
-		A->off = (uint32_t)j_num(d, j_get(d, a, "byteOffset"), 0);
-		A->cnt = (uint32_t)j_num(d, j_get(d, a, "count"), 0);
-		A->comp = (uint32_t)j_num(d, j_get(d, a, "componentType"), 0);
+		A->view = j_index(&L, j_get(d, a, "bufferView"), -1);
+		A->off = j_u32(&L, j_get(d, a, "byteOffset"), 0);
+		A->cnt = j_u32(&L, j_get(d, a, "count"), 0);
+		A->comp = j_u32(&L, j_get(d, a, "componentType"), 0);
 		int ty = j_get(d, a, "type");
 		A->ncomp = j_eq(d, ty, "SCALAR") ? 1 : j_eq(d, ty, "VEC2") ? 2 :
 		  j_eq(d, ty, "VEC3") ? 3 : j_eq(d, ty, "VEC4") ? 4 : 0;
 	}
+	if (L.err)
+		goto out;
 	if (load_materials(&L))
 		goto out;
 	int ma = j_get(d, 0, "meshes");
@@ -702,7 +729,7 @@ int nbh_scene_load_gltf(struct nbh_scene *s, const char *path,
 	}
 	// roots of the default scene (scene, else 0)
 	int sc = j_at(d, j_get(d, 0, "scenes"),
-	  (int)j_num(d, j_get(d, 0, "scene"), 0));
+	  j_index(&L, j_get(d, 0, "scene"), 0));
 	int roots = j_get(d, sc, "nodes");
 	L.seen = calloc((size_t)j_len(d, j_get(d, 0, "nodes")) + 1, 1);
 	if (!L.seen)
@@ -710,7 +737,7 @@ int nbh_scene_load_gltf(struct nbh_scene *s, const char *path,
 	static const float ident[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0,
 	  0, 0, 0, 1};
 	for (int i = 0; i < j_len(d, roots); i++)
-		if (load_nodes(&L, (int)j_num(d, j_at(d, roots, i), -1), ident,
+		if (load_nodes(&L, j_index(&L, j_at(d, roots, i), -1), ident,
 		  0))
 			goto out;
 	if (s->instcnt == 0)
@@ -737,6 +764,8 @@ int nbh_scene_load_gltf(struct nbh_scene *s, const char *path,
 	s->height = 360;
 	s->spp = 1;
 	s->depth = 5;
+	if (L.err)
+		goto out;
 	rc = 0;
 out:
 	if (rc)

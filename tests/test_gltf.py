@@ -282,6 +282,16 @@ def _corruptions(doc, binlen):
          "error"),
         ("matrix of 15 numbers", edit(lambda d: d["nodes"][0].update(
             matrix=[1.0] * 15)), "error"),
+        ("fractional accessor count", edit(lambda d: d["accessors"][0].update(
+            count=d["accessors"][0]["count"] + 0.5)), "error"),
+        ("negative byte offset", edit(lambda d: d["bufferViews"][0].update(
+            byteOffset=-16)), "error"),
+        ("mesh index 1e30", edit(lambda d: [
+            n.update(mesh=1e30) for n in d["nodes"] if "mesh" in n][:1]),
+         "error"),
+        ("material index -1", edit(
+            lambda d: d["meshes"][0]["primitives"][0].update(material=-1)),
+         "error"),
     ]
 
 
